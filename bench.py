@@ -1,0 +1,268 @@
+"""Benchmark of the batched density hot path on the B200.
+
+Default workload (the headline): one batched logjoint + gradient evaluation
+of the large dense logistic regression -- X is 100000 x 100 ~ N(0,1)/sqrt(100),
+y ~ Bernoulli(logistic(X beta_true)), prior normal(0,1) -- over 4096 chains.
+A step is one evaluation of all 4096 chains; the metric is chain-gradient
+evaluations per second.  Data are seeded synthetic stand-ins (no data set is
+shipped).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Multi-GPU: the path does not shard (every chain's gradient needs all of X),
+so N GPUs run N independent replicas (weak scaling) and `value` is the
+aggregate over all ranks divided by the max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_OBS, N_COEF, N_CHAINS = 100_000, 100, 4096
+FLOP_FP32 = 4.0 * N_OBS * N_COEF * N_CHAINS            # two N x D x C contractions (x, +)
+METRIC = "grad evals/s"
+UNIT = "chain-gradient evaluations/s"
+WORKLOAD = ("config-3 logistic regression: batched logjoint+gradient, N=100000 obs, D=100, "
+            "4096 chains, FP32 (3xTF32 tensor-core contraction when available)")
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), float(p["bf16_tflops"]), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    def __init__(self, index=0):
+        self.samples = []
+        self.proc = None
+        self.index = index
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def _data():
+    from uncertaintea_b200.models import BernoulliLogitGLM, logistic_regression_data
+    X, y, _ = logistic_regression_data(N_OBS, N_COEF, seed=3, x_scale=1.0 / np.sqrt(N_COEF))
+    model = BernoulliLogitGLM(N_COEF, coef_mu=0.0, coef_sigma=1.0)
+    params = np.random.default_rng(1).standard_normal((N_CHAINS, N_COEF)).astype(np.float32)
+    return model, X, y, params
+
+
+def cpu_reference_rate(model, X, y, params, budget_s=12.0, threads=0):
+    """Chain-gradient evaluations/s of the CPU restatement of the reference's
+    batched path (chain-parallel, all host threads), on a bounded sample."""
+    import oracle
+    om = oracle.OracleModel(model.lower((X,), {"y": y}))
+    cores = oracle.max_threads() if threads == 0 else threads
+    chunk = max(8, cores * 4)
+    done, t0 = 0, time.perf_counter()
+    while True:
+        om.logjoint_gradient_f32(params[done % N_CHAINS: done % N_CHAINS + chunk], threads=threads)
+        done += chunk
+        el = time.perf_counter() - t0
+        if el >= budget_s or done >= 64 * chunk:
+            break
+    return done / el, cores, f"{done} chain-gradients of the full N=100000 x D=100 model in {el:.1f} s"
+
+
+def run_reference(args):
+    world, rank, _ = _dist()
+    if rank != 0:
+        return
+    model, X, y, params = _data()
+    vals = []
+    for i in range(args.warmup + args.steps):
+        rate, cores, sample = cpu_reference_rate(model, X, y, params, budget_s=4.0)
+        if i >= args.warmup:
+            vals.append(rate)
+    value = float(np.mean(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * N_CHAINS / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "global_batch": N_CHAINS, "parallelism": "replicas"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": sample + " per step (Julia reference not runnable here; C++ restatement)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args):
+    import torch
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from uncertaintea_b200.device import DeviceBatchedWorkspace
+    model, X, y, params = _data()
+    ws = DeviceBatchedWorkspace(model, N_CHAINS, args=(X,), constraints={"y": y})
+    qd = torch.from_numpy(params).cuda()
+    totals = torch.empty(N_CHAINS, device="cuda")
+    grads = torch.empty_like(qd)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    stream = torch.cuda.current_stream()
+
+    def step():
+        ws.logjoint_gradient_device(qd, totals, grads)
+
+    for _ in range(max(args.warmup, 3)):
+        flush.fill_(1.0)
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for s, e in evs:
+        flush.fill_(1.0)  # evict X / params from L2 between steps
+        s.record(stream)
+        step()
+        e.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    step_ms = [s.elapsed_time(e) for s, e in evs]
+    total_ms = float(sum(step_ms))
+    t_max = total_ms
+    if dist:
+        tt = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    clk = clocks.stop()
+    value = world * N_CHAINS * args.steps / (t_max / 1000.0)
+
+    # end to end through the public host-array API: pinned host params in,
+    # host totals + gradients out, every step.
+    pinned = torch.from_numpy(params).pin_memory()   # (C, P) chain-major, page-locked
+    pt = pinned.numpy().T                              # P x C reference-layout view of it
+    for _ in range(2):
+        ws.logjoint_gradient(pt)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    e2e_steps = max(3, args.steps // 2)
+    for _ in range(e2e_steps):
+        vals, g = ws.logjoint_gradient(pt)
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        tt = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    e2e_value = world * N_CHAINS * e2e_steps / e2e_s
+
+    hbm, bf16, peak_kind = _peaks()
+    tc = bool(getattr(ws, "tensor_core_path", lambda: False)())
+    if tc:
+        work = 3.0 * FLOP_FP32 / 1e12          # 3xTF32: three TF32 products per FP32 product
+        peak = bf16 / 2.0                      # dense TF32 = half of dense bf16
+        bound = "tensor"
+    else:
+        work = FLOP_FP32 / 1e12
+        peak = bf16 / 2.0
+        bound = "tensor"
+    avg_s = (total_ms / args.steps) / 1000.0
+    achieved = work / avg_s
+    roof = {"bound": bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "traffic": None, "peak_source": f"{peak_kind} bf16/2 (dense TF32)",
+            "note": ("3xTF32 TF32-FLOPs" if tc else "FP32 CUDA-core FLOPs (no tensor-core path active)")}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, cores, sample = cpu_reference_rate(model, X, y, params, budget_s=args.cpu_seconds)
+        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+    launches = int(ws.launches_per_gradient()) * args.steps if hasattr(ws, "launches_per_gradient") else 2 * args.steps
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "global_batch": N_CHAINS * world, "n_obs": N_OBS,
+                           "n_coefs": N_COEF, "parallelism": f"replicas{world}",
+                           "l2": "flushed between timed steps (256 MB write)"},
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": N_CHAINS * N_COEF * 4,
+                        "d2h_bytes_per_step": N_CHAINS * (N_COEF + 1) * 4},
+                "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches}
+        print(json.dumps(line), flush=True)
+    ws.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,219 @@
+/*
+ * ut_b200.h -- C ABI of the B200 (sm_100a) batched density + sampler library.
+ *
+ * This is the boundary a host language binds (Julia `ccall`, Python `ctypes`).
+ * Every signature uses plain C types: pointers, sizes, and two plain structs.
+ * No C++ or torch types cross it.
+ *
+ * Layout conventions (identical to UncertainTea's column-major Julia arrays):
+ *   - a "P x C" matrix holds C chains, each chain's P unconstrained parameters
+ *     contiguous (chain c, parameter p at index c*P + p);
+ *   - a "C" vector holds one value per chain.
+ *
+ * Host-pointer entry points copy in, run on the current CUDA device, copy out
+ * and synchronise before returning (the reference's `copyto!` + `synchronize`
+ * boundary).  Entry points whose names end in `_device`, and the sampler
+ * iteration entry points, take DEVICE pointers and a `cudaStream_t` passed as
+ * `void*` (NULL = legacy default stream); they return once the work is queued.
+ *
+ * Status codes are returned by every entry point; the message of the last
+ * failure on the calling thread is available through ut_last_error.
+ * No entry point falls back to a CPU path.
+ */
+#ifndef UT_B200_H
+#define UT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define UT_OK                  0
+#define UT_ERR_ARGUMENT        1  /* reference: ArgumentError                    */
+#define UT_ERR_DIMENSION       2  /* reference: DimensionMismatch                */
+#define UT_ERR_UNSUPPORTED     3  /* model not lowerable to a kernel description */
+#define UT_ERR_PRECISION       4  /* precision other than Float32 requested      */
+#define UT_ERR_CUDA            5  /* a CUDA runtime call failed                  */
+#define UT_ERR_NO_DEVICE       6  /* no CUDA device visible                      */
+#define UT_ERR_DEVICE_TIMEOUT  7  /* a bounded in-kernel wait gave up            */
+
+/* ---- model families a kernel description can hold ---------------------- */
+/* Bernoulli-logit GLM: optional intercept ~ normal, coefficients ~ iid normal,
+ * y_i ~ bernoullilogit(intercept + x_i . beta).  Lowered form of the
+ * reference's DeviceBernoulliLogitGLMChoiceStepDyn + DeviceDiagNormalChoiceStepDyn
+ * (src/device/plan/steps.jl:205-225, 334-340). */
+#define UT_FAMILY_GLM_BERNOULLI_LOGIT        1
+/* Non-centred hierarchical normal: mu ~ normal(mu_loc, mu_scale),
+ * tau ~ halfcauchy(tau_scale) (log transform), z_j ~ normal(0, 1),
+ * y_ij ~ normal(mu + tau * z_j, sigma_j).  Semantics of the reference's
+ * `reparam=:noncentered` iid latent (docs/noncentered-reparam.md:22-36). */
+#define UT_FAMILY_HIER_NORMAL_NONCENTERED    2
+
+/* Fixed kernel description: what the host lowers a model's execution plan to
+ * (reference: DeviceExecutionPlan, src/device/plan/steps.jl:482-489, produced
+ * by _lower_device_plan, src/device/plan/lowering.jl:1360).  Parameter rows:
+ *   GLM : [intercept (if has_intercept)] then num_coefs coefficients;
+ *   HIER: [mu, log(tau), z_1 .. z_J]. */
+typedef struct ut_plan_desc {
+    int32_t family;          /* UT_FAMILY_*                                   */
+    int32_t num_params;      /* P, unconstrained parameter count              */
+    int32_t num_obs;         /* N, observations                               */
+    int32_t num_coefs;       /* GLM: D covariates                             */
+    int32_t has_intercept;   /* GLM: 1 if an intercept row leads the params   */
+    int32_t num_groups;      /* HIER: J groups                                */
+    double intercept_mu;     /* GLM: intercept ~ normal(intercept_mu, ...)    */
+    double intercept_sigma;
+    double coef_mu;          /* GLM: beta_d ~ normal(coef_mu, coef_sigma)     */
+    double coef_sigma;
+    double mu_loc;           /* HIER: mu ~ normal(mu_loc, mu_scale)           */
+    double mu_scale;
+    double tau_scale;        /* HIER: tau ~ halfcauchy(tau_scale)             */
+} ut_plan_desc;
+
+typedef struct ut_workspace ut_workspace;
+
+/* ---- library / errors -------------------------------------------------- */
+const char* ut_version(void);
+/* Copies the last error message of this thread into buf (NUL-terminated,
+ * truncated to len) and returns its full length. */
+int32_t ut_last_error(char* buf, size_t len);
+/* Number of visible CUDA devices (0 when none). */
+int32_t ut_device_count(void);
+
+/* ---- lowering report ----------------------------------------------------
+ * reference: device_lowering_report (src/device/workspace.jl:24-35).
+ * Returns UT_OK when the description is supported, else UT_ERR_UNSUPPORTED
+ * with the issue list written to `issues`. */
+int32_t ut_lowering_report(const ut_plan_desc* plan, char* issues, size_t len);
+
+/* ---- workspace ------------------------------------------------------------
+ * reference: DeviceBatchedWorkspace(model, C; backend, precision, args,
+ * constraints) (src/device/workspace.jl:71-137).  `observed` is the staged
+ * observation buffer, one shared column (reference DeviceStagingBundle,
+ * src/device/staging.jl:11-39):
+ *   GLM : observed_rows = N*(D+1): per observation the D covariates then y;
+ *   HIER: observed_rows = N + J:  the N y values group after group, then the
+ *         J fixed sigma_j; trip_counts[j] = n_j and loop_starts[j] = first row
+ *         of group j (num_loops = J).
+ * precision_bits must be 32 (Float32); anything else is UT_ERR_PRECISION. */
+int32_t ut_workspace_create(const ut_plan_desc* plan,
+                            const float* observed, int64_t observed_rows, int64_t observed_cols,
+                            const int32_t* trip_counts, const int32_t* loop_starts, int32_t num_loops,
+                            int32_t batch_size, int32_t precision_bits,
+                            ut_workspace** out);
+int32_t ut_workspace_destroy(ut_workspace* ws);
+int32_t ut_workspace_info(const ut_workspace* ws, int32_t* num_params, int32_t* batch_size);
+
+/* ---- batched density ------------------------------------------------------
+ * reference: device_batched_logjoint! (src/device/workspace.jl:276-307) and
+ * device_batched_logjoint_gradient! (src/device/api.jl:82-107).
+ * Host buffers: params P x C, totals C, gradients P x C. */
+int32_t ut_logjoint(ut_workspace* ws, const float* params, float* totals);
+int32_t ut_logjoint_gradient(ut_workspace* ws, const float* params, float* totals, float* gradients);
+/* Same computations on device-resident buffers (the kernel launch sites of
+ * src/device/workspace.jl:290-301 and src/device/tiled_gradient.jl:292-390). */
+int32_t ut_logjoint_device(ut_workspace* ws, const float* d_params, float* d_totals, void* stream);
+int32_t ut_logjoint_gradient_device(ut_workspace* ws, const float* d_params, float* d_totals,
+                                    float* d_gradients, void* stream);
+
+/* ---- Philox4x32-10 stream ---------------------------------------------------
+ * reference: philox4x32 (src/device/rng.jl:95-119), device_rand_uniform
+ * (:165-174), device_rand_normal (:196-219).  Host buffers; computed on the
+ * GPU.  keys: n x 2, counters: n x 4, out: n x 4 words. */
+int32_t ut_philox4x32(const uint32_t* keys, const uint32_t* counters, int64_t n, uint32_t* out);
+/* out[i] = device_rand_{uniform,normal}(Float32, chain, iteration, stream, draw_start + i) */
+int32_t ut_rand_uniform(uint32_t chain, uint32_t iteration, uint32_t stream, uint32_t draw_start,
+                        int64_t n, float* out);
+int32_t ut_rand_normal(uint32_t chain, uint32_t iteration, uint32_t stream, uint32_t draw_start,
+                       int64_t n, float* out);
+
+/* ---- samplers (device buffers) -------------------------------------------- */
+/* Per-iteration buffers of one HMC / ChEES iteration.  position, gradient and
+ * logjoint hold the chains' current state and are updated in place with the
+ * accepted proposal. */
+typedef struct ut_hmc_buffers {
+    float* position;            /* P x C in/out                                  */
+    float* gradient;            /* P x C in/out                                  */
+    float* logjoint;            /* C in/out                                      */
+    const float* inverse_mass;  /* P   shared diagonal inverse mass              */
+    const float* step;          /* C   per-chain step size                       */
+    float* accept_prob;         /* C out                                         */
+    float* energy;              /* C out: Hamiltonian of the retained state      */
+    float* energy_error;        /* C out: H(proposal) - H(current), +Inf invalid */
+    uint8_t* accepted;          /* C out                                         */
+    uint8_t* divergent;         /* C out                                         */
+    float* proposal;            /* P x C out (optional, NULL): proposal position */
+    float* endpoint_momentum;   /* P x C out (optional, NULL): negated end momentum */
+} ut_hmc_buffers;
+
+/* One batched HMC iteration: Philox momentum (stream 0, draw = parameter),
+ * H0, leapfrog trajectory of num_leapfrog_steps steps, H1, and the
+ * Metropolis accept with a Philox uniform (stream 4, draw 0), applied on
+ * device.  reference: the per-iteration body of _run_device_batched_hmc
+ * (src/device/hmc_kernels.jl:517-590), leapfrog as
+ * _device_leapfrog_integrate_perchain! (:255-287). */
+int32_t ut_hmc_iteration(ut_workspace* ws, const ut_hmc_buffers* buf, int32_t num_leapfrog_steps,
+                         uint32_t iteration_coord, float divergence_threshold, void* stream);
+
+/* One-step leapfrog probe used by the reasonable-step-size search: from the
+ * current state, with momentum drawn at `iteration_coord`, integrate one step
+ * of size trial_step[c] and write log_accept_ratio[c] = H0 - H1 (-Inf when
+ * invalid).  The state is left unchanged.  reference:
+ * _batched_reasonable_log_accept_ratio! (src/inference/nuts/adaptation.jl:389-425). */
+int32_t ut_leapfrog_probe(ut_workspace* ws, const float* d_position, const float* d_gradient,
+                          const float* d_logjoint, const float* d_inverse_mass, const float* d_trial_step,
+                          uint32_t iteration_coord, float* d_log_accept_ratio, void* stream);
+
+/* Per-iteration buffers of one persistent NUTS iteration. */
+typedef struct ut_nuts_buffers {
+    float* position;            /* P x C in/out: replaced by the proposal when moved */
+    float* gradient;            /* P x C in/out                                  */
+    float* logjoint;            /* C in/out                                      */
+    const float* inverse_mass;  /* P                                             */
+    const float* step;          /* C                                             */
+    float* accept_prob;         /* C out  (reference out_real[1, :])             */
+    float* energy;              /* C out  (out_real[2, :], proposal energy)      */
+    float* energy_error;        /* C out  (out_real[3, :])                       */
+    int32_t* tree_depth;        /* C out  (out_int[1, :])                        */
+    int32_t* integration_steps; /* C out  (out_int[2, :])                        */
+    uint8_t* divergent;         /* C out                                         */
+    uint8_t* moved;             /* C out                                         */
+} ut_nuts_buffers;
+
+/* One persistent multinomial-NUTS iteration for every chain in ONE launch.
+ * reference: _device_persistent_nuts_proposals! (src/device/persistent_nuts.jl:678-761)
+ * running _persist_nuts_chain! (:226-491); Philox streams 0-3 as at :70-73. */
+int32_t ut_persistent_nuts_iteration(ut_workspace* ws, const ut_nuts_buffers* buf,
+                                     int32_t max_tree_depth, float divergence_threshold,
+                                     uint32_t iteration_coord, void* stream);
+
+/* ChEES cross-chain trajectory statistics, reduced on device.
+ * reference: _chees_trajectory_update! (src/inference/api_batched_chees.jl:158-228),
+ * device passes _device_chees_proposal_mean! / _device_chees_endpoint_terms!
+ * (src/device/chees_kernels.jl:67-106).  Writes the two host doubles
+ * out[0] = gradient_numerator, out[1] = acceptance_denominator and synchronises. */
+int32_t ut_chees_reduce(ut_workspace* ws, const float* d_initials, const float* d_proposals,
+                        const float* d_endpoint_momentum, const float* d_accept_prob,
+                        const uint8_t* d_divergent, const float* d_inverse_mass,
+                        double* out, void* stream);
+
+/* ---- warmup adaptation on device ------------------------------------------
+ * Pooled running-variance update over the C chains' positions, chain after
+ * chain in index order (Welford with the early-window clip), for the
+ * windowed diagonal mass adaptation.  reference: _update_running_variance!
+ * (src/inference/nuts/adaptation.jl:170-209) with _running_variance_sample!
+ * (:83-101) and the clip constants of src/inference/data_types.jl:189-193.
+ * d_state: double[2P + 3] = mean(P), m2(P), count, weight_sum,
+ * weight_square_sum (updated in place); d_weights: C doubles in [0, 1]
+ * (a zero weight skips the chain). */
+int32_t ut_running_variance_update(const float* d_positions, const double* d_weights, int32_t num_params,
+                                   int32_t num_chains, double* d_state, int32_t window_length, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* UT_B200_H */

@@ -1,0 +1,168 @@
+"""CPU oracle of the batched density + sampler hot path.
+
+TEST INFRASTRUCTURE: only the tests, ``__graft_entry__.smoke`` and the CPU
+baseline leg of ``bench.py`` use this package, as the checker.  The product
+library never calls it.  See oracle.cpp for what each function restates and
+how far parity is pinned (Philox and the ChEES scalar helpers by the
+reference's own known-answer tests; the densities and samplers by closed
+forms and finite differences, not by reference outputs).
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, c_double, c_float, c_int32, c_int64, c_uint32, c_void_p
+
+import numpy as np
+
+from .build_oracle import LIB, build
+
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = build()
+    lib = ctypes.CDLL(path)
+    sig = {
+        "orc_philox4x32": (None, [c_uint32, c_uint32, c_void_p, c_void_p]),
+        "orc_rand_uniform_f32": (None, [c_uint32, c_uint32, c_uint32, c_uint32, c_int64, c_void_p]),
+        "orc_rand_normal_f32": (None, [c_uint32, c_uint32, c_uint32, c_uint32, c_int64, c_void_p]),
+        "orc_rand_uniform_f64": (None, [c_uint32, c_uint32, c_uint32, c_uint32, c_int64, c_void_p]),
+        "orc_rand_normal_f64": (None, [c_uint32, c_uint32, c_uint32, c_uint32, c_int64, c_void_p]),
+        "orc_logjoint_gradient_f64": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p,
+                                                c_void_p, c_int32]),
+        "orc_logjoint_gradient_f32": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p,
+                                                c_void_p, c_int32]),
+        "orc_max_threads": (c_int32, []),
+        "orc_hmc_iteration_f32": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p, c_void_p,
+                                            c_void_p, c_void_p, c_void_p, c_int32, c_uint32, c_float, c_void_p,
+                                            c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32]),
+        "orc_leapfrog_probe_f32": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p, c_void_p,
+                                             c_void_p, c_void_p, c_void_p, c_uint32, c_void_p, c_int32]),
+        "orc_nuts_iteration_f32": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p, c_void_p,
+                                             c_void_p, c_void_p, c_void_p, c_int32, c_float, c_uint32, c_void_p,
+                                             c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32]),
+        "orc_chees_reduce": (None, [c_int32, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                    c_void_p]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def philox4x32(key, counter):
+    out = np.zeros(4, dtype=np.uint32)
+    ctr = np.asarray(counter, dtype=np.uint32)
+    load().orc_philox4x32(int(key[0]), int(key[1]), _p(ctr), _p(out))
+    return tuple(int(v) for v in out)
+
+
+def rand_uniform(chain, iteration, stream, draw_start, n, dtype=np.float32):
+    out = np.empty(n, dtype=dtype)
+    fn = load().orc_rand_uniform_f32 if dtype == np.float32 else load().orc_rand_uniform_f64
+    fn(chain, iteration, stream, draw_start, n, _p(out))
+    return out
+
+
+def rand_normal(chain, iteration, stream, draw_start, n, dtype=np.float32):
+    out = np.empty(n, dtype=dtype)
+    fn = load().orc_rand_normal_f32 if dtype == np.float32 else load().orc_rand_normal_f64
+    fn(chain, iteration, stream, draw_start, n, _p(out))
+    return out
+
+
+class OracleModel:
+    """Wraps a lowered kernel description for the oracle entry points."""
+
+    def __init__(self, lowered):
+        self.lowered = lowered
+        self.plan = lowered.plan
+        self.P = lowered.num_params
+        self.obs = np.ascontiguousarray(lowered.observed, dtype=np.float32)
+        self.tc = np.ascontiguousarray(lowered.trip_counts, dtype=np.int32)
+        self.ls = np.ascontiguousarray(lowered.loop_starts, dtype=np.int32)
+
+    def _common(self):
+        return (ctypes.byref(self.plan), _p(self.obs), _p(self.tc) if self.tc.size else None,
+                _p(self.ls) if self.ls.size else None)
+
+    def logjoint_gradient_f64(self, params_cp, threads=0, want_grad=True):
+        q = np.ascontiguousarray(params_cp, dtype=np.float64)
+        C = q.shape[0]
+        totals = np.empty(C)
+        grads = np.empty_like(q) if want_grad else None
+        load().orc_logjoint_gradient_f64(*self._common(), _p(q), C, _p(totals), _p(grads), threads)
+        return totals, grads
+
+    def logjoint_gradient_f32(self, params_cp, threads=0, want_grad=True):
+        q = np.ascontiguousarray(params_cp, dtype=np.float32)
+        C = q.shape[0]
+        totals = np.empty(C, dtype=np.float32)
+        grads = np.empty_like(q) if want_grad else None
+        load().orc_logjoint_gradient_f32(*self._common(), _p(q), C, _p(totals), _p(grads), threads)
+        return totals, grads
+
+    def hmc_iteration(self, position, gradient, logjoint, inverse_mass, step, L, coord, thr=1000.0,
+                      want_proposal=False, threads=0):
+        C = position.shape[0]
+        out = {k: np.empty(C, dtype=np.float32) for k in ("accept_prob", "energy", "energy_error")}
+        out["accepted"] = np.empty(C, dtype=np.uint8)
+        out["divergent"] = np.empty(C, dtype=np.uint8)
+        prop = np.empty_like(position) if want_proposal else None
+        mom = np.empty_like(position) if want_proposal else None
+        load().orc_hmc_iteration_f32(*self._common(), C, _p(position), _p(gradient), _p(logjoint),
+                                     _p(np.ascontiguousarray(inverse_mass, dtype=np.float32)),
+                                     _p(np.ascontiguousarray(step, dtype=np.float32)), L, coord, thr,
+                                     _p(out["accept_prob"]), _p(out["energy"]), _p(out["energy_error"]),
+                                     _p(out["accepted"]), _p(out["divergent"]), _p(prop), _p(mom), threads)
+        out["proposal"], out["endpoint_momentum"] = prop, mom
+        return out
+
+    def leapfrog_probe(self, position, gradient, logjoint, inverse_mass, trial_step, coord, threads=0):
+        C = position.shape[0]
+        lar = np.empty(C, dtype=np.float32)
+        load().orc_leapfrog_probe_f32(*self._common(), C, _p(position), _p(gradient), _p(logjoint),
+                                      _p(np.ascontiguousarray(inverse_mass, dtype=np.float32)),
+                                      _p(np.ascontiguousarray(trial_step, dtype=np.float32)), coord, _p(lar), threads)
+        return lar
+
+    def nuts_iteration(self, position, gradient, logjoint, inverse_mass, step, max_depth, coord, thr=1000.0,
+                       threads=0):
+        C = position.shape[0]
+        out = {k: np.empty(C, dtype=np.float32) for k in ("accept_prob", "energy", "energy_error")}
+        out["tree_depth"] = np.empty(C, dtype=np.int32)
+        out["integration_steps"] = np.empty(C, dtype=np.int32)
+        out["divergent"] = np.empty(C, dtype=np.uint8)
+        out["moved"] = np.empty(C, dtype=np.uint8)
+        load().orc_nuts_iteration_f32(*self._common(), C, _p(position), _p(gradient), _p(logjoint),
+                                      _p(np.ascontiguousarray(inverse_mass, dtype=np.float32)),
+                                      _p(np.ascontiguousarray(step, dtype=np.float32)), max_depth, thr, coord,
+                                      _p(out["accept_prob"]), _p(out["energy"]), _p(out["energy_error"]),
+                                      _p(out["tree_depth"]), _p(out["integration_steps"]), _p(out["divergent"]),
+                                      _p(out["moved"]), threads)
+        return out
+
+
+def chees_reduce(initials, proposals, momenta, accept_prob, divergent, inverse_mass):
+    C, P = initials.shape
+    out = np.zeros(2)
+    load().orc_chees_reduce(P, C, _p(np.ascontiguousarray(initials, dtype=np.float32)),
+                            _p(np.ascontiguousarray(proposals, dtype=np.float32)),
+                            _p(np.ascontiguousarray(momenta, dtype=np.float32)),
+                            _p(np.ascontiguousarray(accept_prob, dtype=np.float32)),
+                            _p(np.ascontiguousarray(divergent, dtype=np.uint8)),
+                            _p(np.ascontiguousarray(inverse_mass, dtype=np.float32)), _p(out))
+    return out
+
+
+def max_threads():
+    return int(load().orc_max_threads())

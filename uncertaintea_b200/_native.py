@@ -1,0 +1,171 @@
+"""ctypes binding of the C ABI in ``include/ut_b200.h``.
+
+The shared library ``libut_b200.so`` is built in-tree (``__graft_entry__.build``
+or ``python -m uncertaintea_b200.build``).  Loading fails loudly when it is
+missing: there is no CPU fallback for any compute entry point.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_char_p, c_double, c_float, c_int32, c_int64, c_size_t, c_uint8, c_uint32, c_void_p
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBRARY_PATH = os.path.join(_HERE, "libut_b200.so")
+
+UT_OK = 0
+UT_ERR_ARGUMENT = 1
+UT_ERR_DIMENSION = 2
+UT_ERR_UNSUPPORTED = 3
+UT_ERR_PRECISION = 4
+UT_ERR_CUDA = 5
+UT_ERR_NO_DEVICE = 6
+UT_ERR_DEVICE_TIMEOUT = 7
+
+UT_FAMILY_GLM_BERNOULLI_LOGIT = 1
+UT_FAMILY_HIER_NORMAL_NONCENTERED = 2
+
+
+class PlanDesc(ctypes.Structure):
+    _fields_ = [
+        ("family", c_int32),
+        ("num_params", c_int32),
+        ("num_obs", c_int32),
+        ("num_coefs", c_int32),
+        ("has_intercept", c_int32),
+        ("num_groups", c_int32),
+        ("intercept_mu", c_double),
+        ("intercept_sigma", c_double),
+        ("coef_mu", c_double),
+        ("coef_sigma", c_double),
+        ("mu_loc", c_double),
+        ("mu_scale", c_double),
+        ("tau_scale", c_double),
+    ]
+
+
+class HmcBuffers(ctypes.Structure):
+    _fields_ = [
+        ("position", c_void_p),
+        ("gradient", c_void_p),
+        ("logjoint", c_void_p),
+        ("inverse_mass", c_void_p),
+        ("step", c_void_p),
+        ("accept_prob", c_void_p),
+        ("energy", c_void_p),
+        ("energy_error", c_void_p),
+        ("accepted", c_void_p),
+        ("divergent", c_void_p),
+        ("proposal", c_void_p),
+        ("endpoint_momentum", c_void_p),
+    ]
+
+
+class NutsBuffers(ctypes.Structure):
+    _fields_ = [
+        ("position", c_void_p),
+        ("gradient", c_void_p),
+        ("logjoint", c_void_p),
+        ("inverse_mass", c_void_p),
+        ("step", c_void_p),
+        ("accept_prob", c_void_p),
+        ("energy", c_void_p),
+        ("energy_error", c_void_p),
+        ("tree_depth", c_void_p),
+        ("integration_steps", c_void_p),
+        ("divergent", c_void_p),
+        ("moved", c_void_p),
+    ]
+
+
+# (name, restype, argtypes) of every exported entry point, in header order.
+SIGNATURES = [
+    ("ut_version", c_char_p, []),
+    ("ut_last_error", c_int32, [c_char_p, c_size_t]),
+    ("ut_device_count", c_int32, []),
+    ("ut_lowering_report", c_int32, [POINTER(PlanDesc), c_char_p, c_size_t]),
+    ("ut_workspace_create", c_int32,
+     [POINTER(PlanDesc), c_void_p, c_int64, c_int64, c_void_p, c_void_p, c_int32, c_int32, c_int32,
+      POINTER(c_void_p)]),
+    ("ut_workspace_destroy", c_int32, [c_void_p]),
+    ("ut_workspace_info", c_int32, [c_void_p, POINTER(c_int32), POINTER(c_int32)]),
+    ("ut_logjoint", c_int32, [c_void_p, c_void_p, c_void_p]),
+    ("ut_logjoint_gradient", c_int32, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("ut_logjoint_device", c_int32, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("ut_logjoint_gradient_device", c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("ut_philox4x32", c_int32, [c_void_p, c_void_p, c_int64, c_void_p]),
+    ("ut_rand_uniform", c_int32, [c_uint32, c_uint32, c_uint32, c_uint32, c_int64, c_void_p]),
+    ("ut_rand_normal", c_int32, [c_uint32, c_uint32, c_uint32, c_uint32, c_int64, c_void_p]),
+    ("ut_hmc_iteration", c_int32, [c_void_p, POINTER(HmcBuffers), c_int32, c_uint32, c_float, c_void_p]),
+    ("ut_leapfrog_probe", c_int32,
+     [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_uint32, c_void_p, c_void_p]),
+    ("ut_persistent_nuts_iteration", c_int32,
+     [c_void_p, POINTER(NutsBuffers), c_int32, c_float, c_uint32, c_void_p]),
+    ("ut_chees_reduce", c_int32,
+     [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, POINTER(c_double), c_void_p]),
+    ("ut_running_variance_update", c_int32,
+     [c_void_p, c_void_p, c_int32, c_int32, c_void_p, c_int32, c_void_p]),
+]
+
+_lib = None
+
+
+def exported_symbols():
+    """Names of every entry point the binding expects the library to export."""
+    return [name for name, _, _ in SIGNATURES]
+
+
+def load():
+    """Load (once) and return the shared library, with typed entry points."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIBRARY_PATH):
+        raise RuntimeError(
+            f"{LIBRARY_PATH} is missing: build the CUDA extension first "
+            "(python -c 'import __graft_entry__ as g; g.build()'); there is no CPU fallback")
+    lib = ctypes.CDLL(LIBRARY_PATH)
+    for name, restype, argtypes in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = restype
+        fn.argtypes = argtypes
+    _lib = lib
+    return lib
+
+
+class DeviceError(RuntimeError):
+    """A CUDA-side failure reported by the library."""
+
+
+class DeviceTimeoutError(DeviceError):
+    """A bounded in-kernel wait gave up (UT_ERR_DEVICE_TIMEOUT)."""
+
+
+def last_error() -> str:
+    lib = load()
+    buf = ctypes.create_string_buffer(4096)
+    lib.ut_last_error(buf, len(buf))
+    return buf.value.decode("utf-8", "replace")
+
+
+def check(status: int) -> None:
+    """Translate a status code into the reference's exception types."""
+    if status == UT_OK:
+        return
+    msg = last_error()
+    if status in (UT_ERR_ARGUMENT, UT_ERR_UNSUPPORTED, UT_ERR_PRECISION):
+        raise ValueError(msg)  # the reference raises ArgumentError
+    if status == UT_ERR_DIMENSION:
+        raise IndexError(msg)  # the reference raises DimensionMismatch
+    if status == UT_ERR_DEVICE_TIMEOUT:
+        raise DeviceTimeoutError(msg)
+    raise DeviceError(msg)
+
+
+def ptr(t) -> int:
+    """Device or host address of a torch tensor / numpy array (None -> 0)."""
+    if t is None:
+        return 0
+    if hasattr(t, "data_ptr"):
+        return t.data_ptr()
+    return t.ctypes.data

@@ -1,0 +1,725 @@
+// ut_api.cu -- C ABI of the library (declared in include/ut_b200.h): workspace
+// lifetime, kernel-description validation, and the launch sites of every
+// kernel.  No CPU fallback: without a CUDA device every compute entry point
+// returns UT_ERR_NO_DEVICE.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <algorithm>
+
+#include "../../include/ut_b200.h"
+#include "ut_warp_kernels.cuh"
+#include "ut_glm_tiled.cuh"
+#include "ut_lf_batched.cuh"
+#include "ut_tc_glm.cuh"
+
+using namespace ut;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int32_t fail(int32_t code, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define UT_CUDA(call)                                                                          \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess) return fail(UT_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+#define UT_LAUNCHED()                                                                          \
+    do {                                                                                       \
+        cudaError_t e_ = cudaGetLastError();                                                   \
+        if (e_ != cudaSuccess) return fail(UT_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e_)); \
+    } while (0)
+
+enum Path { kPathWarp = 1, kPathTiled = 2 };
+
+constexpr size_t kSmemBudget = 200 * 1024;  // dynamic shared memory per CTA we allow ourselves
+constexpr int kWarpsDensity = 8;            // chains per CTA of the warp kernels
+constexpr int kWarpsNuts = 4;
+
+int inst_k(int P) {
+    int k = (P + 31) / 32;
+    const int ks[] = {1, 2, 3, 4, 8, 17};
+    for (int v : ks)
+        if (k <= v) return v;
+    return -1;
+}
+
+}  // namespace
+
+struct ut_workspace {
+    ut_plan_desc plan;
+    int P = 0, C = 0, N = 0, device = 0;
+    int path = 0;
+    int K = 0, dmax = 16;
+    DevModel dm;
+    // device data
+    float* d_XT = nullptr;   // GLM warp path: D x N
+    float* d_Xa = nullptr;   // GLM tiled path: N x F (ones column first when intercept)
+    float* d_y = nullptr;
+    float* d_sig = nullptr;
+    int32_t* d_start = nullptr;
+    int32_t* d_count = nullptr;
+    // tiled scratch
+    int splits = 0, obs_per_split = 0, fpt = 1;
+    float* d_part_ll = nullptr;
+    float* d_part_g = nullptr;
+    // tensor-core path (GLM, large N)
+    TcGlmPlan tc;
+    // batched leapfrog scratch
+    LfScratch lf = {};
+    // NUTS checkpoint scratch
+    float* d_ckpt = nullptr;
+    int ckpt_depth = -1;
+    // ChEES scratch
+    uint8_t* d_flags = nullptr;
+    double* d_means = nullptr;
+    double* d_terms = nullptr;
+    double* d_out = nullptr;
+    // host-pointer entry buffers
+    float* d_params = nullptr;
+    float* d_totals = nullptr;
+    float* d_grads = nullptr;
+    cudaStream_t stream = nullptr;
+    std::vector<void*> allocations;
+};
+
+namespace {
+
+template <class T>
+int32_t dalloc(ut_workspace* ws, T** p, size_t count) {
+    void* v = nullptr;
+    cudaError_t e = cudaMalloc(&v, std::max<size_t>(count, 1) * sizeof(T));
+    if (e != cudaSuccess) return fail(UT_ERR_CUDA, "cudaMalloc(%zu bytes) failed: %s", count * sizeof(T), cudaGetErrorString(e));
+    ws->allocations.push_back(v);
+    *p = static_cast<T*>(v);
+    return UT_OK;
+}
+
+std::string plan_issues(const ut_plan_desc* p) {
+    std::string s;
+    auto add = [&](const std::string& m) { s += (s.empty() ? "" : "\n") + m; };
+    if (!p) { add("null kernel description"); return s; }
+    if (p->family == UT_FAMILY_GLM_BERNOULLI_LOGIT) {
+        if (p->num_coefs < 1) add("GLM needs at least one covariate (num_coefs >= 1)");
+        if (p->has_intercept != 0 && p->has_intercept != 1) add("has_intercept must be 0 or 1");
+        if (p->num_params != p->num_coefs + (p->has_intercept ? 1 : 0))
+            add("num_params must equal num_coefs + has_intercept");
+        if (p->num_params > kGlmMaxF) add("GLM with more than 256 unconstrained parameters is not supported");
+        if (!(p->coef_sigma > 0.0)) add("coefficient prior scale must be > 0");
+        if (p->has_intercept && !(p->intercept_sigma > 0.0)) add("intercept prior scale must be > 0");
+        if (p->num_obs < 0) add("num_obs must be >= 0");
+    } else if (p->family == UT_FAMILY_HIER_NORMAL_NONCENTERED) {
+        if (p->num_groups < 1) add("hierarchical model needs at least one group (num_groups >= 1)");
+        if (p->num_params != p->num_groups + 2) add("num_params must equal num_groups + 2 (mu, log tau, z_1..z_J)");
+        if (inst_k(p->num_params) < 0) add("hierarchical model with more than 544 parameters is not supported");
+        if (!(p->mu_scale > 0.0)) add("mu prior scale must be > 0");
+        if (!(p->tau_scale > 0.0)) add("tau prior scale must be > 0");
+        if (p->num_obs < 0) add("num_obs must be >= 0");
+    } else {
+        char b[96];
+        snprintf(b, sizeof(b), "unsupported kernel-description family %d", p->family);
+        add(b);
+    }
+    return s;
+}
+
+size_t warp_smem_bytes(const ut_workspace* ws, int warps) {
+    return (size_t)ws->dm.staged_floats * sizeof(float) + (size_t)warps * ws->dm.Ppad * sizeof(float);
+}
+
+int32_t need_device() {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
+        return fail(UT_ERR_NO_DEVICE, "no CUDA device is visible; the B200 backend has no CPU fallback");
+    return UT_OK;
+}
+
+// ---- kernel dispatch over the compile-time slot count K and GLM width DMAX ----
+#define UT_DISPATCH_WARP(ws, KERNEL, ...)                                                                    \
+    do {                                                                                                     \
+        if ((ws)->dm.family == kFamGlm) {                                                                    \
+            if ((ws)->K == 1 && (ws)->dmax == 16) { KERNEL(kFamGlm, 1, 16, __VA_ARGS__); }                   \
+            else if ((ws)->K == 1) { KERNEL(kFamGlm, 1, 32, __VA_ARGS__); }                                  \
+            else { KERNEL(kFamGlm, 2, 32, __VA_ARGS__); }                                                   \
+        } else {                                                                                             \
+            switch ((ws)->K) {                                                                               \
+                case 1: KERNEL(kFamHier, 1, 1, __VA_ARGS__); break;                                          \
+                case 2: KERNEL(kFamHier, 2, 1, __VA_ARGS__); break;                                          \
+                case 3: KERNEL(kFamHier, 3, 1, __VA_ARGS__); break;                                          \
+                case 4: KERNEL(kFamHier, 4, 1, __VA_ARGS__); break;                                          \
+                case 8: KERNEL(kFamHier, 8, 1, __VA_ARGS__); break;                                          \
+                default: KERNEL(kFamHier, 17, 1, __VA_ARGS__); break;                                        \
+            }                                                                                                \
+        }                                                                                                    \
+    } while (0)
+
+template <class Kern>
+cudaError_t launch_dyn(Kern kern, dim3 grid, dim3 block, size_t smem, cudaStream_t st) {
+    (void)st;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+#define LAUNCH_DENSITY(FAM, K, DM, ws, params, totals, grads, st)                                           \
+    {                                                                                                      \
+        auto kern = density_warp_kernel<FAM, K, DM>;                                                        \
+        size_t smem = warp_smem_bytes(ws, kWarpsDensity);                                                   \
+        UT_CUDA(launch_dyn(kern, 0, 0, smem, st));                                                          \
+        kern<<<((ws)->C + kWarpsDensity - 1) / kWarpsDensity, 32 * kWarpsDensity, smem, st>>>((ws)->dm, params, totals, grads, (ws)->C); \
+    }
+
+#define LAUNCH_HMC(FAM, K, DM, ws, args, st)                                                                \
+    {                                                                                                      \
+        auto kern = hmc_warp_kernel<FAM, K, DM>;                                                            \
+        size_t smem = warp_smem_bytes(ws, kWarpsDensity);                                                   \
+        UT_CUDA(launch_dyn(kern, 0, 0, smem, st));                                                          \
+        kern<<<((ws)->C + kWarpsDensity - 1) / kWarpsDensity, 32 * kWarpsDensity, smem, st>>>((ws)->dm, args); \
+    }
+
+#define LAUNCH_PROBE(FAM, K, DM, ws, args, st)                                                              \
+    {                                                                                                      \
+        auto kern = probe_warp_kernel<FAM, K, DM>;                                                          \
+        size_t smem = warp_smem_bytes(ws, kWarpsDensity);                                                   \
+        UT_CUDA(launch_dyn(kern, 0, 0, smem, st));                                                          \
+        kern<<<((ws)->C + kWarpsDensity - 1) / kWarpsDensity, 32 * kWarpsDensity, smem, st>>>((ws)->dm, args); \
+    }
+
+#define LAUNCH_NUTS(FAM, K, DM, ws, args, st)                                                               \
+    {                                                                                                      \
+        auto kern = nuts_warp_kernel<FAM, K, DM>;                                                           \
+        size_t smem = warp_smem_bytes(ws, kWarpsNuts);                                                      \
+        UT_CUDA(launch_dyn(kern, 0, 0, smem, st));                                                          \
+        kern<<<((ws)->C + kWarpsNuts - 1) / kWarpsNuts, 32 * kWarpsNuts, smem, st>>>((ws)->dm, args);     \
+    }
+
+#define UT_K_SWITCH(KV, ...)                                        \
+    switch (KV) {                                                   \
+        case 1: { constexpr int K = 1; __VA_ARGS__; } break;        \
+        case 2: { constexpr int K = 2; __VA_ARGS__; } break;        \
+        case 3: { constexpr int K = 3; __VA_ARGS__; } break;        \
+        case 4: { constexpr int K = 4; __VA_ARGS__; } break;        \
+        default: { constexpr int K = 8; __VA_ARGS__; } break;       \
+    }
+
+size_t tiled_smem_bytes(int F) {
+    return sizeof(float) * ((size_t)F * kGlmCT + (size_t)F * kGlmXS + (size_t)kGlmOT * kGlmRS + kGlmOT + 16 * kGlmCT);
+}
+
+template <bool GRAD>
+int32_t launch_tiled_t(ut_workspace* ws, const float* params, float* totals, float* grads, cudaStream_t st) {
+    GlmTiledArgs a;
+    a.Xa = ws->d_Xa; a.y = ws->d_y; a.params = params;
+    a.part_ll = ws->d_part_ll; a.part_g = ws->d_part_g;
+    a.N = ws->N; a.F = ws->P; a.C = ws->C; a.obs_per_split = ws->obs_per_split;
+    dim3 grid((ws->C + kGlmCT - 1) / kGlmCT, ws->splits);
+    size_t smem = tiled_smem_bytes(ws->P);
+#define TILED_CASE(FPTV)                                                                  \
+    case FPTV: {                                                                          \
+        auto kern = glm_tiled_kernel<GRAD, FPTV>;                                         \
+        UT_CUDA(launch_dyn(kern, 0, 0, smem, st));                                        \
+        kern<<<grid, 256, smem, st>>>(a);                                                 \
+    } break;
+    switch (ws->fpt) {
+        TILED_CASE(1) TILED_CASE(2) TILED_CASE(4) TILED_CASE(7) TILED_CASE(8) TILED_CASE(12)
+        default: TILED_CASE(16)
+    }
+#undef TILED_CASE
+    UT_LAUNCHED();
+    GlmReduceArgs r;
+    r.params = params; r.part_ll = ws->d_part_ll; r.part_g = GRAD ? ws->d_part_g : nullptr;
+    r.totals = totals; r.grads = GRAD ? grads : nullptr;
+    r.S = ws->splits; r.C = ws->C; r.F = ws->P; r.off = ws->plan.has_intercept;
+    r.icpt_mu = (float)ws->plan.intercept_mu; r.icpt_sigma = (float)ws->plan.intercept_sigma;
+    r.coef_mu = (float)ws->plan.coef_mu; r.coef_sigma = (float)ws->plan.coef_sigma;
+    glm_reduce_kernel<<<(ws->C + 7) / 8, 256, 0, st>>>(r);
+    UT_LAUNCHED();
+    return UT_OK;
+}
+
+// Batched density on device buffers, whichever path the workspace uses.
+int32_t density(ut_workspace* ws, const float* params, float* totals, float* grads, cudaStream_t st) {
+    if (ws->path == kPathWarp) {
+        UT_DISPATCH_WARP(ws, LAUNCH_DENSITY, ws, params, totals, grads, st);
+        UT_LAUNCHED();
+        return UT_OK;
+    }
+    if (ws->tc.enabled && grads) return tc_glm_launch(ws->tc, params, totals, grads, st) == cudaSuccess
+                                            ? UT_OK
+                                            : fail(UT_ERR_CUDA, "tensor-core GLM launch failed: %s",
+                                                   cudaGetErrorString(cudaGetLastError()));
+    return grads ? launch_tiled_t<true>(ws, params, totals, grads, st) : launch_tiled_t<false>(ws, params, totals, nullptr, st);
+}
+
+int32_t ensure_lf(ut_workspace* ws) {
+    if (ws->lf.wq) return UT_OK;
+    size_t pc = (size_t)ws->P * ws->C;
+    int32_t rc;
+    if ((rc = dalloc(ws, &ws->lf.wq, pc))) return rc;
+    if ((rc = dalloc(ws, &ws->lf.wp, pc))) return rc;
+    if ((rc = dalloc(ws, &ws->lf.wg, pc))) return rc;
+    if ((rc = dalloc(ws, &ws->lf.wlj, ws->C))) return rc;
+    if ((rc = dalloc(ws, &ws->lf.H0, ws->C))) return rc;
+    if ((rc = dalloc(ws, &ws->lf.valid, ws->C))) return rc;
+    return UT_OK;
+}
+
+int32_t ensure_host_buffers(ut_workspace* ws) {
+    if (ws->d_params) return UT_OK;
+    size_t pc = (size_t)ws->P * ws->C;
+    int32_t rc;
+    if ((rc = dalloc(ws, &ws->d_params, pc))) return rc;
+    if ((rc = dalloc(ws, &ws->d_totals, ws->C))) return rc;
+    if ((rc = dalloc(ws, &ws->d_grads, pc))) return rc;
+    return UT_OK;
+}
+
+int32_t check_ws(const ut_workspace* ws) {
+    if (!ws) return fail(UT_ERR_ARGUMENT, "null workspace handle");
+    return UT_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+const char* ut_version(void) { return "uncertaintea_b200 0.1.0 (sm_100a)"; }
+
+int32_t ut_last_error(char* buf, size_t len) {
+    if (buf && len > 0) {
+        size_t n = std::min(len - 1, g_last_error.size());
+        memcpy(buf, g_last_error.data(), n);
+        buf[n] = '\0';
+    }
+    return (int32_t)g_last_error.size();
+}
+
+int32_t ut_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+int32_t ut_lowering_report(const ut_plan_desc* plan, char* issues, size_t len) {
+    std::string s = plan_issues(plan);
+    if (issues && len > 0) {
+        size_t n = std::min(len - 1, s.size());
+        memcpy(issues, s.data(), n);
+        issues[n] = '\0';
+    }
+    if (!s.empty()) return fail(UT_ERR_UNSUPPORTED, "kernel description cannot be lowered to the device path:\n%s", s.c_str());
+    return UT_OK;
+}
+
+int32_t ut_workspace_create(const ut_plan_desc* plan, const float* observed, int64_t observed_rows,
+                            int64_t observed_cols, const int32_t* trip_counts, const int32_t* loop_starts,
+                            int32_t num_loops, int32_t batch_size, int32_t precision_bits, ut_workspace** out) {
+    if (!out) return fail(UT_ERR_ARGUMENT, "null output handle");
+    *out = nullptr;
+    if (precision_bits != 32)
+        return fail(UT_ERR_PRECISION,
+                    "the B200 backend does not support Float%d arithmetic; request precision=Float32 instead",
+                    (int)precision_bits);
+    std::string issues = plan_issues(plan);
+    if (!issues.empty()) return fail(UT_ERR_UNSUPPORTED, "kernel description cannot be lowered to the device path:\n%s", issues.c_str());
+    if (batch_size < 1) return fail(UT_ERR_ARGUMENT, "batch size must be >= 1, got %d", (int)batch_size);
+    if (observed_cols != 1)
+        return fail(UT_ERR_UNSUPPORTED, "per-chain observation columns (observed_cols=%lld) are not supported; stage one shared column",
+                    (long long)observed_cols);
+    const int N = plan->num_obs;
+    if (plan->family == UT_FAMILY_GLM_BERNOULLI_LOGIT) {
+        int64_t want = (int64_t)N * (plan->num_coefs + 1);
+        if (observed_rows != want)
+            return fail(UT_ERR_DIMENSION, "expected %lld staged observation rows (N*(D+1)), got %lld", (long long)want,
+                        (long long)observed_rows);
+    } else {
+        int64_t want = (int64_t)N + plan->num_groups;
+        if (observed_rows != want)
+            return fail(UT_ERR_DIMENSION, "expected %lld staged observation rows (N+J), got %lld", (long long)want,
+                        (long long)observed_rows);
+        if (num_loops != plan->num_groups || !trip_counts || !loop_starts)
+            return fail(UT_ERR_DIMENSION, "expected %d trip counts / loop starts, got %d", plan->num_groups, (int)num_loops);
+        int64_t total = 0;
+        for (int j = 0; j < num_loops; ++j) {
+            if (trip_counts[j] < 0 || loop_starts[j] < 0 || (int64_t)loop_starts[j] + trip_counts[j] > N)
+                return fail(UT_ERR_ARGUMENT, "group %d has an out-of-range observation block", j);
+            total += trip_counts[j];
+        }
+        if (total != N) return fail(UT_ERR_DIMENSION, "trip counts sum to %lld, expected %d", (long long)total, N);
+    }
+    if (N > 0 && !observed) return fail(UT_ERR_ARGUMENT, "null observation buffer");
+    int32_t rc = need_device();
+    if (rc) return rc;
+
+    ut_workspace* ws = new ut_workspace();
+    ws->plan = *plan;
+    ws->P = plan->num_params;
+    ws->C = batch_size;
+    ws->N = N;
+    cudaGetDevice(&ws->device);
+    auto bail = [&](int32_t code) {
+        ut_workspace_destroy(ws);
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(UT_ERR_CUDA, "cudaStreamCreate failed"));
+
+    DevModel& dm = ws->dm;
+    memset(&dm, 0, sizeof(dm));
+    dm.P = ws->P;
+    ws->K = inst_k(ws->P);
+    dm.Ppad = 32 * ws->K;
+    if (plan->family == UT_FAMILY_GLM_BERNOULLI_LOGIT) {
+        const int D = plan->num_coefs, off = plan->has_intercept ? 1 : 0, F = ws->P;
+        dm.family = kFamGlm;
+        dm.glm.N = N; dm.glm.D = D; dm.glm.off = off;
+        dm.glm.icpt_mu = (float)plan->intercept_mu; dm.glm.icpt_sigma = (float)plan->intercept_sigma;
+        dm.glm.coef_mu = (float)plan->coef_mu; dm.glm.coef_sigma = (float)plan->coef_sigma;
+        std::vector<float> y(N);
+        for (int i = 0; i < N; ++i) y[i] = observed[(size_t)i * (D + 1) + D];
+        if ((rc = dalloc(ws, &ws->d_y, N))) return bail(rc);
+        UT_CUDA(cudaMemcpy(ws->d_y, y.data(), sizeof(float) * N, cudaMemcpyHostToDevice));
+        dm.glm.y = ws->d_y;
+        size_t staged = (size_t)N * (D + 1);
+        bool warp_ok = D <= 32 && (staged * 4 + (size_t)kWarpsDensity * dm.Ppad * 4) <= kSmemBudget;
+        if (warp_ok) {
+            ws->path = kPathWarp;
+            ws->dmax = D <= 16 ? 16 : 32;
+            std::vector<float> XT((size_t)D * N);
+            for (int i = 0; i < N; ++i)
+                for (int d = 0; d < D; ++d) XT[(size_t)d * N + i] = observed[(size_t)i * (D + 1) + d];
+            if ((rc = dalloc(ws, &ws->d_XT, XT.size()))) return bail(rc);
+            UT_CUDA(cudaMemcpy(ws->d_XT, XT.data(), sizeof(float) * XT.size(), cudaMemcpyHostToDevice));
+            dm.glm.XT = ws->d_XT;
+            dm.stage = 1;
+            dm.staged_floats = (int)(((staged + 3) / 4) * 4);
+        } else {
+            ws->path = kPathTiled;
+            std::vector<float> Xa((size_t)N * F);
+            for (int i = 0; i < N; ++i) {
+                if (off) Xa[(size_t)i * F] = 1.0f;
+                for (int d = 0; d < D; ++d) Xa[(size_t)i * F + off + d] = observed[(size_t)i * (D + 1) + d];
+            }
+            if ((rc = dalloc(ws, &ws->d_Xa, Xa.size()))) return bail(rc);
+            UT_CUDA(cudaMemcpy(ws->d_Xa, Xa.data(), sizeof(float) * Xa.size(), cudaMemcpyHostToDevice));
+            int dev_sms = 148;
+            cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, ws->device);
+            int ctiles = (ws->C + kGlmCT - 1) / kGlmCT;
+            int target = 3 * dev_sms;
+            int chunks = std::max(1, (N + kGlmOT - 1) / kGlmOT);
+            int S = std::max(1, std::min(chunks, (target + ctiles - 1) / ctiles));
+            int per = (chunks + S - 1) / S;
+            ws->obs_per_split = per * kGlmOT;
+            ws->splits = std::max(1, (N + ws->obs_per_split - 1) / ws->obs_per_split);
+            int need = (F + 15) / 16;
+            const int fpts[] = {1, 2, 4, 7, 8, 12, 16};
+            for (int v : fpts) if (need <= v) { ws->fpt = v; break; }
+            if ((rc = dalloc(ws, &ws->d_part_ll, (size_t)ws->splits * ws->C))) return bail(rc);
+            if ((rc = dalloc(ws, &ws->d_part_g, (size_t)ws->splits * ws->C * F))) return bail(rc);
+            if ((rc = tc_glm_setup(ws->tc, ws->d_Xa, ws->d_y, N, F, ws->C, off, (float)plan->intercept_mu,
+                                   (float)plan->intercept_sigma, (float)plan->coef_mu, (float)plan->coef_sigma,
+                                   dev_sms, &ws->allocations))) {
+                return bail(fail(UT_ERR_CUDA, "tensor-core GLM setup failed: %s", tc_glm_last_error()));
+            }
+        }
+    } else {
+        const int J = plan->num_groups;
+        dm.family = kFamHier;
+        dm.hier.N = N; dm.hier.J = J;
+        dm.hier.mu_loc = (float)plan->mu_loc; dm.hier.mu_scale = (float)plan->mu_scale;
+        dm.hier.tau_scale = (float)plan->tau_scale;
+        if ((rc = dalloc(ws, &ws->d_y, N + J))) return bail(rc);
+        UT_CUDA(cudaMemcpy(ws->d_y, observed, sizeof(float) * (N + J), cudaMemcpyHostToDevice));
+        if ((rc = dalloc(ws, &ws->d_start, J))) return bail(rc);
+        if ((rc = dalloc(ws, &ws->d_count, J))) return bail(rc);
+        UT_CUDA(cudaMemcpy(ws->d_start, loop_starts, sizeof(int32_t) * J, cudaMemcpyHostToDevice));
+        UT_CUDA(cudaMemcpy(ws->d_count, trip_counts, sizeof(int32_t) * J, cudaMemcpyHostToDevice));
+        dm.hier.y = ws->d_y;
+        dm.hier.sig = ws->d_y + N;
+        dm.hier.start = ws->d_start;
+        dm.hier.count = ws->d_count;
+        ws->path = kPathWarp;
+        size_t staged = (size_t)N + 3 * (size_t)J;
+        dm.stage = (staged * 4 + (size_t)kWarpsDensity * dm.Ppad * 4) <= kSmemBudget ? 1 : 0;
+        dm.staged_floats = dm.stage ? (int)(((staged + 3) / 4) * 4) : 0;
+    }
+    *out = ws;
+    return UT_OK;
+}
+
+int32_t ut_workspace_destroy(ut_workspace* ws) {
+    if (!ws) return UT_OK;
+    for (void* p : ws->allocations) cudaFree(p);
+    if (ws->stream) cudaStreamDestroy(ws->stream);
+    delete ws;
+    return UT_OK;
+}
+
+int32_t ut_workspace_info(const ut_workspace* ws, int32_t* num_params, int32_t* batch_size) {
+    int32_t rc = check_ws(ws);
+    if (rc) return rc;
+    if (num_params) *num_params = ws->P;
+    if (batch_size) *batch_size = ws->C;
+    return UT_OK;
+}
+
+int32_t ut_logjoint_device(ut_workspace* ws, const float* d_params, float* d_totals, void* stream) {
+    int32_t rc = check_ws(ws);
+    if (rc) return rc;
+    if (!d_params || !d_totals) return fail(UT_ERR_ARGUMENT, "null device buffer");
+    return density(ws, d_params, d_totals, nullptr, (cudaStream_t)stream);
+}
+
+int32_t ut_logjoint_gradient_device(ut_workspace* ws, const float* d_params, float* d_totals, float* d_gradients,
+                                    void* stream) {
+    int32_t rc = check_ws(ws);
+    if (rc) return rc;
+    if (!d_params || !d_totals || !d_gradients) return fail(UT_ERR_ARGUMENT, "null device buffer");
+    return density(ws, d_params, d_totals, d_gradients, (cudaStream_t)stream);
+}
+
+int32_t ut_logjoint(ut_workspace* ws, const float* params, float* totals) {
+    int32_t rc = check_ws(ws);
+    if (rc) return rc;
+    if (!params || !totals) return fail(UT_ERR_ARGUMENT, "null host buffer");
+    if ((rc = ensure_host_buffers(ws))) return rc;
+    size_t pc = (size_t)ws->P * ws->C;
+    UT_CUDA(cudaMemcpyAsync(ws->d_params, params, pc * sizeof(float), cudaMemcpyHostToDevice, ws->stream));
+    if ((rc = density(ws, ws->d_params, ws->d_totals, nullptr, ws->stream))) return rc;
+    UT_CUDA(cudaMemcpyAsync(totals, ws->d_totals, ws->C * sizeof(float), cudaMemcpyDeviceToHost, ws->stream));
+    UT_CUDA(cudaStreamSynchronize(ws->stream));
+    return UT_OK;
+}
+
+int32_t ut_logjoint_gradient(ut_workspace* ws, const float* params, float* totals, float* gradients) {
+    int32_t rc = check_ws(ws);
+    if (rc) return rc;
+    if (!params || !totals || !gradients) return fail(UT_ERR_ARGUMENT, "null host buffer");
+    if ((rc = ensure_host_buffers(ws))) return rc;
+    size_t pc = (size_t)ws->P * ws->C;
+    UT_CUDA(cudaMemcpyAsync(ws->d_params, params, pc * sizeof(float), cudaMemcpyHostToDevice, ws->stream));
+    if ((rc = density(ws, ws->d_params, ws->d_totals, ws->d_grads, ws->stream))) return rc;
+    UT_CUDA(cudaMemcpyAsync(totals, ws->d_totals, ws->C * sizeof(float), cudaMemcpyDeviceToHost, ws->stream));
+    UT_CUDA(cudaMemcpyAsync(gradients, ws->d_grads, pc * sizeof(float), cudaMemcpyDeviceToHost, ws->stream));
+    UT_CUDA(cudaStreamSynchronize(ws->stream));
+    return UT_OK;
+}
+
+// ---- Philox ---------------------------------------------------------------
+int32_t ut_philox4x32(const uint32_t* keys, const uint32_t* counters, int64_t n, uint32_t* out) {
+    if (n < 0 || (n > 0 && (!keys || !counters || !out))) return fail(UT_ERR_ARGUMENT, "invalid Philox batch");
+    if (n == 0) return UT_OK;
+    int32_t rc = need_device();
+    if (rc) return rc;
+    uint32_t *dk = nullptr, *dc = nullptr, *dout = nullptr;
+    UT_CUDA(cudaMalloc(&dk, n * 2 * sizeof(uint32_t)));
+    UT_CUDA(cudaMalloc(&dc, n * 4 * sizeof(uint32_t)));
+    UT_CUDA(cudaMalloc(&dout, n * 4 * sizeof(uint32_t)));
+    UT_CUDA(cudaMemcpy(dk, keys, n * 2 * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    UT_CUDA(cudaMemcpy(dc, counters, n * 4 * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    philox_batch_kernel<<<(unsigned)((n + 255) / 256), 256>>>(dk, dc, n, dout);
+    UT_LAUNCHED();
+    UT_CUDA(cudaMemcpy(out, dout, n * 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    cudaFree(dk); cudaFree(dc); cudaFree(dout);
+    return UT_OK;
+}
+
+static int32_t rand_common(uint32_t chain, uint32_t iteration, uint32_t stream, uint32_t draw_start, int64_t n,
+                           float* out, int normal) {
+    if (n < 0 || (n > 0 && !out)) return fail(UT_ERR_ARGUMENT, "invalid draw batch");
+    if (n == 0) return UT_OK;
+    int32_t rc = need_device();
+    if (rc) return rc;
+    float* d = nullptr;
+    UT_CUDA(cudaMalloc(&d, n * sizeof(float)));
+    rand_batch_kernel<<<(unsigned)((n + 255) / 256), 256>>>(chain, iteration, stream, draw_start, n, normal, d);
+    UT_LAUNCHED();
+    UT_CUDA(cudaMemcpy(out, d, n * sizeof(float), cudaMemcpyDeviceToHost));
+    cudaFree(d);
+    return UT_OK;
+}
+
+int32_t ut_rand_uniform(uint32_t chain, uint32_t iteration, uint32_t stream, uint32_t draw_start, int64_t n,
+                        float* out) {
+    return rand_common(chain, iteration, stream, draw_start, n, out, 0);
+}
+int32_t ut_rand_normal(uint32_t chain, uint32_t iteration, uint32_t stream, uint32_t draw_start, int64_t n,
+                       float* out) {
+    return rand_common(chain, iteration, stream, draw_start, n, out, 1);
+}
+
+// ---- HMC ------------------------------------------------------------------
+int32_t ut_hmc_iteration(ut_workspace* ws, const ut_hmc_buffers* buf, int32_t num_leapfrog_steps,
+                         uint32_t iteration_coord, float divergence_threshold, void* stream) {
+    int32_t rc = check_ws(ws);
+    if (rc) return rc;
+    if (!buf || !buf->position || !buf->gradient || !buf->logjoint || !buf->inverse_mass || !buf->step ||
+        !buf->accept_prob || !buf->energy || !buf->energy_error || !buf->accepted || !buf->divergent)
+        return fail(UT_ERR_ARGUMENT, "null HMC buffer");
+    if (num_leapfrog_steps < 1) return fail(UT_ERR_ARGUMENT, "num_leapfrog_steps must be >= 1, got %d", (int)num_leapfrog_steps);
+    cudaStream_t st = (cudaStream_t)stream;
+    HmcArgs a;
+    a.position = buf->position; a.gradient = buf->gradient; a.logjoint = buf->logjoint;
+    a.inverse_mass = buf->inverse_mass; a.step = buf->step;
+    a.accept_prob = buf->accept_prob; a.energy = buf->energy; a.energy_error = buf->energy_error;
+    a.accepted = buf->accepted; a.divergent = buf->divergent;
+    a.proposal = buf->proposal; a.endpoint_momentum = buf->endpoint_momentum;
+    a.C = ws->C; a.L = num_leapfrog_steps; a.coord = iteration_coord; a.thr = divergence_threshold;
+    if (ws->path == kPathWarp) {
+        UT_DISPATCH_WARP(ws, LAUNCH_HMC, ws, a, st);
+        UT_LAUNCHED();
+        return UT_OK;
+    }
+    if ((rc = ensure_lf(ws))) return rc;
+    const int P = ws->P;
+    const unsigned grid = (ws->C + 7) / 8;
+    UT_K_SWITCH(ws->K, lf_begin_kernel<K><<<grid, 256, 0, st>>>(a, ws->lf, P));
+    UT_LAUNCHED();
+    for (int l = 1; l <= num_leapfrog_steps; ++l) {
+        if ((rc = density(ws, ws->lf.wq, ws->lf.wlj, ws->lf.wg, st))) return rc;
+        UT_K_SWITCH(ws->K, lf_step_kernel<K><<<grid, 256, 0, st>>>(a, ws->lf, P, l));
+        UT_LAUNCHED();
+    }
+    return UT_OK;
+}
+
+int32_t ut_leapfrog_probe(ut_workspace* ws, const float* d_position, const float* d_gradient, const float* d_logjoint,
+                          const float* d_inverse_mass, const float* d_trial_step, uint32_t iteration_coord,
+                          float* d_log_accept_ratio, void* stream) {
+    int32_t rc = check_ws(ws);
+    if (rc) return rc;
+    if (!d_position || !d_gradient || !d_logjoint || !d_inverse_mass || !d_trial_step || !d_log_accept_ratio)
+        return fail(UT_ERR_ARGUMENT, "null probe buffer");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (ws->path == kPathWarp) {
+        ProbeArgs a;
+        a.position = d_position; a.gradient = d_gradient; a.logjoint = d_logjoint;
+        a.inverse_mass = d_inverse_mass; a.trial_step = d_trial_step; a.log_accept_ratio = d_log_accept_ratio;
+        a.C = ws->C; a.coord = iteration_coord;
+        UT_DISPATCH_WARP(ws, LAUNCH_PROBE, ws, a, st);
+        UT_LAUNCHED();
+        return UT_OK;
+    }
+    if ((rc = ensure_lf(ws))) return rc;
+    HmcArgs a = {};
+    a.position = const_cast<float*>(d_position); a.gradient = const_cast<float*>(d_gradient);
+    a.logjoint = const_cast<float*>(d_logjoint); a.inverse_mass = d_inverse_mass; a.step = d_trial_step;
+    a.C = ws->C; a.L = 1; a.coord = iteration_coord;
+    const int P = ws->P;
+    const unsigned grid = (ws->C + 7) / 8;
+    UT_K_SWITCH(ws->K, lf_begin_kernel<K><<<grid, 256, 0, st>>>(a, ws->lf, P));
+    UT_LAUNCHED();
+    if ((rc = density(ws, ws->lf.wq, ws->lf.wlj, ws->lf.wg, st))) return rc;
+    UT_K_SWITCH(ws->K, lf_probe_close_kernel<K><<<grid, 256, 0, st>>>(d_inverse_mass, d_trial_step, ws->lf,
+                                                                        d_log_accept_ratio, P, ws->C));
+    UT_LAUNCHED();
+    return UT_OK;
+}
+
+// ---- persistent NUTS --------------------------------------------------------
+int32_t ut_persistent_nuts_iteration(ut_workspace* ws, const ut_nuts_buffers* buf, int32_t max_tree_depth,
+                                     float divergence_threshold, uint32_t iteration_coord, void* stream) {
+    int32_t rc = check_ws(ws);
+    if (rc) return rc;
+    if (!buf || !buf->position || !buf->gradient || !buf->logjoint || !buf->inverse_mass || !buf->step ||
+        !buf->accept_prob || !buf->energy || !buf->energy_error || !buf->tree_depth || !buf->integration_steps ||
+        !buf->divergent || !buf->moved)
+        return fail(UT_ERR_ARGUMENT, "null NUTS buffer");
+    if (max_tree_depth < 1 || max_tree_depth > 30)
+        return fail(UT_ERR_ARGUMENT, "max_tree_depth must be in 1..30, got %d", (int)max_tree_depth);
+    if (ws->path != kPathWarp)
+        return fail(UT_ERR_UNSUPPORTED,
+                    "the persistent NUTS tree needs a per-chain (warp) evaluator; this model's observation data "
+                    "does not fit the warp path (use batched_chees / batched_hmc for it)");
+    if (ws->ckpt_depth < max_tree_depth) {
+        if (ws->d_ckpt) {
+            cudaFree(ws->d_ckpt);
+            ws->allocations.erase(std::remove(ws->allocations.begin(), ws->allocations.end(), (void*)ws->d_ckpt),
+                                  ws->allocations.end());
+            ws->d_ckpt = nullptr;
+        }
+        if ((rc = dalloc(ws, &ws->d_ckpt, (size_t)ws->C * (max_tree_depth + 1) * 2 * 32 * ws->K))) return rc;
+        ws->ckpt_depth = max_tree_depth;
+    }
+    NutsArgs a;
+    a.position = buf->position; a.gradient = buf->gradient; a.logjoint = buf->logjoint;
+    a.inverse_mass = buf->inverse_mass; a.step = buf->step;
+    a.accept_prob = buf->accept_prob; a.energy = buf->energy; a.energy_error = buf->energy_error;
+    a.tree_depth = buf->tree_depth; a.integration_steps = buf->integration_steps;
+    a.divergent = buf->divergent; a.moved = buf->moved;
+    a.ckpt = ws->d_ckpt; a.C = ws->C; a.max_depth = max_tree_depth; a.coord = iteration_coord;
+    a.thr = divergence_threshold;
+    cudaStream_t st = (cudaStream_t)stream;
+    UT_DISPATCH_WARP(ws, LAUNCH_NUTS, ws, a, st);
+    UT_LAUNCHED();
+    return UT_OK;
+}
+
+// ---- ChEES ---------------------------------------------------------------
+int32_t ut_chees_reduce(ut_workspace* ws, const float* d_initials, const float* d_proposals,
+                        const float* d_endpoint_momentum, const float* d_accept_prob, const uint8_t* d_divergent,
+                        const float* d_inverse_mass, double* out, void* stream) {
+    int32_t rc = check_ws(ws);
+    if (rc) return rc;
+    if (!d_initials || !d_proposals || !d_endpoint_momentum || !d_accept_prob || !d_divergent || !d_inverse_mass || !out)
+        return fail(UT_ERR_ARGUMENT, "null ChEES buffer");
+    if (!ws->d_flags) {
+        if ((rc = dalloc(ws, &ws->d_flags, ws->C))) return rc;
+        if ((rc = dalloc(ws, &ws->d_means, 2 * (size_t)ws->P))) return rc;
+        if ((rc = dalloc(ws, &ws->d_terms, 2 * (size_t)ws->C))) return rc;
+        if ((rc = dalloc(ws, &ws->d_out, 2))) return rc;
+    }
+    CheesArgs a;
+    a.initials = d_initials; a.proposals = d_proposals; a.momenta = d_endpoint_momentum;
+    a.accept = d_accept_prob; a.divergent = d_divergent; a.inverse_mass = d_inverse_mass;
+    a.flags = ws->d_flags; a.means = ws->d_means; a.chain_terms = ws->d_terms; a.out = ws->d_out;
+    a.P = ws->P; a.C = ws->C;
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned gw = (ws->C + 7) / 8;
+    chees_flags_kernel<<<gw, 256, 0, st>>>(a);
+    chees_means_kernel<<<ws->P, 256, 0, st>>>(a);
+    chees_terms_kernel<<<gw, 256, 0, st>>>(a);
+    chees_final_kernel<<<1, 256, 0, st>>>(a);
+    UT_LAUNCHED();
+    UT_CUDA(cudaMemcpyAsync(out, ws->d_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    UT_CUDA(cudaStreamSynchronize(st));
+    return UT_OK;
+}
+
+// ---- warmup adaptation ----------------------------------------------------
+int32_t ut_running_variance_update(const float* d_positions, const double* d_weights, int32_t num_params,
+                                   int32_t num_chains, double* d_state, int32_t window_length, void* stream) {
+    if (!d_positions || !d_weights || !d_state) return fail(UT_ERR_ARGUMENT, "null running-variance buffer");
+    if (num_params < 1 || num_params > 1024) return fail(UT_ERR_ARGUMENT, "num_params must be in 1..1024, got %d", (int)num_params);
+    if (num_chains < 0) return fail(UT_ERR_ARGUMENT, "num_chains must be >= 0");
+    if (window_length < 1) return fail(UT_ERR_ARGUMENT, "running variance state requires window_length > 0");
+    if (num_chains == 0) return UT_OK;
+    int threads = ((num_params + 31) / 32) * 32;
+    size_t smem = (size_t)32 * num_params * sizeof(float);
+    UT_CUDA(launch_dyn(running_variance_kernel, 0, 0, smem, nullptr));
+    running_variance_kernel<<<1, threads, smem, (cudaStream_t)stream>>>(d_positions, d_weights, num_params, num_chains,
+                                                                      d_state, window_length);
+    UT_LAUNCHED();
+    return UT_OK;
+}
+
+}  // extern "C"

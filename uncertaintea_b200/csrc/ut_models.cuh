@@ -1,0 +1,167 @@
+// ut_models.cuh -- warp-cooperative logjoint + analytic gradient of ONE chain
+// for each supported kernel-description family.
+//
+// A chain's P unconstrained parameters are spread over the 32 lanes of a warp:
+// parameter p lives in slot k = p / 32 of lane p % 32.  Every function below is
+// called by all 32 lanes with the same chain and returns the same logjoint in
+// every lane (warp_sum is an xor butterfly, so all lanes see bit-identical
+// sums and control flow that depends on them stays warp-uniform).
+#pragma once
+
+#include "ut_common.cuh"
+
+namespace ut {
+
+// Bernoulli-logit GLM (reference steps DeviceBernoulliLogitGLMChoiceStepDyn +
+// DeviceDiagNormalChoiceStepDyn; value at logjoint_kernel.jl:378-399, 514-533;
+// analytic gradient at gradient_kernel.jl:579-627 and 658-681).
+// Observation data is read covariate-major (XT[d * N + i]), so the 32 lanes of
+// a warp, which own consecutive observations, read consecutive addresses.
+struct GlmModel {
+    int N, D, off;  // off = 1 when an intercept row leads the parameters
+    float icpt_mu, icpt_sigma, coef_mu, coef_sigma;
+    const float* XT;  // D x N (covariate-major), shared memory or global
+    const float* y;   // N
+};
+
+// Hierarchical non-centred normal (reference semantics of the iid noncentered
+// latent, docs/noncentered-reparam.md:22-36; value terms of the Normal /
+// HalfCauchy(log) / Noncentered steps, logjoint_kernel.jl:105-129,177-182).
+struct HierModel {
+    int N, J;
+    float mu_loc, mu_scale, tau_scale;
+    const float* y;        // N, group after group
+    const float* sig;      // J
+    const int32_t* start;  // J
+    const int32_t* count;  // J
+};
+
+// Parameters in per-warp shared memory so every lane can read any coefficient
+// with a broadcast load.  `qs` has room for P floats.
+template <int K, int DMAX>
+__device__ __forceinline__ float glm_lj_grad(const GlmModel& m, int P, const float (&q)[K], float (&g)[K],
+                                             float* qs, bool want_grad) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        int p = lane + 32 * k;
+        if (p < P) qs[p] = q[k];
+    }
+    __syncwarp();
+    const int D = m.D, off = m.off, N = m.N;
+    const float a = off ? qs[0] : 0.0f;
+    float gacc[DMAX];
+    float gicpt = 0.0f;
+#pragma unroll
+    for (int d = 0; d < DMAX; ++d) gacc[d] = 0.0f;
+    float ll = 0.0f;
+    for (int i = lane; i < N; i += 32) {
+        float eta = a;
+#pragma unroll
+        for (int d = 0; d < DMAX; ++d)
+            if (d < D) eta = fmaf(qs[off + d], m.XT[(size_t)d * N + i], eta);
+        float yv = m.y[i];
+        ll += bernoullilogit_logpdf(eta, yv);
+        if (want_grad) {
+            float r = yv - logistic(eta);
+            gicpt += r;
+#pragma unroll
+            for (int d = 0; d < DMAX; ++d)
+                if (d < D) gacc[d] = fmaf(r, m.XT[(size_t)d * N + i], gacc[d]);
+        }
+    }
+    // prior terms by the owner lane of each parameter
+    float prior = 0.0f;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        int p = lane + 32 * k;
+        if (p < P) {
+            if (off && p == 0) prior += normal_logpdf(m.icpt_mu, m.icpt_sigma, q[k]);
+            else prior += normal_logpdf(m.coef_mu, m.coef_sigma, q[k]);
+        }
+    }
+    float total = warp_sum(ll + prior);
+    if (want_grad) {
+        gicpt = warp_sum(gicpt);
+#pragma unroll
+        for (int d = 0; d < DMAX; ++d)
+            if (d < D) gacc[d] = warp_sum(gacc[d]);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            int p = lane + 32 * k;
+            float gv = 0.0f;
+            if (p < P) {
+                if (off && p == 0) {
+                    gv = gicpt - (q[k] - m.icpt_mu) / (m.icpt_sigma * m.icpt_sigma);
+                } else {
+                    int d = p - off;
+#pragma unroll
+                    for (int dd = 0; dd < DMAX; ++dd)
+                        if (dd == d) gv = gacc[dd];
+                    gv -= (q[k] - m.coef_mu) / (m.coef_sigma * m.coef_sigma);
+                }
+            }
+            g[k] = gv;
+        }
+    }
+    __syncwarp();
+    return total;
+}
+
+template <int K>
+__device__ __forceinline__ float hier_lj_grad(const HierModel& m, int P, const float (&q)[K], float (&g)[K],
+                                              bool want_grad) {
+    const int lane = threadIdx.x & 31;
+    const float mu = __shfl_sync(UT_FULL_MASK, q[0], 0);
+    const float u = __shfl_sync(UT_FULL_MASK, q[0], 1);
+    const float tau = expf(u);
+    float ll = 0.0f, gmu = 0.0f, gtz = 0.0f;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        int p = lane + 32 * k;
+        float gv = 0.0f;
+        if (p >= 2 && p < P) {
+            int j = p - 2;
+            float z = q[k];
+            ll += normal_logpdf(0.0f, 1.0f, z);
+            float theta = mu + tau * z;
+            float sj = m.sig[j];
+            float inv_s2 = 1.0f / (sj * sj);
+            float ls = -logf(sj) - kHalfLog2Pi;
+            float inv_s = 1.0f / sj;
+            float dtheta = 0.0f, sq = 0.0f;
+            const int s0 = m.start[j], n = m.count[j];
+            for (int t = 0; t < n; ++t) {
+                float r = m.y[s0 + t] - theta;
+                sq = fmaf(r, r, sq);
+                dtheta += r;
+            }
+            // sum_t normal_logpdf(theta, sj, y_t) = n*ls - sq/(2 sj^2)
+            ll += (float)n * ls - 0.5f * sq * inv_s * inv_s;
+            dtheta *= inv_s2;
+            gmu += dtheta;
+            gtz += z * dtheta;
+            gv = -z + tau * dtheta;
+        }
+        g[k] = gv;
+    }
+    float prior = 0.0f;
+    if (lane == 0) prior += normal_logpdf(m.mu_loc, m.mu_scale, mu);
+    if (lane == 1) {
+        float z = tau / m.tau_scale;
+        prior += kLog2 - kLogPi - logf(m.tau_scale) - log1pf(z * z) + u;  // halfcauchy + log|J| = u
+    }
+    float total = warp_sum(ll + prior);
+    if (want_grad) {
+        gmu = warp_sum(gmu);
+        gtz = warp_sum(gtz);
+        if (lane == 0) g[0] = gmu - (mu - m.mu_loc) / (m.mu_scale * m.mu_scale);
+        if (lane == 1) {
+            float s2 = m.tau_scale * m.tau_scale;
+            g[0] = 1.0f - 2.0f * tau * tau / (s2 + tau * tau) + tau * gtz;
+        }
+    }
+    return total;
+}
+
+}  // namespace ut

@@ -1,0 +1,204 @@
+"""Model specifications and their lowering to the fixed kernel description.
+
+The reference lowers a ``@tea static`` model's execution plan into an
+``isbits`` ``DeviceExecutionPlan`` (src/device/plan/lowering.jl:1360) and
+stages its observations into a dense buffer (src/device/staging.jl:499).  A
+``TeaModelSpec`` here plays the role of that already-parsed model: it names a
+kernel-description family and its priors, and ``lower(args, constraints)``
+produces the ``PlanDesc`` plus the staged observation buffer that
+``ut_workspace_create`` takes.
+
+Calls mirror the reference: ``args`` carries the model's data arguments and
+``constraints`` the observed choices, e.g. for the logistic regression
+``args = (X,)`` and ``constraints = {"y": y}``.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native as nat
+
+
+@dataclass
+class Lowered:
+    plan: nat.PlanDesc
+    observed: np.ndarray            # float32, staged rows (one shared column)
+    trip_counts: np.ndarray         # int32 (may be empty)
+    loop_starts: np.ndarray         # int32 (may be empty)
+    num_params: int
+
+
+class TeaModelSpec:
+    """Base class: a model whose density lowers to a device kernel description."""
+
+    name = "model"
+
+    def parameter_names(self, args=(), constraints=None):
+        raise NotImplementedError
+
+    def lower(self, args=(), constraints=None) -> Lowered:
+        raise NotImplementedError
+
+    def num_params(self, args=(), constraints=None) -> int:
+        return len(self.parameter_names(args, constraints))
+
+    def constrain(self, unconstrained: np.ndarray, args=(), constraints=None) -> np.ndarray:
+        """Unconstrained draws (..., P) -> constrained values (..., P_constrained)."""
+        return np.asarray(unconstrained)
+
+    def initial_positions(self, rng: np.random.Generator, num_chains: int, args=(), constraints=None,
+                          init_strategy: str = "prior") -> np.ndarray:
+        raise NotImplementedError
+
+
+def _observed_value(constraints, key):
+    if constraints is None or key not in constraints:
+        raise ValueError(f"missing observed choice {key!r} in constraints")
+    return np.asarray(constraints[key], dtype=np.float64)
+
+
+@dataclass
+class BernoulliLogitGLM(TeaModelSpec):
+    """``beta ~ iid normal(coef_mu, coef_sigma)`` (+ optional intercept),
+    ``y_i ~ bernoullilogit(intercept + x_i . beta)``.
+
+    args = (X,) with X of shape (N, D) (observation-major; the reference's own
+    covariate matrix is D x N, ``X[:, i]`` being observation i -- pass
+    ``X.T`` of such a matrix).  constraints = {"y": y} with y in {0, 1}.
+    """
+
+    num_coefs: int
+    intercept: bool = False
+    coef_mu: float = 0.0
+    coef_sigma: float = 1.0
+    intercept_mu: float = 0.0
+    intercept_sigma: float = 2.5
+    name: str = "bernoulli_logit_glm"
+
+    def parameter_names(self, args=(), constraints=None):
+        names = ["alpha"] if self.intercept else []
+        return names + [f"beta[{d + 1}]" for d in range(self.num_coefs)]
+
+    def lower(self, args=(), constraints=None) -> Lowered:
+        if len(args) != 1:
+            raise ValueError(f"{self.name} expects args=(X,), got {len(args)} argument(s)")
+        X = np.asarray(args[0], dtype=np.float32)
+        if X.ndim != 2 or X.shape[1] != self.num_coefs:
+            raise IndexError(f"expected X of shape (N, {self.num_coefs}), got {X.shape}")
+        y = _observed_value(constraints, "y").astype(np.float32)
+        N = X.shape[0]
+        if y.shape != (N,):
+            raise IndexError(f"expected y of length {N}, got shape {y.shape}")
+        staged = np.empty((N, self.num_coefs + 1), dtype=np.float32)
+        staged[:, : self.num_coefs] = X
+        staged[:, self.num_coefs] = y
+        P = self.num_coefs + (1 if self.intercept else 0)
+        plan = nat.PlanDesc(
+            family=nat.UT_FAMILY_GLM_BERNOULLI_LOGIT, num_params=P, num_obs=N, num_coefs=self.num_coefs,
+            has_intercept=1 if self.intercept else 0, num_groups=0,
+            intercept_mu=self.intercept_mu, intercept_sigma=self.intercept_sigma,
+            coef_mu=self.coef_mu, coef_sigma=self.coef_sigma, mu_loc=0.0, mu_scale=1.0, tau_scale=1.0)
+        empty = np.zeros(0, dtype=np.int32)
+        return Lowered(plan, np.ascontiguousarray(staged.reshape(-1)), empty, empty, P)
+
+    def initial_positions(self, rng, num_chains, args=(), constraints=None, init_strategy="prior"):
+        P = self.num_params(args, constraints)
+        if init_strategy == "uniform":
+            return rng.uniform(-2.0, 2.0, size=(num_chains, P))
+        out = rng.normal(self.coef_mu, self.coef_sigma, size=(num_chains, P))
+        if self.intercept:
+            out[:, 0] = rng.normal(self.intercept_mu, self.intercept_sigma, size=num_chains)
+        return out
+
+
+@dataclass
+class HierarchicalNormalNoncentered(TeaModelSpec):
+    """``mu ~ normal(mu_loc, mu_scale)``, ``tau ~ halfcauchy(tau_scale)``,
+    ``theta ~ iid(normal(mu, tau), J; reparam=:noncentered)``,
+    ``y[j][i] ~ normal(theta[j], sigma[j])``.
+
+    Unconstrained parameters: [mu, log(tau), z_1 .. z_J]; the constrained
+    vector is [mu, tau, theta_1 .. theta_J] with theta_j = mu + tau z_j
+    (docs/noncentered-reparam.md:22-36).
+    args = (sigma, group_sizes); constraints = {"y": y} with y the
+    concatenated observations, group after group.
+    """
+
+    num_groups: int
+    mu_loc: float = 0.0
+    mu_scale: float = 5.0
+    tau_scale: float = 2.5
+    name: str = "hierarchical_normal_noncentered"
+
+    def parameter_names(self, args=(), constraints=None):
+        return ["mu", "tau"] + [f"theta[{j + 1}]" for j in range(self.num_groups)]
+
+    def lower(self, args=(), constraints=None) -> Lowered:
+        if len(args) != 2:
+            raise ValueError(f"{self.name} expects args=(sigma, group_sizes), got {len(args)} argument(s)")
+        sigma = np.asarray(args[0], dtype=np.float32)
+        sizes = np.asarray(args[1], dtype=np.int64)
+        J = self.num_groups
+        if sigma.shape != (J,) or sizes.shape != (J,):
+            raise IndexError(f"expected sigma and group_sizes of length {J}, got {sigma.shape} and {sizes.shape}")
+        if np.any(sizes < 0):
+            raise ValueError("group sizes must be >= 0")
+        y = _observed_value(constraints, "y").astype(np.float32)
+        N = int(sizes.sum())
+        if y.shape != (N,):
+            raise IndexError(f"expected {N} observations (sum of group sizes), got shape {y.shape}")
+        starts = np.zeros(J, dtype=np.int32)
+        starts[1:] = np.cumsum(sizes)[:-1]
+        observed = np.concatenate([y, sigma]).astype(np.float32)
+        plan = nat.PlanDesc(
+            family=nat.UT_FAMILY_HIER_NORMAL_NONCENTERED, num_params=J + 2, num_obs=N, num_coefs=0,
+            has_intercept=0, num_groups=J, intercept_mu=0.0, intercept_sigma=1.0, coef_mu=0.0, coef_sigma=1.0,
+            mu_loc=self.mu_loc, mu_scale=self.mu_scale, tau_scale=self.tau_scale)
+        return Lowered(plan, observed, sizes.astype(np.int32), starts, J + 2)
+
+    def constrain(self, unconstrained, args=(), constraints=None):
+        u = np.asarray(unconstrained)
+        out = np.empty_like(u)
+        mu = u[..., 0]
+        tau = np.exp(u[..., 1])
+        out[..., 0] = mu
+        out[..., 1] = tau
+        out[..., 2:] = mu[..., None] + tau[..., None] * u[..., 2:]
+        return out
+
+    def initial_positions(self, rng, num_chains, args=(), constraints=None, init_strategy="prior"):
+        P = self.num_groups + 2
+        if init_strategy == "uniform":
+            return rng.uniform(-2.0, 2.0, size=(num_chains, P))
+        out = np.empty((num_chains, P))
+        out[:, 0] = rng.normal(self.mu_loc, self.mu_scale, size=num_chains)
+        tau = np.abs(self.tau_scale * rng.standard_cauchy(size=num_chains))
+        out[:, 1] = np.log(np.maximum(tau, 1e-30))
+        out[:, 2:] = rng.normal(0.0, 1.0, size=(num_chains, self.num_groups))
+        return out
+
+
+# ---- synthetic workloads (seeded stand-ins for the benchmark data sets) -----
+
+def logistic_regression_data(num_obs: int, num_coefs: int, seed: int, x_scale: float = 1.0):
+    """X ~ N(0,1) * x_scale (N x D), beta_true ~ N(0,1), y ~ Bernoulli(logistic(X beta))."""
+    rng = np.random.default_rng(seed)
+    X = (rng.standard_normal((num_obs, num_coefs)) * x_scale).astype(np.float32)
+    beta = rng.standard_normal(num_coefs)
+    eta = X.astype(np.float64) @ beta
+    y = (rng.uniform(size=num_obs) < 1.0 / (1.0 + np.exp(-eta))).astype(np.float32)
+    return X, y, beta
+
+
+def hierarchical_data(num_groups: int, group_sizes, seed: int, mu_loc=0.0, mu_scale=5.0, tau_scale=2.5):
+    """sigma_j ~ U(0.5, 2); y drawn from the prior predictive at `seed`."""
+    rng = np.random.default_rng(seed)
+    sizes = np.broadcast_to(np.asarray(group_sizes, dtype=np.int64), (num_groups,)).copy()
+    sigma = rng.uniform(0.5, 2.0, size=num_groups).astype(np.float32)
+    mu = rng.normal(mu_loc, mu_scale)
+    tau = abs(tau_scale * rng.standard_cauchy())
+    theta = mu + tau * rng.standard_normal(num_groups)
+    y = np.concatenate([rng.normal(theta[j], sigma[j], size=sizes[j]) for j in range(num_groups)]).astype(np.float32)
+    return y, sigma, sizes, {"mu": mu, "tau": tau, "theta": theta}
