@@ -106,6 +106,15 @@ int32_t ut_workspace_create(const ut_plan_desc* plan,
                             ut_workspace** out);
 int32_t ut_workspace_destroy(ut_workspace* ws);
 int32_t ut_workspace_info(const ut_workspace* ws, int32_t* num_params, int32_t* batch_size);
+/* Which kernel family evaluates this workspace's density: 1 = one warp per
+ * chain (observation data staged in shared memory), 2 = CUDA-core
+ * observation-tiled GEMM path, 3 = tensor-core (tcgen05, 3xTF32) path. */
+int32_t ut_workspace_path(const ut_workspace* ws);
+/* Synchronises the workspace's work and reports the sticky device error word:
+ * UT_ERR_DEVICE_TIMEOUT when a bounded in-kernel wait gave up since the last
+ * check (the word is cleared by this call), else UT_OK.  Until it is cleared,
+ * kernels that wait on barriers return early instead of waiting. */
+int32_t ut_workspace_check(ut_workspace* ws, void* stream);
 
 /* ---- batched density ------------------------------------------------------
  * reference: device_batched_logjoint! (src/device/workspace.jl:276-307) and

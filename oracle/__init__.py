@@ -95,6 +95,9 @@ class OracleModel:
         return (ctypes.byref(self.plan), _p(self.obs), _p(self.tc) if self.tc.size else None,
                 _p(self.ls) if self.ls.size else None)
 
+    # Every array handed to the library is bound to a local name first, so it
+    # stays alive until the call returns.
+
     def logjoint_gradient_f64(self, params_cp, threads=0, want_grad=True):
         q = np.ascontiguousarray(params_cp, dtype=np.float64)
         C = q.shape[0]
@@ -114,14 +117,15 @@ class OracleModel:
     def hmc_iteration(self, position, gradient, logjoint, inverse_mass, step, L, coord, thr=1000.0,
                       want_proposal=False, threads=0):
         C = position.shape[0]
+        inverse_mass = np.ascontiguousarray(inverse_mass, dtype=np.float32)  # held for the call
+        step = np.ascontiguousarray(step, dtype=np.float32)
         out = {k: np.empty(C, dtype=np.float32) for k in ("accept_prob", "energy", "energy_error")}
         out["accepted"] = np.empty(C, dtype=np.uint8)
         out["divergent"] = np.empty(C, dtype=np.uint8)
         prop = np.empty_like(position) if want_proposal else None
         mom = np.empty_like(position) if want_proposal else None
         load().orc_hmc_iteration_f32(*self._common(), C, _p(position), _p(gradient), _p(logjoint),
-                                     _p(np.ascontiguousarray(inverse_mass, dtype=np.float32)),
-                                     _p(np.ascontiguousarray(step, dtype=np.float32)), L, coord, thr,
+                                     _p(inverse_mass), _p(step), L, coord, thr,
                                      _p(out["accept_prob"]), _p(out["energy"]), _p(out["energy_error"]),
                                      _p(out["accepted"]), _p(out["divergent"]), _p(prop), _p(mom), threads)
         out["proposal"], out["endpoint_momentum"] = prop, mom
@@ -130,22 +134,24 @@ class OracleModel:
     def leapfrog_probe(self, position, gradient, logjoint, inverse_mass, trial_step, coord, threads=0):
         C = position.shape[0]
         lar = np.empty(C, dtype=np.float32)
+        inverse_mass = np.ascontiguousarray(inverse_mass, dtype=np.float32)
+        trial_step = np.ascontiguousarray(trial_step, dtype=np.float32)
         load().orc_leapfrog_probe_f32(*self._common(), C, _p(position), _p(gradient), _p(logjoint),
-                                      _p(np.ascontiguousarray(inverse_mass, dtype=np.float32)),
-                                      _p(np.ascontiguousarray(trial_step, dtype=np.float32)), coord, _p(lar), threads)
+                                      _p(inverse_mass), _p(trial_step), coord, _p(lar), threads)
         return lar
 
     def nuts_iteration(self, position, gradient, logjoint, inverse_mass, step, max_depth, coord, thr=1000.0,
                        threads=0):
         C = position.shape[0]
+        inverse_mass = np.ascontiguousarray(inverse_mass, dtype=np.float32)
+        step = np.ascontiguousarray(step, dtype=np.float32)
         out = {k: np.empty(C, dtype=np.float32) for k in ("accept_prob", "energy", "energy_error")}
         out["tree_depth"] = np.empty(C, dtype=np.int32)
         out["integration_steps"] = np.empty(C, dtype=np.int32)
         out["divergent"] = np.empty(C, dtype=np.uint8)
         out["moved"] = np.empty(C, dtype=np.uint8)
         load().orc_nuts_iteration_f32(*self._common(), C, _p(position), _p(gradient), _p(logjoint),
-                                      _p(np.ascontiguousarray(inverse_mass, dtype=np.float32)),
-                                      _p(np.ascontiguousarray(step, dtype=np.float32)), max_depth, thr, coord,
+                                      _p(inverse_mass), _p(step), max_depth, thr, coord,
                                       _p(out["accept_prob"]), _p(out["energy"]), _p(out["energy_error"]),
                                       _p(out["tree_depth"]), _p(out["integration_steps"]), _p(out["divergent"]),
                                       _p(out["moved"]), threads)
@@ -155,12 +161,10 @@ class OracleModel:
 def chees_reduce(initials, proposals, momenta, accept_prob, divergent, inverse_mass):
     C, P = initials.shape
     out = np.zeros(2)
-    load().orc_chees_reduce(P, C, _p(np.ascontiguousarray(initials, dtype=np.float32)),
-                            _p(np.ascontiguousarray(proposals, dtype=np.float32)),
-                            _p(np.ascontiguousarray(momenta, dtype=np.float32)),
-                            _p(np.ascontiguousarray(accept_prob, dtype=np.float32)),
-                            _p(np.ascontiguousarray(divergent, dtype=np.uint8)),
-                            _p(np.ascontiguousarray(inverse_mass, dtype=np.float32)), _p(out))
+    held = [np.ascontiguousarray(a, dtype=dt) for a, dt in ((initials, np.float32), (proposals, np.float32),
+                                                            (momenta, np.float32), (accept_prob, np.float32),
+                                                            (divergent, np.uint8), (inverse_mass, np.float32))]
+    load().orc_chees_reduce(P, C, *[_p(a) for a in held], _p(out))
     return out
 
 

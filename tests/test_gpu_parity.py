@@ -192,11 +192,27 @@ def _hmc_gpu(ws, qd, g, t, im, step, L, coord, want=False):
     return res
 
 
+def _glm_mode(X, y, sigma=1.0, iters=25):
+    """Posterior mode of the logistic regression by Newton's method (float64)."""
+    X = X.astype(np.float64)
+    b = np.zeros(X.shape[1])
+    for _ in range(iters):
+        pr = 1 / (1 + np.exp(-X @ b))
+        g = X.T @ (y - pr) - b / sigma ** 2
+        H = -(X.T * (pr * (1 - pr))) @ X - np.eye(X.shape[1]) / sigma ** 2
+        b = b - np.linalg.solve(H, g)
+    return b
+
+
 @pytest.mark.parametrize("case", ["glm_c1", "glm_tiled", "hier"])
 def test_hmc_iteration_vs_oracle(lib, case):
+    """One HMC iteration from near-posterior states with stable step sizes:
+    the same Philox momenta and accept uniforms on both sides."""
+    r = np.random.default_rng(3)
     if case == "glm_c1":
-        m, args, cons, q = _glm_case(1000, 10, 256, False, 1)
-        q *= 0.3
+        m, args, cons, _ = _glm_case(1000, 10, 256, False, 1)
+        mode = _glm_mode(args[0], cons["y"])
+        q = (mode + 0.05 * r.standard_normal((256, 10))).astype(np.float32)
         step, L = 0.05, 8
     elif case == "glm_tiled":
         m, args, cons, q = _glm_case(4000, 48, 96, True, 5, 0.2)
@@ -205,9 +221,15 @@ def test_hmc_iteration_vs_oracle(lib, case):
     else:
         y, sig, sizes, _ = hierarchical_data(64, 20, 7)
         m, args, cons = HierarchicalNormalNoncentered(64), (sig, sizes), {"y": y}
-        q = (np.random.default_rng(3).standard_normal((256, 66)) * 0.5).astype(np.float32)
-        q[:, 0] += 1.0
-        step, L = 0.02, 6
+        # near the posterior mode: theta_j at the group means, z_j = (ybar_j - mu) / tau
+        starts = np.concatenate([[0], np.cumsum(sizes)[:-1]])
+        ybar = np.array([y[s:s + n].mean() for s, n in zip(starts, sizes)])
+        mu0, tau0 = ybar.mean(), ybar.std()
+        q = np.empty((256, 66), dtype=np.float32)
+        q[:, 0] = mu0 + 0.1 * r.standard_normal(256)
+        q[:, 1] = np.log(tau0) + 0.02 * r.standard_normal(256)
+        q[:, 2:] = (ybar - mu0) / tau0 + 0.02 * r.standard_normal((256, 64))
+        step, L = 0.004, 6
     C, P = q.shape
     ws = _ws(m, args, cons, C)
     qd, g, t = _state(ws, q)
@@ -217,33 +239,38 @@ def test_hmc_iteration_vs_oracle(lib, case):
     qo, go, to = qd.cpu().numpy().copy(), g.cpu().numpy().copy(), t.cpu().numpy().copy()
     gpu = _hmc_gpu(ws, qd, g, t, im, steps, L, 12345, want=True)
     ref = om.hmc_iteration(qo, go, to, im, steps, L, 12345, want_proposal=True)
-    same = gpu["accepted"] == ref["accepted"]
+    same = (gpu["accepted"] == ref["accepted"]) & (gpu["divergent"] == ref["divergent"])
     assert same.mean() >= 0.98
-    assert np.array_equal(gpu["divergent"], ref["divergent"])
-    np.testing.assert_allclose(gpu["proposal"], ref["proposal"], rtol=1e-3, atol=1e-4)
-    np.testing.assert_allclose(gpu["endpoint_momentum"], ref["endpoint_momentum"], rtol=1e-3, atol=1e-3)
+    assert ref["divergent"].mean() <= 0.02
+    ok = same & (ref["divergent"] == 0)
+    np.testing.assert_allclose(gpu["proposal"][ok], ref["proposal"][ok], rtol=1e-3, atol=1e-4)
+    np.testing.assert_allclose(gpu["endpoint_momentum"][ok], ref["endpoint_momentum"][ok], rtol=1e-3, atol=1e-3)
     np.testing.assert_allclose(gpu["position"][same], qo[same], rtol=1e-3, atol=1e-4)
-    np.testing.assert_allclose(gpu["accept_prob"], ref["accept_prob"], atol=2e-3)
+    np.testing.assert_allclose(gpu["accept_prob"][ok], ref["accept_prob"][ok], atol=2e-3)
+    np.testing.assert_allclose(gpu["energy_error"][ok], ref["energy_error"][ok], rtol=1e-3, atol=5e-3)
     ws.close()
 
 
 def test_leapfrog_probe_vs_oracle(lib):
-    m, args, cons, q = _glm_case(1000, 10, 64, False, 2)
-    q *= 0.3
+    m, args, cons, _ = _glm_case(1000, 10, 64, False, 2)
+    mode = _glm_mode(args[0], cons["y"])
+    q = (mode + 0.05 * np.random.default_rng(1).standard_normal((64, 10))).astype(np.float32)
     ws = _ws(m, args, cons, 64)
     qd, g, t = _state(ws, q)
     im = np.ones(10, dtype=np.float32)
-    trial = np.geomspace(1e-3, 2.0, 64).astype(np.float32)
+    trial = np.geomspace(1e-3, 0.1, 64).astype(np.float32)
+    imd = torch.from_numpy(im).cuda()          # kept alive until the kernel has run
+    trd = torch.from_numpy(trial).cuda()
     out = torch.empty(64, dtype=torch.float32, device="cuda")
-    nat.check(nat.load().ut_leapfrog_probe(ws.handle, nat.ptr(qd), nat.ptr(g), nat.ptr(t),
-                                           nat.ptr(torch.from_numpy(im).cuda()), nat.ptr(torch.from_numpy(trial).cuda()),
-                                           777, nat.ptr(out), None))
+    nat.check(nat.load().ut_leapfrog_probe(ws.handle, nat.ptr(qd), nat.ptr(g), nat.ptr(t), nat.ptr(imd),
+                                           nat.ptr(trd), 777, nat.ptr(out), None))
+    torch.cuda.synchronize()
     ref = oracle.OracleModel(ws.lowered).leapfrog_probe(qd.cpu().numpy(), g.cpu().numpy(), t.cpu().numpy(), im, trial,
                                                         777)
     gpu = out.cpu().numpy()
-    fin = np.isfinite(ref)
-    assert np.array_equal(fin, np.isfinite(gpu))
-    np.testing.assert_allclose(gpu[fin], ref[fin], rtol=1e-3, atol=1e-3)
+    assert np.all(np.isfinite(ref)) and np.all(np.isfinite(gpu))
+    # H ~ |logjoint| ~ 6e2: FP32 rounding of H0 - H1 is ~1e-4 absolute
+    np.testing.assert_allclose(gpu, ref, rtol=1e-3, atol=5e-4)
     ws.close()
 
 
@@ -345,3 +372,35 @@ def test_running_variance_vs_sequential(lib):
     np.testing.assert_allclose(m2, M2, rtol=1e-12, atol=1e-12)
     assert count == n == rv.count
     assert ws_ == pytest.approx(S, rel=1e-14) and wss == pytest.approx(SS, rel=1e-14)
+
+
+@pytest.mark.parametrize("N,D,C,intercept", [
+    (100000, 100, 4096, False),   # config 3
+    (5003, 100, 200, True),       # ragged obs tile and chain tile, F=101 -> 104 padded features
+    (777, 64, 128, False),
+    (70, 3, 5, True),             # tiny: one observation tile, one partial chain tile
+])
+def test_tensor_core_path_vs_cuda_core_and_oracle(lib, N, D, C, intercept, monkeypatch):
+    """The tcgen05 3xTF32 kernel against the CUDA-core tiled kernel and the FP64
+    oracle (same tolerances as the other density tests)."""
+    m, args, cons, q = _glm_case(N, D, C, intercept, 21, 1.0 / np.sqrt(D))
+    ws_tc = _ws(m, args, cons, C)
+    assert ws_tc.kernel_path() in ("tensor_core", "warp")
+    monkeypatch.setenv("UT_DISABLE_TENSOR_CORES", "1")
+    ws_cc = _ws(m, args, cons, C)
+    monkeypatch.delenv("UT_DISABLE_TENSOR_CORES")
+    qd = torch.from_numpy(q).cuda()
+    t1, g1 = ws_tc.logjoint_gradient_device(qd)
+    t0 = ws_tc.logjoint_device(qd)
+    ws_tc.check()
+    t2, g2 = ws_cc.logjoint_gradient_device(qd)
+    torch.cuda.synchronize()
+    t1, g1, t0, t2, g2 = (x.cpu().numpy() for x in (t1, g1, t0, t2, g2))
+    idx = np.unique(np.linspace(0, C - 1, min(C, 16)).astype(int))
+    t64, g64 = oracle.OracleModel(ws_tc.lowered).logjoint_gradient_f64(q[idx].astype(np.float64))
+    assert _lj_err(t1[idx], t64) <= 1e-5 and _grad_err(g1[idx], g64) <= 1e-5
+    assert _lj_err(t0[idx], t64) <= 1e-5
+    assert _lj_err(t2[idx], t64) <= 1e-5 and _grad_err(g2[idx], g64) <= 1e-5
+    assert _lj_err(t1, t2.astype(np.float64)) <= 2e-5
+    ws_tc.close()
+    ws_cc.close()

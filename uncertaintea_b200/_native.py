@@ -89,6 +89,8 @@ SIGNATURES = [
       POINTER(c_void_p)]),
     ("ut_workspace_destroy", c_int32, [c_void_p]),
     ("ut_workspace_info", c_int32, [c_void_p, POINTER(c_int32), POINTER(c_int32)]),
+    ("ut_workspace_path", c_int32, [c_void_p]),
+    ("ut_workspace_check", c_int32, [c_void_p, c_void_p]),
     ("ut_logjoint", c_int32, [c_void_p, c_void_p, c_void_p]),
     ("ut_logjoint_gradient", c_int32, [c_void_p, c_void_p, c_void_p, c_void_p]),
     ("ut_logjoint_device", c_int32, [c_void_p, c_void_p, c_void_p, c_void_p]),

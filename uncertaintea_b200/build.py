@@ -35,7 +35,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     newest = max(os.path.getmtime(s) for s in sources())
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= newest:
         return LIB
-    cmd = [nvcc()] + NVCC_FLAGS + ["-o", LIB + ".tmp", os.path.join(HERE, "csrc", "ut_api.cu"), "-lcuda"]
+    cmd = [nvcc()] + NVCC_FLAGS + ["-o", LIB + ".tmp", os.path.join(HERE, "csrc", "ut_api.cu")]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     subprocess.run(cmd, check=True)

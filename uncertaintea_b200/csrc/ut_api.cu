@@ -259,7 +259,7 @@ int32_t density(ut_workspace* ws, const float* params, float* totals, float* gra
         UT_LAUNCHED();
         return UT_OK;
     }
-    if (ws->tc.enabled && grads) return tc_glm_launch(ws->tc, params, totals, grads, st) == cudaSuccess
+    if (ws->tc.enabled) return tc_glm_launch(ws->tc, params, totals, grads, st) == cudaSuccess
                                             ? UT_OK
                                             : fail(UT_ERR_CUDA, "tensor-core GLM launch failed: %s",
                                                    cudaGetErrorString(cudaGetLastError()));
@@ -482,6 +482,29 @@ int32_t ut_workspace_info(const ut_workspace* ws, int32_t* num_params, int32_t* 
     return UT_OK;
 }
 
+int32_t ut_workspace_path(const ut_workspace* ws) {
+    if (!ws) return 0;
+    if (ws->path == kPathWarp) return 1;
+    return ws->tc.enabled ? 3 : 2;
+}
+
+int32_t ut_workspace_check(ut_workspace* ws, void* stream) {
+    int32_t rc = check_ws(ws);
+    if (rc) return rc;
+    UT_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    UT_CUDA(cudaStreamSynchronize(ws->stream));
+    if (ws->tc.err) {
+        int h = 0;
+        UT_CUDA(cudaMemcpy(&h, ws->tc.err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (h) {
+            UT_CUDA(cudaMemset(ws->tc.err, 0, sizeof(int)));
+            return fail(UT_ERR_DEVICE_TIMEOUT, "a bounded wait inside the tensor-core GLM kernel gave up; "
+                                               "its results are invalid");
+        }
+    }
+    return UT_OK;
+}
+
 int32_t ut_logjoint_device(ut_workspace* ws, const float* d_params, float* d_totals, void* stream) {
     int32_t rc = check_ws(ws);
     if (rc) return rc;
@@ -507,7 +530,7 @@ int32_t ut_logjoint(ut_workspace* ws, const float* params, float* totals) {
     if ((rc = density(ws, ws->d_params, ws->d_totals, nullptr, ws->stream))) return rc;
     UT_CUDA(cudaMemcpyAsync(totals, ws->d_totals, ws->C * sizeof(float), cudaMemcpyDeviceToHost, ws->stream));
     UT_CUDA(cudaStreamSynchronize(ws->stream));
-    return UT_OK;
+    return ut_workspace_check(ws, ws->stream);
 }
 
 int32_t ut_logjoint_gradient(ut_workspace* ws, const float* params, float* totals, float* gradients) {
@@ -521,7 +544,7 @@ int32_t ut_logjoint_gradient(ut_workspace* ws, const float* params, float* total
     UT_CUDA(cudaMemcpyAsync(totals, ws->d_totals, ws->C * sizeof(float), cudaMemcpyDeviceToHost, ws->stream));
     UT_CUDA(cudaMemcpyAsync(gradients, ws->d_grads, pc * sizeof(float), cudaMemcpyDeviceToHost, ws->stream));
     UT_CUDA(cudaStreamSynchronize(ws->stream));
-    return UT_OK;
+    return ut_workspace_check(ws, ws->stream);
 }
 
 // ---- Philox ---------------------------------------------------------------

@@ -1,27 +1,632 @@
-// ut_tc_glm.cuh -- tensor-core (tcgen05, 3xTF32) GLM logjoint + gradient.
-// Placeholder until the sm_100a kernel lands: `enabled` stays false and the
-// CUDA-core tiled kernel serves the large-N path.
+// ut_tc_glm.cuh -- Bernoulli-logit GLM logjoint + gradient on the 5th-gen
+// tensor cores (tcgen05, TF32 with FP32 accumulation in TMEM), FP32-accurate
+// through the 3xTF32 split a*b ~ a_hi*b_hi + a_hi*b_lo + a_lo*b_hi, where
+// hi = tf32_round(x) and lo = tf32_round(x - hi).
+//
+// One CTA owns a tile of 128 chains and a contiguous range of 32-observation
+// tiles.  Per observation tile t:
+//   GEMM1:  H^T[c, n]  = sum_f Theta[c, f] X[n, f]      M=128 chains, N=32 obs, K=Fp
+//           A = Theta (hi/lo) resident in TMEM, B = X tile (K-major, SMEM)
+//   epilogue (thread = chain c = TMEM lane c):
+//           r = y_n - logistic(h),  ll_c += y_n h - log1p_exp(h)
+//           r -> (r_hi, r_lo) written back into TMEM
+//   GEMM2:  G^T[c, f] += sum_n R^T[c, n] X[n, f]         M=128, N=Fp, K=32 obs
+//           A = R (TMEM), B = X tile (MN-major, SMEM)
+// so the per-chain log-likelihood is a thread-local sum and the residual tile
+// never touches shared memory.
+//
+// Warp roles (192 threads): warp 0 = TMA producer, warp 1 = MMA issuer (and
+// TMEM owner), warps 2-5 = epilogue (TMEM lane quadrants 2,3,0,1).
+// Pipelines: 3 X stages, 2 H/R TMEM buffers, so GEMM1 of tile t+1 runs on the
+// tensor cores while the epilogue of tile t runs on the CUDA cores / SFUs.
+//
+// Every mbarrier wait is bounded (~2^31 clocks).  A wait that gives up sets the
+// error word, the role stops issuing, all threads meet at the final barrier and
+// the TMEM owner frees TMEM before the CTA exits.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cstdint>
+#include <cstring>
+#include <string>
 #include <vector>
+
+#include "ut_common.cuh"
 
 namespace ut {
 
-struct TcGlmPlan {
-    bool enabled = false;
+constexpr int kTcChains = 128;          // M of both GEMMs (TMEM lanes)
+constexpr int kTcObs = 32;              // observations per tile (N of GEMM1, K of GEMM2)
+constexpr int kTcMaxFp = 128;           // padded feature count the TMEM plan holds (3 Fp + 128 <= 512)
+constexpr int kTcThreads = 192;
+constexpr long long kTcWaitClocks = 1ll << 31;
+
+struct TcGlmParams {
+    const float* y;        // N
+    float* part_ll;        // S x C
+    float* part_g;         // S x C x F
+    int* err;              // device error word (1 = a bounded wait gave up)
+    int N, F, Fp, C;
+    int tiles_per_split;   // observation tiles per CTA
+    int num_tiles;         // total observation tiles
+    int want_grad;
 };
 
-inline const char* tc_glm_last_error() { return ""; }
+// ---------------------------------------------------------------------------
+// PTX helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
 
-inline int tc_glm_setup(TcGlmPlan& plan, const float*, const float*, int, int, int, int, float, float, float, float,
-                        int, std::vector<void*>*) {
-    plan.enabled = false;
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: returns false (and raises the error word) when it gives up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (true) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (clock64() - t0 > kTcWaitClocks) {
+            atomicExch(err, 1);
+            return false;
+        }
+        if (*((volatile int*)err)) return false;  // another role already gave up
+    }
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
+                 "r"(ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols));
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// D[tmem] (+)= A[smem] * B[smem]
+__device__ __forceinline__ void mma_ss(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(d), "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+// D[tmem] (+)= A[tmem] * B[smem]
+__device__ __forceinline__ void mma_ts(uint32_t d, uint32_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}"
+        ::"r"(d), "r"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+        "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+        "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};"
+        ::"r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+          "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]),
+          "r"(r[16]), "r"(r[17]), "r"(r[18]), "r"(r[19]), "r"(r[20]), "r"(r[21]), "r"(r[22]), "r"(r[23]),
+          "r"(r[24]), "r"(r[25]), "r"(r[26]), "r"(r[27]), "r"(r[28]), "r"(r[29]), "r"(r[30]), "r"(r[31])
+        : "memory");
+}
+
+__device__ __forceinline__ uint32_t tf32_bits(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+
+// Shared-memory matrix descriptor, SWIZZLE_32B layout.
+__device__ __forceinline__ uint64_t sdesc_sw32(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;   // descriptor version (sm_100)
+    d |= (uint64_t)6 << 61;   // SWIZZLE_32B
+    return d;
+}
+
+// Instruction descriptor: D=F32, A=B=TF32, dense, M x N.
+__host__ __device__ constexpr uint32_t idesc_tf32(int M, int N, int b_mn_major) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)b_mn_major << 16) | ((uint32_t)(N >> 3) << 17) |
+           ((uint32_t)(M >> 4) << 24);
+}
+
+// ---------------------------------------------------------------------------
+// the kernel
+// ---------------------------------------------------------------------------
+// TMEM columns (512 allocated), Fp = padded features (multiple of 16, <= 128):
+//   Theta_hi [0, Fp)   Theta_lo [Fp, 2Fp)   D2 = G^T [2Fp, 3Fp)
+//   buffer b (0,1): H^T / R_hi [3Fp + 64b, +32)   R_lo [3Fp + 64b + 32, +32)
+// Shared memory per pipeline stage (3 stages), Fp features x 32 observations:
+//   XK_hi, XK_lo : K-major SWIZZLE_32B, Fp/8 blocks of [32 rows][32 B]     (GEMM1 B)
+//   XM_hi, XM_lo : MN-major SWIZZLE_128B_BASE32B, Fp/32 atoms of [32 rows][128 B] (GEMM2 B)
+// (TF32 operands that are MN-major must use the 128B_BASE32B layout, which no
+// K-major layout shares, so each X tile is loaded twice, once per view.)
+constexpr int kTcStages = 3;
+constexpr int kTcDrainTiles = 4;   // observation tiles per TMEM gradient accumulation run
+
+__host__ __device__ inline int tc_kblocks(int Fp) { return Fp / 8; }
+__host__ __device__ inline int tc_matoms(int Fp) { return (Fp + 31) / 32; }
+__host__ __device__ inline int tc_xk_bytes(int Fp) { return tc_kblocks(Fp) * kTcObs * 32; }
+__host__ __device__ inline int tc_xm_bytes(int Fp) { return tc_matoms(Fp) * kTcObs * 128; }
+__host__ __device__ inline int tc_stage_bytes(int Fp) { return 2 * tc_xk_bytes(Fp) + 2 * tc_xm_bytes(Fp); }
+
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+        "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};"
+        ::"r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+          "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Shared-memory descriptor, SWIZZLE_128B_BASE32B (layout type 1).
+__device__ __forceinline__ uint64_t sdesc_sw128b32(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)1 << 61;
+    return d;
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+    tc_glm_kernel(const __grid_constant__ CUtensorMap map_xk_hi, const __grid_constant__ CUtensorMap map_xk_lo,
+                  const __grid_constant__ CUtensorMap map_xm_hi, const __grid_constant__ CUtensorMap map_xm_lo,
+                  const float* __restrict__ params, TcGlmParams p) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int Fp = p.Fp;
+    const int KB = tc_kblocks(Fp), MA = tc_matoms(Fp);
+    const int xk_bytes = tc_xk_bytes(Fp), xm_bytes = tc_xm_bytes(Fp), stage_bytes = tc_stage_bytes(Fp);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kTcStages * stage_bytes);
+    uint64_t* bar_xfull = bars;                    // [3]
+    uint64_t* bar_xempty = bars + 3;               // [3]
+    uint64_t* bar_d1full = bars + 6;               // [2]
+    uint64_t* bar_rfull = bars + 8;                // [2]
+    uint64_t* bar_d2full = bars + 10;
+    uint64_t* bar_theta = bars + 11;
+    uint64_t* bar_d2empty = bars + 12;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 13);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ctile = blockIdx.y;
+    const int split = blockIdx.x;
+    const int t_begin = split * p.tiles_per_split;
+    const int t_end = min(p.num_tiles, t_begin + p.tiles_per_split);
+    const int ntiles = max(0, t_end - t_begin);
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < kTcStages; ++i) {
+            mbar_init(bar_xfull + i, 1);
+            mbar_init(bar_xempty + i, 1);
+        }
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(bar_d1full + i, 1);
+            mbar_init(bar_rfull + i, 128);
+        }
+        mbar_init(bar_d2full, 1);
+        mbar_init(bar_theta, 128);
+        mbar_init(bar_d2empty, 128);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) tmem_alloc(tmem_slot, 512);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t col_thi = 0, col_tlo = Fp, col_d2 = 2 * Fp, col_buf = 3 * Fp;
+
+    if (warp == 0) {
+        // ---------------- TMA producer ----------------
+        if (lane == 0) {
+            for (int i = 0; i < ntiles; ++i) {
+                const int s = i % kTcStages;
+                if (i >= kTcStages && !mbar_wait(bar_xempty + s, ((i / kTcStages) - 1) & 1, p.err)) break;
+                uint8_t* st = smem + s * stage_bytes;
+                mbar_expect_tx(bar_xfull + s, stage_bytes);
+                const int n0 = (t_begin + i) * kTcObs;
+                for (int kb = 0; kb < KB; ++kb) {
+                    tma_load_2d(st + kb * (kTcObs * 32), &map_xk_hi, bar_xfull + s, kb * 8, n0);
+                    tma_load_2d(st + xk_bytes + kb * (kTcObs * 32), &map_xk_lo, bar_xfull + s, kb * 8, n0);
+                }
+                for (int a = 0; a < MA; ++a) {
+                    tma_load_2d(st + 2 * xk_bytes + a * (kTcObs * 128), &map_xm_hi, bar_xfull + s, a * 32, n0);
+                    tma_load_2d(st + 2 * xk_bytes + xm_bytes + a * (kTcObs * 128), &map_xm_lo, bar_xfull + s, a * 32,
+                                n0);
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0 && ntiles > 0) {
+            const uint32_t id1 = idesc_tf32(kTcChains, kTcObs, 0);
+            const uint32_t id2 = idesc_tf32(kTcChains, Fp, 1);
+            bool ok = mbar_wait(bar_theta, 0, p.err);
+            tc_fence_after();
+            // GEMM2 of tile j.  The G^T accumulator in TMEM restarts every
+            // kTcDrainTiles tiles: the epilogue drains it into FP32 registers
+            // (round-to-nearest adds) so only a short run of tensor-core
+            // accumulations ever lands in one TMEM value.
+            auto gemm2 = [&](int j) -> bool {
+                const int s = j % kTcStages, b = j & 1;
+                const int group = j / kTcDrainTiles;
+                if (j % kTcDrainTiles == 0 && group > 0) {
+                    if (!mbar_wait(bar_d2empty, (group - 1) & 1, p.err)) return false;
+                    tc_fence_after();
+                }
+                const uint32_t xm = smem_u32(smem + s * stage_bytes + 2 * xk_bytes);
+                const uint32_t rhi = tmem + col_buf + b * 64, rlo = rhi + 32;
+                for (int kk = 0; kk < kTcObs / 8; ++kk) {
+                    const uint64_t bh = sdesc_sw128b32(xm + kk * 1024, kTcObs * 128, 512);
+                    const uint64_t bl = sdesc_sw128b32(xm + xm_bytes + kk * 1024, kTcObs * 128, 512);
+                    const uint32_t first = (j % kTcDrainTiles == 0 && kk == 0) ? 0u : 1u;
+                    mma_ts(tmem + col_d2, rhi + kk * 8, bh, id2, first);
+                    mma_ts(tmem + col_d2, rlo + kk * 8, bh, id2, 1u);
+                    mma_ts(tmem + col_d2, rhi + kk * 8, bl, id2, 1u);
+                }
+                if ((j + 1) % kTcDrainTiles == 0 || j == ntiles - 1) mma_commit(bar_d2full);
+                return true;
+            };
+            for (int i = 0; ok && i < ntiles; ++i) {
+                const int s = i % kTcStages, b = i & 1;
+                if (!mbar_wait(bar_xfull + s, (i / kTcStages) & 1, p.err)) { ok = false; break; }
+                tc_fence_after();
+                const uint32_t xk = smem_u32(smem + s * stage_bytes);
+                const uint32_t d1 = tmem + col_buf + b * 64;
+                for (int kb = 0; kb < KB; ++kb) {
+                    const uint64_t bh = sdesc_sw32(xk + kb * (kTcObs * 32), 16, 256);
+                    const uint64_t bl = sdesc_sw32(xk + xk_bytes + kb * (kTcObs * 32), 16, 256);
+                    mma_ts(d1, tmem + col_thi + kb * 8, bh, id1, kb > 0 ? 1u : 0u);
+                    mma_ts(d1, tmem + col_thi + kb * 8, bl, id1, 1u);
+                    mma_ts(d1, tmem + col_tlo + kb * 8, bh, id1, 1u);
+                }
+                mma_commit(bar_d1full + b);
+                if (i > 0) {
+                    const int j = i - 1;
+                    if (!mbar_wait(bar_rfull + (j & 1), (j >> 1) & 1, p.err)) { ok = false; break; }
+                    tc_fence_after();
+                    if (p.want_grad && !gemm2(j)) { ok = false; break; }
+                    mma_commit(bar_xempty + (j % kTcStages));
+                }
+            }
+            if (ok) {
+                const int j = ntiles - 1;
+                if (mbar_wait(bar_rfull + (j & 1), (j >> 1) & 1, p.err)) {
+                    tc_fence_after();
+                    if (p.want_grad) gemm2(j);
+                    mma_commit(bar_xempty + (j % kTcStages));
+                }
+            }
+        }
+    } else {
+        // ---------------- epilogue: thread = chain (TMEM lane) ----------------
+        const int q = warp & 3;
+        const int c_local = q * 32 + lane;
+        const int c = ctile * kTcChains + c_local;
+        const uint32_t lane_off = (uint32_t)(q * 32) << 16;
+        // Theta row of this chain -> TF32 hi / lo in TMEM (A operand of GEMM1)
+        for (int f0 = 0; f0 < Fp; f0 += 16) {
+            uint32_t hi[16], lo[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int f = f0 + j;
+                const float x = (c < p.C && f < p.F) ? __ldg(params + (size_t)c * p.F + f) : 0.0f;
+                hi[j] = tf32_bits(x);
+                lo[j] = tf32_bits(x - __uint_as_float(hi[j]));
+            }
+            tmem_st16(tmem + lane_off + col_thi + f0, hi);
+            tmem_st16(tmem + lane_off + col_tlo + f0, lo);
+        }
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+        tc_fence_before();
+        mbar_arrive(bar_theta);
+
+        float ll = 0.0f;
+        float gacc[kTcMaxFp];
+#pragma unroll
+        for (int f = 0; f < kTcMaxFp; ++f) gacc[f] = 0.0f;
+        bool ok = ntiles > 0;
+        for (int i = 0; ok && i < ntiles; ++i) {
+            const int b = i & 1;
+            if (!mbar_wait(bar_d1full + b, (i >> 1) & 1, p.err)) { ok = false; break; }
+            tc_fence_after();
+            const int n0 = (t_begin + i) * kTcObs;
+            const uint32_t d1 = tmem + lane_off + col_buf + b * 64;
+            float h[32];
+            tmem_ld32(d1, h);
+            uint32_t rh[32], rl[32];
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                const int n = n0 + j;
+                const bool live = n < p.N;
+                const float yv = live ? __ldg(p.y + n) : 0.0f;
+                const float hv = h[j];
+                const float e = expf(-fabsf(hv));
+                const float l1 = log1pf(e);
+                const float lpe = fmaxf(hv, 0.0f) + l1;              // log1p_exp(h)
+                const float inv = 1.0f / (1.0f + e);
+                const float sig = hv >= 0.0f ? inv : e * inv;         // logistic(h)
+                const bool sup = (yv == 0.0f) | (yv == 1.0f);
+                ll += live ? (sup ? yv * hv - lpe : -INFINITY) : 0.0f;
+                const float r = live ? yv - sig : 0.0f;
+                const uint32_t hb = tf32_bits(r);
+                rh[j] = hb;
+                rl[j] = tf32_bits(r - __uint_as_float(hb));
+            }
+            tmem_st32(d1, rh);        // R_hi overwrites the consumed H^T columns
+            tmem_st32(d1 + 32, rl);
+            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+            tc_fence_before();
+            mbar_arrive(bar_rfull + b);
+            if (p.want_grad && ((i + 1) % kTcDrainTiles == 0 || i == ntiles - 1)) {
+                // drain the G^T accumulator of this group of tiles into registers
+                if (!mbar_wait(bar_d2full, (i / kTcDrainTiles) & 1, p.err)) { ok = false; break; }
+                tc_fence_after();
+#pragma unroll
+                for (int f0 = 0; f0 < kTcMaxFp; f0 += 16) {
+                    if (f0 < Fp) {
+                        float g[16];
+                        tmem_ld16(tmem + lane_off + col_d2 + f0, g);
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) gacc[f0 + j] += g[j];
+                    }
+                }
+                tc_fence_before();
+                mbar_arrive(bar_d2empty);
+            }
+        }
+        if (ok) {
+            if (c < p.C) p.part_ll[(size_t)split * p.C + c] = ll;
+            if (p.want_grad && c < p.C) {
+                float* dst = p.part_g + ((size_t)split * p.C + c) * p.F;
+#pragma unroll
+                for (int f = 0; f < kTcMaxFp; ++f)
+                    if (f < p.F) dst[f] = gacc[f];
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 1) tmem_dealloc(tmem, 512);
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+struct TcGlmPlan {
+    bool enabled = false;
+    int N = 0, F = 0, Fp = 0, C = 0, S = 0, tiles_per_split = 0, num_tiles = 0;
+    float* xhi = nullptr;
+    float* xlo = nullptr;
+    float* part_ll = nullptr;
+    float* part_g = nullptr;
+    int* err = nullptr;
+    const float* y = nullptr;
+    int off = 0;
+    float icpt_mu = 0, icpt_sigma = 1, coef_mu = 0, coef_sigma = 1;
+    CUtensorMap map_xk_hi, map_xk_lo, map_xm_hi, map_xm_lo;
+    size_t smem = 0;
+};
+
+inline std::string& tc_err_string() {
+    static thread_local std::string s;
+    return s;
+}
+inline const char* tc_glm_last_error() { return tc_err_string().c_str(); }
+
+typedef CUresult (*PFN_encodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+inline PFN_encodeTiled tc_encode_fn() {
+    static PFN_encodeTiled fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_encodeTiled>(p);
+    }
+    return fn;
+}
+
+// 2D fp32 map over a rows x Fp row-major matrix with box = box_cols x box_rows.
+inline bool tc_make_map(CUtensorMap* m, float* base, int rows, int Fp, int box_cols, int box_rows,
+                        CUtensorMapSwizzle swz) {
+    PFN_encodeTiled enc = tc_encode_fn();
+    if (!enc) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)Fp, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)Fp * sizeof(float)};
+    cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+__global__ void tc_split_x_kernel(const float* __restrict__ Xa, float* __restrict__ hi, float* __restrict__ lo,
+                                  long long N, int F, int Fp) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N * Fp) return;
+    const long long n = i / Fp;
+    const int f = (int)(i % Fp);
+    const float x = f < F ? Xa[n * F + f] : 0.0f;
+    const uint32_t h = tf32_bits(x);
+    hi[i] = __uint_as_float(h);
+    lo[i] = __uint_as_float(tf32_bits(x - __uint_as_float(h)));
+}
+
+inline int tc_glm_setup(TcGlmPlan& t, const float* d_Xa, const float* d_y, int N, int F, int C, int off,
+                        float icpt_mu, float icpt_sigma, float coef_mu, float coef_sigma, int sms,
+                        std::vector<void*>* allocs) {
+    t.enabled = false;
+    const char* env = getenv("UT_DISABLE_TENSOR_CORES");
+    if (env && env[0] == '1') return 0;
+    int dev = 0, major = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    const int Fp = ((F + 15) / 16) * 16;
+    if (major != 10 || Fp > kTcMaxFp || N < 1 || C < 1) return 0;  // the CUDA-core tiled path serves the rest
+    t.N = N; t.F = F; t.Fp = Fp; t.C = C; t.y = d_y; t.off = off;
+    t.icpt_mu = icpt_mu; t.icpt_sigma = icpt_sigma; t.coef_mu = coef_mu; t.coef_sigma = coef_sigma;
+    t.num_tiles = (N + kTcObs - 1) / kTcObs;
+    const int ctiles = (C + kTcChains - 1) / kTcChains;
+    // one CTA per SM (shared memory), 8 waves of (chain tile, observation split) work units
+    int S = (8 * sms + ctiles - 1) / ctiles;
+    S = std::max(1, std::min(S, std::max(1, t.num_tiles / 8)));
+    t.tiles_per_split = (t.num_tiles + S - 1) / S;
+    t.S = (t.num_tiles + t.tiles_per_split - 1) / t.tiles_per_split;
+    auto alloc = [&](void** p, size_t bytes) {
+        if (cudaMalloc(p, bytes) != cudaSuccess) return false;
+        allocs->push_back(*p);
+        return true;
+    };
+    const size_t xbytes = (size_t)N * Fp * sizeof(float);
+    if (!alloc((void**)&t.xhi, xbytes) || !alloc((void**)&t.xlo, xbytes) ||
+        !alloc((void**)&t.part_ll, (size_t)t.S * C * sizeof(float)) ||
+        !alloc((void**)&t.part_g, (size_t)t.S * C * F * sizeof(float)) || !alloc((void**)&t.err, sizeof(int))) {
+        tc_err_string() = "cudaMalloc failed";
+        return 1;
+    }
+    cudaMemset(t.err, 0, sizeof(int));
+    const long long total = (long long)N * Fp;
+    tc_split_x_kernel<<<(unsigned)((total + 255) / 256), 256>>>(d_Xa, t.xhi, t.xlo, N, F, Fp);
+    if (cudaDeviceSynchronize() != cudaSuccess) {
+        tc_err_string() = "splitting X into TF32 hi/lo failed";
+        return 1;
+    }
+    if (!tc_make_map(&t.map_xk_hi, t.xhi, N, Fp, 8, kTcObs, CU_TENSOR_MAP_SWIZZLE_32B) ||
+        !tc_make_map(&t.map_xk_lo, t.xlo, N, Fp, 8, kTcObs, CU_TENSOR_MAP_SWIZZLE_32B) ||
+        !tc_make_map(&t.map_xm_hi, t.xhi, N, Fp, 32, kTcObs, CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B) ||
+        !tc_make_map(&t.map_xm_lo, t.xlo, N, Fp, 32, kTcObs, CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B)) {
+        tc_err_string() = "cuTensorMapEncodeTiled failed";
+        return 1;
+    }
+    t.smem = 1024 + (size_t)kTcStages * tc_stage_bytes(Fp) + 128;
+    if (cudaFuncSetAttribute(tc_glm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem) != cudaSuccess) {
+        tc_err_string() = "shared-memory opt-in failed";
+        return 1;
+    }
+    t.enabled = true;
     return 0;
 }
 
-inline cudaError_t tc_glm_launch(const TcGlmPlan&, const float*, float*, float*, cudaStream_t) {
-    return cudaErrorNotSupported;
+// Prior terms + deterministic fold of the S partials (same reduce as the CUDA-core path).
+__global__ void tc_reduce_kernel(const float* params, const float* part_ll, const float* part_g, float* totals,
+                                 float* grads, int S, int C, int F, int off, float icpt_mu, float icpt_sigma,
+                                 float coef_mu, float coef_sigma) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c = blockIdx.x * 8 + warp;
+    if (c >= C) return;
+    float prior = 0.0f;
+    for (int f = lane; f < F; f += 32) {
+        const float th = params[(size_t)c * F + f];
+        const bool icpt = off && f == 0;
+        const float mu = icpt ? icpt_mu : coef_mu, sg = icpt ? icpt_sigma : coef_sigma;
+        prior += normal_logpdf(mu, sg, th);
+        if (grads) {
+            float gs = 0.0f;
+            for (int s = 0; s < S; ++s) gs += part_g[((size_t)s * C + c) * F + f];
+            grads[(size_t)c * F + f] = gs - (th - mu) / (sg * sg);
+        }
+    }
+    prior = warp_sum(prior);
+    if (lane == 0) {
+        float tsum = 0.0f;
+        for (int s = 0; s < S; ++s) tsum += part_ll[(size_t)s * C + c];
+        totals[c] = tsum + prior;
+    }
+}
+
+inline cudaError_t tc_glm_launch(const TcGlmPlan& t, const float* params, float* totals, float* grads,
+                                 cudaStream_t st) {
+    TcGlmParams p;
+    p.y = t.y; p.part_ll = t.part_ll; p.part_g = t.part_g; p.err = t.err;
+    p.N = t.N; p.F = t.F; p.Fp = t.Fp; p.C = t.C;
+    p.tiles_per_split = t.tiles_per_split; p.num_tiles = t.num_tiles; p.want_grad = grads ? 1 : 0;
+    dim3 grid(t.S, (t.C + kTcChains - 1) / kTcChains);
+    tc_glm_kernel<<<grid, kTcThreads, t.smem, st>>>(t.map_xk_hi, t.map_xk_lo, t.map_xm_hi, t.map_xm_lo, params, p);
+    tc_reduce_kernel<<<(t.C + 7) / 8, 256, 0, st>>>(params, t.part_ll, grads ? t.part_g : nullptr, totals, grads,
+                                                     t.S, t.C, t.F, t.off, t.icpt_mu, t.icpt_sigma, t.coef_mu,
+                                                     t.coef_sigma);
+    return cudaGetLastError();
 }
 
 }  // namespace ut

@@ -553,7 +553,7 @@ class _DeviceRun:
         """log accept ratio of one leapfrog step per chain (momentum fixed by `coord`)."""
         torch = self.torch
         im = torch.from_numpy(np.asarray(inverse_mass, dtype=np.float32)).to(self.device)
-        ts = torch.from_numpy(np.ascontiguousarray(np.broadcast_to(
+        ts = torch.from_numpy(np.array(np.broadcast_to(
             np.asarray(trial_steps, dtype=np.float32), (self.C,)))).to(self.device)
         out = torch.empty(self.C, dtype=torch.float32, device=self.device)
         nat.check(self.lib.ut_leapfrog_probe(self.ws.handle, nat.ptr(self.position), nat.ptr(self.gradient),

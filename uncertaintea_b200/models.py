@@ -192,11 +192,12 @@ def logistic_regression_data(num_obs: int, num_coefs: int, seed: int, x_scale: f
     return X, y, beta
 
 
-def hierarchical_data(num_groups: int, group_sizes, seed: int, mu_loc=0.0, mu_scale=5.0, tau_scale=2.5):
-    """sigma_j ~ U(0.5, 2); y drawn from the prior predictive at `seed`."""
+def hierarchical_data(num_groups: int, group_sizes, seed: int, mu_loc=0.0, mu_scale=5.0, tau_scale=2.5,
+                      sigma_range=(0.5, 2.0)):
+    """sigma_j ~ U(sigma_range); y drawn from the prior predictive at `seed`."""
     rng = np.random.default_rng(seed)
     sizes = np.broadcast_to(np.asarray(group_sizes, dtype=np.int64), (num_groups,)).copy()
-    sigma = rng.uniform(0.5, 2.0, size=num_groups).astype(np.float32)
+    sigma = rng.uniform(sigma_range[0], sigma_range[1], size=num_groups).astype(np.float32)
     mu = rng.normal(mu_loc, mu_scale)
     tau = abs(tau_scale * rng.standard_cauchy())
     theta = mu + tau * rng.standard_normal(num_groups)
