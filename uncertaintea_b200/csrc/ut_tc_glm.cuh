@@ -15,8 +15,9 @@
 // so the per-chain log-likelihood is a thread-local sum and the residual tile
 // never touches shared memory.
 //
-// Warp roles (192 threads): warp 0 = TMA producer, warp 1 = MMA issuer (and
-// TMEM owner), warps 2-5 = epilogue (TMEM lane quadrants 2,3,0,1).
+// Warp roles (320 threads): warp 0 = TMA producer, warp 1 = MMA issuer (and
+// TMEM owner), warps 2-9 = epilogue: two warps per TMEM lane quadrant, each
+// owning half of a tile's observation columns and half of the gradient columns.
 // Pipelines: 3 X stages, 2 H/R TMEM buffers, so GEMM1 of tile t+1 runs on the
 // tensor cores while the epilogue of tile t runs on the CUDA cores / SFUs.
 //
@@ -39,7 +40,8 @@ namespace ut {
 constexpr int kTcChains = 128;          // M of both GEMMs (TMEM lanes)
 constexpr int kTcObs = 32;              // observations per tile (N of GEMM1, K of GEMM2)
 constexpr int kTcMaxFp = 128;           // padded feature count the TMEM plan holds (3 Fp + 128 <= 512)
-constexpr int kTcThreads = 192;
+constexpr int kTcThreads = 320;         // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
+constexpr int kTcEpiThreads = 256;
 constexpr long long kTcWaitClocks = 1ll << 31;
 
 struct TcGlmParams {
@@ -264,8 +266,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 13);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int ctile = blockIdx.y;
-    const int split = blockIdx.x;
+    const int ctile = blockIdx.x;   // chain tiles fastest: concurrent CTAs share X ranges in L2
+    const int split = blockIdx.y;
     const int t_begin = split * p.tiles_per_split;
     const int t_end = min(p.num_tiles, t_begin + p.tiles_per_split);
     const int ntiles = max(0, t_end - t_begin);
@@ -277,11 +279,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
         for (int i = 0; i < 2; ++i) {
             mbar_init(bar_d1full + i, 1);
-            mbar_init(bar_rfull + i, 128);
+            mbar_init(bar_rfull + i, kTcEpiThreads);
         }
         mbar_init(bar_d2full, 1);
-        mbar_init(bar_theta, 128);
-        mbar_init(bar_d2empty, 128);
+        mbar_init(bar_theta, kTcEpiThreads);
+        mbar_init(bar_d2empty, kTcEpiThreads);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) tmem_alloc(tmem_slot, 512);
@@ -375,12 +377,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
     } else {
         // ---------------- epilogue: thread = chain (TMEM lane) ----------------
-        const int q = warp & 3;
+        const int q = warp & 3;                 // TMEM lane quadrant
+        const int half = (warp - 2) >> 2;       // which half of the columns this warp owns
         const int c_local = q * 32 + lane;
         const int c = ctile * kTcChains + c_local;
         const uint32_t lane_off = (uint32_t)(q * 32) << 16;
-        // Theta row of this chain -> TF32 hi / lo in TMEM (A operand of GEMM1)
-        for (int f0 = 0; f0 < Fp; f0 += 16) {
+        // Theta row of this chain -> TF32 hi / lo in TMEM (A operand of GEMM1); 16-column chunks alternate halves
+        for (int f0 = 16 * half; f0 < Fp; f0 += 32) {
             uint32_t hi[16], lo[16];
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
@@ -397,30 +400,32 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         mbar_arrive(bar_theta);
 
         float ll = 0.0f;
-        float gacc[kTcMaxFp];
+        constexpr int kHalfCols = kTcMaxFp / 2;    // gradient columns owned: chunks f0 = 16*half + 32*k
+        float gacc[kHalfCols];
 #pragma unroll
-        for (int f = 0; f < kTcMaxFp; ++f) gacc[f] = 0.0f;
+        for (int f = 0; f < kHalfCols; ++f) gacc[f] = 0.0f;
         bool ok = ntiles > 0;
         for (int i = 0; ok && i < ntiles; ++i) {
             const int b = i & 1;
             if (!mbar_wait(bar_d1full + b, (i >> 1) & 1, p.err)) { ok = false; break; }
             tc_fence_after();
-            const int n0 = (t_begin + i) * kTcObs;
-            const uint32_t d1 = tmem + lane_off + col_buf + b * 64;
-            float h[32];
-            tmem_ld32(d1, h);
-            uint32_t rh[32], rl[32];
+            const int n0 = (t_begin + i) * kTcObs + 16 * half;
+            const uint32_t d1 = tmem + lane_off + col_buf + b * 64 + 16 * half;
+            float h[16];
+            tmem_ld16(d1, h);
+            uint32_t rh[16], rl[16];
 #pragma unroll
-            for (int j = 0; j < 32; ++j) {
+            for (int j = 0; j < 16; ++j) {
                 const int n = n0 + j;
                 const bool live = n < p.N;
                 const float yv = live ? __ldg(p.y + n) : 0.0f;
                 const float hv = h[j];
-                const float e = expf(-fabsf(hv));
-                const float l1 = log1pf(e);
-                const float lpe = fmaxf(hv, 0.0f) + l1;              // log1p_exp(h)
-                const float inv = 1.0f / (1.0f + e);
-                const float sig = hv >= 0.0f ? inv : e * inv;         // logistic(h)
+                // log1p_exp(h) = max(h,0) + log1p(exp(-|h|)); logistic(h) from the same exp (math.jl:202-224)
+                const float e = __expf(-fabsf(hv));
+                const float onepe = 1.0f + e;
+                const float lpe = fmaxf(hv, 0.0f) + __logf(onepe);
+                const float inv = __frcp_rn(onepe);
+                const float sig = hv >= 0.0f ? inv : e * inv;
                 const bool sup = (yv == 0.0f) | (yv == 1.0f);
                 ll += live ? (sup ? yv * hv - lpe : -INFINITY) : 0.0f;
                 const float r = live ? yv - sig : 0.0f;
@@ -428,8 +433,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 rh[j] = hb;
                 rl[j] = tf32_bits(r - __uint_as_float(hb));
             }
-            tmem_st32(d1, rh);        // R_hi overwrites the consumed H^T columns
-            tmem_st32(d1 + 32, rl);
+            tmem_st16(d1, rh);        // R_hi overwrites the consumed H^T columns
+            tmem_st16(d1 + 32, rl);
             asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             tc_fence_before();
             mbar_arrive(bar_rfull + b);
@@ -438,25 +443,35 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 if (!mbar_wait(bar_d2full, (i / kTcDrainTiles) & 1, p.err)) { ok = false; break; }
                 tc_fence_after();
 #pragma unroll
-                for (int f0 = 0; f0 < kTcMaxFp; f0 += 16) {
+                for (int k = 0; k < kHalfCols / 16; ++k) {
+                    const int f0 = 16 * half + 32 * k;
                     if (f0 < Fp) {
                         float g[16];
                         tmem_ld16(tmem + lane_off + col_d2 + f0, g);
 #pragma unroll
-                        for (int j = 0; j < 16; ++j) gacc[f0 + j] += g[j];
+                        for (int j = 0; j < 16; ++j) gacc[16 * k + j] += g[j];
                     }
                 }
                 tc_fence_before();
                 mbar_arrive(bar_d2empty);
             }
         }
+        // combine the two halves' log-likelihoods through shared memory
+        float* ll_half = reinterpret_cast<float*>(tmem_slot + 4);
+        if (half == 1) ll_half[c_local] = ll;
+        asm volatile("bar.sync 1, %0;" ::"n"(kTcEpiThreads));
         if (ok) {
-            if (c < p.C) p.part_ll[(size_t)split * p.C + c] = ll;
+            if (half == 0 && c < p.C) p.part_ll[(size_t)split * p.C + c] = ll + ll_half[c_local];
             if (p.want_grad && c < p.C) {
                 float* dst = p.part_g + ((size_t)split * p.C + c) * p.F;
 #pragma unroll
-                for (int f = 0; f < kTcMaxFp; ++f)
-                    if (f < p.F) dst[f] = gacc[f];
+                for (int k = 0; k < kHalfCols / 16; ++k) {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        const int f = 16 * half + 32 * k + j;
+                        if (f < p.F) dst[f] = gacc[16 * k + j];
+                    }
+                }
             }
         }
     }
@@ -579,7 +594,7 @@ inline int tc_glm_setup(TcGlmPlan& t, const float* d_Xa, const float* d_y, int N
         tc_err_string() = "cuTensorMapEncodeTiled failed";
         return 1;
     }
-    t.smem = 1024 + (size_t)kTcStages * tc_stage_bytes(Fp) + 128;
+    t.smem = 1024 + (size_t)kTcStages * tc_stage_bytes(Fp) + 128 + 16 + kTcChains * sizeof(float);
     if (cudaFuncSetAttribute(tc_glm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem) != cudaSuccess) {
         tc_err_string() = "shared-memory opt-in failed";
         return 1;
@@ -621,7 +636,7 @@ inline cudaError_t tc_glm_launch(const TcGlmPlan& t, const float* params, float*
     p.y = t.y; p.part_ll = t.part_ll; p.part_g = t.part_g; p.err = t.err;
     p.N = t.N; p.F = t.F; p.Fp = t.Fp; p.C = t.C;
     p.tiles_per_split = t.tiles_per_split; p.num_tiles = t.num_tiles; p.want_grad = grads ? 1 : 0;
-    dim3 grid(t.S, (t.C + kTcChains - 1) / kTcChains);
+    dim3 grid((t.C + kTcChains - 1) / kTcChains, t.S);
     tc_glm_kernel<<<grid, kTcThreads, t.smem, st>>>(t.map_xk_hi, t.map_xk_lo, t.map_xm_hi, t.map_xm_lo, params, p);
     tc_reduce_kernel<<<(t.C + 7) / 8, 256, 0, st>>>(params, t.part_ll, grads ? t.part_g : nullptr, totals, grads,
                                                      t.S, t.C, t.F, t.off, t.icpt_mu, t.icpt_sigma, t.coef_mu,
