@@ -15,9 +15,9 @@
 // so the per-chain log-likelihood is a thread-local sum and the residual tile
 // never touches shared memory.
 //
-// Warp roles (320 threads): warp 0 = TMA producer, warp 1 = MMA issuer (and
-// TMEM owner), warps 2-9 = epilogue: two warps per TMEM lane quadrant, each
-// owning half of a tile's observation columns and half of the gradient columns.
+// Warp roles (576 threads): warp 0 = TMA producer, warp 1 = MMA issuer (and
+// TMEM owner), warps 2-17 = epilogue: four warps per TMEM lane quadrant, each
+// owning 8 of a tile's observation columns and a quarter of the gradient columns.
 // Pipelines: 3 X stages, 2 H/R TMEM buffers, so GEMM1 of tile t+1 runs on the
 // tensor cores while the epilogue of tile t runs on the CUDA cores / SFUs.
 //
@@ -40,8 +40,8 @@ namespace ut {
 constexpr int kTcChains = 128;          // M of both GEMMs (TMEM lanes)
 constexpr int kTcObs = 32;              // observations per tile (N of GEMM1, K of GEMM2)
 constexpr int kTcMaxFp = 128;           // padded feature count the TMEM plan holds (3 Fp + 128 <= 512)
-constexpr int kTcThreads = 320;         // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
-constexpr int kTcEpiThreads = 256;
+constexpr int kTcThreads = 576;         // warp 0 TMA, warp 1 MMA, warps 2-17 epilogue
+constexpr int kTcEpiThreads = 512;
 constexpr long long kTcWaitClocks = 1ll << 31;
 
 struct TcGlmParams {
@@ -88,16 +88,20 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Bounded wait: returns false (and raises the error word) when it gives up.
+// The clock and the (global) error word are only looked at every 1024 spins,
+// so a wait that succeeds within a few polls costs no memory round trip.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
-    while (true) {
+    for (uint32_t it = 1;; ++it) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (clock64() - t0 > kTcWaitClocks) {
-            atomicExch(err, 1);
-            return false;
+        if ((it & 1023u) == 0) {
+            if (clock64() - t0 > kTcWaitClocks) {
+                atomicExch(err, 1);
+                return false;
+            }
+            if (*((volatile int*)err)) return false;  // another role already gave up
         }
-        if (*((volatile int*)err)) return false;  // another role already gave up
     }
 }
 
@@ -106,6 +110,13 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
         "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
         ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
         : "memory");
+}
+
+// Plain (untiled) bulk copy global -> shared, completing on an mbarrier.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
 }
 
 __device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
@@ -211,7 +222,7 @@ __host__ __device__ inline int tc_kblocks(int Fp) { return Fp / 8; }
 __host__ __device__ inline int tc_matoms(int Fp) { return (Fp + 31) / 32; }
 __host__ __device__ inline int tc_xk_bytes(int Fp) { return tc_kblocks(Fp) * kTcObs * 32; }
 __host__ __device__ inline int tc_xm_bytes(int Fp) { return tc_matoms(Fp) * kTcObs * 128; }
-__host__ __device__ inline int tc_stage_bytes(int Fp) { return 2 * tc_xk_bytes(Fp) + 2 * tc_xm_bytes(Fp); }
+__host__ __device__ inline int tc_stage_bytes(int Fp) { return 2 * tc_xk_bytes(Fp) + 2 * tc_xm_bytes(Fp) + 1024; }  // + y tile (128 B used)
 
 __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
     asm volatile(
@@ -233,6 +244,22 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&r)[8]) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};"
+                 ::"r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 // Shared-memory descriptor, SWIZZLE_128B_BASE32B (layout type 1).
@@ -300,7 +327,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 const int s = i % kTcStages;
                 if (i >= kTcStages && !mbar_wait(bar_xempty + s, ((i / kTcStages) - 1) & 1, p.err)) break;
                 uint8_t* st = smem + s * stage_bytes;
-                mbar_expect_tx(bar_xfull + s, stage_bytes);
+                mbar_expect_tx(bar_xfull + s, stage_bytes - 1024 + kTcObs * 4);
                 const int n0 = (t_begin + i) * kTcObs;
                 for (int kb = 0; kb < KB; ++kb) {
                     tma_load_2d(st + kb * (kTcObs * 32), &map_xk_hi, bar_xfull + s, kb * 8, n0);
@@ -311,6 +338,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     tma_load_2d(st + 2 * xk_bytes + xm_bytes + a * (kTcObs * 128), &map_xm_lo, bar_xfull + s, a * 32,
                                 n0);
                 }
+                bulk_load(st + 2 * xk_bytes + 2 * xm_bytes, p.y + n0, kTcObs * 4, bar_xfull + s);
             }
         }
     } else if (warp == 1) {
@@ -378,12 +406,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     } else {
         // ---------------- epilogue: thread = chain (TMEM lane) ----------------
         const int q = warp & 3;                 // TMEM lane quadrant
-        const int half = (warp - 2) >> 2;       // which half of the columns this warp owns
+        const int slot = (warp - 2) >> 2;       // which quarter of the columns this warp owns
         const int c_local = q * 32 + lane;
         const int c = ctile * kTcChains + c_local;
         const uint32_t lane_off = (uint32_t)(q * 32) << 16;
-        // Theta row of this chain -> TF32 hi / lo in TMEM (A operand of GEMM1); 16-column chunks alternate halves
-        for (int f0 = 16 * half; f0 < Fp; f0 += 32) {
+        // Theta row of this chain -> TF32 hi / lo in TMEM (A operand of GEMM1);
+        // 16-column chunks f0 = 16*slot + 64*k belong to this warp (also for the gradient)
+        for (int f0 = 16 * slot; f0 < Fp; f0 += 64) {
             uint32_t hi[16], lo[16];
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
@@ -400,25 +429,31 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         mbar_arrive(bar_theta);
 
         float ll = 0.0f;
-        constexpr int kHalfCols = kTcMaxFp / 2;    // gradient columns owned: chunks f0 = 16*half + 32*k
-        float gacc[kHalfCols];
+        constexpr int kOwnCols = kTcMaxFp / 4;     // gradient columns owned by this warp
+        float gacc[kOwnCols];
 #pragma unroll
-        for (int f = 0; f < kHalfCols; ++f) gacc[f] = 0.0f;
+        for (int f = 0; f < kOwnCols; ++f) gacc[f] = 0.0f;
         bool ok = ntiles > 0;
         for (int i = 0; ok && i < ntiles; ++i) {
-            const int b = i & 1;
+            const int b = i & 1, s = i % kTcStages;
+            // the y tile arrived with the X stage; d1_full(i) implies GEMM1(i) consumed stage s,
+            // which the producer only refills after GEMM2(i) -- after this tile's r_full
             if (!mbar_wait(bar_d1full + b, (i >> 1) & 1, p.err)) { ok = false; break; }
             tc_fence_after();
-            const int n0 = (t_begin + i) * kTcObs + 16 * half;
-            const uint32_t d1 = tmem + lane_off + col_buf + b * 64 + 16 * half;
-            float h[16];
-            tmem_ld16(d1, h);
-            uint32_t rh[16], rl[16];
+            const int n0 = (t_begin + i) * kTcObs + 8 * slot;
+            const float* ys = reinterpret_cast<const float*>(smem + s * stage_bytes + 2 * xk_bytes + 2 * xm_bytes) +
+                              8 * slot;
+            const uint32_t d1 = tmem + lane_off + col_buf + b * 64 + 8 * slot;
+            float h[8];
+            tmem_ld8(d1, h);
+            const float4 y0 = *reinterpret_cast<const float4*>(ys);
+            const float4 y1 = *reinterpret_cast<const float4*>(ys + 4);
+            const float yt[8] = {y0.x, y0.y, y0.z, y0.w, y1.x, y1.y, y1.z, y1.w};
+            uint32_t rh[8], rl[8];
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int n = n0 + j;
-                const bool live = n < p.N;
-                const float yv = live ? __ldg(p.y + n) : 0.0f;
+            for (int j = 0; j < 8; ++j) {
+                const bool live = n0 + j < p.N;
+                const float yv = live ? yt[j] : 0.0f;
                 const float hv = h[j];
                 // log1p_exp(h) = max(h,0) + log1p(exp(-|h|)); logistic(h) from the same exp (math.jl:202-224)
                 const float e = __expf(-fabsf(hv));
@@ -433,8 +468,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 rh[j] = hb;
                 rl[j] = tf32_bits(r - __uint_as_float(hb));
             }
-            tmem_st16(d1, rh);        // R_hi overwrites the consumed H^T columns
-            tmem_st16(d1 + 32, rl);
+            tmem_st8(d1, rh);        // R_hi overwrites the consumed H^T columns
+            tmem_st8(d1 + 32, rl);
             asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             tc_fence_before();
             mbar_arrive(bar_rfull + b);
@@ -443,8 +478,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 if (!mbar_wait(bar_d2full, (i / kTcDrainTiles) & 1, p.err)) { ok = false; break; }
                 tc_fence_after();
 #pragma unroll
-                for (int k = 0; k < kHalfCols / 16; ++k) {
-                    const int f0 = 16 * half + 32 * k;
+                for (int k = 0; k < kOwnCols / 16; ++k) {
+                    const int f0 = 16 * slot + 64 * k;
                     if (f0 < Fp) {
                         float g[16];
                         tmem_ld16(tmem + lane_off + col_d2 + f0, g);
@@ -456,19 +491,21 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 mbar_arrive(bar_d2empty);
             }
         }
-        // combine the two halves' log-likelihoods through shared memory
-        float* ll_half = reinterpret_cast<float*>(tmem_slot + 4);
-        if (half == 1) ll_half[c_local] = ll;
+        // combine the four column quarters' log-likelihoods through shared memory
+        float* ll_part = reinterpret_cast<float*>(tmem_slot + 4);   // [4][128]
+        ll_part[slot * kTcChains + c_local] = ll;
         asm volatile("bar.sync 1, %0;" ::"n"(kTcEpiThreads));
         if (ok) {
-            if (half == 0 && c < p.C) p.part_ll[(size_t)split * p.C + c] = ll + ll_half[c_local];
+            if (slot == 0 && c < p.C)
+                p.part_ll[(size_t)split * p.C + c] = ((ll_part[c_local] + ll_part[kTcChains + c_local]) +
+                                                      ll_part[2 * kTcChains + c_local]) + ll_part[3 * kTcChains + c_local];
             if (p.want_grad && c < p.C) {
                 float* dst = p.part_g + ((size_t)split * p.C + c) * p.F;
 #pragma unroll
-                for (int k = 0; k < kHalfCols / 16; ++k) {
+                for (int k = 0; k < kOwnCols / 16; ++k) {
 #pragma unroll
                     for (int j = 0; j < 16; ++j) {
-                        const int f = 16 * half + 32 * k + j;
+                        const int f = 16 * slot + 64 * k + j;
                         if (f < p.F) dst[f] = gacc[16 * k + j];
                     }
                 }
@@ -492,7 +529,7 @@ struct TcGlmPlan {
     float* part_ll = nullptr;
     float* part_g = nullptr;
     int* err = nullptr;
-    const float* y = nullptr;
+    const float* y = nullptr;     // N rounded up to whole observation tiles, zero padded
     int off = 0;
     float icpt_mu = 0, icpt_sigma = 1, coef_mu = 0, coef_sigma = 1;
     CUtensorMap map_xk_hi, map_xk_lo, map_xm_hi, map_xm_lo;
@@ -559,7 +596,7 @@ inline int tc_glm_setup(TcGlmPlan& t, const float* d_Xa, const float* d_y, int N
     cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
     const int Fp = ((F + 15) / 16) * 16;
     if (major != 10 || Fp > kTcMaxFp || N < 1 || C < 1) return 0;  // the CUDA-core tiled path serves the rest
-    t.N = N; t.F = F; t.Fp = Fp; t.C = C; t.y = d_y; t.off = off;
+    t.N = N; t.F = F; t.Fp = Fp; t.C = C; t.off = off;
     t.icpt_mu = icpt_mu; t.icpt_sigma = icpt_sigma; t.coef_mu = coef_mu; t.coef_sigma = coef_sigma;
     t.num_tiles = (N + kTcObs - 1) / kTcObs;
     const int ctiles = (C + kTcChains - 1) / kTcChains;
@@ -581,6 +618,17 @@ inline int tc_glm_setup(TcGlmPlan& t, const float* d_Xa, const float* d_y, int N
         return 1;
     }
     cudaMemset(t.err, 0, sizeof(int));
+    {
+        float* yp = nullptr;
+        const size_t ybytes = (size_t)t.num_tiles * kTcObs * sizeof(float);
+        if (!alloc((void**)&yp, ybytes)) {
+            tc_err_string() = "cudaMalloc failed";
+            return 1;
+        }
+        cudaMemset(yp, 0, ybytes);
+        cudaMemcpy(yp, d_y, (size_t)N * sizeof(float), cudaMemcpyDeviceToDevice);
+        t.y = yp;
+    }
     const long long total = (long long)N * Fp;
     tc_split_x_kernel<<<(unsigned)((total + 255) / 256), 256>>>(d_Xa, t.xhi, t.xlo, N, F, Fp);
     if (cudaDeviceSynchronize() != cudaSuccess) {
@@ -594,7 +642,7 @@ inline int tc_glm_setup(TcGlmPlan& t, const float* d_Xa, const float* d_y, int N
         tc_err_string() = "cuTensorMapEncodeTiled failed";
         return 1;
     }
-    t.smem = 1024 + (size_t)kTcStages * tc_stage_bytes(Fp) + 128 + 16 + kTcChains * sizeof(float);
+    t.smem = 1024 + (size_t)kTcStages * tc_stage_bytes(Fp) + 128 + 16 + 4 * kTcChains * sizeof(float);
     if (cudaFuncSetAttribute(tc_glm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem) != cudaSuccess) {
         tc_err_string() = "shared-memory opt-in failed";
         return 1;
