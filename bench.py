@@ -249,6 +249,22 @@ def run_b200(args):
         dist.destroy_process_group()
 
 
+def run_kernel_only(args):
+    """Only the device evaluations (no L2 flush, no e2e, no CPU leg): the
+    command the ncu summaries under profiles/ were captured with."""
+    import torch
+    from uncertaintea_b200.device import DeviceBatchedWorkspace
+    model, X, y, params = _data()
+    ws = DeviceBatchedWorkspace(model, N_CHAINS, args=(X,), constraints={"y": y})
+    qd = torch.from_numpy(params).cuda()
+    for _ in range(args.warmup + args.steps):
+        t, g = ws.logjoint_gradient_device(qd)
+    torch.cuda.synchronize()
+    ws.check()
+    print(json.dumps({"kernel_path": ws.kernel_path(), "evaluations": args.warmup + args.steps}))
+    ws.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -257,8 +273,11 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--kernel-only", action="store_true")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.kernel_only:
+        run_kernel_only(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_b200(args)
