@@ -221,6 +221,29 @@ int32_t ut_chees_reduce(ut_workspace* ws, const float* d_initials, const float* 
 int32_t ut_running_variance_update(const float* d_positions, const double* d_weights, int32_t num_params,
                                    int32_t num_chains, double* d_state, int32_t window_length, void* stream);
 
+/* ---- allocation-free GLM logjoint + gradient ------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory when they need a gradient (a host whose device memory all comes from
+ * its own pool or a fixed budget, or a latency-critical loop that cannot take
+ * the synchronisation cudaMalloc / cudaFree may imply): the Bernoulli-logit GLM
+ * logjoint and gradient of C chains with every buffer supplied by the caller
+ * on the device and no device memory allocated.
+ *   d_design   : N x P row-major design matrix (a leading column of ones when
+ *                has_intercept = 1, then the covariates)
+ *   d_y        : N outcomes in {0, 1}
+ *   d_params   : C x P chain-major parameters;  d_totals: C;  d_gradients: C x P
+ * Scratch memory is a fixed 16 MiB device array owned by the library (held by
+ * every GPU that loads it until exit): C * (P + 1) may be at most 4,194,304,
+ * larger batches are rejected with UT_ERR_ARGUMENT.  The first call on a device
+ * performs a one-time set-up for that device; make it before any stream
+ * capture.  All calls share the array, so calls that overlap on the GPU race:
+ * serialise them.  Returns once the work is queued on `stream`. */
+int32_t ut_glm_logjoint_gradient_noalloc(const float* d_design, const float* d_y, int64_t num_obs,
+                                         int32_t num_params, int32_t has_intercept, double intercept_mu,
+                                         double intercept_sigma, double coef_mu, double coef_sigma,
+                                         const float* d_params, int32_t num_chains, float* d_totals,
+                                         float* d_gradients, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,7 +1,8 @@
 """Builds the sm_100a CUDA library in-tree: uncertaintea_b200/libut_b200.so.
 
-All kernels and the C ABI are one translation unit (csrc/ut_api.cu), compiled
-by nvcc for sm_100a only.  Run: python -m uncertaintea_b200.build [--force]
+The C ABI and its kernels are compiled by nvcc for sm_100a only, from
+csrc/ut_api.cu and csrc/ut_noalloc.cu (the allocation-free entry point, whose
+kernels are private to its file).  Run: python -m uncertaintea_b200.build [--force]
 """
 from __future__ import annotations
 
@@ -35,7 +36,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     newest = max(os.path.getmtime(s) for s in sources())
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= newest:
         return LIB
-    cmd = [nvcc()] + NVCC_FLAGS + ["-o", LIB + ".tmp", os.path.join(HERE, "csrc", "ut_api.cu")]
+    cmd = [nvcc()] + NVCC_FLAGS + ["-o", LIB + ".tmp", os.path.join(HERE, "csrc", "ut_api.cu"),
+                                   os.path.join(HERE, "csrc", "ut_noalloc.cu")]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     subprocess.run(cmd, check=True)

@@ -59,6 +59,9 @@ int inst_k(int P) {
 
 }  // namespace
 
+// Lets the library's other translation unit report through ut_last_error.
+void ut_internal_set_last_error(const char* msg) { g_last_error = msg; }
+
 struct ut_workspace {
     ut_plan_desc plan;
     int P = 0, C = 0, N = 0, device = 0;
