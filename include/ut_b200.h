@@ -244,6 +244,74 @@ int32_t ut_glm_logjoint_gradient_noalloc(const float* d_design, const float* d_y
                                          const float* d_params, int32_t num_chains, float* d_totals,
                                          float* d_gradients, void* stream);
 
+/* ---- learned gradient surrogate ------------------------------------------ */
+/* No counterpart in the reference.  An MLP  P -> 256 -> 256 -> P  with SiLU
+ * hidden layers maps an unconstrained position to an approximation of the
+ * logjoint gradient.  Weights are FP32 (updated by Adam); the matmuls run in
+ * BF16 with FP32 accumulation.  Inputs are normalised per coordinate as
+ * (theta - in_mean) / in_scale and outputs de-normalised as
+ * y * out_scale + out_mean.  It is trained on (theta, gradient) pairs that an
+ * exact sampler produced (typically its warmup) and then drives leapfrog
+ * trajectories whose Metropolis accept uses the exact logjoint, so the target
+ * distribution stays exact.  1 <= P <= 128.
+ *
+ * Weight layout (one flat FP32 array; Pp = P rounded up to 16; entries at
+ * row or column index >= P are zero and stay zero):
+ *   W1 [256][Pp], b1 [256], W2 [256][256], b2 [256], W3 [Pp][256], b3 [Pp]. */
+typedef struct ut_surrogate ut_surrogate;
+
+/* Allocates the weights on the current device, initialised as
+ * U(-1/sqrt(fan_in), 1/sqrt(fan_in)) from Philox (key = (seed, layer)), zero
+ * biases, identity normalisation. */
+int32_t ut_surrogate_create(int32_t num_params, uint32_t seed, ut_surrogate** out);
+int32_t ut_surrogate_destroy(ut_surrogate* s);
+/* Length of the flat weight array. */
+int32_t ut_surrogate_num_weights(const ut_surrogate* s, int64_t* out);
+/* Host copies of the FP32 weights.  set_weights also resets the Adam state. */
+int32_t ut_surrogate_get_weights(const ut_surrogate* s, float* out, int64_t n);
+int32_t ut_surrogate_set_weights(ut_surrogate* s, const float* in, int64_t n);
+/* Normalisation as 4*P host floats: in_mean, in_scale, out_mean, out_scale. */
+int32_t ut_surrogate_get_normalization(const ut_surrogate* s, float* out);
+int32_t ut_surrogate_set_normalization(ut_surrogate* s, const float* in);
+/* Sets the normalisation to the per-coordinate means and standard deviations
+ * of num_pairs device pairs (d_theta, d_gradient: num_pairs x P each). */
+int32_t ut_surrogate_fit_normalization(ut_surrogate* s, const float* d_theta, const float* d_gradient,
+                                       int64_t num_pairs, void* stream);
+/* num_steps Adam steps (beta1 0.9, beta2 0.999, eps 1e-8) on the mean squared
+ * error between the normalised network output and the normalised gradient,
+ * loss = sum over batch rows and coordinates of (y - t)^2 / batch.  The
+ * learning rate goes geometrically from learning_rate to final_learning_rate.
+ * Step k uses the pair rows d_batch_index[k*batch .. k*batch+batch) when
+ * d_batch_index is given (indices outside [0, num_pairs) are skipped and
+ * reported by ut_surrogate_check), else rows drawn uniformly with
+ * replacement from Philox (key = (seed, Adam step count)).  d_losses
+ * (optional, num_steps floats) receives each step's loss.  1 <= batch <= 65536. */
+int32_t ut_surrogate_train(ut_surrogate* s, const float* d_theta, const float* d_gradient, int64_t num_pairs,
+                           const int32_t* d_batch_index, int32_t batch, int32_t num_steps, float learning_rate,
+                           float final_learning_rate, uint32_t seed, float* d_losses, void* stream);
+/* The loss of one batch and its gradient with respect to the weights (flat
+ * layout above), without updating anything. */
+int32_t ut_surrogate_loss_gradient(ut_surrogate* s, const float* d_theta, const float* d_gradient, int64_t num_pairs,
+                                   const int32_t* d_batch_index, int32_t batch, float* d_weight_gradient,
+                                   float* d_loss, void* stream);
+/* Surrogate gradient at n positions: d_out (n x P) = network(d_theta). */
+int32_t ut_surrogate_gradient(const ut_surrogate* s, const float* d_theta, int64_t n, float* d_out, void* stream);
+/* Synchronises `stream` and reports batch indices that were out of range. */
+int32_t ut_surrogate_check(ut_surrogate* s, void* stream);
+
+/* One batched HMC iteration whose leapfrog kicks all use the surrogate
+ * gradient (at the start, at every intermediate point and at the end), with
+ * the Metropolis accept on the exact logjoint of the workspace's model: the
+ * leapfrog map of any position-only force field is volume-preserving and
+ * reversible, so the chain keeps the exact target.  Same momentum and accept
+ * Philox streams and the same buffers as ut_hmc_iteration, except that
+ * buf->gradient is neither read nor written (recompute it with
+ * ut_logjoint_gradient_device before an exact iteration).  Per iteration: L+1
+ * surrogate evaluations and one logjoint-only evaluation of the model. */
+int32_t ut_surrogate_hmc_iteration(ut_workspace* ws, const ut_surrogate* s, const ut_hmc_buffers* buf,
+                                   int32_t num_leapfrog_steps, uint32_t iteration_coord,
+                                   float divergence_threshold, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

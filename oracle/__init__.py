@@ -46,6 +46,14 @@ def load():
                                              c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32]),
         "orc_chees_reduce": (None, [c_int32, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                     c_void_p]),
+        "orc_mlp_num_weights": (c_int64, [c_int32]),
+        "orc_mlp_forward": (None, [c_void_p, c_void_p, c_int32, c_void_p, c_int64, c_void_p, c_int32]),
+        "orc_mlp_loss_gradient": (None, [c_void_p, c_void_p, c_int32, c_void_p, c_void_p, c_int64, c_void_p, c_int32,
+                                         c_void_p, c_void_p, c_int32]),
+        "orc_surrogate_hmc_iteration_f32": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p,
+                                                      c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_void_p,
+                                                      c_int32, c_uint32, c_float, c_void_p, c_void_p, c_void_p,
+                                                      c_void_p, c_void_p, c_void_p, c_void_p, c_int32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -140,6 +148,28 @@ class OracleModel:
                                       _p(inverse_mass), _p(trial_step), coord, _p(lar), threads)
         return lar
 
+    def surrogate_hmc_iteration(self, weights, norm, position, logjoint, inverse_mass, step, L, coord, thr=1000.0,
+                                bf16=True, want_proposal=False, threads=0):
+        """Surrogate-driven HMC iteration (kicks from the MLP oracle, exact accept);
+        position and logjoint are updated in place."""
+        C = position.shape[0]
+        weights = np.ascontiguousarray(weights, dtype=np.float32)
+        norm = np.ascontiguousarray(norm, dtype=np.float32)
+        inverse_mass = np.ascontiguousarray(inverse_mass, dtype=np.float32)
+        step = np.ascontiguousarray(step, dtype=np.float32)
+        out = {k: np.empty(C, dtype=np.float32) for k in ("accept_prob", "energy", "energy_error")}
+        out["accepted"] = np.empty(C, dtype=np.uint8)
+        out["divergent"] = np.empty(C, dtype=np.uint8)
+        prop = np.empty_like(position) if want_proposal else None
+        mom = np.empty_like(position) if want_proposal else None
+        load().orc_surrogate_hmc_iteration_f32(*self._common(), C, _p(weights), _p(norm), int(bool(bf16)),
+                                               _p(position), _p(logjoint), _p(inverse_mass), _p(step), L, coord,
+                                               thr, _p(out["accept_prob"]), _p(out["energy"]),
+                                               _p(out["energy_error"]), _p(out["accepted"]), _p(out["divergent"]),
+                                               _p(prop), _p(mom), threads)
+        out["proposal"], out["endpoint_momentum"] = prop, mom
+        return out
+
     def nuts_iteration(self, position, gradient, logjoint, inverse_mass, step, max_depth, coord, thr=1000.0,
                        threads=0):
         C = position.shape[0]
@@ -166,6 +196,36 @@ def chees_reduce(initials, proposals, momenta, accept_prob, divergent, inverse_m
                                                             (divergent, np.uint8), (inverse_mass, np.float32))]
     load().orc_chees_reduce(P, C, *[_p(a) for a in held], _p(out))
     return out
+
+
+def mlp_num_weights(P):
+    return int(load().orc_mlp_num_weights(P))
+
+
+def mlp_forward(weights, norm, theta, bf16=True):
+    """Surrogate MLP restatement: gradient estimates at the rows of theta (n x P)."""
+    theta = np.ascontiguousarray(theta, dtype=np.float32)
+    weights = np.ascontiguousarray(weights, dtype=np.float32)
+    norm = np.ascontiguousarray(norm, dtype=np.float32)
+    n, P = theta.shape
+    out = np.empty((n, P), dtype=np.float32)
+    load().orc_mlp_forward(_p(weights), _p(norm), P, _p(theta), n, _p(out), int(bool(bf16)))
+    return out
+
+
+def mlp_loss_gradient(weights, norm, theta, grad, index, bf16=True):
+    """Loss and FP64 weight gradient of the batch of pair rows `index`."""
+    theta = np.ascontiguousarray(theta, dtype=np.float32)
+    grad = np.ascontiguousarray(grad, dtype=np.float32)
+    weights = np.ascontiguousarray(weights, dtype=np.float32)
+    norm = np.ascontiguousarray(norm, dtype=np.float32)
+    index = np.ascontiguousarray(index, dtype=np.int32)
+    n, P = theta.shape
+    wg = np.empty(weights.size, dtype=np.float64)
+    loss = np.zeros(1)
+    load().orc_mlp_loss_gradient(_p(weights), _p(norm), P, _p(theta), _p(grad), n, _p(index), index.size, _p(wg),
+                                 _p(loss), int(bool(bf16)))
+    return float(loss[0]), wg
 
 
 def max_threads():

@@ -1,7 +1,7 @@
 """Build recipe of the CPU oracle (test infrastructure only).
 
-Compiles oracle/oracle.cpp into oracle/_build/liboracle.so with g++ and
-OpenMP.  Run: python oracle/build_oracle.py
+Compiles oracle/oracle.cpp and oracle/oracle_mlp.cpp into
+oracle/_build/liboracle.so with g++ and OpenMP.  Run: python oracle/build_oracle.py
 """
 from __future__ import annotations
 
@@ -15,12 +15,12 @@ LIB = os.path.join(OUT_DIR, "liboracle.so")
 
 
 def build(force: bool = False) -> str:
-    src = os.path.join(HERE, "oracle.cpp")
-    hdr = os.path.join(HERE, "..", "include", "ut_b200.h")
-    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(src), os.path.getmtime(hdr)):
+    srcs = [os.path.join(HERE, "oracle.cpp"), os.path.join(HERE, "oracle_mlp.cpp")]
+    deps = srcs + [os.path.join(HERE, "oracle_mlp.h"), os.path.join(HERE, "..", "include", "ut_b200.h")]
+    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(d) for d in deps):
         return LIB
     os.makedirs(OUT_DIR, exist_ok=True)
-    cmd = ["g++", "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", src, "-o", LIB]
+    cmd = ["g++", "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared"] + srcs + ["-o", LIB]
     subprocess.run(cmd, check=True)
     return LIB
 

@@ -26,6 +26,7 @@
 #endif
 
 #include "../include/ut_b200.h"
+#include "oracle_mlp.h"
 
 namespace {
 
@@ -608,6 +609,75 @@ int orc_hmc_iteration_f32(const ut_plan_desc* plan, const float* observed, const
         if (acc) {
             for (int k = 0; k < P; ++k) { position[(size_t)c * P + k] = q[k]; gradient[(size_t)c * P + k] = g[k]; }
             logjoint[c] = t.lj1;
+        }
+    }
+    return 0;
+}
+
+// One surrogate-driven HMC iteration (f32): the same Philox momentum, leapfrog
+// and accept as orc_hmc_iteration_f32, except that every kick (start,
+// intermediate, end) uses the MLP surrogate gradient (oracle_mlp, BF16
+// rounding points when bf16 != 0) and only the end point's exact logjoint is
+// evaluated, for the accept.  No reference counterpart: the project's
+// surrogate HMC.  The gradient array is not used.
+int orc_surrogate_hmc_iteration_f32(const ut_plan_desc* plan, const float* observed, const int32_t* trip_counts,
+                                    const int32_t* loop_starts, int32_t C, const float* mlp_weights,
+                                    const float* mlp_norm, int32_t bf16, float* position, float* logjoint,
+                                    const float* inverse_mass, const float* step, int32_t L, uint32_t coord,
+                                    float thr, float* accept_prob, float* energy, float* energy_error,
+                                    uint8_t* accepted, uint8_t* divergent, float* proposal,
+                                    float* endpoint_momentum, int32_t threads) {
+    ModelData m = make_model(plan, observed, trip_counts, loop_starts);
+    const int P = plan->num_params;
+    const oracle_mlp::Evaluator net(mlp_weights, mlp_norm, P, bf16);
+    set_threads(threads);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int c = 0; c < C; ++c) {
+        std::vector<float> q(position + (size_t)c * P, position + (size_t)(c + 1) * P);
+        std::vector<float> g(P), p(P);
+        for (int k = 0; k < P; ++k)
+            p[k] = rand_normal<float>((uint32_t)c, coord, kStreamMomentum, (uint32_t)k) / std::sqrt(inverse_mass[k]);
+        const float H0 = kinetic(p.data(), inverse_mass, P) - logjoint[c];
+        const float h = step[c], half = 0.5f * h;
+        bool valid = true;
+        float lj1 = 0.0f;
+        net(q.data(), g.data());
+        if (!all_finite(g.data(), P)) valid = false;
+        if (valid) for (int k = 0; k < P; ++k) p[k] += half * g[k];
+        for (int l = 1; l <= L && valid; ++l) {
+            for (int k = 0; k < P; ++k) q[k] += h * inverse_mass[k] * p[k];
+            net(q.data(), g.data());
+            if (l < L) {
+                if (!all_finite(g.data(), P)) { valid = false; break; }
+                for (int k = 0; k < P; ++k) p[k] += h * g[k];
+            } else {
+                const float lj = (float)logjoint_grad<float, double>(m, q.data(), nullptr);
+                if (!all_finite(g.data(), P) || !std::isfinite(lj)) { valid = false; break; }
+                lj1 = lj;
+            }
+        }
+        if (valid) for (int k = 0; k < P; ++k) p[k] = -(p[k] + half * g[k]);
+        const float H1 = valid ? kinetic(p.data(), inverse_mass, P) - lj1 : std::numeric_limits<float>::infinity();
+        bool acc = false, div = true;
+        float ap = 0.0f, ee = std::numeric_limits<float>::infinity();
+        if (valid) {
+            const float lar = H0 - H1;
+            ee = H1 - H0;
+            div = !std::isfinite(ee) || ee > thr;
+            ap = !std::isfinite(lar) ? 0.0f : (lar >= 0.0f ? 1.0f : std::exp(lar));
+            const float uacc = rand_uniform<float>((uint32_t)c, coord, kStreamAccept, 0u);
+            acc = std::log(uacc) < std::min(0.0f, lar);
+        }
+        accept_prob[c] = ap;
+        energy_error[c] = ee;
+        accepted[c] = acc ? 1 : 0;
+        divergent[c] = div ? 1 : 0;
+        energy[c] = acc ? H1 : H0;
+        if (proposal) for (int k = 0; k < P; ++k) proposal[(size_t)c * P + k] = q[k];
+        if (endpoint_momentum) for (int k = 0; k < P; ++k) endpoint_momentum[(size_t)c * P + k] = p[k];
+        if (acc) {
+            for (int k = 0; k < P; ++k) position[(size_t)c * P + k] = q[k];
+            logjoint[c] = lj1;
         }
     }
     return 0;

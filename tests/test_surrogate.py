@@ -1,0 +1,343 @@
+"""Learned gradient surrogate: the MLP oracle (CPU) and the device kernels
+(GPU, through the C ABI) against it.
+
+The surrogate has no counterpart in the reference; its oracle is the
+project's CPU restatement of the same network (oracle/oracle_mlp.cpp), which
+follows the device kernels' BF16 rounding points and accumulates in FP64.
+
+Tolerances (stated per test):
+* oracle FP64 weight gradient vs central finite differences: relative 1e-4.
+* device forward vs BF16 oracle: relative Frobenius error <= 2e-3 (FP32 vs FP64
+  accumulation plus rare one-ulp BF16 flips of an intermediate activation).
+* device weight gradient vs BF16 oracle: relative Frobenius error per weight
+  block <= 1e-2; loss relative error <= 1e-4.
+* one Adam step: weights within 1e-6 of the closed form applied to the
+  device's own gradient.
+* surrogate HMC iteration vs the oracle's, same Philox streams: >= 95% of
+  chains with the same accept decision; their proposals within rtol 1e-2.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import oracle
+from uncertaintea_b200 import _native as nat
+from uncertaintea_b200.surrogate import weight_layout
+
+
+def _random_weights(P, seed, scale=1.0):
+    r = np.random.default_rng(seed)
+    lay = weight_layout(P)
+    pp = lay["padded_params"]
+    w = np.zeros(lay["total"], dtype=np.float32)
+
+    def put(name, arr):
+        sl, shape = lay[name]
+        w[sl] = np.asarray(arr, dtype=np.float32).reshape(-1)
+
+    W1 = np.zeros((256, pp))
+    W1[:, :P] = r.standard_normal((256, P)) * scale / np.sqrt(P)
+    W3 = np.zeros((pp, 256))
+    W3[:P] = r.standard_normal((P, 256)) * scale / 16.0
+    b3 = np.zeros(pp)
+    b3[:P] = 0.1 * r.standard_normal(P)
+    put("W1", W1)
+    put("b1", 0.1 * r.standard_normal(256))
+    put("W2", r.standard_normal((256, 256)) * scale / 16.0)
+    put("b2", 0.1 * r.standard_normal(256))
+    put("W3", W3)
+    put("b3", b3)
+    return w
+
+
+def _random_norm(P, seed):
+    r = np.random.default_rng(seed + 1)
+    return np.concatenate([0.3 * r.standard_normal(P), 0.5 + r.random(P), 0.3 * r.standard_normal(P),
+                           0.5 + 2 * r.random(P)]).astype(np.float32)
+
+
+# ------------------------------------------------------------------ CPU -----
+@pytest.mark.parametrize("P", [5, 19])
+def test_oracle_weight_gradient_matches_finite_differences(P):
+    r = np.random.default_rng(P)
+    w = _random_weights(P, P)
+    norm = _random_norm(P, P)
+    th = r.standard_normal((24, P)).astype(np.float32)
+    g = r.standard_normal((24, P)).astype(np.float32)
+    idx = np.array([0, 3, 3, 7, 11, 23, 5, 2], dtype=np.int32)
+    _, wg = oracle.mlp_loss_gradient(w, norm, th, g, idx, bf16=False)
+    lay = weight_layout(P)
+    live = np.nonzero(w)[0]
+    picks = list(r.choice(live, 30, replace=False)) + [lay["b1"][0].start + 3, lay["b3"][0].start]
+    for k in picks:
+        h = np.float32(1e-2 * max(abs(float(w[k])), 1e-2))
+        wp, wm = w.copy(), w.copy()
+        wp[k] += h
+        wm[k] -= h
+        lp = oracle.mlp_loss_gradient(wp, norm, th, g, idx, bf16=False)[0]
+        lm = oracle.mlp_loss_gradient(wm, norm, th, g, idx, bf16=False)[0]
+        fd = (lp - lm) / (float(wp[k]) - float(wm[k]))
+        assert abs(fd - wg[k]) <= 1e-4 * max(abs(wg[k]), 1e-3), (k, fd, wg[k])
+
+
+def test_oracle_bf16_mode_is_close_to_fp64():
+    P = 12
+    r = np.random.default_rng(0)
+    w, norm = _random_weights(P, 1), _random_norm(P, 1)
+    th = r.standard_normal((64, P)).astype(np.float32)
+    f64 = oracle.mlp_forward(w, norm, th, bf16=False)
+    f16 = oracle.mlp_forward(w, norm, th, bf16=True)
+    err = np.linalg.norm(f16 - f64) / np.linalg.norm(f64)
+    assert 1e-5 < err < 3e-2  # BF16 rounding is visible but small
+
+
+def test_oracle_skips_out_of_range_rows():
+    P = 4
+    r = np.random.default_rng(1)
+    w, norm = _random_weights(P, 2), _random_norm(P, 2)
+    th = r.standard_normal((10, P)).astype(np.float32)
+    g = r.standard_normal((10, P)).astype(np.float32)
+    l1, g1 = oracle.mlp_loss_gradient(w, norm, th, g, np.array([1, 2, -1, 10], np.int32))
+    l2, g2 = oracle.mlp_loss_gradient(w, norm, th, g, np.array([1, 2], np.int32))
+    # same rows, batch size 4 vs 2 in the 1/B factor
+    np.testing.assert_allclose(l1 * 4, l2 * 2, rtol=1e-12)
+
+
+# ------------------------------------------------------------------ GPU -----
+def _torch():
+    return pytest.importorskip("torch")
+
+
+def _surrogate(P, w=None, norm=None):
+    from uncertaintea_b200.surrogate import GradientSurrogate
+    s = GradientSurrogate(P, seed=7)
+    if w is not None:
+        s.set_weights(w)
+    if norm is not None:
+        s.set_normalization(norm)
+    return s
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("P,n", [(100, 1000), (7, 45), (33, 64), (128, 96)])
+def test_forward_vs_oracle(lib, P, n):
+    torch = _torch()
+    r = np.random.default_rng(P)
+    w, norm = _random_weights(P, P), _random_norm(P, P)
+    s = _surrogate(P, w, norm)
+    th = r.standard_normal((n, P)).astype(np.float32)
+    got = s.gradient(torch.from_numpy(th).cuda()).cpu().numpy()
+    ref = oracle.mlp_forward(w, norm, th, bf16=True)
+    assert np.linalg.norm(got - ref) <= 2e-3 * np.linalg.norm(ref)
+    assert np.max(np.abs(got - ref)) <= 1e-2 * np.max(np.abs(ref))
+    ref64 = oracle.mlp_forward(w, norm, th, bf16=False)
+    assert np.linalg.norm(got - ref64) <= 3e-2 * np.linalg.norm(ref64)
+    assert np.array_equal(s.get_weights(), w) and np.array_equal(s.get_normalization().reshape(-1), norm)
+    s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("P,batch", [(100, 512), (9, 77)])
+def test_loss_gradient_vs_oracle(lib, P, batch):
+    torch = _torch()
+    r = np.random.default_rng(10 + P)
+    w, norm = _random_weights(P, 3), _random_norm(P, 3)
+    s = _surrogate(P, w, norm)
+    n = 600
+    th = r.standard_normal((n, P)).astype(np.float32)
+    g = (2.0 * r.standard_normal((n, P))).astype(np.float32)
+    idx = r.integers(0, n, batch).astype(np.int32)
+    loss, wg = s.loss_gradient(torch.from_numpy(th).cuda(), torch.from_numpy(g).cuda(), torch.from_numpy(idx).cuda())
+    loss, wg = float(loss.cpu()[0]), wg.cpu().numpy().astype(np.float64)
+    lref, wref = oracle.mlp_loss_gradient(w, norm, th, g, idx, bf16=True)
+    assert abs(loss - lref) <= 1e-4 * abs(lref)
+    lay = weight_layout(P)
+    for name in ("W1", "b1", "W2", "b2", "W3", "b3"):
+        sl = lay[name][0]
+        assert np.linalg.norm(wg[sl] - wref[sl]) <= 1e-2 * np.linalg.norm(wref[sl]), name
+    s.check()
+    s.close()
+
+
+@pytest.mark.gpu
+def test_out_of_range_batch_index_is_skipped_and_reported(lib):
+    torch = _torch()
+    P = 6
+    r = np.random.default_rng(5)
+    w, norm = _random_weights(P, 4), _random_norm(P, 4)
+    s = _surrogate(P, w, norm)
+    th = r.standard_normal((20, P)).astype(np.float32)
+    g = r.standard_normal((20, P)).astype(np.float32)
+    idx = np.array([3, 20, -5, 7], dtype=np.int32)
+    loss, wg = s.loss_gradient(torch.from_numpy(th).cuda(), torch.from_numpy(g).cuda(), torch.from_numpy(idx).cuda())
+    with pytest.raises(ValueError):
+        s.check()
+    s.check()  # the flag was cleared
+    lref, wref = oracle.mlp_loss_gradient(w, norm, th, g, idx, bf16=True)
+    assert abs(float(loss.cpu()[0]) - lref) <= 1e-4 * abs(lref)
+    wg = wg.cpu().numpy()
+    assert np.linalg.norm(wg - wref) <= 1e-2 * np.linalg.norm(wref)
+    s.close()
+
+
+@pytest.mark.gpu
+def test_adam_step_closed_form(lib):
+    """First Adam step from zero moments: w1 = w0 - lr * g / (|g| + eps)."""
+    torch = _torch()
+    P = 20
+    r = np.random.default_rng(8)
+    w, norm = _random_weights(P, 5), _random_norm(P, 5)
+    s = _surrogate(P, w, norm)
+    th = torch.from_numpy(r.standard_normal((256, P)).astype(np.float32)).cuda()
+    g = torch.from_numpy(r.standard_normal((256, P)).astype(np.float32)).cuda()
+    idx = torch.from_numpy(r.integers(0, 256, 128).astype(np.int32)).cuda()
+    _, wg = s.loss_gradient(th, g, idx)
+    gd = wg.cpu().numpy().astype(np.float64)
+    lr = 1e-3
+    s.train(th, g, steps=1, batch=128, learning_rate=lr, final_learning_rate=lr, index=idx)
+    got = s.get_weights().astype(np.float64)
+    exp = w.astype(np.float64) - lr * gd / (np.abs(gd) + 1e-8)
+    assert np.max(np.abs(got - exp)) <= 1e-6
+    lay = weight_layout(P)
+    assert np.all(got[lay["W1"][0]].reshape(256, -1)[:, P:] == 0)  # padded columns stay zero
+    s.close()
+
+
+@pytest.mark.gpu
+def test_training_learns_a_gaussian_score(lib):
+    """Pairs from a correlated Gaussian: the trained surrogate reproduces the
+    score -Sigma^{-1}(theta - mu) on held-out points."""
+    torch = _torch()
+    P = 24
+    r = np.random.default_rng(11)
+    A = r.standard_normal((P, P)) / np.sqrt(P)
+    cov = A @ A.T + 0.5 * np.eye(P)
+    prec = np.linalg.inv(cov)
+    mu = r.standard_normal(P)
+    n = 1 << 16
+    th = r.multivariate_normal(mu, cov, size=n + 4096)
+    sc = -(th - mu) @ prec
+    tt = torch.from_numpy(th[:n].astype(np.float32)).cuda()
+    gg = torch.from_numpy(sc[:n].astype(np.float32)).cuda()
+    s = _surrogate(P)
+    s.fit_normalization(tt, gg)
+    nrm = s.get_normalization()
+    np.testing.assert_allclose(nrm[0], th[:n].mean(0), atol=2e-3 * np.abs(th).max())
+    np.testing.assert_allclose(nrm[1], th[:n].std(0), rtol=1e-3)
+    losses = s.train(tt, gg, steps=1500, batch=1024, learning_rate=2e-3, final_learning_rate=5e-5, seed=3)
+    losses = losses.cpu().numpy()
+    assert np.all(np.isfinite(losses)) and losses[-50:].mean() < 0.05 * losses[:10].mean()
+    hold_t = torch.from_numpy(th[n:].astype(np.float32)).cuda()
+    hold_g = torch.from_numpy(sc[n:].astype(np.float32)).cuda()
+    err = s.relative_error(hold_t, hold_g)
+    assert err < 0.05, err
+    s.close()
+
+
+def _glm_model(N, D, C, seed):
+    from uncertaintea_b200.models import BernoulliLogitGLM, logistic_regression_data
+    X, y, _ = logistic_regression_data(N, D, seed=seed)
+    return BernoulliLogitGLM(D), (X,), {"y": y}
+
+
+def _glm_mode(X, y, iters=25):
+    X = X.astype(np.float64)
+    b = np.zeros(X.shape[1])
+    for _ in range(iters):
+        pr = 1 / (1 + np.exp(-X @ b))
+        g = X.T @ (y - pr) - b
+        H = -(X.T * (pr * (1 - pr))) @ X - np.eye(X.shape[1])
+        b = b - np.linalg.solve(H, g)
+    return b, H
+
+
+def _trained_glm_surrogate(ws, X, y, n_pairs=1 << 14, steps=800, seed=0):
+    """A surrogate trained on exact gradients at Laplace-approximation draws."""
+    torch = _torch()
+    mode, H = _glm_mode(X, y)
+    cov = np.linalg.inv(-H)
+    r = np.random.default_rng(seed)
+    th = r.multivariate_normal(mode, 2.0 * cov, size=n_pairs).astype(np.float32)
+    tt = torch.from_numpy(th).cuda()
+    gg = torch.empty_like(tt)
+    C = ws.batch_size
+    for i in range(0, n_pairs, C):
+        _, gi = ws.logjoint_gradient_device(tt[i:i + C].contiguous())
+        gg[i:i + C] = gi
+    s = _surrogate(ws.parameter_count)
+    s.fit_normalization(tt, gg)
+    s.train(tt, gg, steps=steps, batch=1024, learning_rate=2e-3, final_learning_rate=5e-5, seed=seed)
+    return s, mode, cov
+
+
+@pytest.mark.gpu
+def test_surrogate_hmc_iteration_vs_oracle(lib):
+    torch = _torch()
+    from uncertaintea_b200.device import DeviceBatchedWorkspace
+    C, N, D = 256, 1000, 10
+    m, args, cons = _glm_model(N, D, C, 1)
+    ws = DeviceBatchedWorkspace(m, C, args=args, constraints=cons)
+    X, y = args[0], cons["y"]
+    s, mode, cov = _trained_glm_surrogate(ws, X, y)
+    r = np.random.default_rng(4)
+    q = r.multivariate_normal(mode, cov, size=C).astype(np.float32)
+    qd = torch.from_numpy(q).cuda()
+    t, g = ws.logjoint_gradient_device(qd)
+    im = np.ascontiguousarray(np.diag(cov).astype(np.float32))
+    steps = (0.5 * np.linspace(0.8, 1.2, C)).astype(np.float32)
+    L = 6
+    f = lambda: torch.zeros(C, dtype=torch.float32, device="cuda")  # noqa: E731
+    out = {"accept_prob": f(), "energy": f(), "energy_error": f(),
+           "accepted": torch.zeros(C, dtype=torch.uint8, device="cuda"),
+           "divergent": torch.zeros(C, dtype=torch.uint8, device="cuda")}
+    prop, mom = torch.zeros_like(qd), torch.zeros_like(qd)
+    imd, sd = torch.from_numpy(im).cuda(), torch.from_numpy(steps).cuda()
+    q0, t0, g0 = qd.cpu().numpy().copy(), t.cpu().numpy().copy(), g.cpu().numpy().copy()
+    buf = nat.HmcBuffers(nat.ptr(qd), nat.ptr(g), nat.ptr(t), nat.ptr(imd), nat.ptr(sd), nat.ptr(out["accept_prob"]),
+                         nat.ptr(out["energy"]), nat.ptr(out["energy_error"]), nat.ptr(out["accepted"]),
+                         nat.ptr(out["divergent"]), nat.ptr(prop), nat.ptr(mom))
+    nat.check(lib.ut_surrogate_hmc_iteration(ws.handle, s.handle, ctypes.byref(buf), L, 777, 1000.0, None))
+    torch.cuda.synchronize()
+    gpu = {k: v.cpu().numpy() for k, v in out.items()}
+    assert np.array_equal(g.cpu().numpy(), g0)  # the gradient buffer is not touched
+    om = oracle.OracleModel(ws.lowered)
+    qo, to = q0.copy(), t0.copy()
+    ref = om.surrogate_hmc_iteration(s.get_weights(), s.get_normalization(), qo, to, im, steps, L, 777,
+                                     want_proposal=True)
+    assert ref["accept_prob"].mean() > 0.5  # the trained surrogate makes useful trajectories
+    same = (gpu["accepted"] == ref["accepted"]) & (gpu["divergent"] == ref["divergent"])
+    assert same.mean() >= 0.95
+    ok = same & (ref["divergent"] == 0)
+    np.testing.assert_allclose(prop.cpu().numpy()[ok], ref["proposal"][ok], rtol=1e-2, atol=1e-3)
+    # accepted chains carry the exact logjoint of their new position
+    acc = gpu["accepted"].astype(bool)
+    t_exact, _ = ws.logjoint_gradient_device(qd)
+    np.testing.assert_allclose(t.cpu().numpy()[acc], t_exact.cpu().numpy()[acc], rtol=1e-6, atol=1e-3)
+    np.testing.assert_array_equal(qd.cpu().numpy()[~acc], q0[~acc])
+    s.close()
+    ws.close()
+
+
+@pytest.mark.gpu
+def test_surrogate_validation_errors(lib):
+    torch = _torch()
+    from uncertaintea_b200.surrogate import GradientSurrogate
+    with pytest.raises(ValueError):
+        GradientSurrogate(129)
+    s = GradientSurrogate(10)
+    w = s.get_weights()
+    lay = weight_layout(10)
+    w[lay["W1"][0]][11] = 1.0  # padded column 11 of row 0
+    with pytest.raises(ValueError):
+        s.set_weights(w)
+    with pytest.raises(IndexError):
+        s.set_weights(w[:-1])
+    bad = s.get_normalization()
+    bad[1, 0] = 0.0
+    with pytest.raises(ValueError):
+        s.set_normalization(bad)
+    x = torch.zeros((4, 10), device="cuda")
+    with pytest.raises(ValueError):
+        s.train(x, x, steps=0, batch=4)
+    s.close()

@@ -3,7 +3,8 @@
 Public surface mirrors the reference's ``UncertainTea.Device`` and
 ``UncertainTea.Inference`` facades (src/UncertainTea.jl:101-200) for the
 device path: batched logjoint / gradient, batched HMC, persistent NUTS,
-ChEES-HMC, the Philox4x32-10 stream and the R-hat / ESS diagnostics.
+ChEES-HMC, the Philox4x32-10 stream and the R-hat / ESS diagnostics; plus
+the learned gradient surrogate for ChEES-HMC (no reference counterpart).
 """
 from .models import (BernoulliLogitGLM, HierarchicalNormalNoncentered, TeaModelSpec, hierarchical_data,
                      logistic_regression_data)
@@ -11,6 +12,7 @@ from .device import (DeviceBatchedWorkspace, device_batched_logjoint, device_bat
                      device_batched_logjoint_gradient, device_batched_logjoint_gradient_, device_lowering_report)
 from .inference import HMCChains, batched_chees, batched_hmc, batched_nuts, posterior_array
 from .diagnostics import ess, min_ess_per_second, rhat, summarize
+from .surrogate import GradientSurrogate, batched_chees_surrogate
 from . import rng
 
 __all__ = [
@@ -18,5 +20,5 @@ __all__ = [
     "logistic_regression_data", "DeviceBatchedWorkspace", "device_batched_logjoint", "device_batched_logjoint_",
     "device_batched_logjoint_gradient", "device_batched_logjoint_gradient_", "device_lowering_report", "HMCChains",
     "batched_chees", "batched_hmc", "batched_nuts", "posterior_array", "ess", "min_ess_per_second", "rhat",
-    "summarize", "rng",
+    "summarize", "rng", "GradientSurrogate", "batched_chees_surrogate",
 ]

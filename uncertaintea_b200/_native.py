@@ -110,6 +110,23 @@ SIGNATURES = [
     ("ut_glm_logjoint_gradient_noalloc", c_int32,
      [c_void_p, c_void_p, c_int64, c_int32, c_int32, c_double, c_double, c_double, c_double, c_void_p, c_int32,
       c_void_p, c_void_p, c_void_p]),
+    ("ut_surrogate_create", c_int32, [c_int32, c_uint32, POINTER(c_void_p)]),
+    ("ut_surrogate_destroy", c_int32, [c_void_p]),
+    ("ut_surrogate_num_weights", c_int32, [c_void_p, POINTER(c_int64)]),
+    ("ut_surrogate_get_weights", c_int32, [c_void_p, c_void_p, c_int64]),
+    ("ut_surrogate_set_weights", c_int32, [c_void_p, c_void_p, c_int64]),
+    ("ut_surrogate_get_normalization", c_int32, [c_void_p, c_void_p]),
+    ("ut_surrogate_set_normalization", c_int32, [c_void_p, c_void_p]),
+    ("ut_surrogate_fit_normalization", c_int32, [c_void_p, c_void_p, c_void_p, c_int64, c_void_p]),
+    ("ut_surrogate_train", c_int32,
+     [c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_int32, c_int32, c_float, c_float, c_uint32, c_void_p,
+      c_void_p]),
+    ("ut_surrogate_loss_gradient", c_int32,
+     [c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_int32, c_void_p, c_void_p, c_void_p]),
+    ("ut_surrogate_gradient", c_int32, [c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),
+    ("ut_surrogate_check", c_int32, [c_void_p, c_void_p]),
+    ("ut_surrogate_hmc_iteration", c_int32,
+     [c_void_p, c_void_p, POINTER(HmcBuffers), c_int32, c_uint32, c_float, c_void_p]),
 ]
 
 _lib = None

@@ -1,8 +1,9 @@
 """Builds the sm_100a CUDA library in-tree: uncertaintea_b200/libut_b200.so.
 
 The C ABI and its kernels are compiled by nvcc for sm_100a only, from
-csrc/ut_api.cu and csrc/ut_noalloc.cu (the allocation-free entry point, whose
-kernels are private to its file).  Run: python -m uncertaintea_b200.build [--force]
+csrc/ut_api.cu, csrc/ut_noalloc.cu (the allocation-free entry point, whose
+kernels are private to its file) and csrc/ut_surrogate.cu (the learned
+gradient surrogate).  Run: python -m uncertaintea_b200.build [--force]
 """
 from __future__ import annotations
 
@@ -37,7 +38,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= newest:
         return LIB
     cmd = [nvcc()] + NVCC_FLAGS + ["-o", LIB + ".tmp", os.path.join(HERE, "csrc", "ut_api.cu"),
-                                   os.path.join(HERE, "csrc", "ut_noalloc.cu")]
+                                   os.path.join(HERE, "csrc", "ut_noalloc.cu"),
+                                   os.path.join(HERE, "csrc", "ut_surrogate.cu")]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     subprocess.run(cmd, check=True)

@@ -628,6 +628,50 @@ int32_t ut_hmc_iteration(ut_workspace* ws, const ut_hmc_buffers* buf, int32_t nu
     return UT_OK;
 }
 
+// Defined in ut_surrogate.cu (C++ linkage: not part of the exported C ABI).
+extern "C++" int ut_internal_surrogate_num_params(const ut_surrogate* s);
+extern "C++" int32_t ut_internal_surrogate_forward(const ut_surrogate* s, const float* x, int64_t n, float* out,
+                                                   cudaStream_t st);
+
+int32_t ut_surrogate_hmc_iteration(ut_workspace* ws, const ut_surrogate* s, const ut_hmc_buffers* buf,
+                                   int32_t num_leapfrog_steps, uint32_t iteration_coord, float divergence_threshold,
+                                   void* stream) {
+    int32_t rc = check_ws(ws);
+    if (rc) return rc;
+    if (!s) return fail(UT_ERR_ARGUMENT, "null surrogate handle");
+    if (ut_internal_surrogate_num_params(s) != ws->P)
+        return fail(UT_ERR_DIMENSION, "surrogate has %d parameters, the model %d", ut_internal_surrogate_num_params(s),
+                    ws->P);
+    if (!buf || !buf->position || !buf->logjoint || !buf->inverse_mass || !buf->step || !buf->accept_prob ||
+        !buf->energy || !buf->energy_error || !buf->accepted || !buf->divergent)
+        return fail(UT_ERR_ARGUMENT, "null HMC buffer");
+    if (num_leapfrog_steps < 1) return fail(UT_ERR_ARGUMENT, "num_leapfrog_steps must be >= 1, got %d", (int)num_leapfrog_steps);
+    if ((rc = ensure_lf(ws))) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    HmcArgs a;
+    a.position = buf->position; a.logjoint = buf->logjoint;
+    // the kicks read the surrogate gradient from lf.wg; the accept copies the
+    // accepted row of lf.wg onto itself, so buf->gradient is never touched
+    a.gradient = ws->lf.wg;
+    a.inverse_mass = buf->inverse_mass; a.step = buf->step;
+    a.accept_prob = buf->accept_prob; a.energy = buf->energy; a.energy_error = buf->energy_error;
+    a.accepted = buf->accepted; a.divergent = buf->divergent;
+    a.proposal = buf->proposal; a.endpoint_momentum = buf->endpoint_momentum;
+    a.C = ws->C; a.L = num_leapfrog_steps; a.coord = iteration_coord; a.thr = divergence_threshold;
+    const int P = ws->P;
+    const unsigned grid = (ws->C + 7) / 8;
+    if ((rc = ut_internal_surrogate_forward(s, buf->position, ws->C, ws->lf.wg, st))) return rc;
+    UT_K_SWITCH(ws->K, lf_begin_kernel<K><<<grid, 256, 0, st>>>(a, ws->lf, P));
+    UT_LAUNCHED();
+    for (int l = 1; l <= num_leapfrog_steps; ++l) {
+        if ((rc = ut_internal_surrogate_forward(s, ws->lf.wq, ws->C, ws->lf.wg, st))) return rc;
+        if (l == num_leapfrog_steps && (rc = density(ws, ws->lf.wq, ws->lf.wlj, nullptr, st))) return rc;
+        UT_K_SWITCH(ws->K, lf_step_kernel<K><<<grid, 256, 0, st>>>(a, ws->lf, P, l));
+        UT_LAUNCHED();
+    }
+    return UT_OK;
+}
+
 int32_t ut_leapfrog_probe(ut_workspace* ws, const float* d_position, const float* d_gradient, const float* d_logjoint,
                           const float* d_inverse_mass, const float* d_trial_step, uint32_t iteration_coord,
                           float* d_log_accept_ratio, void* stream) {

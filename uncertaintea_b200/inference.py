@@ -432,6 +432,7 @@ class HMCChains:
     sampling_seconds: float
     trajectory_length: float = float("nan")
     gradient_evaluations: int = 0
+    surrogate: object = None  # report of the learned gradient surrogate, when one drove the run
 
     @property
     def num_chains(self):
@@ -916,6 +917,8 @@ def batched_chees(model, args=(), constraints=None, *, num_chains, num_samples, 
     total = num_warmup + num_samples
     divergences = 0
     grad_evals = 0
+    if _surrogate is not None:
+        _surrogate.setup(run, num_warmup)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     t_sample = None
@@ -931,11 +934,13 @@ def batched_chees(model, args=(), constraints=None, *, num_chains, num_samples, 
         if warm and adapt_trajectory_length:
             initials.copy_(run.position)
         if _surrogate is not None:
-            _surrogate.iteration(run, L, it, divergence_threshold)
+            grad_evals += _surrogate.iteration(run, L, it, divergence_threshold, warm,
+                                               proposal if (warm and adapt_traj) else None,
+                                               momentum if (warm and adapt_traj) else None)
         else:
             run.hmc_iteration(L, it, divergence_threshold, proposal if (warm and adapt_traj) else None,
                               momentum if (warm and adapt_traj) else None)
-        grad_evals += L * C
+            grad_evals += L * C
         if warm:
             ap = run.accept_prob.double().cpu().numpy()
             acc = run.accepted.cpu().numpy().astype(bool)
@@ -954,14 +959,22 @@ def batched_chees(model, args=(), constraints=None, *, num_chains, num_samples, 
                 _chees_apply_trajectory_gradient(traj, num, den, jitter, driver.step_size)
                 if _trajectory_trace is not None:
                     _trajectory_trace.append(traj.trajectory_length)
+            if _surrogate is not None:
+                _surrogate.after_warmup_iteration(run, it)
             if it == num_warmup:
                 driver.warmup_finalize()
+                if _surrogate is not None:
+                    # Philox coordinates past the run's own iterations
+                    _surrogate.end_warmup(run, driver, traj, lambda i: _chees_jitter_value(jitter_amount, i),
+                                          _chees_leapfrog_steps_from_jitter, divergence_threshold, total + 1)
             _invoke_callback(callback, callback_every, "warmup", it, num_warmup, driver.step_size, divergences)
         else:
             draws.record(it - num_warmup - 1, integration_steps=L)
             draws.ist[it - num_warmup - 1].fill_(L)
             _invoke_callback(callback, callback_every, "sample", it - num_warmup, num_samples, driver.step_size,
                              divergences)
+    if _surrogate is not None:
+        _surrogate.finish(run)
     torch.cuda.synchronize()
     t1 = time.perf_counter()
     if t_sample is None:
