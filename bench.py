@@ -9,6 +9,13 @@ shipped).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
+At N=1 the line also carries `surrogate_chees`: the learned-gradient-surrogate
+workload on the same model (min ESS/s of surrogate-driven ChEES-HMC vs plain
+ChEES-HMC, both at R-hat < 1.01; skipped with --no-surrogate), and
+`uneven_batch`: 512 hierarchical models of uneven sizes in one batched
+persistent-NUTS run (aggregate ESS/s, per-model time to R-hat < 1.01;
+skipped with --no-uneven).
+
 Multi-GPU: the path does not shard (every chain's gradient needs all of X),
 so N GPUs run N independent replicas (weak scaling) and `value` is the
 aggregate over all ranks divided by the max-over-ranks time.
@@ -233,6 +240,12 @@ def run_b200(args):
         rate, cores, sample = cpu_reference_rate(model, X, y, params, budget_s=args.cpu_seconds)
         cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
     launches = int(ws.launches_per_gradient()) * args.steps if hasattr(ws, "launches_per_gradient") else 2 * args.steps
+    ws.close()
+    sur = uneven = None
+    if rank == 0 and world == 1 and not args.no_surrogate:
+        sur = surrogate_comparison()
+    if rank == 0 and world == 1 and not args.no_uneven:
+        uneven = uneven_batch()
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -243,10 +256,95 @@ def run_b200(args):
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": N_CHAINS * N_COEF * 4,
                         "d2h_bytes_per_step": N_CHAINS * (N_COEF + 1) * 4},
                 "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches}
+        if sur is not None:
+            line["surrogate_chees"] = sur
+        if uneven is not None:
+            line["uneven_batch"] = uneven
         print(json.dumps(line), flush=True)
-    ws.close()
     if dist:
         dist.destroy_process_group()
+
+
+def surrogate_comparison(num_chains=4096, num_warmup=500, num_samples=500):
+    """The learned-surrogate workload on the same model: ChEES-HMC with exact
+    gradients vs ChEES-HMC whose trajectories the trained MLP drives (exact
+    logjoint in the accept), same seeds and settings (16 initial leapfrog
+    steps, trajectory length and step size adapted in warmup).  The surrogate
+    is trained on 2^20 (theta, gradient) pairs of the last 256 warmup
+    iterations.  Min ESS over the 100 coefficients per second of sampling
+    (warmup, training and step-size re-tuning excluded, reported apart)."""
+    from uncertaintea_b200 import batched_chees, batched_chees_surrogate, ess, rhat
+    model, X, y, _ = _data()
+    kw = dict(num_chains=num_chains, num_samples=num_samples, num_warmup=num_warmup, num_leapfrog_steps=16, rng=1)
+    out = {}
+    runs = {"plain": batched_chees(model, (X,), {"y": y}, **kw),
+            "surrogate": batched_chees_surrogate(model, (X,), {"y": y}, **kw)}
+    for name, ch in runs.items():
+        e, r = ess(ch, space="unconstrained"), rhat(ch, space="unconstrained")
+        out[name] = {"min_ess_per_s": float(np.min(e) / ch.sampling_seconds), "min_ess": float(np.min(e)),
+                     "max_rhat": float(np.max(r)), "sampling_s": ch.sampling_seconds, "warmup_s": ch.warmup_seconds,
+                     "mean_leapfrog_steps": float(ch.integration_steps.mean()),
+                     "mean_accept": float(ch.accept_prob.mean()), "step_size": float(np.mean(ch.step_size))}
+    rep = runs["surrogate"].surrogate
+    out["surrogate"].update({"pairs": rep.num_pairs, "train_steps": rep.train_steps,
+                             "train_s": rep.train_seconds, "relative_error": rep.relative_error_after_training,
+                             "fallback_at": rep.fallback_at})
+    up = runs["plain"].unconstrained.reshape(-1, N_COEF)
+    us = runs["surrogate"].unconstrained.reshape(-1, N_COEF)
+    out["max_mean_diff_in_sd"] = float(np.max(np.abs(up.mean(0) - us.mean(0)) / up.std(0)))
+    out["ratio"] = out["surrogate"]["min_ess_per_s"] / out["plain"]["min_ess_per_s"]
+    out["metric"] = "min ESS/s (R-hat<1.01), surrogate ChEES-HMC vs plain ChEES-HMC"
+    out["unit"] = "effective samples/s"
+    out["config"] = (f"config-4: learned gradient surrogate on the config-3 model, {num_chains} chains, "
+                     f"{num_warmup} warmup + {num_samples} sampling iterations")
+    return out
+
+
+def uneven_models(num_models=512, seed=5):
+    """The uneven-batch workload: num_models independent non-centred
+    hierarchical normal models with J ~ UniformInt[8, 512] groups and
+    UniformInt[5, 100] observations per group, sigma_j ~ U(0.5, 2), y drawn
+    from the prior predictive (seeded)."""
+    from uncertaintea_b200.models import HierarchicalNormalNoncentered, hierarchical_data
+    r = np.random.default_rng(seed)
+    models = []
+    for i in range(num_models):
+        J = int(r.integers(8, 513))
+        sizes = r.integers(5, 101, size=J)
+        y, sig, sz, _ = hierarchical_data(J, sizes, 1000 + i)
+        models.append((HierarchicalNormalNoncentered(J), (sig, sz), {"y": y}))
+    return models
+
+
+def uneven_batch(num_models=512, chains=64, num_warmup=500, num_samples=500):
+    """All models in one batched persistent-NUTS run (one launch per
+    parameter-slot class per iteration, replayed from a CUDA graph, launch
+    shapes from the autotuner): aggregate min-ESS per sampling second and the
+    per-model time to R-hat < 1.01 (checked every 50 draws)."""
+    from uncertaintea_b200.multi import batched_nuts_multi
+    models = uneven_models(num_models)
+    res = batched_nuts_multi(models, chains_per_model=chains, num_warmup=num_warmup, num_samples=num_samples,
+                             rng=1, rhat_check_every=50)
+    p50, p99 = res.time_to_rhat_quantiles()
+    s50, s99 = res.time_to_rhat_quantiles(from_sampling=True)
+    cls = res.classes
+    out = {"metric": "aggregate min-ESS/s; per-model time to R-hat<1.01 (p50/p99 over models)",
+           "unit": "effective samples/s; s", "aggregate_ess_per_s": res.aggregate_ess_per_second,
+           "time_to_rhat_p50_s": p50, "time_to_rhat_p99_s": p99,
+           "sampling_time_to_rhat_p50_s": s50, "sampling_time_to_rhat_p99_s": s99,
+           "converged_fraction": res.converged_fraction, "median_model_min_ess": float(np.median(res.min_ess)),
+           "warmup_s": res.warmup_seconds, "sampling_s": res.sampling_seconds,
+           "ms_per_iteration": 1000.0 * res.sampling_seconds / num_samples,
+           "mean_tree_depth": res.mean_tree_depth, "divergences": res.divergences,
+           "total_obs": int(sum(int(m[1][1].sum()) for m in models)), "total_chains": int(res.num_chains.sum()),
+           "classes": {"slots": cls["slots"].tolist(), "models": cls["models"].tolist(),
+                       "chains_per_block": cls["chains_per_block"].tolist(),
+                       "stage_limit_bytes": cls["stage_limit_bytes"].tolist()},
+           "config": (f"config-5: {num_models} non-centred hierarchical models, J~U[8,512], obs/group~U[5,100], "
+                      f"{chains} chains each, max tree depth 10, {num_warmup} warmup + {num_samples} draws, "
+                      "CUDA graph replay, autotuned launch shapes")}
+    res.batch.close()
+    return out
 
 
 def run_kernel_only(args):
@@ -274,6 +372,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--kernel-only", action="store_true")
+    ap.add_argument("--no-surrogate", action="store_true",
+                    help="skip the learned-surrogate ChEES comparison (about a minute) in the output line")
+    ap.add_argument("--no-uneven", action="store_true",
+                    help="skip the uneven-batch run (512 hierarchical models, about two minutes)")
     args = ap.parse_args()
     if args.kernel_only:
         run_kernel_only(args)

@@ -312,6 +312,87 @@ int32_t ut_surrogate_hmc_iteration(ut_workspace* ws, const ut_surrogate* s, cons
                                    int32_t num_leapfrog_steps, uint32_t iteration_coord,
                                    float divergence_threshold, void* stream);
 
+/* ---- uneven batching: many hierarchical models in one batched launch ------ */
+/* No counterpart in the reference.  A batch of independent non-centred
+ * hierarchical normal models (UT_FAMILY_HIER_NORMAL_NONCENTERED), each with
+ * its own groups, group sizes, priors and chain count, sampled together by
+ * batched persistent NUTS: one launch per parameter-slot class per iteration
+ * (the classes run concurrently), per-model step-size and diagonal-mass
+ * adaptation on the device, and the iterations replayed from a captured CUDA
+ * graph.  State layout: model m's chains own the C_m x P_m chain-major block
+ * starting at state_offsets[m] of the position / gradient / draw arrays, its
+ * per-chain entries start at chain_offsets[m], its inverse mass at
+ * param_offsets[m]. */
+typedef struct ut_multi ut_multi;
+
+/* Device pointers into a batch's state (owned by the batch). */
+typedef struct ut_multi_view {
+    float* position;            /* state_floats                                  */
+    float* gradient;            /* state_floats                                  */
+    float* logjoint;            /* total_chains                                  */
+    float* step;                /* total_chains                                  */
+    float* inverse_mass;        /* param_floats                                  */
+    float* accept_prob;         /* total_chains, last iteration                  */
+    int32_t* tree_depth;        /* total_chains, last iteration                  */
+    int32_t* integration_steps; /* total_chains, last iteration                  */
+    uint8_t* divergent;         /* total_chains, last iteration                  */
+    float* draws;               /* draws_capacity x state_floats                 */
+    float* draw_accept;         /* draws_capacity x total_chains                 */
+    int32_t* draw_tree_depth;   /* draws_capacity x total_chains                 */
+    uint8_t* draw_divergent;    /* draws_capacity x total_chains                 */
+    int32_t* iteration;         /* iterations run since ut_multi_begin           */
+    int64_t state_floats;
+    int64_t total_chains;
+    int64_t param_floats;
+    int32_t draws_capacity;
+} ut_multi_view;
+
+/* plans[m]: the model's kernel description (num_params = num_groups + 2 <=
+ * 544).  observed: the models' staged blocks one after another, model m's at
+ * observed_offsets[m] (num_models + 1 entries), each num_obs y values group
+ * after group then num_groups sigma values.  trip_counts / loop_starts: every
+ * model's num_groups entries one model after another, loop_starts relative to
+ * the model's own block.  chains[m]: chain count of model m. */
+int32_t ut_multi_create(int32_t num_models, const ut_plan_desc* plans, const float* observed,
+                        const int64_t* observed_offsets, const int32_t* trip_counts, const int32_t* loop_starts,
+                        const int32_t* chains, int32_t max_tree_depth, ut_multi** out);
+int32_t ut_multi_destroy(ut_multi* mm);
+/* Offsets of every model (num_models + 1 entries each; any may be NULL). */
+int32_t ut_multi_layout(const ut_multi* mm, int64_t* state_offsets, int64_t* chain_offsets, int64_t* param_offsets);
+/* Per slot-count class (8 entries each; any may be NULL): slots per lane K
+ * (models with P <= 32 K), models, chains, chains per CTA and the staging
+ * limit in bytes (a model's data is staged in shared memory when it fits). */
+int32_t ut_multi_class_info(const ut_multi* mm, int32_t* slot_counts, int32_t* num_models, int64_t* num_chains,
+                            int32_t* chains_per_block, int32_t* stage_limit_bytes);
+/* Sets one class's launch configuration: 1..4 chains per CTA, staging limit 0..204800 bytes. */
+int32_t ut_multi_configure(ut_multi* mm, int32_t klass, int32_t chains_per_block, int32_t stage_limit_bytes);
+/* Copies state_floats device positions in and evaluates logjoint + gradient there. */
+int32_t ut_multi_set_positions(ut_multi* mm, const float* d_positions, void* stream);
+/* Starts a run: iteration counter 0, unit inverse masses, every step size
+ * initial_step, dual averaging towards target_accept (pooled over each model's
+ * chains), warmup_actions[i] for warmup iteration i (bit 0: add the positions
+ * to the model's Welford window, bit 1: the window ends and sets the inverse
+ * mass, bit 2: final step size), and room for draws_capacity sampling draws.
+ * The Philox iteration coordinate of iteration i is seed + i. */
+int32_t ut_multi_begin(ut_multi* mm, int32_t num_warmup, int32_t num_samples, uint32_t seed, float target_accept,
+                       float initial_step, float divergence_threshold, const uint8_t* warmup_actions,
+                       int32_t draws_capacity);
+/* Runs the next num_iterations iterations (warmup first, then sampling, whose
+ * positions are recorded as draws), from a captured CUDA graph when
+ * use_graph != 0.  Ordered after prior work on `stream`; later work on
+ * `stream` waits for it. */
+int32_t ut_multi_run(ut_multi* mm, int32_t num_iterations, int32_t use_graph, void* stream);
+/* Autotuner: for every class, times each (chains per CTA in {1, 2, 4}) x
+ * (staging off / on) candidate on the next iteration from the current state
+ * (restored after every trial; results do not depend on the choice) and
+ * keeps the fastest.  timings_ms (optional, 8 x 6 floats): class k's
+ * candidate (w, s) at [6 k + 2 w + s], -1 for empty classes.  Synchronises. */
+int32_t ut_multi_autotune(ut_multi* mm, int32_t trials, float* timings_ms, void* stream);
+/* Max split R-hat over each model's parameters from its first num_draws
+ * recorded draws (d_out: num_models floats). */
+int32_t ut_multi_split_rhat(ut_multi* mm, int32_t num_draws, float* d_out, void* stream);
+int32_t ut_multi_buffers(const ut_multi* mm, ut_multi_view* view);
+
 #ifdef __cplusplus
 }
 #endif

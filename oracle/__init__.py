@@ -44,6 +44,10 @@ def load():
         "orc_nuts_iteration_f32": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p, c_void_p,
                                              c_void_p, c_void_p, c_void_p, c_int32, c_float, c_uint32, c_void_p,
                                              c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32]),
+        "orc_nuts_iteration_keyed_f32": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_uint32,
+                                                   c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32,
+                                                   c_float, c_uint32, c_void_p, c_void_p, c_void_p, c_void_p,
+                                                   c_void_p, c_void_p, c_void_p, c_int32]),
         "orc_chees_reduce": (None, [c_int32, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                     c_void_p]),
         "orc_mlp_num_weights": (c_int64, [c_int32]),
@@ -171,7 +175,7 @@ class OracleModel:
         return out
 
     def nuts_iteration(self, position, gradient, logjoint, inverse_mass, step, max_depth, coord, thr=1000.0,
-                       threads=0):
+                       threads=0, chain_key_offset=0):
         C = position.shape[0]
         inverse_mass = np.ascontiguousarray(inverse_mass, dtype=np.float32)
         step = np.ascontiguousarray(step, dtype=np.float32)
@@ -180,7 +184,8 @@ class OracleModel:
         out["integration_steps"] = np.empty(C, dtype=np.int32)
         out["divergent"] = np.empty(C, dtype=np.uint8)
         out["moved"] = np.empty(C, dtype=np.uint8)
-        load().orc_nuts_iteration_f32(*self._common(), C, _p(position), _p(gradient), _p(logjoint),
+        load().orc_nuts_iteration_keyed_f32(*self._common(), C, int(chain_key_offset), _p(position), _p(gradient),
+                                            _p(logjoint),
                                       _p(inverse_mass), _p(step), max_depth, thr, coord,
                                       _p(out["accept_prob"]), _p(out["energy"]), _p(out["energy_error"]),
                                       _p(out["tree_depth"]), _p(out["integration_steps"]), _p(out["divergent"]),

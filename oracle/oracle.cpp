@@ -708,12 +708,32 @@ int orc_leapfrog_probe_f32(const ut_plan_desc* plan, const float* observed, cons
 
 // One persistent-NUTS iteration for C chains (f32).  State arrays C x P / C,
 // updated in place with the proposal when moved.
+int orc_nuts_iteration_keyed_f32(const ut_plan_desc* plan, const float* observed, const int32_t* trip_counts,
+                                 const int32_t* loop_starts, int32_t C, uint32_t chain_key_offset, float* position,
+                                 float* gradient, float* logjoint, const float* inverse_mass, const float* step,
+                                 int32_t max_depth, float thr, uint32_t coord, float* accept_prob, float* energy,
+                                 float* energy_error, int32_t* tree_depth, int32_t* integration_steps,
+                                 uint8_t* divergent, uint8_t* moved, int32_t threads);
+
 int orc_nuts_iteration_f32(const ut_plan_desc* plan, const float* observed, const int32_t* trip_counts,
                            const int32_t* loop_starts, int32_t C, float* position, float* gradient,
                            float* logjoint, const float* inverse_mass, const float* step, int32_t max_depth,
                            float thr, uint32_t coord, float* accept_prob, float* energy, float* energy_error,
                            int32_t* tree_depth, int32_t* integration_steps, uint8_t* divergent, uint8_t* moved,
                            int32_t threads) {
+    return orc_nuts_iteration_keyed_f32(plan, observed, trip_counts, loop_starts, C, 0u, position, gradient,
+                                        logjoint, inverse_mass, step, max_depth, thr, coord, accept_prob, energy,
+                                        energy_error, tree_depth, integration_steps, divergent, moved, threads);
+}
+
+// The same with chain c's Philox streams keyed by chain_key_offset + c (a
+// model whose chains sit at an offset of a larger batch).
+int orc_nuts_iteration_keyed_f32(const ut_plan_desc* plan, const float* observed, const int32_t* trip_counts,
+                                 const int32_t* loop_starts, int32_t C, uint32_t chain_key_offset, float* position,
+                                 float* gradient, float* logjoint, const float* inverse_mass, const float* step,
+                                 int32_t max_depth, float thr, uint32_t coord, float* accept_prob, float* energy,
+                                 float* energy_error, int32_t* tree_depth, int32_t* integration_steps,
+                                 uint8_t* divergent, uint8_t* moved, int32_t threads) {
     ModelData m = make_model(plan, observed, trip_counts, loop_starts);
     const int P = plan->num_params;
     set_threads(threads);
@@ -721,7 +741,8 @@ int orc_nuts_iteration_f32(const ut_plan_desc* plan, const float* observed, cons
     for (int c = 0; c < C; ++c) {
         std::vector<float> g0(gradient + (size_t)c * P, gradient + (size_t)(c + 1) * P);
         float lj = logjoint[c];
-        NutsOut o = nuts_chain(m, P, (uint32_t)c, coord, position + (size_t)c * P, gradient + (size_t)c * P, lj,
+        NutsOut o = nuts_chain(m, P, chain_key_offset + (uint32_t)c, coord, position + (size_t)c * P,
+                               gradient + (size_t)c * P, lj,
                                inverse_mass, step[c], max_depth, thr);
         if (!o.moved) for (int k = 0; k < P; ++k) gradient[(size_t)c * P + k] = g0[k];
         logjoint[c] = lj;

@@ -4,7 +4,8 @@ Public surface mirrors the reference's ``UncertainTea.Device`` and
 ``UncertainTea.Inference`` facades (src/UncertainTea.jl:101-200) for the
 device path: batched logjoint / gradient, batched HMC, persistent NUTS,
 ChEES-HMC, the Philox4x32-10 stream and the R-hat / ESS diagnostics; plus
-the learned gradient surrogate for ChEES-HMC (no reference counterpart).
+the learned gradient surrogate for ChEES-HMC and many-model batched NUTS
+(no reference counterparts).
 """
 from .models import (BernoulliLogitGLM, HierarchicalNormalNoncentered, TeaModelSpec, hierarchical_data,
                      logistic_regression_data)
@@ -13,6 +14,7 @@ from .device import (DeviceBatchedWorkspace, device_batched_logjoint, device_bat
 from .inference import HMCChains, batched_chees, batched_hmc, batched_nuts, posterior_array
 from .diagnostics import ess, min_ess_per_second, rhat, summarize
 from .surrogate import GradientSurrogate, batched_chees_surrogate
+from .multi import MultiChains, MultiModelBatch, batched_nuts_multi
 from . import rng
 
 __all__ = [
@@ -20,5 +22,6 @@ __all__ = [
     "logistic_regression_data", "DeviceBatchedWorkspace", "device_batched_logjoint", "device_batched_logjoint_",
     "device_batched_logjoint_gradient", "device_batched_logjoint_gradient_", "device_lowering_report", "HMCChains",
     "batched_chees", "batched_hmc", "batched_nuts", "posterior_array", "ess", "min_ess_per_second", "rhat",
-    "summarize", "rng", "GradientSurrogate", "batched_chees_surrogate",
+    "summarize", "rng", "GradientSurrogate", "batched_chees_surrogate", "MultiChains", "MultiModelBatch",
+    "batched_nuts_multi",
 ]

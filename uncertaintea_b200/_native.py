@@ -78,6 +78,29 @@ class NutsBuffers(ctypes.Structure):
     ]
 
 
+class MultiView(ctypes.Structure):
+    _fields_ = [
+        ("position", c_void_p),
+        ("gradient", c_void_p),
+        ("logjoint", c_void_p),
+        ("step", c_void_p),
+        ("inverse_mass", c_void_p),
+        ("accept_prob", c_void_p),
+        ("tree_depth", c_void_p),
+        ("integration_steps", c_void_p),
+        ("divergent", c_void_p),
+        ("draws", c_void_p),
+        ("draw_accept", c_void_p),
+        ("draw_tree_depth", c_void_p),
+        ("draw_divergent", c_void_p),
+        ("iteration", c_void_p),
+        ("state_floats", c_int64),
+        ("total_chains", c_int64),
+        ("param_floats", c_int64),
+        ("draws_capacity", c_int32),
+    ]
+
+
 # (name, restype, argtypes) of every exported entry point, in header order.
 SIGNATURES = [
     ("ut_version", c_char_p, []),
@@ -127,6 +150,19 @@ SIGNATURES = [
     ("ut_surrogate_check", c_int32, [c_void_p, c_void_p]),
     ("ut_surrogate_hmc_iteration", c_int32,
      [c_void_p, c_void_p, POINTER(HmcBuffers), c_int32, c_uint32, c_float, c_void_p]),
+    ("ut_multi_create", c_int32,
+     [c_int32, POINTER(PlanDesc), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, POINTER(c_void_p)]),
+    ("ut_multi_destroy", c_int32, [c_void_p]),
+    ("ut_multi_layout", c_int32, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("ut_multi_class_info", c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("ut_multi_configure", c_int32, [c_void_p, c_int32, c_int32, c_int32]),
+    ("ut_multi_set_positions", c_int32, [c_void_p, c_void_p, c_void_p]),
+    ("ut_multi_begin", c_int32,
+     [c_void_p, c_int32, c_int32, c_uint32, c_float, c_float, c_float, c_void_p, c_int32]),
+    ("ut_multi_run", c_int32, [c_void_p, c_int32, c_int32, c_void_p]),
+    ("ut_multi_autotune", c_int32, [c_void_p, c_int32, c_void_p, c_void_p]),
+    ("ut_multi_split_rhat", c_int32, [c_void_p, c_int32, c_void_p, c_void_p]),
+    ("ut_multi_buffers", c_int32, [c_void_p, POINTER(MultiView)]),
 ]
 
 _lib = None

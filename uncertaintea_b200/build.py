@@ -2,8 +2,8 @@
 
 The C ABI and its kernels are compiled by nvcc for sm_100a only, from
 csrc/ut_api.cu, csrc/ut_noalloc.cu (the allocation-free entry point, whose
-kernels are private to its file) and csrc/ut_surrogate.cu (the learned
-gradient surrogate).  Run: python -m uncertaintea_b200.build [--force]
+kernels are private to its file), csrc/ut_surrogate.cu (the learned
+gradient surrogate) and csrc/ut_multi.cu (many models in one batched launch).  Run: python -m uncertaintea_b200.build [--force]
 """
 from __future__ import annotations
 
@@ -39,7 +39,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
         return LIB
     cmd = [nvcc()] + NVCC_FLAGS + ["-o", LIB + ".tmp", os.path.join(HERE, "csrc", "ut_api.cu"),
                                    os.path.join(HERE, "csrc", "ut_noalloc.cu"),
-                                   os.path.join(HERE, "csrc", "ut_surrogate.cu")]
+                                   os.path.join(HERE, "csrc", "ut_surrogate.cu"),
+                                   os.path.join(HERE, "csrc", "ut_multi.cu")]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     subprocess.run(cmd, check=True)

@@ -320,26 +320,41 @@ __device__ __forceinline__ bool is_turning_lr(const float (&Lq)[K], const float 
     return ld <= 0.0f || rd <= 0.0f;
 }
 
-template <int FAM, int K, int DMAX>
-__global__ void __launch_bounds__(128) nuts_warp_kernel(DevModel dm, NutsArgs a) {
-    extern __shared__ float smem[];
-    stage_model<FAM>(dm, smem);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int c = blockIdx.x * (blockDim.x >> 5) + warp;
-    if (c >= a.C) return;
-    float* qs = smem + dm.staged_floats + warp * dm.Ppad;
-    const int P = dm.P;
-    const uint32_t chain = (uint32_t)c, it = a.coord;
+// One chain's state and outputs for one persistent-NUTS iteration: pointers to
+// its position / gradient rows (P floats) and to its entry of each per-chain
+// array.
+struct NutsChainIO {
+    float* position;
+    float* gradient;
+    float* logjoint;
+    const float* inverse_mass;
+    float step;
+    float* accept_prob;
+    float* energy;
+    float* energy_error;
+    int32_t* tree_depth;
+    int32_t* integration_steps;
+    uint8_t* divergent;
+    uint8_t* moved;
+};
+
+// One persistent-NUTS iteration of one chain by one warp (persistent_nuts.jl:226-491).
+// eval(q, g) returns the logjoint at q and writes its gradient to g; `chain`
+// keys the chain's Philox streams, `it` is the iteration coordinate, ck the
+// chain's checkpoint stack ((max_depth + 1) x 2 x 32K floats).
+template <int K, class Eval>
+__device__ __forceinline__ void nuts_chain(const Eval& eval, int P, const NutsChainIO& io, uint32_t chain,
+                                           uint32_t it, int max_depth, float thr, float* ck) {
+    const int lane = threadIdx.x & 31;
     const int VS = 32 * K;
-    float* ck = a.ckpt + (size_t)c * (a.max_depth + 1) * 2 * VS;
 
     float q[K], g[K], p[K], im[K];
     float Lq[K], Lp[K], Lg[K], Rq[K], Rp[K], Rg[K], Sq[K], Sg[K], PPq[K], PPg[K], q0[K], g0[K];
-    load_vec(q, a.position + (size_t)c * P, P);
-    load_vec(g, a.gradient + (size_t)c * P, P);
-    load_vec(im, a.inverse_mass, P);
-    const float h = a.step[c];
-    const float lj0 = a.logjoint[c];
+    load_vec(q, io.position, P);
+    load_vec(g, io.gradient, P);
+    load_vec(im, io.inverse_mass, P);
+    const float h = io.step;
+    const float lj0 = *io.logjoint;
 
 #pragma unroll
     for (int k = 0; k < K; ++k) {
@@ -372,7 +387,7 @@ __global__ void __launch_bounds__(128) nuts_warp_kernel(DevModel dm, NutsArgs a)
             p[k] = fmaf(half, g[k], p[k]);
             q[k] = fmaf(hs, im[k] * p[k], q[k]);
         }
-        float lj1 = eval_lj<FAM, K, DMAX>(dm, q, g, qs, true);
+        float lj1 = eval(q, g);
         bool ok1 = isfinite(lj1) && own_finite(g, P);
         if (!ok1) {
             divergent = true;
@@ -391,7 +406,7 @@ __global__ void __launch_bounds__(128) nuts_warp_kernel(DevModel dm, NutsArgs a)
             float pe = kinetic(p, im) - lj1;
             float delta = pe - H0;
             isteps = 1;
-            if (!isfinite(delta) || delta > a.thr) {
+            if (!isfinite(delta) || delta > thr) {
                 divergent = true;
             } else {
                 accept_sum += fminf(1.0f, expf(fminf(0.0f, -delta)));
@@ -412,7 +427,7 @@ __global__ void __launch_bounds__(128) nuts_warp_kernel(DevModel dm, NutsArgs a)
     }
 
     // ---- doubling loop (persistent_nuts.jl:341-475) ----
-    while (depth < a.max_depth && !divergent && !turning) {
+    while (depth < max_depth && !divergent && !turning) {
         const int round = depth;
         float ud = rand_uniform(chain, it, kStreamDirection, (uint32_t)round);
         float dir = ud < 0.5f ? -1.0f : 1.0f;
@@ -438,7 +453,7 @@ __global__ void __launch_bounds__(128) nuts_warp_kernel(DevModel dm, NutsArgs a)
                 p[k] = fmaf(half, g[k], p[k]);
                 q[k] = fmaf(hs, im[k] * p[k], q[k]);
             }
-            float ljc = eval_lj<FAM, K, DMAX>(dm, q, g, qs, true);
+            float ljc = eval(q, g);
             if (!(isfinite(ljc) && own_finite(g, P))) { sub_div = true; break; }
 #pragma unroll
             for (int k = 0; k < K; ++k) p[k] = fmaf(half, g[k], p[k]);
@@ -446,7 +461,7 @@ __global__ void __launch_bounds__(128) nuts_warp_kernel(DevModel dm, NutsArgs a)
             sub_int += 1;
             float pe = kinetic(p, im) - ljc;
             float delta = pe - H0;
-            if (!isfinite(delta) || delta > a.thr) { sub_div = true; break; }
+            if (!isfinite(delta) || delta > thr) { sub_div = true; break; }
             sub_acc += fminf(1.0f, expf(fminf(0.0f, -delta)));
             sub_acc_n += 1;
             float cand = -pe;
@@ -536,20 +551,47 @@ __global__ void __launch_bounds__(128) nuts_warp_kernel(DevModel dm, NutsArgs a)
         if (lane + 32 * k < P && PPq[k] != q0[k]) moved_l = true;
     const bool moved = __any_sync(UT_FULL_MASK, moved_l);
     if (moved) {
-        store_vec(a.position + (size_t)c * P, PPq, P);
-        store_vec(a.gradient + (size_t)c * P, PPg, P);
+        store_vec(io.position, PPq, P);
+        store_vec(io.gradient, PPg, P);
     }
     if (lane == 0) {
-        if (moved) a.logjoint[c] = prop_lj;
-        a.moved[c] = moved ? 1 : 0;
-        a.accept_prob[c] = accept_count == 0 ? 0.0f : accept_sum / (float)accept_count;
-        a.energy[c] = prop_energy;
-        a.energy_error[c] = prop_error;
-        a.divergent[c] = divergent ? 1 : 0;
-        a.tree_depth[c] = depth;
-        a.integration_steps[c] = isteps;
+        if (moved) *io.logjoint = prop_lj;
+        *io.moved = moved ? 1 : 0;
+        *io.accept_prob = accept_count == 0 ? 0.0f : accept_sum / (float)accept_count;
+        *io.energy = prop_energy;
+        *io.energy_error = prop_error;
+        *io.divergent = divergent ? 1 : 0;
+        *io.tree_depth = depth;
+        *io.integration_steps = isteps;
     }
     (void)g0;
+}
+
+template <int FAM, int K, int DMAX>
+__global__ void __launch_bounds__(128) nuts_warp_kernel(DevModel dm, NutsArgs a) {
+    extern __shared__ float smem[];
+    stage_model<FAM>(dm, smem);
+    const int warp = threadIdx.x >> 5;
+    const int c = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (c >= a.C) return;
+    const int P = dm.P;
+    NutsChainIO io;
+    io.position = a.position + (size_t)c * P;
+    io.gradient = a.gradient + (size_t)c * P;
+    io.logjoint = a.logjoint + c;
+    io.inverse_mass = a.inverse_mass;
+    io.step = a.step[c];
+    io.accept_prob = a.accept_prob + c;
+    io.energy = a.energy + c;
+    io.energy_error = a.energy_error + c;
+    io.tree_depth = a.tree_depth + c;
+    io.integration_steps = a.integration_steps + c;
+    io.divergent = a.divergent + c;
+    io.moved = a.moved + c;
+    float* qs = smem + dm.staged_floats + warp * dm.Ppad;
+    float* ck = a.ckpt + (size_t)c * (a.max_depth + 1) * 2 * (32 * K);
+    auto eval = [&](const float (&qq)[K], float (&gg)[K]) { return eval_lj<FAM, K, DMAX>(dm, qq, gg, qs, true); };
+    nuts_chain<K>(eval, P, io, (uint32_t)c, a.coord, a.max_depth, a.thr, ck);
 }
 
 }  // namespace ut

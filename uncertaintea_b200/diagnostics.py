@@ -11,6 +11,13 @@ from __future__ import annotations
 import numpy as np
 from scipy.special import ndtri
 
+try:  # multi-threaded FFTs when scipy provides them
+    import scipy.fft as _fft
+    _FFT_KW = {"workers": -1}
+except ImportError:  # pragma: no cover
+    _fft = np.fft
+    _FFT_KW = {}
+
 
 def _split_chain_draws(draws: np.ndarray) -> np.ndarray:
     """(C, S) -> (2C, S//2): first and second half of every chain (diagnostics.jl:500-511)."""
@@ -51,8 +58,8 @@ def _split_ess_of(split: np.ndarray) -> float:
         return 0.0
     x = split - means[:, None]
     n = 1 << int(np.ceil(np.log2(2 * S)))
-    f = np.fft.rfft(x, n=n, axis=1)
-    acov = np.fft.irfft(f * np.conj(f), n=n, axis=1)[:, :S] / S
+    f = _fft.rfft(x, n=n, axis=1, **_FFT_KW)
+    acov = _fft.irfft((f * np.conj(f)).real, n=n, axis=1, **_FFT_KW)[:, :S] / S
     mean_acov = acov.mean(axis=0)
     rho = 1.0 - (W - mean_acov) / var_plus
     rho[0] = 1.0

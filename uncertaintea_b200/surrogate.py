@@ -185,9 +185,11 @@ class SurrogateChEESController:
     """Hooks the surrogate into batched_chees.
 
     Warmup: exact iterations; the (position, exact gradient) pairs of the
-    last iterations are copied into a device pair buffer, ``num_pairs`` rows
-    in total.  End of warmup: normalisation, ``train_epochs`` passes of Adam
-    over the pairs, then ``readapt_iterations`` surrogate iterations that
+    last iterations (at most the last 60% of warmup, so the initial transient
+    is left out) are copied into a device pair buffer, ``num_pairs`` rows at
+    most.  End of warmup: normalisation, Adam over the pairs
+    (max(``min_train_steps``, ``train_epochs`` passes) steps of ``batch``
+    rows), then ``readapt_iterations`` surrogate iterations that
     re-tune the step size by dual averaging (the surrogate's energy error
     differs from the exact one).  Sampling: surrogate iterations; when the
     mean accept probability over the last ``fallback_window`` iterations falls
@@ -196,11 +198,12 @@ class SurrogateChEESController:
     the surrogate is compared with the exact gradient at the current
     positions (one extra exact gradient evaluation)."""
 
-    def __init__(self, *, num_pairs=2 ** 20, train_epochs=8, batch=4096, learning_rate=2e-3,
+    def __init__(self, *, num_pairs=2 ** 20, train_epochs=8, min_train_steps=1000, batch=4096, learning_rate=2e-3,
                  final_learning_rate=5e-5, readapt_iterations=100, fallback_accept=0.2, fallback_window=20,
                  error_check_every=0, seed=0, surrogate=None, train=True):
         self.num_pairs = int(num_pairs)
         self.train_epochs = float(train_epochs)
+        self.min_train_steps = int(min_train_steps)
         self.batch = int(batch)
         self.learning_rate = float(learning_rate)
         self.final_learning_rate = float(final_learning_rate)
@@ -228,7 +231,7 @@ class SurrogateChEESController:
         elif self.surrogate.P != run.P:
             raise IndexError(f"surrogate has {self.surrogate.P} parameters, the model {run.P}")
         if self.do_train:
-            iters = max(1, min(num_warmup, math.ceil(self.num_pairs / run.C)))
+            iters = max(1, min(math.ceil(0.6 * num_warmup), math.ceil(self.num_pairs / run.C)))
             self.num_pairs = min(self.num_pairs, iters * run.C)
             self.record_from = num_warmup - iters + 1
             self.pairs_theta = torch.empty((self.num_pairs, run.P), dtype=torch.float32, device=run.device)
@@ -253,7 +256,7 @@ class SurrogateChEESController:
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             self.surrogate.fit_normalization(theta, grad)
-            steps = max(1, int(round(self.train_epochs * self.filled / self.batch)))
+            steps = max(self.min_train_steps, int(round(self.train_epochs * self.filled / self.batch)))
             losses = self.surrogate.train(theta, grad, steps=steps, batch=self.batch,
                                           learning_rate=self.learning_rate,
                                           final_learning_rate=self.final_learning_rate, seed=self.seed)
@@ -323,7 +326,8 @@ class SurrogateChEESController:
 
 
 def batched_chees_surrogate(model, args=(), constraints=None, *, num_chains, num_samples, num_warmup=500,
-                            num_pairs=2 ** 20, train_epochs=8, train_batch=4096, learning_rate=2e-3,
+                            num_pairs=2 ** 20, train_epochs=8, min_train_steps=1000, train_batch=4096,
+                            learning_rate=2e-3,
                             final_learning_rate=5e-5, readapt_iterations=100, fallback_accept=0.2,
                             fallback_window=20, error_check_every=0, surrogate=None, surrogate_seed=0, **kwargs):
     """batched_chees whose sampling trajectories are driven by a learned
@@ -335,7 +339,8 @@ def batched_chees_surrogate(model, args=(), constraints=None, *, num_chains, num
     if num_warmup < 1 and surrogate is None:
         raise ValueError("the surrogate is trained on warmup pairs: num_warmup must be >= 1 "
                          "(or pass a trained surrogate)")
-    ctl = SurrogateChEESController(num_pairs=num_pairs, train_epochs=train_epochs, batch=train_batch,
+    ctl = SurrogateChEESController(num_pairs=num_pairs, train_epochs=train_epochs,
+                                   min_train_steps=min_train_steps, batch=train_batch,
                                    learning_rate=learning_rate, final_learning_rate=final_learning_rate,
                                    readapt_iterations=readapt_iterations, fallback_accept=fallback_accept,
                                    fallback_window=fallback_window, error_check_every=error_check_every,
