@@ -369,11 +369,15 @@ int32_t ut_multi_configure(ut_multi* mm, int32_t klass, int32_t chains_per_block
 /* Copies state_floats device positions in and evaluates logjoint + gradient there. */
 int32_t ut_multi_set_positions(ut_multi* mm, const float* d_positions, void* stream);
 /* Starts a run: iteration counter 0, unit inverse masses, every step size
- * initial_step, dual averaging towards target_accept (pooled over each model's
- * chains), warmup_actions[i] for warmup iteration i (bit 0: add the positions
- * to the model's Welford window, bit 1: the window ends and sets the inverse
- * mass, bit 2: final step size), and room for draws_capacity sampling draws.
- * The Philox iteration coordinate of iteration i is seed + i. */
+ * initial_step, warmup_actions[i] for warmup iteration i (bit 0: add the
+ * model's non-divergent positions to its Welford window, bit 1: the window
+ * ends and sets the model's inverse mass, bit 2: final step sizes), and room
+ * for draws_capacity sampling draws.  Warmup adapts as the reference's default
+ * batched NUTS: every chain searches a reasonable step size at the first
+ * iteration and after every window (one momentum draw at Philox coordinate
+ * seed + 2^31 + iteration), then dual-averages it towards target_accept on its
+ * own accept statistic (0 when divergent).  The Philox iteration coordinate of
+ * iteration i is seed + i. */
 int32_t ut_multi_begin(ut_multi* mm, int32_t num_warmup, int32_t num_samples, uint32_t seed, float target_accept,
                        float initial_step, float divergence_threshold, const uint8_t* warmup_actions,
                        int32_t draws_capacity);

@@ -934,6 +934,7 @@ def batched_chees(model, args=(), constraints=None, *, num_chains, num_samples, 
         if warm and adapt_trajectory_length:
             initials.copy_(run.position)
         if _surrogate is not None:
+            L = _surrogate.cap_steps(L)
             grad_evals += _surrogate.iteration(run, L, it, divergence_threshold, warm,
                                                proposal if (warm and adapt_traj) else None,
                                                momentum if (warm and adapt_traj) else None)

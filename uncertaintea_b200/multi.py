@@ -4,10 +4,11 @@ sizes, priors and chain count, sampled together by batched persistent NUTS on
 one GPU.
 
 Per iteration the library launches one persistent-NUTS kernel per
-parameter-slot class (the classes run concurrently), then per-model warmup
-adaptation (dual averaging of the step size pooled over the model's chains,
-windowed diagonal mass) or draw recording, all on the device, replayed from a
-captured CUDA graph.  Chains per CTA and shared-memory staging of each
+parameter-slot class (the classes run concurrently), then the warmup
+adaptation of the reference's default batched NUTS (a dual-averaged step per
+chain after a reasonable-step search, a pooled windowed diagonal mass per
+model) or draw recording, all on the device, replayed from a captured CUDA
+graph.  Chains per CTA and shared-memory staging of each
 class's model data come from the library's autotuner, which times every
 candidate on the same iteration.  The host only checks convergence at
 checkpoints: per-model split R-hat on the device, from which the time each

@@ -177,7 +177,7 @@ class SurrogateReport:
     relative_error_checks: list = field(default_factory=list)
     surrogate_iterations: int = 0
     exact_iterations_after_warmup: int = 0
-    fallback_at: int | None = None
+    fallback_at: int | str | None = None  # sampling iteration, "training" or "readapt"
     readapted_step_size: float = float("nan")
 
 
@@ -196,11 +196,15 @@ class SurrogateChEESController:
     below ``fallback_accept``, the exact gradient is recomputed and every
     later iteration is exact.  Every ``error_check_every`` sampling iterations
     the surrogate is compared with the exact gradient at the current
-    positions (one extra exact gradient evaluation)."""
+    positions (one extra exact gradient evaluation).  A surrogate whose
+    relative error after training is not below ``max_relative_error`` is not
+    used, and neither is one whose step-size re-tuning fails (accept rate
+    below ``fallback_accept`` over ``fallback_window`` iterations, or the step
+    shrinking 64-fold): the run then continues with exact gradients."""
 
-    def __init__(self, *, num_pairs=2 ** 20, train_epochs=8, min_train_steps=1000, batch=4096, learning_rate=2e-3,
-                 final_learning_rate=5e-5, readapt_iterations=100, fallback_accept=0.2, fallback_window=20,
-                 error_check_every=0, seed=0, surrogate=None, train=True):
+    def __init__(self, *, num_pairs=2 ** 20, train_epochs=8, min_train_steps=10000, batch=4096, learning_rate=2e-3,
+                 final_learning_rate=1e-5, readapt_iterations=100, fallback_accept=0.2, fallback_window=20,
+                 error_check_every=0, seed=0, surrogate=None, train=True, max_relative_error=0.5):
         self.num_pairs = int(num_pairs)
         self.train_epochs = float(train_epochs)
         self.min_train_steps = int(min_train_steps)
@@ -222,6 +226,8 @@ class SurrogateChEESController:
         self.active = False
         self.fallen_back = False
         self.recent_accept = []
+        self.max_steps = 1000
+        self.max_relative_error = float(max_relative_error)
 
     # ---- warmup ----
     def setup(self, run, num_warmup):
@@ -267,24 +273,45 @@ class SurrogateChEESController:
             rep.final_loss = float(losses[-min(steps, 32):].mean())
             self.pairs_theta = self.pairs_grad = None  # release the pair buffer
         rep.relative_error_after_training = self.surrogate.relative_error(run.position, run.gradient)
+        self.max_steps = int(traj.max_leapfrog_steps)
+        if not rep.relative_error_after_training < self.max_relative_error:
+            self._fall_back(run, "training")  # too inaccurate to drive trajectories
+            return 0
         self.active = True
-        # step-size re-tuning on surrogate dynamics (trajectory length fixed)
-        from .inference import DualAveraging
+        # step-size re-tuning on surrogate dynamics (trajectory length fixed);
+        # given up (exact gradients from then on) when the surrogate's accept
+        # rate stays below fallback_accept or the step collapses
+        from .inference import DualAveraging, _chees_harmonic_mean_accept
         dual = DualAveraging(driver.step_size, driver.target_accept)
-        eps = driver.step_size
+        eps0 = eps = driver.step_size
+        accepts = []
         for k in range(self.readapt_iterations):
             it = first_iteration + k
             run.set_mass_and_step(driver.inverse_mass_matrix, eps)
-            L = steps_fn(jitter_fn(it), traj.trajectory_length, eps)
+            L = self.cap_steps(steps_fn(jitter_fn(it), traj.trajectory_length, eps))
             self._surrogate_iteration(run, L, it, thr)
             ap = run.accept_prob.double().cpu().numpy()
             div = run.divergent.cpu().numpy().astype(bool)
-            from .inference import _chees_harmonic_mean_accept
+            accepts.append(float(ap.mean()))
             eps = float(dual.update(_chees_harmonic_mean_accept(ap, div)))
+            window = accepts[-self.fallback_window:]
+            if (len(window) == self.fallback_window and np.mean(window) < self.fallback_accept) or eps < eps0 / 64:
+                self._fall_back(run, "readapt")
+                return k + 1
         if self.readapt_iterations > 0:
             driver.step_size = float(dual.final())
         rep.readapted_step_size = driver.step_size
         return self.readapt_iterations
+
+    def cap_steps(self, L: int) -> int:
+        """Leapfrog steps of a surrogate trajectory, at most max_leapfrog_steps."""
+        return int(min(L, self.max_steps)) if self.active and not self.fallen_back else int(L)
+
+    def _fall_back(self, run, where):
+        self.fallen_back = True
+        self.report.fallback_at = where
+        # exact state for the exact iterations that follow
+        run.ws.logjoint_gradient_device(run.position, run.logjoint, run.gradient)
 
     # ---- iterations ----
     def _surrogate_iteration(self, run, L, it, thr, proposal=None, momentum=None):
@@ -312,10 +339,7 @@ class SurrogateChEESController:
             cost += run.C
         if (len(self.recent_accept) == self.fallback_window
                 and float(np.mean(self.recent_accept)) < self.fallback_accept):
-            self.fallen_back = True
-            self.report.fallback_at = it
-            # exact state for the exact iterations that follow
-            run.ws.logjoint_gradient_device(run.position, run.logjoint, run.gradient)
+            self._fall_back(run, it)
             cost += run.C
         return cost
 
@@ -326,10 +350,11 @@ class SurrogateChEESController:
 
 
 def batched_chees_surrogate(model, args=(), constraints=None, *, num_chains, num_samples, num_warmup=500,
-                            num_pairs=2 ** 20, train_epochs=8, min_train_steps=1000, train_batch=4096,
+                            num_pairs=2 ** 20, train_epochs=8, min_train_steps=10000, train_batch=4096,
                             learning_rate=2e-3,
-                            final_learning_rate=5e-5, readapt_iterations=100, fallback_accept=0.2,
-                            fallback_window=20, error_check_every=0, surrogate=None, surrogate_seed=0, **kwargs):
+                            final_learning_rate=1e-5, readapt_iterations=100, fallback_accept=0.2,
+                            fallback_window=20, error_check_every=0, max_relative_error=0.5, surrogate=None,
+                            surrogate_seed=0, **kwargs):
     """batched_chees whose sampling trajectories are driven by a learned
     gradient surrogate (exact logjoint in the accept).  Extra keyword
     arguments are those of batched_chees.  The returned chains carry a
@@ -344,7 +369,8 @@ def batched_chees_surrogate(model, args=(), constraints=None, *, num_chains, num
                                    learning_rate=learning_rate, final_learning_rate=final_learning_rate,
                                    readapt_iterations=readapt_iterations, fallback_accept=fallback_accept,
                                    fallback_window=fallback_window, error_check_every=error_check_every,
-                                   seed=surrogate_seed, surrogate=surrogate, train=surrogate is None)
+                                   seed=surrogate_seed, surrogate=surrogate, train=surrogate is None,
+                                   max_relative_error=max_relative_error)
     chains = batched_chees(model, args, constraints, num_chains=num_chains, num_samples=num_samples,
                            num_warmup=num_warmup, _surrogate=ctl, **kwargs)
     chains.surrogate = ctl.report
