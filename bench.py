@@ -9,7 +9,9 @@ shipped).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-At N=1 the line also carries `surrogate_chees`: the learned-gradient-surrogate
+At N=1 the line also carries `hbm_sweep`: the same design at 1, 4, 8 and 16
+chains, where an evaluation is bound by reading X from HBM (achieved GB/s
+against the measured HBM bandwidth), `surrogate_chees`: the learned-gradient-surrogate
 workload on the same model (min ESS/s of surrogate-driven ChEES-HMC vs plain
 ChEES-HMC, both at R-hat < 1.01; skipped with --no-surrogate), and
 `uneven_batch`: 512 hierarchical models of uneven sizes in one batched
@@ -241,7 +243,9 @@ def run_b200(args):
         cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
     launches = int(ws.launches_per_gradient()) * args.steps if hasattr(ws, "launches_per_gradient") else 2 * args.steps
     ws.close()
-    sur = uneven = None
+    sur = uneven = sweep = None
+    if rank == 0 and world == 1:
+        sweep = hbm_sweep()
     if rank == 0 and world == 1 and not args.no_surrogate:
         sur = surrogate_comparison()
     if rank == 0 and world == 1 and not args.no_uneven:
@@ -256,6 +260,8 @@ def run_b200(args):
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": N_CHAINS * N_COEF * 4,
                         "d2h_bytes_per_step": N_CHAINS * (N_COEF + 1) * 4},
                 "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches}
+        if sweep is not None:
+            line["hbm_sweep"] = sweep
         if sur is not None:
             line["surrogate_chees"] = sur
         if uneven is not None:
@@ -263,6 +269,52 @@ def run_b200(args):
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
+
+
+def hbm_sweep(chain_counts=(1, 4, 8, 16), steps=20, warmup=5):
+    """Few-chain logjoint + gradient on the same 100000 x 100 design, where one
+    evaluation must read all of X from HBM: achieved bytes per second against the
+    measured HBM copy bandwidth.  Algorithmic bytes per evaluation = X (N*F*4) +
+    y (N*4) + parameters in and gradients out (2*C*F*4) + values out (C*4).  L2 is
+    flushed (256 MB write) before every timed evaluation; per-step CUDA events."""
+    import torch
+    from uncertaintea_b200.device import DeviceBatchedWorkspace
+    model, X, y, params = _data()
+    hbm, _, kind = _peaks()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    out = []
+    for C in chain_counts:
+        ws = DeviceBatchedWorkspace(model, C, args=(X,), constraints={"y": y})
+        qd = torch.from_numpy(params[:C].copy()).cuda()
+        totals = torch.empty(C, device="cuda")
+        grads = torch.empty_like(qd)
+        row = {"chains": C, "kernel_path": ws.kernel_path()}
+        for name, grad in (("logjoint_gradient", True), ("logjoint", False)):
+            def step():
+                if grad:
+                    ws.logjoint_gradient_device(qd, totals, grads)
+                else:
+                    ws.logjoint_device(qd, totals)
+            for _ in range(max(warmup, 3)):
+                flush.fill_(1.0)
+                step()
+            evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+            for a, b in evs:
+                flush.fill_(1.0)
+                a.record(stream)
+                step()
+                b.record(stream)
+            torch.cuda.synchronize()
+            ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
+            nbytes = N_OBS * N_COEF * 4 + N_OBS * 4 + (2 if grad else 1) * C * N_COEF * 4 + C * 4
+            gbs = nbytes / (ms / 1000.0) / 1e9
+            row[name] = {"ms": ms, "bytes": nbytes, "GB/s": gbs, "frac": gbs / hbm}
+        out.append(row)
+        ws.close()
+    return {"metric": "few-chain logjoint(+gradient) HBM roofline", "peak_GB/s": hbm,
+            "peak_source": f"{kind} HBM copy bandwidth", "l2": "flushed before every timed evaluation",
+            "rows": out}
 
 
 def surrogate_comparison(num_chains=4096, num_warmup=500, num_samples=500):

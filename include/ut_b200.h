@@ -108,7 +108,9 @@ int32_t ut_workspace_destroy(ut_workspace* ws);
 int32_t ut_workspace_info(const ut_workspace* ws, int32_t* num_params, int32_t* batch_size);
 /* Which kernel family evaluates this workspace's density: 1 = one warp per
  * chain (observation data staged in shared memory), 2 = CUDA-core
- * observation-tiled GEMM path, 3 = tensor-core (tcgen05, 3xTF32) path. */
+ * observation-tiled GEMM path, 3 = tensor-core (tcgen05, 3xTF32) path,
+ * 4 = HBM-streaming path for a few chains (C <= 16, GLM with P % 4 == 0 and
+ * P <= 128). */
 int32_t ut_workspace_path(const ut_workspace* ws);
 /* Synchronises the workspace's work and reports the sticky device error word:
  * UT_ERR_DEVICE_TIMEOUT when a bounded in-kernel wait gave up since the last

@@ -404,3 +404,42 @@ def test_tensor_core_path_vs_cuda_core_and_oracle(lib, N, D, C, intercept, monke
     assert _lj_err(t1, t2.astype(np.float64)) <= 2e-5
     ws_tc.close()
     ws_cc.close()
+
+
+@pytest.mark.parametrize("N,D,C,intercept", [
+    (100000, 100, 1, False),      # config-3 design, one chain
+    (100000, 100, 16, False),     # config-3 design, 16 chains
+    (5003, 99, 8, True),          # F = 100, ragged last chunk (5003 = 78 x 64 + 11)
+    (1000, 63, 3, True),          # F = 64, chains padded to 4
+    (130, 35, 5, True),           # F = 36, three chunks
+])
+def test_streaming_path_vs_oracle_and_tiled(lib, N, D, C, intercept, monkeypatch):
+    """The HBM-streaming kernel for a few chains against the FP64 oracle (same
+    tolerances as the other density tests) and the CUDA-core tiled kernel."""
+    m, args, cons, q = _glm_case(N, D, C, intercept, 33, 1.0 / np.sqrt(D))
+    ws = _ws(m, args, cons, C)
+    assert ws.kernel_path() == "stream"
+    monkeypatch.setenv("UT_DISABLE_STREAM_KERNEL", "1")
+    ws_t = _ws(m, args, cons, C)
+    monkeypatch.delenv("UT_DISABLE_STREAM_KERNEL")
+    assert ws_t.kernel_path() != "stream"
+    qd = torch.from_numpy(q).cuda()
+    t1, g1 = ws.logjoint_gradient_device(qd)
+    t0 = ws.logjoint_device(qd)
+    t2, g2 = ws_t.logjoint_gradient_device(qd)
+    torch.cuda.synchronize()
+    t1, g1, t0, t2, g2 = (x.cpu().numpy() for x in (t1, g1, t0, t2, g2))
+    t64, g64 = oracle.OracleModel(ws.lowered).logjoint_gradient_f64(q.astype(np.float64))
+    assert _lj_err(t1, t64) <= 1e-5 and _lj_err(t0, t64) <= 1e-5
+    assert _grad_err(g1, g64) <= 1e-5
+    np.testing.assert_allclose(t1, t2, rtol=2e-6)
+    np.testing.assert_allclose(g1, g2, rtol=1e-4, atol=1e-4 * np.abs(g64).max())
+    ws.close()
+    ws_t.close()
+
+
+def test_streaming_path_needs_feature_count_multiple_of_four(lib):
+    m, args, cons, q = _glm_case(2000, 101, 4, False, 34, 0.1)
+    ws = _ws(m, args, cons, 4)
+    assert ws.kernel_path() != "stream"
+    ws.close()

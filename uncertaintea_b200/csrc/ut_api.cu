@@ -3,6 +3,7 @@
 // kernel.  No CPU fallback: without a CUDA device every compute entry point
 // returns UT_ERR_NO_DEVICE.
 #include <cstdarg>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -14,6 +15,7 @@
 #include "ut_glm_tiled.cuh"
 #include "ut_lf_batched.cuh"
 #include "ut_tc_glm.cuh"
+#include "ut_glm_stream.cuh"
 
 using namespace ut;
 
@@ -81,6 +83,11 @@ struct ut_workspace {
     float* d_part_g = nullptr;
     // tensor-core path (GLM, large N)
     TcGlmPlan tc;
+    // streaming path (GLM, few chains)
+    bool streaming = false;
+    int stream_cb = 16, stream_splits = 0, stream_warps = 8;
+    float* d_spart_ll = nullptr;
+    float* d_spart_g = nullptr;
     // batched leapfrog scratch
     LfScratch lf = {};
     // NUTS checkpoint scratch
@@ -255,8 +262,37 @@ int32_t launch_tiled_t(ut_workspace* ws, const float* params, float* totals, flo
     return UT_OK;
 }
 
+int32_t launch_stream(ut_workspace* ws, const float* params, float* totals, float* grads, cudaStream_t st) {
+    GlmStreamArgs a;
+    a.Xa = ws->d_Xa; a.y = ws->d_y; a.params = params; a.part_ll = ws->d_spart_ll; a.part_g = ws->d_spart_g;
+    a.N = ws->N; a.F = ws->P; a.C = ws->C;
+    const size_t smem = glm_stream_smem(ws->stream_cb, ws->P, ws->stream_warps);
+#define STREAM_CASE(CBV)                                                                            \
+    case CBV: {                                                                                     \
+        auto kern = grads ? glm_stream_kernel<CBV, true> : glm_stream_kernel<CBV, false>;          \
+        UT_CUDA(launch_dyn(kern, 0, 0, smem, st));                                                  \
+        kern<<<ws->stream_splits, 32 * ws->stream_warps, smem, st>>>(a);                            \
+    } break;
+    switch (ws->stream_cb) {
+        STREAM_CASE(1) STREAM_CASE(2) STREAM_CASE(4) STREAM_CASE(8)
+        default: STREAM_CASE(16)
+    }
+#undef STREAM_CASE
+    UT_LAUNCHED();
+    GlmStreamFoldArgs r;
+    r.params = params; r.part_ll = ws->d_spart_ll; r.part_g = grads ? ws->d_spart_g : nullptr;
+    r.totals = totals; r.grads = grads;
+    r.S = ws->stream_splits; r.C = ws->C; r.F = ws->P; r.off = ws->plan.has_intercept;
+    r.icpt_mu = (float)ws->plan.intercept_mu; r.icpt_sigma = (float)ws->plan.intercept_sigma;
+    r.coef_mu = (float)ws->plan.coef_mu; r.coef_sigma = (float)ws->plan.coef_sigma;
+    glm_stream_fold_kernel<<<ws->C, 1024, 0, st>>>(r);
+    UT_LAUNCHED();
+    return UT_OK;
+}
+
 // Batched density on device buffers, whichever path the workspace uses.
 int32_t density(ut_workspace* ws, const float* params, float* totals, float* grads, cudaStream_t st) {
+    if (ws->streaming) return launch_stream(ws, params, totals, grads, st);
     if (ws->path == kPathWarp) {
         UT_DISPATCH_WARP(ws, LAUNCH_DENSITY, ws, params, totals, grads, st);
         UT_LAUNCHED();
@@ -438,9 +474,19 @@ int32_t ut_workspace_create(const ut_plan_desc* plan, const float* observed, int
             for (int v : fpts) if (need <= v) { ws->fpt = v; break; }
             if ((rc = dalloc(ws, &ws->d_part_ll, (size_t)ws->splits * ws->C))) return bail(rc);
             if ((rc = dalloc(ws, &ws->d_part_g, (size_t)ws->splits * ws->C * F))) return bail(rc);
-            if ((rc = tc_glm_setup(ws->tc, ws->d_Xa, ws->d_y, N, F, ws->C, off, (float)plan->intercept_mu,
-                                   (float)plan->intercept_sigma, (float)plan->coef_mu, (float)plan->coef_sigma,
-                                   dev_sms, &ws->allocations))) {
+            // few chains: the HBM-streaming kernel (UT_DISABLE_STREAM_KERNEL=1 keeps the tiled one)
+            const char* no_stream = getenv("UT_DISABLE_STREAM_KERNEL");
+            if (ws->C <= kStreamMaxC && F % 4 == 0 && F <= kStreamMaxF && !(no_stream && no_stream[0] == '1')) {
+                ws->streaming = true;
+                const int C = ws->C;
+                ws->stream_cb = C <= 1 ? 1 : C <= 2 ? 2 : C <= 4 ? 4 : C <= 8 ? 8 : 16;
+                ws->stream_warps = glm_stream_warps(ws->stream_cb, F);
+                ws->stream_splits = dev_sms;  // one CTA per SM; its warps take chunks round-robin
+                if ((rc = dalloc(ws, &ws->d_spart_ll, (size_t)ws->stream_splits * C))) return bail(rc);
+                if ((rc = dalloc(ws, &ws->d_spart_g, (size_t)ws->stream_splits * C * F))) return bail(rc);
+            } else if ((rc = tc_glm_setup(ws->tc, ws->d_Xa, ws->d_y, N, F, ws->C, off, (float)plan->intercept_mu,
+                                          (float)plan->intercept_sigma, (float)plan->coef_mu,
+                                          (float)plan->coef_sigma, dev_sms, &ws->allocations))) {
                 return bail(fail(UT_ERR_CUDA, "tensor-core GLM setup failed: %s", tc_glm_last_error()));
             }
         }
@@ -488,6 +534,7 @@ int32_t ut_workspace_info(const ut_workspace* ws, int32_t* num_params, int32_t* 
 int32_t ut_workspace_path(const ut_workspace* ws) {
     if (!ws) return 0;
     if (ws->path == kPathWarp) return 1;
+    if (ws->streaming) return 4;
     return ws->tc.enabled ? 3 : 2;
 }
 

@@ -106,14 +106,15 @@ class DeviceBatchedWorkspace:
 
     def kernel_path(self) -> str:
         """'warp' (one warp per chain), 'tiled' (CUDA-core GEMM tiles) or 'tensor_core' (tcgen05 3xTF32)."""
-        return {1: "warp", 2: "tiled", 3: "tensor_core"}.get(self.lib.ut_workspace_path(self.handle), "unknown")
+        return {1: "warp", 2: "tiled", 3: "tensor_core", 4: "stream"}.get(self.lib.ut_workspace_path(self.handle),
+                                                                             "unknown")
 
     def tensor_core_path(self) -> bool:
         return self.kernel_path() == "tensor_core"
 
     def launches_per_gradient(self) -> int:
         """Kernels one logjoint+gradient call launches (the bench's launch count)."""
-        return {"warp": 1, "tiled": 2, "tensor_core": 3}[self.kernel_path()]
+        return {"warp": 1, "tiled": 2, "tensor_core": 3, "stream": 2}[self.kernel_path()]
 
     def check(self):
         """Synchronise and raise if a bounded in-kernel wait gave up."""
