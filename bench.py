@@ -377,13 +377,15 @@ def uneven_batch(num_models=512, chains=64, num_warmup=500, num_samples=500):
     models = uneven_models(num_models)
     res = batched_nuts_multi(models, chains_per_model=chains, num_warmup=num_warmup, num_samples=num_samples,
                              rng=1, rhat_check_every=50)
-    p50, p99 = res.time_to_rhat_quantiles()
-    s50, s99 = res.time_to_rhat_quantiles(from_sampling=True)
+    fin = lambda v: v if np.isfinite(v) else None  # noqa: E731  (null: not reached within the run)
+    p50, p99 = (fin(v) for v in res.time_to_rhat_quantiles())
+    s50, s99 = (fin(v) for v in res.time_to_rhat_quantiles(from_sampling=True))
     cls = res.classes
     out = {"metric": "aggregate min-ESS/s; per-model time to R-hat<1.01 (p50/p99 over models)",
            "unit": "effective samples/s; s", "aggregate_ess_per_s": res.aggregate_ess_per_second,
            "time_to_rhat_p50_s": p50, "time_to_rhat_p99_s": p99,
            "sampling_time_to_rhat_p50_s": s50, "sampling_time_to_rhat_p99_s": s99,
+           "time_to_rhat_note": "null = that share of models did not reach R-hat < 1.01 within the run",
            "converged_fraction": res.converged_fraction, "median_model_min_ess": float(np.median(res.min_ess)),
            "warmup_s": res.warmup_seconds, "sampling_s": res.sampling_seconds,
            "ms_per_iteration": 1000.0 * res.sampling_seconds / num_samples,
