@@ -11,7 +11,9 @@ shipped).
 
 At N=1 the line also carries `hbm_sweep`: the same design at 1, 4, 8 and 16
 chains, where an evaluation is bound by reading X from HBM (achieved GB/s
-against the measured HBM bandwidth), `surrogate_chees`: the learned-gradient-surrogate
+against the measured HBM bandwidth), `samplers`: the config-1 HMC and config-2
+persistent-NUTS runs (min ESS/s, R-hat, gradient evaluations/s; skipped with
+--no-samplers), `surrogate_chees`: the learned-gradient-surrogate
 workload on the same model (min ESS/s of surrogate-driven ChEES-HMC vs plain
 ChEES-HMC, both at R-hat < 1.01; skipped with --no-surrogate), and
 `uneven_batch`: 512 hierarchical models of uneven sizes in one batched
@@ -243,9 +245,11 @@ def run_b200(args):
         cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
     launches = int(ws.launches_per_gradient()) * args.steps if hasattr(ws, "launches_per_gradient") else 2 * args.steps
     ws.close()
-    sur = uneven = sweep = None
+    sur = uneven = sweep = samplers = None
     if rank == 0 and world == 1:
         sweep = hbm_sweep()
+        if not args.no_samplers:
+            samplers = sampler_configs()
     if rank == 0 and world == 1 and not args.no_surrogate:
         sur = surrogate_comparison()
     if rank == 0 and world == 1 and not args.no_uneven:
@@ -262,6 +266,8 @@ def run_b200(args):
                 "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches}
         if sweep is not None:
             line["hbm_sweep"] = sweep
+        if samplers is not None:
+            line["samplers"] = samplers
         if sur is not None:
             line["surrogate_chees"] = sur
         if uneven is not None:
@@ -315,6 +321,35 @@ def hbm_sweep(chain_counts=(1, 4, 8, 16), steps=20, warmup=5):
     return {"metric": "few-chain logjoint(+gradient) HBM roofline", "peak_GB/s": hbm,
             "peak_source": f"{kind} HBM copy bandwidth", "l2": "flushed before every timed evaluation",
             "rows": out}
+
+
+def sampler_configs():
+    """The two sampler workloads of the small models, timed end to end: config 1
+    (batched HMC on the 1000 x 10 logistic regression, 256 chains, 8 leapfrog
+    steps, step 0.05 without step adaptation, 1000 warmup + 1000 draws, seed 1) and
+    config 2 (batched persistent NUTS on the non-centred hierarchical model with
+    J = 64 groups x 20 observations, sigma_j ~ U(0.5, 2), y from the prior at seed 7;
+    4096 chains, max tree depth 10, 1000 warmup + 1000 draws).  Min bulk ESS over
+    parameters per second of sampling, max split R-hat, gradient evaluations/s."""
+    from uncertaintea_b200 import (BernoulliLogitGLM, HierarchicalNormalNoncentered, batched_hmc, batched_nuts, ess,
+                                   hierarchical_data, logistic_regression_data, rhat)
+    out = {}
+    X, y, _ = logistic_regression_data(1000, 10, seed=1)
+    c1 = batched_hmc(BernoulliLogitGLM(10), (X,), {"y": y}, num_chains=256, num_samples=1000, num_warmup=1000,
+                     step_size=0.05, num_leapfrog_steps=8, adapt_step_size=False, rng=1)
+    yh, sig, sizes, _ = hierarchical_data(64, 20, 7)
+    c2 = batched_nuts(HierarchicalNormalNoncentered(64), (sig, sizes), {"y": yh}, num_chains=4096, num_samples=1000,
+                      num_warmup=1000, max_tree_depth=10, rng=7)
+    for name, ch, cfg in (("config1_hmc", c1, "256 chains, L=8, step 0.05, 1000+1000, GLM 1000x10"),
+                          ("config2_nuts", c2, "4096 chains, depth 10, 1000+1000, hierarchical J=64 x 20")):
+        e, r = ess(ch, space="unconstrained"), rhat(ch, space="unconstrained")
+        total_s = ch.warmup_seconds + ch.sampling_seconds
+        out[name] = {"min_ess_per_s": float(np.min(e) / ch.sampling_seconds), "min_ess": float(np.min(e)),
+                     "max_rhat": float(np.max(r)), "warmup_s": ch.warmup_seconds, "sampling_s": ch.sampling_seconds,
+                     "grad_evals_per_s": ch.gradient_evaluations / total_s, "mean_accept": float(ch.accept_prob.mean()),
+                     "config": cfg}
+    out["config2_nuts"]["mean_tree_depth"] = float(c2.tree_depth.mean())
+    return out
 
 
 def surrogate_comparison(num_chains=4096, num_warmup=500, num_samples=500):
@@ -428,6 +463,8 @@ def main():
     ap.add_argument("--kernel-only", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true",
                     help="skip the learned-surrogate ChEES comparison (about a minute) in the output line")
+    ap.add_argument("--no-samplers", action="store_true",
+                    help="skip the config-1 HMC and config-2 NUTS sampler runs in the output line")
     ap.add_argument("--no-uneven", action="store_true",
                     help="skip the uneven-batch run (512 hierarchical models, about two minutes)")
     args = ap.parse_args()
