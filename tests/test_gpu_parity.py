@@ -443,3 +443,69 @@ def test_streaming_path_needs_feature_count_multiple_of_four(lib):
     ws = _ws(m, args, cons, 4)
     assert ws.kernel_path() != "stream"
     ws.close()
+
+
+
+def _nuts_call(fn, ws, qd, g, t, im, step, depth, coord):
+    C = qd.shape[0]
+    f = lambda dt=torch.float32: torch.zeros(C, dtype=dt, device="cuda")  # noqa: E731
+    o = {"accept_prob": f(), "energy": f(), "energy_error": f(), "tree_depth": f(torch.int32),
+         "integration_steps": f(torch.int32), "divergent": f(torch.uint8), "moved": f(torch.uint8)}
+    imd = torch.from_numpy(im.astype(np.float32)).cuda()
+    sd = torch.from_numpy(step.astype(np.float32)).cuda()
+    buf = nat.NutsBuffers(nat.ptr(qd), nat.ptr(g), nat.ptr(t), nat.ptr(imd), nat.ptr(sd), nat.ptr(o["accept_prob"]),
+                          nat.ptr(o["energy"]), nat.ptr(o["energy_error"]), nat.ptr(o["tree_depth"]),
+                          nat.ptr(o["integration_steps"]), nat.ptr(o["divergent"]), nat.ptr(o["moved"]))
+    nat.check(fn(ws.handle, ctypes.byref(buf), depth, 1000.0, coord, None))
+    torch.cuda.synchronize()
+    res = {k: v.cpu().numpy() for k, v in o.items()}
+    res["position"], res["gradient"], res["logjoint"] = qd.cpu().numpy(), g.cpu().numpy(), t.cpu().numpy()
+    return res
+
+
+@pytest.mark.parametrize("case", ["glm", "hier"])
+def test_lockstep_nuts_matches_persistent_bitwise(lib, case):
+    """Where both strategies apply (a per-chain evaluator), the lockstep tree and
+    the persistent tree are the same computation: identical states and outputs."""
+    if case == "glm":
+        m, args, cons, q = _glm_case(1000, 10, 96, False, 1)
+        q *= 0.3
+        step = 0.08
+    else:
+        y, sig, sizes, _ = hierarchical_data(64, 20, 7)
+        m, args, cons = HierarchicalNormalNoncentered(64), (sig, sizes), {"y": y}
+        q = (np.random.default_rng(8).standard_normal((64, 66)) * 0.5).astype(np.float32)
+        step = 0.05
+    C, P = q.shape
+    ws = _ws(m, args, cons, C)
+    im, steps = np.linspace(0.7, 1.3, P), np.full(C, step) * np.linspace(0.9, 1.1, C)
+    outs = []
+    for fn in (lib.ut_persistent_nuts_iteration, lib.ut_lockstep_nuts_iteration):
+        qd, g, t = _state(ws, q)
+        outs.append(_nuts_call(fn, ws, qd, g, t, im, steps, 8, 515))
+    for k in outs[0]:
+        assert np.array_equal(outs[0][k], outs[1][k]), k
+    assert outs[0]["tree_depth"].max() >= 3
+    ws.close()
+
+
+def test_lockstep_nuts_on_tensor_core_path_vs_oracle(lib):
+    """Lockstep NUTS over the tensor-core batched gradient against the oracle's
+    NUTS (same Philox streams); the gradients differ in the last bits, so the
+    trees agree for most chains."""
+    m, args, cons, q = _glm_case(20000, 100, 128, False, 7, 0.1)
+    X, y = args[0], cons["y"]
+    mode = _glm_mode(X, y)
+    q = (mode + 0.02 * np.random.default_rng(9).standard_normal((128, 100))).astype(np.float32)
+    ws = _ws(m, args, cons, 128)
+    assert ws.kernel_path() == "tensor_core"
+    qd, g, t = _state(ws, q)
+    qo, go, to = qd.cpu().numpy().copy(), g.cpu().numpy().copy(), t.cpu().numpy().copy()
+    im, steps = np.ones(100), np.full(128, 0.02)
+    gpu = _nuts_call(lib.ut_lockstep_nuts_iteration, ws, qd, g, t, im, steps, 6, 77)
+    ref = oracle.OracleModel(ws.lowered).nuts_iteration(qo, go, to, im, steps, 6, 77)
+    same = (gpu["tree_depth"] == ref["tree_depth"]) & (gpu["integration_steps"] == ref["integration_steps"]) & \
+        (gpu["moved"] == ref["moved"])
+    assert same.mean() >= 0.9, same.mean()
+    np.testing.assert_allclose(gpu["position"][same], qo[same], rtol=1e-3, atol=1e-3)
+    ws.close()

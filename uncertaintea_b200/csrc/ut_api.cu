@@ -16,6 +16,7 @@
 #include "ut_lf_batched.cuh"
 #include "ut_tc_glm.cuh"
 #include "ut_glm_stream.cuh"
+#include "ut_nuts_lockstep.cuh"
 
 using namespace ut;
 
@@ -93,6 +94,19 @@ struct ut_workspace {
     // NUTS checkpoint scratch
     float* d_ckpt = nullptr;
     int ckpt_depth = -1;
+    // lockstep NUTS state machine
+    float* ls_vec = nullptr;
+    float* ls_f = nullptr;
+    int32_t* ls_i = nullptr;
+    float* ls_ckpt = nullptr;
+    int32_t* ls_active = nullptr;  // live-chain count (device)
+    int32_t* h_active = nullptr;   // pinned host copy of the live-chain count
+    uint8_t* ls_act = nullptr;     // per-chain live flags
+    int32_t* ls_idx = nullptr;     // compacted live chains
+    float* ls_cq = nullptr;        // compacted positions / gradients / logjoints
+    float* ls_cg = nullptr;
+    float* ls_clj = nullptr;
+    int ls_depth = -1;
     // ChEES scratch
     uint8_t* d_flags = nullptr;
     double* d_means = nullptr;
@@ -518,6 +532,7 @@ int32_t ut_workspace_create(const ut_plan_desc* plan, const float* observed, int
 int32_t ut_workspace_destroy(ut_workspace* ws) {
     if (!ws) return UT_OK;
     for (void* p : ws->allocations) cudaFree(p);
+    if (ws->h_active) cudaFreeHost(ws->h_active);
     if (ws->stream) cudaStreamDestroy(ws->stream);
     delete ws;
     return UT_OK;
@@ -788,6 +803,94 @@ int32_t ut_persistent_nuts_iteration(ut_workspace* ws, const ut_nuts_buffers* bu
     cudaStream_t st = (cudaStream_t)stream;
     UT_DISPATCH_WARP(ws, LAUNCH_NUTS, ws, a, st);
     UT_LAUNCHED();
+    return UT_OK;
+}
+
+// ---- lockstep (masked) NUTS ------------------------------------------------
+int32_t ut_lockstep_nuts_iteration(ut_workspace* ws, const ut_nuts_buffers* buf, int32_t max_tree_depth,
+                                   float divergence_threshold, uint32_t iteration_coord, void* stream) {
+    int32_t rc = check_ws(ws);
+    if (rc) return rc;
+    if (!buf || !buf->position || !buf->gradient || !buf->logjoint || !buf->inverse_mass || !buf->step ||
+        !buf->accept_prob || !buf->energy || !buf->energy_error || !buf->tree_depth || !buf->integration_steps ||
+        !buf->divergent || !buf->moved)
+        return fail(UT_ERR_ARGUMENT, "null NUTS buffer");
+    if (max_tree_depth < 1 || max_tree_depth > 16)
+        return fail(UT_ERR_ARGUMENT, "max_tree_depth must be in 1..16 for the lockstep tree, got %d",
+                    (int)max_tree_depth);
+    if (ws->P > 256) return fail(UT_ERR_UNSUPPORTED, "the lockstep NUTS tree supports up to 256 parameters");
+    if ((rc = ensure_lf(ws))) return rc;
+    const size_t C = ws->C, P = ws->P;
+    const int K = ws->P <= 32 ? 1 : ws->P <= 64 ? 2 : ws->P <= 96 ? 3 : ws->P <= 128 ? 4 : 8;
+    if (!ws->ls_vec) {
+        if ((rc = dalloc(ws, &ws->ls_vec, (size_t)kLsNumVec * C * P))) return rc;
+        if ((rc = dalloc(ws, &ws->ls_f, (size_t)kLsNumF * C))) return rc;
+        if ((rc = dalloc(ws, &ws->ls_i, (size_t)kLsNumI * C))) return rc;
+        if ((rc = dalloc(ws, &ws->ls_active, 1))) return rc;
+        if ((rc = dalloc(ws, &ws->ls_act, C))) return rc;
+        if ((rc = dalloc(ws, &ws->ls_idx, C))) return rc;
+        if (ws->tc.enabled) {
+            if ((rc = dalloc(ws, &ws->ls_cq, C * P))) return rc;
+            if ((rc = dalloc(ws, &ws->ls_cg, C * P))) return rc;
+            if ((rc = dalloc(ws, &ws->ls_clj, C))) return rc;
+            UT_CUDA(cudaMemset(ws->ls_cq, 0, C * P * sizeof(float)));
+        }
+        void* hp = nullptr;
+        UT_CUDA(cudaMallocHost(&hp, sizeof(int32_t)));
+        ws->h_active = static_cast<int32_t*>(hp);
+    }
+    if (ws->ls_depth < max_tree_depth) {
+        if (ws->ls_ckpt) {
+            cudaFree(ws->ls_ckpt);
+            ws->allocations.erase(std::remove(ws->allocations.begin(), ws->allocations.end(), (void*)ws->ls_ckpt),
+                                  ws->allocations.end());
+            ws->ls_ckpt = nullptr;
+        }
+        if ((rc = dalloc(ws, &ws->ls_ckpt, C * (max_tree_depth + 1) * 2 * 32 * K))) return rc;
+        ws->ls_depth = max_tree_depth;
+    }
+    LsArgs a;
+    a.n.position = buf->position; a.n.gradient = buf->gradient; a.n.logjoint = buf->logjoint;
+    a.n.inverse_mass = buf->inverse_mass; a.n.step = buf->step;
+    a.n.accept_prob = buf->accept_prob; a.n.energy = buf->energy; a.n.energy_error = buf->energy_error;
+    a.n.tree_depth = buf->tree_depth; a.n.integration_steps = buf->integration_steps;
+    a.n.divergent = buf->divergent; a.n.moved = buf->moved;
+    a.n.ckpt = nullptr; a.n.C = ws->C; a.n.max_depth = max_tree_depth; a.n.coord = iteration_coord;
+    a.n.thr = divergence_threshold;
+    a.s.vec = ws->ls_vec; a.s.f = ws->ls_f; a.s.i = ws->ls_i; a.s.ckpt = ws->ls_ckpt;
+    a.s.wq = ws->lf.wq; a.s.wg = ws->lf.wg; a.s.wlj = ws->lf.wlj; a.s.act = ws->ls_act;
+    a.P = ws->P;
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned grid = (unsigned)((C + 3) / 4);
+    UT_K_SWITCH(K, ls_init_kernel<K><<<grid, 128, 0, st>>>(a));
+    UT_LAUNCHED();
+    // at most 2^max_depth - 1 leaves per tree; every 4 leaves the host stops once no
+    // chain is still growing
+    const int max_steps = (1 << max_tree_depth) - 1;
+    const bool compact = ws->tc.enabled;
+    const unsigned rows_grid = (unsigned)std::min<size_t>((C * P + 255) / 256, 4096);
+    for (int step = 0; step < max_steps; ++step) {
+        ls_compact_kernel<<<1, 1024, 0, st>>>(ws->ls_act, (int)C, ws->ls_idx, ws->ls_active);
+        UT_LAUNCHED();
+        if (step > 0 && (step & 3) == 0) {
+            UT_CUDA(cudaMemcpyAsync(ws->h_active, ws->ls_active, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+            UT_CUDA(cudaStreamSynchronize(st));
+            if (*ws->h_active == 0) break;
+        }
+        if (compact) {
+            ls_gather_kernel<<<rows_grid, 256, 0, st>>>(ws->lf.wq, ws->ls_idx, ws->ls_active, (int)P, ws->ls_cq);
+            UT_LAUNCHED();
+            if (tc_glm_launch(ws->tc, ws->ls_cq, ws->ls_clj, ws->ls_cg, st, ws->ls_active) != cudaSuccess)
+                return fail(UT_ERR_CUDA, "tensor-core GLM launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+            ls_scatter_kernel<<<rows_grid, 256, 0, st>>>(ws->ls_cg, ws->ls_clj, ws->ls_idx, ws->ls_active, (int)P,
+                                                         ws->lf.wg, ws->lf.wlj);
+            UT_LAUNCHED();
+        } else if ((rc = density(ws, ws->lf.wq, ws->lf.wlj, ws->lf.wg, st))) {
+            return rc;
+        }
+        UT_K_SWITCH(K, ls_step_kernel<K><<<grid, 128, 0, st>>>(a));
+        UT_LAUNCHED();
+    }
     return UT_OK;
 }
 

@@ -53,6 +53,7 @@ struct TcGlmParams {
     int tiles_per_split;   // observation tiles per CTA
     int num_tiles;         // total observation tiles
     int want_grad;
+    const int* nact;       // optional: only the first *nact chains are live (later chain tiles exit at once)
 };
 
 // ---------------------------------------------------------------------------
@@ -298,6 +299,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int t_begin = split * p.tiles_per_split;
     const int t_end = min(p.num_tiles, t_begin + p.tiles_per_split);
     const int ntiles = max(0, t_end - t_begin);
+    // a chain tile holding no live chain has nothing to do (before any barrier or TMEM exists)
+    if (p.nact && ctile * kTcChains >= *p.nact) return;
 
     if (threadIdx.x == 0) {
         for (int i = 0; i < kTcStages; ++i) {
@@ -654,10 +657,10 @@ inline int tc_glm_setup(TcGlmPlan& t, const float* d_Xa, const float* d_y, int N
 // Prior terms + deterministic fold of the S partials (same reduce as the CUDA-core path).
 __global__ void tc_reduce_kernel(const float* params, const float* part_ll, const float* part_g, float* totals,
                                  float* grads, int S, int C, int F, int off, float icpt_mu, float icpt_sigma,
-                                 float coef_mu, float coef_sigma) {
+                                 float coef_mu, float coef_sigma, const int* nact) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int c = blockIdx.x * 8 + warp;
-    if (c >= C) return;
+    if (c >= C || (nact && c >= *nact)) return;
     float prior = 0.0f;
     for (int f = lane; f < F; f += 32) {
         const float th = params[(size_t)c * F + f];
@@ -678,17 +681,20 @@ __global__ void tc_reduce_kernel(const float* params, const float* part_ll, cons
     }
 }
 
+// nact (optional, device): evaluate only the first *nact chains of params
+// (the totals / gradients of later chains are left untouched).
 inline cudaError_t tc_glm_launch(const TcGlmPlan& t, const float* params, float* totals, float* grads,
-                                 cudaStream_t st) {
+                                 cudaStream_t st, const int* nact = nullptr) {
     TcGlmParams p;
     p.y = t.y; p.part_ll = t.part_ll; p.part_g = t.part_g; p.err = t.err;
     p.N = t.N; p.F = t.F; p.Fp = t.Fp; p.C = t.C;
     p.tiles_per_split = t.tiles_per_split; p.num_tiles = t.num_tiles; p.want_grad = grads ? 1 : 0;
+    p.nact = nact;
     dim3 grid((t.C + kTcChains - 1) / kTcChains, t.S);
     tc_glm_kernel<<<grid, kTcThreads, t.smem, st>>>(t.map_xk_hi, t.map_xk_lo, t.map_xm_hi, t.map_xm_lo, params, p);
     tc_reduce_kernel<<<(t.C + 7) / 8, 256, 0, st>>>(params, t.part_ll, grads ? t.part_g : nullptr, totals, grads,
                                                      t.S, t.C, t.F, t.off, t.icpt_mu, t.icpt_sigma, t.coef_mu,
-                                                     t.coef_sigma);
+                                                     t.coef_sigma, nact);
     return cudaGetLastError();
 }
 

@@ -527,8 +527,8 @@ class _DeviceRun:
     def set_mass_and_step(self, inverse_mass, step):
         torch = self.torch
         self.inverse_mass.copy_(torch.from_numpy(np.asarray(inverse_mass, dtype=np.float32)))
-        st = np.broadcast_to(np.asarray(step, dtype=np.float32), (self.C,))
-        self.step.copy_(torch.from_numpy(np.ascontiguousarray(st)))
+        st = np.array(np.broadcast_to(np.asarray(step, dtype=np.float32), (self.C,)))
+        self.step.copy_(torch.from_numpy(st))
 
     def hmc_buffers(self, proposal=None, endpoint_momentum=None):
         return nat.HmcBuffers(
@@ -541,14 +541,15 @@ class _DeviceRun:
         nat.check(self.lib.ut_hmc_iteration(self.ws.handle, ctypes.byref(buf), int(L), self.coord(iteration),
                                             float(thr), _stream_handle()))
 
-    def nuts_iteration(self, max_depth, iteration, thr):
+    def nuts_iteration(self, max_depth, iteration, thr, strategy="persistent"):
         buf = nat.NutsBuffers(
             nat.ptr(self.position), nat.ptr(self.gradient), nat.ptr(self.logjoint), nat.ptr(self.inverse_mass),
             nat.ptr(self.step), nat.ptr(self.accept_prob), nat.ptr(self.energy), nat.ptr(self.energy_error),
             nat.ptr(self.tree_depth), nat.ptr(self.integration_steps), nat.ptr(self.divergent),
             nat.ptr(self.moved if hasattr(self, "moved") else self.accepted))
-        nat.check(self.lib.ut_persistent_nuts_iteration(self.ws.handle, ctypes.byref(buf), int(max_depth),
-                                                        float(thr), self.coord(iteration), _stream_handle()))
+        fn = self.lib.ut_lockstep_nuts_iteration if strategy == "masked" else self.lib.ut_persistent_nuts_iteration
+        nat.check(fn(self.ws.handle, ctypes.byref(buf), int(max_depth), float(thr), self.coord(iteration),
+                     _stream_handle()))
 
     def probe(self, trial_steps, inverse_mass, coord):
         """log accept ratio of one leapfrog step per chain (momentum fixed by `coord`)."""
@@ -785,8 +786,8 @@ def batched_nuts(model, args=(), constraints=None, *, num_chains, num_samples, n
                  backend="cuda", precision=None, persistent_gradient="auto", rng=None) -> HMCChains:
     if tree_strategy not in ("hybrid", "masked", "persistent"):
         raise ValueError(f"batched_nuts tree_strategy must be :hybrid, :masked, or :persistent, got {tree_strategy!r}")
-    if tree_strategy != "persistent":
-        raise ValueError(f"the B200 backend implements tree_strategy=:persistent; got {tree_strategy!r}")
+    if tree_strategy == "hybrid":  # api_batched_nuts.jl:99-102
+        raise ValueError("batched_nuts device backend requires tree_strategy=:masked or :persistent, got :hybrid")
     if persistent_gradient not in ("auto", "scalar", "wide"):
         raise ValueError("batched_nuts persistent_gradient must be :auto, :scalar, or :wide")
     if max_tree_depth < 1:
@@ -829,7 +830,7 @@ def batched_nuts(model, args=(), constraints=None, *, num_chains, num_samples, n
         if it == num_warmup + 1:
             torch.cuda.synchronize()
             t_sample = time.perf_counter()
-        run.nuts_iteration(max_tree_depth, it, divergence_threshold)
+        run.nuts_iteration(max_tree_depth, it, divergence_threshold, tree_strategy)
         grad_evals += run.integration_steps.sum()
         if it <= num_warmup:
             ap = run.accept_prob.double().cpu().numpy()
