@@ -53,8 +53,34 @@ struct TcGlmParams {
     int tiles_per_split;   // observation tiles per CTA
     int num_tiles;         // total observation tiles
     int want_grad;
-    const int* nact;       // optional: only the first *nact chains are live (later chain tiles exit at once)
+    int ctiles, S, sms;    // chain tiles, observation splits of the full grid, SMs
+    const int* nact;       // optional: only the first *nact chains are live
 };
+
+// Work split of one launch.  Without nact: the (chain tile, split) grid of the
+// plan and partial rows of C chains.  With nact: only ceil(nact / 128) chain
+// tiles are live, and when they are few the observations are cut into more
+// splits so the launch still fills the SMs (at most the plan's grid size
+// CTAs); partial rows then hold nt * 128 chains.
+struct TcSplit {
+    int nt, S, tps, Cl;
+};
+
+__device__ __forceinline__ TcSplit tc_split(const TcGlmParams& p) {
+    TcSplit r;
+    if (!p.nact) {
+        r.nt = p.ctiles; r.S = p.S; r.tps = p.tiles_per_split; r.Cl = p.C;
+        return r;
+    }
+    const int n = *p.nact;
+    r.nt = max(1, (n + kTcChains - 1) / kTcChains);
+    int S = max(p.S, min(p.ctiles * p.S, p.sms) / r.nt);
+    S = min(S, p.num_tiles);
+    r.tps = (p.num_tiles + S - 1) / S;
+    r.S = (p.num_tiles + r.tps - 1) / r.tps;
+    r.Cl = r.nt * kTcChains;
+    return r;
+}
 
 // ---------------------------------------------------------------------------
 // PTX helpers
@@ -294,13 +320,16 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 13);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int ctile = blockIdx.x;   // chain tiles fastest: concurrent CTAs share X ranges in L2
-    const int split = blockIdx.y;
-    const int t_begin = split * p.tiles_per_split;
-    const int t_end = min(p.num_tiles, t_begin + p.tiles_per_split);
+    // chain tiles fastest: concurrent CTAs share X ranges in L2
+    const TcSplit sp = tc_split(p);
+    const int b = blockIdx.y * gridDim.x + blockIdx.x;
+    // with nact, CTAs beyond the live work leave before any barrier or TMEM exists
+    if (p.nact && (*p.nact <= 0 || b >= sp.S * sp.nt)) return;
+    const int ctile = p.nact ? b % sp.nt : blockIdx.x;
+    const int split = p.nact ? b / sp.nt : blockIdx.y;
+    const int t_begin = split * sp.tps;
+    const int t_end = min(p.num_tiles, t_begin + sp.tps);
     const int ntiles = max(0, t_end - t_begin);
-    // a chain tile holding no live chain has nothing to do (before any barrier or TMEM exists)
-    if (p.nact && ctile * kTcChains >= *p.nact) return;
 
     if (threadIdx.x == 0) {
         for (int i = 0; i < kTcStages; ++i) {
@@ -500,10 +529,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         asm volatile("bar.sync 1, %0;" ::"n"(kTcEpiThreads));
         if (ok) {
             if (slot == 0 && c < p.C)
-                p.part_ll[(size_t)split * p.C + c] = ((ll_part[c_local] + ll_part[kTcChains + c_local]) +
+                p.part_ll[(size_t)split * sp.Cl + c] = ((ll_part[c_local] + ll_part[kTcChains + c_local]) +
                                                       ll_part[2 * kTcChains + c_local]) + ll_part[3 * kTcChains + c_local];
             if (p.want_grad && c < p.C) {
-                float* dst = p.part_g + ((size_t)split * p.C + c) * p.F;
+                float* dst = p.part_g + ((size_t)split * sp.Cl + c) * p.F;
 #pragma unroll
                 for (int k = 0; k < kOwnCols / 16; ++k) {
 #pragma unroll
@@ -526,7 +555,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 // ---------------------------------------------------------------------------
 struct TcGlmPlan {
     bool enabled = false;
-    int N = 0, F = 0, Fp = 0, C = 0, S = 0, tiles_per_split = 0, num_tiles = 0;
+    int N = 0, F = 0, Fp = 0, C = 0, S = 0, tiles_per_split = 0, num_tiles = 0, ctiles = 0, sms = 0;
     float* xhi = nullptr;
     float* xlo = nullptr;
     float* part_ll = nullptr;
@@ -608,6 +637,10 @@ inline int tc_glm_setup(TcGlmPlan& t, const float* d_Xa, const float* d_y, int N
     S = std::max(1, std::min(S, std::max(1, t.num_tiles / 8)));
     t.tiles_per_split = (t.num_tiles + S - 1) / S;
     t.S = (t.num_tiles + t.tiles_per_split - 1) / t.tiles_per_split;
+    t.ctiles = ctiles;
+    t.sms = sms;
+    // partial rows for every split plan tc_split can pick: at most ctiles * S CTAs of 128 chains
+    const size_t part_rows = (size_t)ctiles * t.S * kTcChains;
     auto alloc = [&](void** p, size_t bytes) {
         if (cudaMalloc(p, bytes) != cudaSuccess) return false;
         allocs->push_back(*p);
@@ -615,8 +648,8 @@ inline int tc_glm_setup(TcGlmPlan& t, const float* d_Xa, const float* d_y, int N
     };
     const size_t xbytes = (size_t)N * Fp * sizeof(float);
     if (!alloc((void**)&t.xhi, xbytes) || !alloc((void**)&t.xlo, xbytes) ||
-        !alloc((void**)&t.part_ll, (size_t)t.S * C * sizeof(float)) ||
-        !alloc((void**)&t.part_g, (size_t)t.S * C * F * sizeof(float)) || !alloc((void**)&t.err, sizeof(int))) {
+        !alloc((void**)&t.part_ll, part_rows * sizeof(float)) ||
+        !alloc((void**)&t.part_g, part_rows * F * sizeof(float)) || !alloc((void**)&t.err, sizeof(int))) {
         tc_err_string() = "cudaMalloc failed";
         return 1;
     }
@@ -654,30 +687,40 @@ inline int tc_glm_setup(TcGlmPlan& t, const float* d_Xa, const float* d_y, int N
     return 0;
 }
 
-// Prior terms + deterministic fold of the S partials (same reduce as the CUDA-core path).
-__global__ void tc_reduce_kernel(const float* params, const float* part_ll, const float* part_g, float* totals,
-                                 float* grads, int S, int C, int F, int off, float icpt_mu, float icpt_sigma,
-                                 float coef_mu, float coef_sigma, const int* nact) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int c = blockIdx.x * 8 + warp;
-    if (c >= C || (nact && c >= *nact)) return;
+// Prior terms + deterministic fold of the split partials, one 128-thread CTA
+// per chain (thread = feature; F <= 128 on this path), fixed summation order.
+__global__ void __launch_bounds__(128) tc_reduce_kernel(const float* params, float* totals, float* grads,
+                                                        TcGlmParams p, int off, float icpt_mu, float icpt_sigma,
+                                                        float coef_mu, float coef_sigma) {
+    const int c = blockIdx.x;
+    if (c >= p.C || (p.nact && c >= *p.nact)) return;
+    const TcSplit sp = tc_split(p);
+    const int f = threadIdx.x, warp = f >> 5, lane = f & 31;
+    const int F = p.F;
+    __shared__ float wsum[4];
     float prior = 0.0f;
-    for (int f = lane; f < F; f += 32) {
+    if (f < F) {
         const float th = params[(size_t)c * F + f];
         const bool icpt = off && f == 0;
         const float mu = icpt ? icpt_mu : coef_mu, sg = icpt ? icpt_sigma : coef_sigma;
-        prior += normal_logpdf(mu, sg, th);
+        prior = normal_logpdf(mu, sg, th);
         if (grads) {
+            const float* pg = p.part_g + (size_t)c * F + f;
+            const size_t stride = (size_t)sp.Cl * F;
             float gs = 0.0f;
-            for (int s = 0; s < S; ++s) gs += part_g[((size_t)s * C + c) * F + f];
+#pragma unroll 8
+            for (int s = 0; s < sp.S; ++s) gs += pg[s * stride];
             grads[(size_t)c * F + f] = gs - (th - mu) / (sg * sg);
         }
     }
     prior = warp_sum(prior);
-    if (lane == 0) {
-        float tsum = 0.0f;
-        for (int s = 0; s < S; ++s) tsum += part_ll[(size_t)s * C + c];
-        totals[c] = tsum + prior;
+    if (lane == 0) wsum[warp] = prior;
+    __syncthreads();
+    if (warp == 0) {
+        float ll = 0.0f;
+        for (int s = lane; s < sp.S; s += 32) ll += p.part_ll[(size_t)s * sp.Cl + c];
+        ll = warp_sum(ll);
+        if (lane == 0) totals[c] = ll + (((wsum[0] + wsum[1]) + wsum[2]) + wsum[3]);
     }
 }
 
@@ -689,12 +732,12 @@ inline cudaError_t tc_glm_launch(const TcGlmPlan& t, const float* params, float*
     p.y = t.y; p.part_ll = t.part_ll; p.part_g = t.part_g; p.err = t.err;
     p.N = t.N; p.F = t.F; p.Fp = t.Fp; p.C = t.C;
     p.tiles_per_split = t.tiles_per_split; p.num_tiles = t.num_tiles; p.want_grad = grads ? 1 : 0;
+    p.ctiles = t.ctiles; p.S = t.S; p.sms = t.sms;
     p.nact = nact;
-    dim3 grid((t.C + kTcChains - 1) / kTcChains, t.S);
+    dim3 grid(t.ctiles, t.S);
     tc_glm_kernel<<<grid, kTcThreads, t.smem, st>>>(t.map_xk_hi, t.map_xk_lo, t.map_xm_hi, t.map_xm_lo, params, p);
-    tc_reduce_kernel<<<(t.C + 7) / 8, 256, 0, st>>>(params, t.part_ll, grads ? t.part_g : nullptr, totals, grads,
-                                                     t.S, t.C, t.F, t.off, t.icpt_mu, t.icpt_sigma, t.coef_mu,
-                                                     t.coef_sigma, nact);
+    tc_reduce_kernel<<<t.C, 128, 0, st>>>(params, totals, grads, p, t.off, t.icpt_mu, t.icpt_sigma, t.coef_mu,
+                                          t.coef_sigma);
     return cudaGetLastError();
 }
 
