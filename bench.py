@@ -11,11 +11,12 @@ shipped).
 
 At N=1 the line also carries `hbm_sweep`: the same design at 1, 4, 8 and 16
 chains, where an evaluation is bound by reading X from HBM (achieved GB/s
-against the measured HBM bandwidth), `samplers`: the config-1 HMC and config-2
-persistent-NUTS runs (min ESS/s, R-hat, gradient evaluations/s; skipped with
---no-samplers), `surrogate_chees`: the learned-gradient-surrogate
-workload on the same model (min ESS/s of surrogate-driven ChEES-HMC vs plain
-ChEES-HMC, both at R-hat < 1.01; skipped with --no-surrogate), and
+against the measured HBM bandwidth), `samplers`: the config-1 HMC, config-2
+persistent-NUTS and config-3 masked-NUTS runs (min ESS/s, R-hat, gradient
+evaluations/s; skipped with --no-samplers), `surrogate_chees`: the
+learned-gradient-surrogate workload on the same model (min ESS/s of
+surrogate-driven ChEES-HMC vs plain ChEES-HMC and vs the plain masked NUTS run,
+all at R-hat < 1.01; skipped with --no-surrogate), and
 `uneven_batch`: 512 hierarchical models of uneven sizes in one batched
 persistent-NUTS run (aggregate ESS/s, per-model time to R-hat < 1.01;
 skipped with --no-uneven).
@@ -250,8 +251,14 @@ def run_b200(args):
         sweep = hbm_sweep()
         if not args.no_samplers:
             samplers = sampler_configs()
+            samplers["config3_nuts"] = config3_nuts()
     if rank == 0 and world == 1 and not args.no_surrogate:
         sur = surrogate_comparison()
+        if samplers is not None:
+            # the headline comparison: surrogate-driven trajectories vs plain NUTS on the same model
+            nuts = samplers["config3_nuts"]
+            sur["plain_nuts"] = {k: nuts[k] for k in ("min_ess_per_s", "min_ess", "max_rhat", "sampling_s")}
+            sur["ratio_vs_plain_nuts"] = sur["surrogate"]["min_ess_per_s"] / nuts["min_ess_per_s"]
     if rank == 0 and world == 1 and not args.no_uneven:
         uneven = uneven_batch()
     if rank == 0:
@@ -350,6 +357,27 @@ def sampler_configs():
                      "config": cfg}
     out["config2_nuts"]["mean_tree_depth"] = float(c2.tree_depth.mean())
     return out
+
+
+def config3_nuts(num_chains=4096, num_warmup=200, num_samples=200):
+    """Masked (lockstep) NUTS on the large logistic regression, 4096 chains, max
+    tree depth 10: every leaf is one batched tensor-core gradient over the chains
+    whose trees are still growing (compacted).  Fewer iterations than configs 1-2
+    (200 + 200) keep the bench within minutes; the draws are still nearly
+    independent (min ESS at the draw count)."""
+    from uncertaintea_b200 import batched_nuts, ess, rhat
+    model, X, y, _ = _data()
+    ch = batched_nuts(model, (X,), {"y": y}, num_chains=num_chains, num_samples=num_samples, num_warmup=num_warmup,
+                      max_tree_depth=10, tree_strategy="masked", rng=1)
+    e, r = ess(ch, space="unconstrained"), rhat(ch, space="unconstrained")
+    total_s = ch.warmup_seconds + ch.sampling_seconds
+    return {"min_ess_per_s": float(np.min(e) / ch.sampling_seconds), "min_ess": float(np.min(e)),
+            "max_rhat": float(np.max(r)), "warmup_s": ch.warmup_seconds, "sampling_s": ch.sampling_seconds,
+            "ms_per_sampling_iteration": 1e3 * ch.sampling_seconds / num_samples,
+            "grad_evals_per_s": ch.gradient_evaluations / total_s, "mean_accept": float(ch.accept_prob.mean()),
+            "mean_tree_depth": float(ch.tree_depth.mean()), "max_tree_depth": int(ch.tree_depth.max()),
+            "mean_leapfrog_steps": float(ch.integration_steps.mean()),
+            "config": f"{num_chains} chains, masked NUTS depth 10, {num_warmup}+{num_samples}, GLM 100000x100"}
 
 
 def surrogate_comparison(num_chains=4096, num_warmup=500, num_samples=500):
