@@ -426,9 +426,12 @@ def test_streaming_path_vs_oracle_and_tiled(lib, N, D, C, intercept, monkeypatch
     qd = torch.from_numpy(q).cuda()
     t1, g1 = ws.logjoint_gradient_device(qd)
     t0 = ws.logjoint_device(qd)
+    t1b, g1b = ws.logjoint_gradient_device(qd)  # the fold's tickets were reset: same bits again
     t2, g2 = ws_t.logjoint_gradient_device(qd)
     torch.cuda.synchronize()
+    ws.check()
     t1, g1, t0, t2, g2 = (x.cpu().numpy() for x in (t1, g1, t0, t2, g2))
+    assert np.array_equal(t1, t1b.cpu().numpy()) and np.array_equal(g1, g1b.cpu().numpy())
     t64, g64 = oracle.OracleModel(ws.lowered).logjoint_gradient_f64(q.astype(np.float64))
     assert _lj_err(t1, t64) <= 1e-5 and _lj_err(t0, t64) <= 1e-5
     assert _grad_err(g1, g64) <= 1e-5

@@ -86,9 +86,13 @@ struct ut_workspace {
     TcGlmPlan tc;
     // streaming path (GLM, few chains)
     bool streaming = false;
-    int stream_cb = 16, stream_splits = 0, stream_warps = 8;
-    float* d_spart_ll = nullptr;
-    float* d_spart_g = nullptr;
+    int stream_cb = 16, stream_splits = 0, stream_stages = 2;
+    size_t stream_smem = 0;
+    float* d_ypad = nullptr;        // y rounded up to whole 32-row chunks, zero padded
+    float* d_spart = nullptr;       // per-CTA partials
+    float* d_sgpart = nullptr;      // per-group partials
+    unsigned* d_stickets = nullptr; // fold tickets (zero between launches)
+    int* d_serr = nullptr;          // sticky error word of the streaming kernel
     // batched leapfrog scratch
     LfScratch lf = {};
     // NUTS checkpoint scratch
@@ -278,28 +282,24 @@ int32_t launch_tiled_t(ut_workspace* ws, const float* params, float* totals, flo
 
 int32_t launch_stream(ut_workspace* ws, const float* params, float* totals, float* grads, cudaStream_t st) {
     GlmStreamArgs a;
-    a.Xa = ws->d_Xa; a.y = ws->d_y; a.params = params; a.part_ll = ws->d_spart_ll; a.part_g = ws->d_spart_g;
-    a.N = ws->N; a.F = ws->P; a.C = ws->C;
-    const size_t smem = glm_stream_smem(ws->stream_cb, ws->P, ws->stream_warps);
+    a.Xa = ws->d_Xa; a.ypad = ws->d_ypad; a.params = params;
+    a.part = ws->d_spart; a.gpart = ws->d_sgpart; a.tickets = ws->d_stickets; a.err = ws->d_serr;
+    a.totals = totals; a.grads = grads;
+    a.N = ws->N; a.F = ws->P; a.C = ws->C; a.stages = ws->stream_stages; a.off = ws->plan.has_intercept;
+    a.icpt_mu = (float)ws->plan.intercept_mu; a.icpt_sigma = (float)ws->plan.intercept_sigma;
+    a.coef_mu = (float)ws->plan.coef_mu; a.coef_sigma = (float)ws->plan.coef_sigma;
+    const size_t smem = ws->stream_smem;
 #define STREAM_CASE(CBV)                                                                            \
     case CBV: {                                                                                     \
         auto kern = grads ? glm_stream_kernel<CBV, true> : glm_stream_kernel<CBV, false>;          \
         UT_CUDA(launch_dyn(kern, 0, 0, smem, st));                                                  \
-        kern<<<ws->stream_splits, 32 * ws->stream_warps, smem, st>>>(a);                            \
+        kern<<<ws->stream_splits, kStreamThreads, smem, st>>>(a);                                   \
     } break;
     switch (ws->stream_cb) {
         STREAM_CASE(1) STREAM_CASE(2) STREAM_CASE(4) STREAM_CASE(8)
         default: STREAM_CASE(16)
     }
 #undef STREAM_CASE
-    UT_LAUNCHED();
-    GlmStreamFoldArgs r;
-    r.params = params; r.part_ll = ws->d_spart_ll; r.part_g = grads ? ws->d_spart_g : nullptr;
-    r.totals = totals; r.grads = grads;
-    r.S = ws->stream_splits; r.C = ws->C; r.F = ws->P; r.off = ws->plan.has_intercept;
-    r.icpt_mu = (float)ws->plan.intercept_mu; r.icpt_sigma = (float)ws->plan.intercept_sigma;
-    r.coef_mu = (float)ws->plan.coef_mu; r.coef_sigma = (float)ws->plan.coef_sigma;
-    glm_stream_fold_kernel<<<ws->C, 1024, 0, st>>>(r);
     UT_LAUNCHED();
     return UT_OK;
 }
@@ -494,10 +494,27 @@ int32_t ut_workspace_create(const ut_plan_desc* plan, const float* observed, int
                 ws->streaming = true;
                 const int C = ws->C;
                 ws->stream_cb = C <= 1 ? 1 : C <= 2 ? 2 : C <= 4 ? 4 : C <= 8 ? 8 : 16;
-                ws->stream_warps = glm_stream_warps(ws->stream_cb, F);
-                ws->stream_splits = dev_sms;  // one CTA per SM; its warps take chunks round-robin
-                if ((rc = dalloc(ws, &ws->d_spart_ll, (size_t)ws->stream_splits * C))) return bail(rc);
-                if ((rc = dalloc(ws, &ws->d_spart_g, (size_t)ws->stream_splits * C * F))) return bail(rc);
+                ws->stream_splits = dev_sms;  // one CTA per SM, each a contiguous range of 32-row chunks
+                int optin = 0;
+                cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ws->device);
+                const int chunks = (N + kStreamRows - 1) / kStreamRows;
+                const int per_cta = (chunks + dev_sms - 1) / dev_sms;
+                ws->stream_stages = glm_stream_stages(ws->stream_cb, F, (size_t)std::max(0, optin - 1024), per_cta);
+                ws->stream_smem = glm_stream_smem(ws->stream_cb, F, ws->stream_stages);
+                if (ws->stream_smem + 1024 > (size_t)optin)
+                    return bail(fail(UT_ERR_UNSUPPORTED, "streaming kernel needs %zu bytes of shared memory",
+                                     ws->stream_smem));
+                const int groups = glm_stream_groups(ws->stream_splits);
+                const size_t ypad = (size_t)chunks * kStreamRows;
+                if ((rc = dalloc(ws, &ws->d_ypad, ypad))) return bail(rc);
+                UT_CUDA(cudaMemset(ws->d_ypad, 0, ypad * sizeof(float)));
+                UT_CUDA(cudaMemcpy(ws->d_ypad, ws->d_y, (size_t)N * sizeof(float), cudaMemcpyDeviceToDevice));
+                if ((rc = dalloc(ws, &ws->d_spart, (size_t)ws->stream_splits * C * (F + 1)))) return bail(rc);
+                if ((rc = dalloc(ws, &ws->d_sgpart, (size_t)groups * C * (F + 1)))) return bail(rc);
+                if ((rc = dalloc(ws, &ws->d_stickets, (size_t)groups + 1))) return bail(rc);
+                if ((rc = dalloc(ws, &ws->d_serr, 1))) return bail(rc);
+                UT_CUDA(cudaMemset(ws->d_stickets, 0, ((size_t)groups + 1) * sizeof(unsigned)));
+                UT_CUDA(cudaMemset(ws->d_serr, 0, sizeof(int)));
             } else if ((rc = tc_glm_setup(ws->tc, ws->d_Xa, ws->d_y, N, F, ws->C, off, (float)plan->intercept_mu,
                                           (float)plan->intercept_sigma, (float)plan->coef_mu,
                                           (float)plan->coef_sigma, dev_sms, &ws->allocations))) {
@@ -564,6 +581,15 @@ int32_t ut_workspace_check(ut_workspace* ws, void* stream) {
         if (h) {
             UT_CUDA(cudaMemset(ws->tc.err, 0, sizeof(int)));
             return fail(UT_ERR_DEVICE_TIMEOUT, "a bounded wait inside the tensor-core GLM kernel gave up; "
+                                               "its results are invalid");
+        }
+    }
+    if (ws->d_serr) {
+        int h = 0;
+        UT_CUDA(cudaMemcpy(&h, ws->d_serr, sizeof(int), cudaMemcpyDeviceToHost));
+        if (h) {
+            UT_CUDA(cudaMemset(ws->d_serr, 0, sizeof(int)));
+            return fail(UT_ERR_DEVICE_TIMEOUT, "a bounded wait inside the streaming GLM kernel gave up; "
                                                "its results are invalid");
         }
     }

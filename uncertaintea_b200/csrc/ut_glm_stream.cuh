@@ -2,96 +2,108 @@
 // few chains (C <= 16): an HBM-streaming kernel.
 //
 // With few chains every element of X is used 2C times (C for eta, C for the
-// gradient), so the evaluation is bound by reading X once from HBM.  Every
-// warp streams its own 32-row chunks of the row-major X (N x F, F % 4 == 0,
-// F <= 128) through a private two-stage cp.async pipeline (16-byte pieces:
-// the next chunk is in flight while the current one is used) -- no block-wide
-// barrier inside the loop, so the warps of an SM overlap each other's load
-// latency and arithmetic.  Per chunk:
+// gradient), so the evaluation is bound by reading X once from HBM.  One CTA
+// per SM owns a contiguous range of 32-row chunks of the row-major X
+// (N x F, F % 4 == 0, F <= 128).  A producer thread keeps a deep ring of
+// shared-memory stages filled with plain bulk copies (cp.async.bulk, one per
+// chunk for X and one for y, completing on the stage's mbarrier): at launch the
+// ring requests most of the CTA's range at once, so the whole GPU has tens of
+// MB in flight.  Eight consumer warps take the chunks round-robin (chunk i ->
+// warp i mod 8, a fixed assignment, so every sum has a fixed order):
 //   lane = row      eta_c = x_row . theta_c (theta broadcast from shared
 //                   memory), r_c = y - logistic(eta_c), log-likelihood terms;
-//   lane = feature  G_c[f4] += sum_rows r_c(row) x_row[f4] (r by warp shuffle,
-//   group (of 4)    X rows read as float4, conflict-free).
-// At the end the warps' partials are added in warp order into one per-CTA
-// partial; glm_stream_fold_kernel folds the CTAs' partials in a fixed order and
-// adds the priors (deterministic).
+//   lane = feature  G_c[f4] += sum_rows r_c(row) x_row[f4] (r broadcast from
+//   group (of 4)    shared memory, X rows read as float4, conflict-free);
+// then release the stage to the producer.
+// The fold is fused: each CTA adds its warps' partials in warp order into a
+// per-CTA partial; the last CTA of each group of kStreamGroup CTAs (an atomic
+// ticket) folds its group's partials in CTA order; the last group to finish
+// folds the group partials in group order and adds the priors.  Deterministic:
+// which CTA folds depends on timing, the order of every sum does not.
 #pragma once
 
+#include <algorithm>
+
 #include "ut_common.cuh"
+#include "ut_tc_glm.cuh"
 
 namespace ut {
 
-constexpr int kStreamRows = 32;      // observations per chunk (one per lane)
-constexpr int kStreamMaxC = 16;      // chains
-constexpr int kStreamMaxF = 128;     // features (a multiple of 4): one float4 group per lane
-constexpr int kStreamStages = 2;  // chunks in flight per warp
+constexpr int kStreamRows = 32;       // observations per chunk (one per lane)
+constexpr int kStreamMaxC = 16;       // chains
+constexpr int kStreamMaxF = 128;      // features (a multiple of 4): one float4 group per lane
+constexpr int kStreamWarps = 8;       // consumer warps (plus one producer warp)
+constexpr int kStreamThreads = 32 * (kStreamWarps + 1);
+constexpr int kStreamGroup = 12;      // CTAs per first-level fold group
+constexpr int kStreamMaxStages = 48;
+constexpr int kStreamHeader = 1024;   // mbarriers (2 x kStreamMaxStages x 8 B), rounded up
 
 struct GlmStreamArgs {
-    const float* Xa;      // N x F row-major (ones column first when intercept), F % 4 == 0
-    const float* y;       // N
+    const float* Xa;      // N x F row-major (ones column first when intercept), F % 4 == 0, 16-byte aligned
+    const float* ypad;    // N rounded up to whole chunks, zero padded
     const float* params;  // C x F
-    float* part_ll;       // S x C
-    float* part_g;        // S x C x F (only when GRAD)
-    int N, F, C;
+    float* part;          // S x C x Wd  per-CTA partials (Wd = F + 1 with the gradient, else 1): [ll, g_0..g_F-1]
+    float* gpart;         // groups x C x Wd
+    unsigned* tickets;    // groups + 1 counters, zero between launches
+    int* err;             // sticky error word (a bounded wait gave up)
+    float* totals;        // C
+    float* grads;         // C x F (GRAD)
+    int N, F, C, stages, off;
+    float icpt_mu, icpt_sigma, coef_mu, coef_sigma;
 };
 
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+__host__ __device__ inline size_t glm_stream_stage_floats(int F) { return (size_t)kStreamRows * F + kStreamRows; }
+// header | theta (CB x F) | residuals (warps x 32 x CB) | stages
+__host__ __device__ inline size_t glm_stream_fixed_bytes(int CB, int F) {
+    return kStreamHeader + sizeof(float) * ((size_t)CB * F + (size_t)kStreamWarps * kStreamRows * CB);
 }
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+__host__ __device__ inline size_t glm_stream_smem(int CB, int F, int stages) {
+    return glm_stream_fixed_bytes(CB, F) + sizeof(float) * (size_t)stages * glm_stream_stage_floats(F);
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-
-// Shared memory: theta (CB x F), then per warp kStreamStages x (32 x F X rows
-// + 32 y) floats.  After the loop the warp areas hold the warps' partials
-// (CB + CB * F floats <= the area since CB <= 16 < 2 * 32).
-__host__ __device__ inline size_t glm_stream_warp_floats(int F) {
-    return (size_t)kStreamStages * kStreamRows * (F + 1);
-}
-__host__ __device__ inline size_t glm_stream_smem(int CB, int F, int warps) {
-    return sizeof(float) * ((size_t)CB * F + (size_t)warps * glm_stream_warp_floats(F));
-}
-// Warps per CTA: as many as fit in 220 KB of shared memory (at most 8).
-__host__ __device__ inline int glm_stream_warps(int CB, int F) {
-    int w = 8;
-    while (w > 1 && glm_stream_smem(CB, F, w) > 220 * 1024) --w;
-    return w;
+inline int glm_stream_groups(int S) { return (S + kStreamGroup - 1) / kStreamGroup; }
+// Stages: as many as fit in smem_limit bytes, at most the CTA's chunk count and
+// kStreamMaxStages, at least 2; the ring must also hold the warps' partials.
+inline int glm_stream_stages(int CB, int F, size_t smem_limit, int max_chunks) {
+    const size_t fixed = glm_stream_fixed_bytes(CB, F), per = sizeof(float) * glm_stream_stage_floats(F);
+    int s = smem_limit > fixed ? (int)((smem_limit - fixed) / per) : 0;
+    s = std::min(s, std::min(kStreamMaxStages, std::max(2, max_chunks)));
+    s = std::max(2, s);
+    const size_t partial_floats = (size_t)kStreamWarps * CB * (F + 1);
+    while ((size_t)s * glm_stream_stage_floats(F) < partial_floats) ++s;
+    return s;
 }
 
 template <int CB, bool GRAD>
-__global__ void __launch_bounds__(256) glm_stream_kernel(GlmStreamArgs a) {
-    extern __shared__ __align__(16) float sm[];
-    const int F = a.F, F4 = F / 4, N = a.N, C = a.C;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, W = blockDim.x >> 5;
-    float* Th = sm;  // [CB][F]
-    for (int i = threadIdx.x; i < CB * F; i += blockDim.x) {
+__global__ void __launch_bounds__(kStreamThreads, 1) glm_stream_kernel(GlmStreamArgs a) {
+    extern __shared__ __align__(1024) uint8_t stream_smem[];
+    __shared__ int s_last;
+    const int F = a.F, F4 = F / 4, N = a.N, C = a.C, NS = a.stages;
+    const int Wd = GRAD ? F + 1 : 1;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    uint64_t* full = reinterpret_cast<uint64_t*>(stream_smem);
+    uint64_t* empty = full + kStreamMaxStages;
+    float* Th = reinterpret_cast<float*>(stream_smem + kStreamHeader);    // [CB][F]
+    float* R = Th + CB * F;                                                // [warps][32][CB]
+    float* ring = R + kStreamWarps * kStreamRows * CB;                     // [NS][32 x F X rows, 32 y]
+    const size_t stage_floats = glm_stream_stage_floats(F);
+
+    const int NC = (N + kStreamRows - 1) / kStreamRows;
+    const int c0 = (int)((long long)blockIdx.x * NC / gridDim.x);
+    const int c1 = (int)((long long)(blockIdx.x + 1) * NC / gridDim.x);
+    const int n = c1 - c0;
+
+    if (tid == 0) {
+        for (int s = 0; s < NS; ++s) {
+            mbar_init(full + s, 1);
+            mbar_init(empty + s, 1);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int i = tid; i < CB * F; i += blockDim.x) {
         const int c = i / F, f = i % F;
         Th[i] = c < C ? a.params[(size_t)c * F + f] : 0.0f;
     }
     __syncthreads();
-    const size_t wf = glm_stream_warp_floats(F);
-    float* Wb = sm + CB * F + warp * wf;  // this warp's stages
-    const int nchunks = (N + kStreamRows - 1) / kStreamRows;
-    const int gw = blockIdx.x * W + warp, GW = gridDim.x * W;
-
-    auto stage_x = [&](int st) { return Wb + st * kStreamRows * (F + 1); };  // 32 x F rows
-    auto stage_y = [&](int st) { return Wb + st * kStreamRows * (F + 1) + kStreamRows * F; };
-    auto issue = [&](int chunk, int st) {
-        if (chunk < nchunks) {
-            const int r0 = chunk * kStreamRows;
-            const int nrows = min(kStreamRows, N - r0);
-            const float* src = a.Xa + (size_t)r0 * F;
-            float* dst = stage_x(st);
-            for (int i = lane; i < nrows * F4; i += 32) cp_async16(dst + 4 * i, src + 4 * i);
-            if (lane < nrows) cp_async4(stage_y(st) + lane, a.y + r0 + lane);
-        }
-        cp_async_commit();  // one group per call (empty past the end) keeps the counts exact
-    };
 
     float ll[CB];
     float4 g[CB];
@@ -100,164 +112,172 @@ __global__ void __launch_bounds__(256) glm_stream_kernel(GlmStreamArgs a) {
         ll[c] = 0.0f;
         g[c] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
-    const float4* Th4 = reinterpret_cast<const float4*>(Th);
 
-    int it = 0;
+    if (warp == kStreamWarps) {
+        // ---------------- producer ----------------
+        if (lane == 0) {
+            for (int i = 0; i < n; ++i) {
+                const int s = i % NS;
+                if (i >= NS && !mbar_wait(empty + s, ((i / NS) - 1) & 1, a.err)) break;
+                const int r0 = (c0 + i) * kStreamRows;
+                const int nrows = min(kStreamRows, N - r0);
+                float* st = ring + s * stage_floats;
+                const uint32_t xbytes = (uint32_t)(nrows * F * 4);
+                mbar_expect_tx(full + s, xbytes + kStreamRows * 4);
+                bulk_load(st, a.Xa + (size_t)r0 * F, xbytes, full + s);
+                bulk_load(st + kStreamRows * F, a.ypad + r0, kStreamRows * 4, full + s);
+            }
+        }
+    } else {
+        // ---------------- consumers ----------------
+        const float4* Th4 = reinterpret_cast<const float4*>(Th);
+        float* Rw = R + warp * kStreamRows * CB;
+        for (int i = warp; i < n; i += kStreamWarps) {
+            const int s = i % NS;
+            if (!mbar_wait(full + s, (i / NS) & 1, a.err)) break;
+            const int nrows = min(kStreamRows, N - (c0 + i) * kStreamRows);
+            const float* st = ring + s * stage_floats;
+            const float4* X4 = reinterpret_cast<const float4*>(st);
+            // lane = row: eta (four independent component sums per chain), residual, log-likelihood
+            {
+                float4 e4[CB];
 #pragma unroll
-    for (int p = 0; p < kStreamStages - 1; ++p) issue(gw + p * GW, p);  // the pipeline's first chunks
-    for (int chunk = gw; chunk < nchunks; chunk += GW, ++it) {
-        const int st = it % kStreamStages;
-        issue(chunk + (kStreamStages - 1) * GW, (it + kStreamStages - 1) % kStreamStages);
-        cp_async_wait<kStreamStages - 1>();
-        __syncwarp();
-        const int nrows = min(kStreamRows, N - chunk * kStreamRows);
-        const float4* X4 = reinterpret_cast<const float4*>(stage_x(st));
-        // lane = row: eta (four independent component sums per chain), residual,
-        // log-likelihood
-        float r[CB];
-        {
-            float4 e4[CB];
+                for (int c = 0; c < CB; ++c) e4[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+                const bool live = lane < nrows;
+                if (live) {
+                    for (int f4 = 0; f4 < F4; ++f4) {
+                        const float4 x = X4[lane * F4 + f4];
 #pragma unroll
-            for (int c = 0; c < CB; ++c) e4[c] = make_float4(0.f, 0.f, 0.f, 0.f);
-            const bool live = lane < nrows;
-            if (live) {
-                for (int f4 = 0; f4 < F4; ++f4) {
-                    const float4 x = X4[lane * F4 + f4];
+                        for (int c = 0; c < CB; ++c) {
+                            const float4 t = Th4[c * F4 + f4];
+                            e4[c].x = fmaf(x.x, t.x, e4[c].x);
+                            e4[c].y = fmaf(x.y, t.y, e4[c].y);
+                            e4[c].z = fmaf(x.z, t.z, e4[c].z);
+                            e4[c].w = fmaf(x.w, t.w, e4[c].w);
+                        }
+                    }
+                }
+                const float yo = live ? st[kStreamRows * F + lane] : 0.0f;
+                float r[CB];
 #pragma unroll
-                    for (int c = 0; c < CB; ++c) {
-                        const float4 t = Th4[c * F4 + f4];
-                        e4[c].x = fmaf(x.x, t.x, e4[c].x);
-                        e4[c].y = fmaf(x.y, t.y, e4[c].y);
-                        e4[c].z = fmaf(x.z, t.z, e4[c].z);
-                        e4[c].w = fmaf(x.w, t.w, e4[c].w);
+                for (int c = 0; c < CB; ++c) {
+                    const float e = (e4[c].x + e4[c].y) + (e4[c].z + e4[c].w);
+                    const bool use = live && c < C;
+                    ll[c] += use ? bernoullilogit_logpdf(e, yo) : 0.0f;
+                    r[c] = use ? (yo - logistic(e)) : 0.0f;
+                }
+                if constexpr (CB % 4 == 0) {
+#pragma unroll
+                    for (int c4 = 0; c4 < CB / 4; ++c4)
+                        reinterpret_cast<float4*>(Rw + lane * CB)[c4] =
+                            make_float4(r[4 * c4], r[4 * c4 + 1], r[4 * c4 + 2], r[4 * c4 + 3]);
+                } else {
+#pragma unroll
+                    for (int c = 0; c < CB; ++c) Rw[lane * CB + c] = r[c];
+                }
+            }
+            __syncwarp();
+            // lane = feature group: gradient
+            if (GRAD && lane < F4) {
+                for (int rr = 0; rr < nrows; ++rr) {
+                    const float4 x = X4[rr * F4 + lane];
+                    const float* Rr = Rw + rr * CB;
+                    if constexpr (CB % 4 == 0) {
+#pragma unroll
+                        for (int c4 = 0; c4 < CB / 4; ++c4) {
+                            const float4 r = reinterpret_cast<const float4*>(Rr)[c4];
+                            const float rv[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+                            for (int u = 0; u < 4; ++u) {
+                                float4& gc = g[4 * c4 + u];
+                                gc.x = fmaf(rv[u], x.x, gc.x);
+                                gc.y = fmaf(rv[u], x.y, gc.y);
+                                gc.z = fmaf(rv[u], x.z, gc.z);
+                                gc.w = fmaf(rv[u], x.w, gc.w);
+                            }
+                        }
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < CB; ++c) {
+                            const float rv = Rr[c];
+                            g[c].x = fmaf(rv, x.x, g[c].x);
+                            g[c].y = fmaf(rv, x.y, g[c].y);
+                            g[c].z = fmaf(rv, x.z, g[c].z);
+                            g[c].w = fmaf(rv, x.w, g[c].w);
+                        }
                     }
                 }
             }
-            float e[CB];
-#pragma unroll
-            for (int c = 0; c < CB; ++c) e[c] = (e4[c].x + e4[c].y) + (e4[c].z + e4[c].w);
-            const float yo = live ? stage_y(st)[lane] : 0.0f;
-#pragma unroll
-            for (int c = 0; c < CB; ++c) {
-                const bool use = live && c < C;
-                ll[c] += use ? bernoullilogit_logpdf(e[c], yo) : 0.0f;
-                r[c] = use ? (yo - logistic(e[c])) : 0.0f;
-            }
+            __syncwarp();  // the stage and the residual rows are free again
+            if (lane == 0) mbar_arrive(empty + s);
         }
-        // lane = feature group: gradient
-        if (GRAD) {
-            for (int rr = 0; rr < nrows; ++rr) {
-                const float4 x = lane < F4 ? X4[rr * F4 + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-                for (int c = 0; c < CB; ++c) {
-                    const float rv = __shfl_sync(UT_FULL_MASK, r[c], rr);
-                    g[c].x = fmaf(rv, x.x, g[c].x);
-                    g[c].y = fmaf(rv, x.y, g[c].y);
-                    g[c].z = fmaf(rv, x.z, g[c].z);
-                    g[c].w = fmaf(rv, x.w, g[c].w);
-                }
-            }
-        }
-        __syncwarp();  // the stage is refilled by the next iteration's issue
     }
-    cp_async_wait<0>();  // (only empty groups can remain)
+    __syncthreads();  // every chunk consumed: the ring is free
 
-    // per-warp partials into the warp's area, then added in warp order
-#pragma unroll
-    for (int c = 0; c < CB; ++c) ll[c] = warp_sum(ll[c]);
-    float* mine = Wb;  // [CB] ll, then [CB][F] gradient
-    if (lane == 0) {
-#pragma unroll
-        for (int c = 0; c < CB; ++c) mine[c] = ll[c];
-    }
-    if (GRAD && lane < F4) {
+    // warp partials into the ring ([warp][CB][Wd]), then added in warp order
+    if (warp < kStreamWarps) {
+        float* mine = ring + (size_t)warp * CB * Wd;
 #pragma unroll
         for (int c = 0; c < CB; ++c) {
-            float* dst = mine + CB + c * F + 4 * lane;
-            dst[0] = g[c].x; dst[1] = g[c].y; dst[2] = g[c].z; dst[3] = g[c].w;
+            const float l = warp_sum(ll[c]);
+            if (lane == 0) mine[c * Wd] = l;
+            if (GRAD && lane < F4) {
+                float* dst = mine + c * Wd + 1 + 4 * lane;
+                dst[0] = g[c].x; dst[1] = g[c].y; dst[2] = g[c].z; dst[3] = g[c].w;
+            }
         }
     }
     __syncthreads();
-    const int s = blockIdx.x;
-    for (int c = threadIdx.x; c < C; c += blockDim.x) {
+    const int S = gridDim.x, b = blockIdx.x, CW = C * Wd;
+    for (int i = tid; i < CW; i += blockDim.x) {
         float t = 0.0f;
-        for (int w = 0; w < W; ++w) t += (sm + CB * F + w * wf)[c];
-        a.part_ll[(size_t)s * C + c] = t;
+        for (int w = 0; w < kStreamWarps; ++w) t += ring[(size_t)w * CB * Wd + i];
+        a.part[(size_t)b * CW + i] = t;
     }
-    if (GRAD) {
-        for (int i = threadIdx.x; i < C * F; i += blockDim.x) {
-            float t = 0.0f;
-            for (int w = 0; w < W; ++w) t += (sm + CB * F + w * wf)[CB + i];
-            a.part_g[(size_t)s * C * F + i] = t;
-        }
-    }
-}
 
-// Fold of the streaming kernel's S per-CTA partials, one 1024-thread CTA per
-// chain: thread (s-group g, feature f) adds partials s = g, g + G, ... (G =
-// 1024 / Fw groups, Fw = F rounded up to 32) in 4 interleaved accumulators;
-// the G group sums are then added in group order, the log-likelihood partials
-// likewise by 1024 threads and a fixed tree; the prior terms are added last
-// (glm_reduce_kernel's formulas).  Deterministic: every sum's order is fixed.
-struct GlmStreamFoldArgs {
-    const float* params;
-    const float* part_ll;  // S x C
-    const float* part_g;   // S x C x F (or null)
-    float* totals;
-    float* grads;          // C x F (or null)
-    int S, C, F, off;
-    float icpt_mu, icpt_sigma, coef_mu, coef_sigma;
-};
+    // first-level fold: the last CTA of this group adds the group's partials in CTA order
+    __threadfence();
+    __syncthreads();
+    const int grp = b / kStreamGroup, g0 = grp * kStreamGroup, g1 = min(S, g0 + kStreamGroup);
+    if (tid == 0) s_last = atomicAdd(a.tickets + grp, 1u) == (unsigned)(g1 - g0 - 1);
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    for (int i = tid; i < CW; i += blockDim.x) {
+        float t = 0.0f;
+        for (int q = g0; q < g1; ++q) t += __ldcg(a.part + (size_t)q * CW + i);
+        a.gpart[(size_t)grp * CW + i] = t;
+    }
+    __threadfence();
+    __syncthreads();
+    const int NG = (S + kStreamGroup - 1) / kStreamGroup;
+    if (tid == 0) s_last = atomicAdd(a.tickets + NG, 1u) == (unsigned)(NG - 1);
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
 
-__global__ void __launch_bounds__(1024) glm_stream_fold_kernel(GlmStreamFoldArgs a) {
-    __shared__ float part[1024];
-    const int c = blockIdx.x, tid = threadIdx.x, F = a.F, S = a.S, C = a.C;
-    const int Fw = (F + 31) / 32 * 32;
-    const int G = 1024 / Fw;
-    float l = 0.0f;
-    for (int s = tid; s < S; s += 1024) l += a.part_ll[(size_t)s * C + c];
-    part[tid] = l;
-    __syncthreads();
-    for (int w = 512; w > 0; w >>= 1) {
-        if (tid < w) part[tid] += part[tid + w];
-        __syncthreads();
+    // second level (one CTA): group partials in group order, then the priors
+    float* V = ring;  // [C][Wd]
+    for (int i = tid; i < CW; i += blockDim.x) {
+        float t = 0.0f;
+        for (int q = 0; q < NG; ++q) t += __ldcg(a.gpart + (size_t)q * CW + i);
+        V[i] = t;
     }
-    const float ll = part[0];
     __syncthreads();
-    const int g = tid / Fw, f = tid % Fw;
-    float gs = 0.0f;
-    if (a.grads && g < G && f < F) {
-        float acc[4] = {0.f, 0.f, 0.f, 0.f};
-        int s = g;
-        for (; s + 3 * G < S; s += 4 * G) {
-#pragma unroll
-            for (int u = 0; u < 4; ++u) acc[u] += a.part_g[((size_t)(s + u * G) * C + c) * F + f];
+    for (int c = warp; c < C; c += blockDim.x >> 5) {
+        float prior = 0.0f;
+        for (int f = lane; f < F; f += 32) {
+            const float th = Th[c * F + f];
+            const bool icpt = a.off && f == 0;
+            const float mu = icpt ? a.icpt_mu : a.coef_mu, sg = icpt ? a.icpt_sigma : a.coef_sigma;
+            prior += normal_logpdf(mu, sg, th);
+            if (GRAD) a.grads[(size_t)c * F + f] = V[c * Wd + 1 + f] - (th - mu) / (sg * sg);
         }
-        for (int u = 0; s < S; s += G, ++u) acc[u] += a.part_g[((size_t)s * C + c) * F + f];
-        gs = (acc[0] + acc[1]) + (acc[2] + acc[3]);
+        prior = warp_sum(prior);
+        if (lane == 0) a.totals[c] = V[c * Wd] + prior;
     }
-    if (g < G) part[g * Fw + f] = gs;
-    __syncthreads();
-    float prior = 0.0f;
-    if (tid < F) {
-        const float th = a.params[(size_t)c * F + tid];
-        const bool icpt = a.off && tid == 0;
-        const float mu = icpt ? a.icpt_mu : a.coef_mu, sg = icpt ? a.icpt_sigma : a.coef_sigma;
-        prior = normal_logpdf(mu, sg, th);
-        if (a.grads) {
-            float gsum = 0.0f;
-            for (int h = 0; h < G; ++h) gsum += part[h * Fw + tid];
-            a.grads[(size_t)c * F + tid] = gsum - (th - mu) / (sg * sg);
-        }
-    }
-    __syncthreads();
-    part[tid] = prior;  // priors: a fixed tree over the feature threads
-    __syncthreads();
-    for (int w = 512; w > 0; w >>= 1) {
-        if (tid < w) part[tid] += part[tid + w];
-        __syncthreads();
-    }
-    if (tid == 0) a.totals[c] = ll + part[0];
+    // every CTA has taken its tickets: reset them for the next launch
+    for (int i = tid; i <= NG; i += blockDim.x) a.tickets[i] = 0u;
 }
 
 }  // namespace ut

@@ -105,7 +105,8 @@ class DeviceBatchedWorkspace:
         self.batch_size = int(num_chains)
 
     def kernel_path(self) -> str:
-        """'warp' (one warp per chain), 'tiled' (CUDA-core GEMM tiles) or 'tensor_core' (tcgen05 3xTF32)."""
+        """'warp' (one warp per chain), 'tiled' (CUDA-core GEMM tiles), 'tensor_core' (tcgen05 3xTF32) or
+        'stream' (few chains: the HBM-streaming kernel)."""
         return {1: "warp", 2: "tiled", 3: "tensor_core", 4: "stream"}.get(self.lib.ut_workspace_path(self.handle),
                                                                              "unknown")
 
@@ -114,7 +115,7 @@ class DeviceBatchedWorkspace:
 
     def launches_per_gradient(self) -> int:
         """Kernels one logjoint+gradient call launches (the bench's launch count)."""
-        return {"warp": 1, "tiled": 2, "tensor_core": 3, "stream": 2}[self.kernel_path()]
+        return {"warp": 1, "tiled": 2, "tensor_core": 3, "stream": 1}[self.kernel_path()]
 
     def check(self):
         """Synchronise and raise if a bounded in-kernel wait gave up."""
