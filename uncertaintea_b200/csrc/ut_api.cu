@@ -86,7 +86,7 @@ struct ut_workspace {
     TcGlmPlan tc;
     // streaming path (GLM, few chains)
     bool streaming = false;
-    int stream_cb = 16, stream_splits = 0, stream_stages = 2;
+    int stream_cb = 16, stream_splits = 0, stream_stages = 2, stream_slots = 1;
     size_t stream_smem = 0;
     float* d_ypad = nullptr;        // y rounded up to whole 32-row chunks, zero padded
     float* d_spart = nullptr;       // per-CTA partials
@@ -285,7 +285,7 @@ int32_t launch_stream(ut_workspace* ws, const float* params, float* totals, floa
     a.Xa = ws->d_Xa; a.ypad = ws->d_ypad; a.params = params;
     a.part = ws->d_spart; a.gpart = ws->d_sgpart; a.tickets = ws->d_stickets; a.err = ws->d_serr;
     a.totals = totals; a.grads = grads;
-    a.N = ws->N; a.F = ws->P; a.C = ws->C; a.stages = ws->stream_stages; a.off = ws->plan.has_intercept;
+    a.N = ws->N; a.F = ws->P; a.C = ws->C; a.stages = ws->stream_stages; a.slots = ws->stream_slots; a.off = ws->plan.has_intercept;
     a.icpt_mu = (float)ws->plan.intercept_mu; a.icpt_sigma = (float)ws->plan.intercept_sigma;
     a.coef_mu = (float)ws->plan.coef_mu; a.coef_sigma = (float)ws->plan.coef_sigma;
     const size_t smem = ws->stream_smem;
@@ -498,12 +498,10 @@ int32_t ut_workspace_create(const ut_plan_desc* plan, const float* observed, int
                 int optin = 0;
                 cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ws->device);
                 const int chunks = (N + kStreamRows - 1) / kStreamRows;
-                const int per_cta = (chunks + dev_sms - 1) / dev_sms;
-                ws->stream_stages = glm_stream_stages(ws->stream_cb, F, (size_t)std::max(0, optin - 1024), per_cta);
+                if (!glm_stream_plan(ws->stream_cb, F, (size_t)std::max(0, optin - 1024), &ws->stream_stages,
+                                     &ws->stream_slots))
+                    return bail(fail(UT_ERR_UNSUPPORTED, "streaming kernel: shared memory too small"));
                 ws->stream_smem = glm_stream_smem(ws->stream_cb, F, ws->stream_stages);
-                if (ws->stream_smem + 1024 > (size_t)optin)
-                    return bail(fail(UT_ERR_UNSUPPORTED, "streaming kernel needs %zu bytes of shared memory",
-                                     ws->stream_smem));
                 const int groups = glm_stream_groups(ws->stream_splits);
                 const size_t ypad = (size_t)chunks * kStreamRows;
                 if ((rc = dalloc(ws, &ws->d_ypad, ypad))) return bail(rc);
