@@ -51,12 +51,20 @@ extern "C" {
  * y_ij ~ normal(mu + tau * z_j, sigma_j).  Semantics of the reference's
  * `reparam=:noncentered` iid latent (docs/noncentered-reparam.md:22-36). */
 #define UT_FAMILY_HIER_NORMAL_NONCENTERED    2
+/* Normal location/scale with a gamma scale: mu ~ normal(mu_loc, mu_scale),
+ * s ~ gamma(scale_shape, scale_rate) (log transform, log|J| = log s),
+ * y_i ~ normal(mu, s) for i = 1..N.  The reference's device-lowerable
+ * gaussian model (DeviceNormalChoiceStep + DeviceGammaChoiceStep + a
+ * DeviceLoopStep of normal observations, src/device/plan/steps.jl:6-44,
+ * 445-449; scored at src/device/logjoint_kernel.jl:105-111, 146-151). */
+#define UT_FAMILY_NORMAL_LOCATION_SCALE      3
 
 /* Fixed kernel description: what the host lowers a model's execution plan to
  * (reference: DeviceExecutionPlan, src/device/plan/steps.jl:482-489, produced
  * by _lower_device_plan, src/device/plan/lowering.jl:1360).  Parameter rows:
  *   GLM : [intercept (if has_intercept)] then num_coefs coefficients;
- *   HIER: [mu, log(tau), z_1 .. z_J]. */
+ *   HIER: [mu, log(tau), z_1 .. z_J];
+ *   NLS : [mu, log(s)]. */
 typedef struct ut_plan_desc {
     int32_t family;          /* UT_FAMILY_*                                   */
     int32_t num_params;      /* P, unconstrained parameter count              */
@@ -71,6 +79,8 @@ typedef struct ut_plan_desc {
     double mu_loc;           /* HIER: mu ~ normal(mu_loc, mu_scale)           */
     double mu_scale;
     double tau_scale;        /* HIER: tau ~ halfcauchy(tau_scale)             */
+    double scale_shape;      /* NLS: s ~ gamma(scale_shape, scale_rate)       */
+    double scale_rate;       /*      (mu uses mu_loc / mu_scale)              */
 } ut_plan_desc;
 
 typedef struct ut_workspace ut_workspace;
@@ -97,7 +107,8 @@ int32_t ut_lowering_report(const ut_plan_desc* plan, char* issues, size_t len);
  *   GLM : observed_rows = N*(D+1): per observation the D covariates then y;
  *   HIER: observed_rows = N + J:  the N y values group after group, then the
  *         J fixed sigma_j; trip_counts[j] = n_j and loop_starts[j] = first row
- *         of group j (num_loops = J).
+ *         of group j (num_loops = J);
+ *   NLS : observed_rows = N: the y values (no loops are passed).
  * precision_bits must be 32 (Float32); anything else is UT_ERR_PRECISION. */
 int32_t ut_workspace_create(const ut_plan_desc* plan,
                             const float* observed, int64_t observed_rows, int64_t observed_cols,

@@ -120,6 +120,13 @@ template <class T> inline T bernoullilogit_logpdf(T eta, T x) {  // math.jl:212-
     return in_support ? base : -std::numeric_limits<T>::infinity();
 }
 template <class T> inline T logistic(T eta) { return std::exp(-log1p_exp(-eta)); }  // math.jl:224
+// math.jl:103-107 (support: a positive normal float, math.jl:66); the
+// normaliser uses the C library's lgamma in double, where the reference's
+// device code uses its own Lanczos loggamma (math.jl:30-50).
+template <class T> inline T gamma_logpdf(T shape, T rate, T x) {
+    T base = shape * std::log(rate) - (T)std::lgamma((double)shape) + (shape - T(1)) * std::log(x) - rate * x;
+    return x >= std::numeric_limits<T>::min() ? base : -std::numeric_limits<T>::infinity();
+}
 
 // ---------------------------------------------------------------------------
 // Models: unconstrained logjoint + analytic gradient of one chain.
@@ -145,6 +152,8 @@ ModelData make_model(const ut_plan_desc* plan, const float* observed, const int3
             for (int d = 0; d < D; ++d) m.X[(size_t)i * D + d] = observed[(size_t)i * (D + 1) + d];
             m.y[i] = observed[(size_t)i * (D + 1) + D];
         }
+    } else if (plan->family == UT_FAMILY_NORMAL_LOCATION_SCALE) {
+        m.y.assign(observed, observed + N);
     } else {
         const int J = plan->num_groups;
         m.y.assign(observed, observed + N);
@@ -227,9 +236,35 @@ W hier_logjoint_grad(const ModelData& m, const T* q, T* g) {
     return total;
 }
 
+// Normal location/scale (steps: Normal on mu, Gamma on s with log transform,
+// lad = u (math.jl:1144-1146), then the loop of normal observations;
+// logjoint_kernel.jl:105-111, 146-151).  Every observation term is scored
+// separately, in order.
+template <class T, class W>
+W gauss_logjoint_grad(const ModelData& m, const T* q, T* g) {
+    const ut_plan_desc& p = m.plan;
+    const int N = p.num_obs;
+    T mu = q[0], u = q[1];
+    T s = std::exp(u);
+    W total = (W)normal_logpdf<T>(T(p.mu_loc), T(p.mu_scale), mu);
+    total += (W)gamma_logpdf<T>(T(p.scale_shape), T(p.scale_rate), s) + (W)u;
+    W gmu = -(W)(mu - T(p.mu_loc)) / ((W)p.mu_scale * (W)p.mu_scale);
+    W gu = (W)p.scale_shape - (W)p.scale_rate * (W)s;  // gamma prior + lad, d/du
+    for (int i = 0; i < N; ++i) {
+        T yv = (T)m.y[i];
+        total += (W)normal_logpdf<T>(mu, s, yv);
+        W r = (W)yv - (W)mu;
+        gmu += r / ((W)s * (W)s);
+        gu += r * r / ((W)s * (W)s) - W(1);
+    }
+    if (g) { g[0] = (T)gmu; g[1] = (T)gu; }
+    return total;
+}
+
 template <class T, class W>
 W logjoint_grad(const ModelData& m, const T* q, T* g) {
     if (m.plan.family == UT_FAMILY_GLM_BERNOULLI_LOGIT) return glm_logjoint_grad<T, W>(m, q, g);
+    if (m.plan.family == UT_FAMILY_NORMAL_LOCATION_SCALE) return gauss_logjoint_grad<T, W>(m, q, g);
     return hier_logjoint_grad<T, W>(m, q, g);
 }
 

@@ -19,8 +19,8 @@ import pytest
 
 import oracle
 from uncertaintea_b200 import _native as nat
-from uncertaintea_b200.models import (BernoulliLogitGLM, HierarchicalNormalNoncentered, hierarchical_data,
-                                      logistic_regression_data)
+from uncertaintea_b200.models import (BernoulliLogitGLM, HierarchicalNormalNoncentered, NormalLocationScale,
+                                      gauss_data, hierarchical_data, logistic_regression_data)
 
 pytestmark = pytest.mark.gpu
 
@@ -127,6 +127,26 @@ def test_hier_density_vs_fp64_oracle(lib, J, n, C):
     ws.close()
 
 
+@pytest.mark.parametrize("n,C", [(5, 4), (1000, 300), (20000, 37), (0, 8)])
+def test_gauss_density_vs_fp64_oracle(lib, n, C):
+    """The normal location/scale family (the reference's gaussian device model);
+    n = 5, C = 4 is the reference's own parity case (device_lowering_parity.jl:131-134)."""
+    if n == 5:
+        y = np.array([0.4, -0.7, 1.1, 0.2, 0.9], dtype=np.float32)
+        q = np.array([[0.5, 0.1], [-0.3, 0.7], [1.2, -0.2], [0.05, 0.4]], dtype=np.float32)
+    else:
+        y, _ = gauss_data(n, 9)
+        q = (np.random.default_rng(5).standard_normal((C, 2)) * 0.6).astype(np.float32)
+    m = NormalLocationScale()
+    ws = _ws(m, (n,), {"y": y}, C)
+    assert ws.kernel_path() == "warp"
+    t, g = ws.logjoint_gradient(q.T)
+    t64, g64 = oracle.OracleModel(ws.lowered).logjoint_gradient_f64(q.astype(np.float64))
+    assert _lj_err(t, t64) <= 1e-5
+    assert _grad_err(np.asarray(g.T), g64) <= 1e-5
+    ws.close()
+
+
 def test_hier_ragged_groups_with_empty_group(lib):
     J = 6
     sizes = np.array([3, 0, 9, 1, 0, 4])
@@ -204,7 +224,16 @@ def _glm_mode(X, y, sigma=1.0, iters=25):
     return b
 
 
-@pytest.mark.parametrize("case", ["glm_c1", "glm_tiled", "hier"])
+def _gauss_near_mode(n, C, seed, spread):
+    y, _ = gauss_data(n, 3)
+    r = np.random.default_rng(seed)
+    q = np.empty((C, 2), dtype=np.float32)
+    q[:, 0] = y.mean() + spread * r.standard_normal(C)
+    q[:, 1] = np.log(y.std()) + spread * r.standard_normal(C)
+    return NormalLocationScale(), (n,), {"y": y}, q
+
+
+@pytest.mark.parametrize("case", ["glm_c1", "glm_tiled", "hier", "gauss"])
 def test_hmc_iteration_vs_oracle(lib, case):
     """One HMC iteration from near-posterior states with stable step sizes:
     the same Philox momenta and accept uniforms on both sides."""
@@ -230,6 +259,9 @@ def test_hmc_iteration_vs_oracle(lib, case):
         q[:, 1] = np.log(tau0) + 0.02 * r.standard_normal(256)
         q[:, 2:] = (ybar - mu0) / tau0 + 0.02 * r.standard_normal((256, 64))
         step, L = 0.004, 6
+    if case == "gauss":
+        m, args, cons, q = _gauss_near_mode(200, 256, 3, 0.05)
+        step, L = 0.05, 8
     C, P = q.shape
     ws = _ws(m, args, cons, C)
     qd, g, t = _state(ws, q)
@@ -291,9 +323,12 @@ def _nuts_gpu(ws, qd, g, t, im, step, depth, coord):
     return res
 
 
-@pytest.mark.parametrize("case", ["hier", "glm"])
+@pytest.mark.parametrize("case", ["hier", "glm", "gauss"])
 def test_persistent_nuts_iteration_vs_oracle(lib, case):
-    if case == "hier":
+    if case == "gauss":
+        m, args, cons, q = _gauss_near_mode(200, 128, 8, 0.1)
+        step = 0.1
+    elif case == "hier":
         y, sig, sizes, _ = hierarchical_data(64, 20, 7)
         m, args, cons = HierarchicalNormalNoncentered(64), (sig, sizes), {"y": y}
         q = (np.random.default_rng(8).standard_normal((128, 66)) * 0.5).astype(np.float32)
@@ -466,11 +501,14 @@ def _nuts_call(fn, ws, qd, g, t, im, step, depth, coord):
     return res
 
 
-@pytest.mark.parametrize("case", ["glm", "hier"])
+@pytest.mark.parametrize("case", ["glm", "hier", "gauss"])
 def test_lockstep_nuts_matches_persistent_bitwise(lib, case):
     """Where both strategies apply (a per-chain evaluator), the lockstep tree and
     the persistent tree are the same computation: identical states and outputs."""
-    if case == "glm":
+    if case == "gauss":
+        m, args, cons, q = _gauss_near_mode(200, 64, 9, 0.3)
+        step = 0.1
+    elif case == "glm":
         m, args, cons, q = _glm_case(1000, 10, 96, False, 1)
         q *= 0.3
         step = 0.08

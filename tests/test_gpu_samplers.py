@@ -12,8 +12,9 @@ instead, with the reason stated at the assertion."""
 import numpy as np
 import pytest
 
-from uncertaintea_b200 import (BernoulliLogitGLM, HierarchicalNormalNoncentered, batched_chees, batched_hmc,
-                               batched_nuts, ess, hierarchical_data, logistic_regression_data, rhat)
+from uncertaintea_b200 import (BernoulliLogitGLM, HierarchicalNormalNoncentered, NormalLocationScale, batched_chees,
+                               batched_hmc, batched_nuts, ess, gauss_data, hierarchical_data,
+                               logistic_regression_data, rhat)
 
 pytestmark = pytest.mark.gpu
 
@@ -120,6 +121,38 @@ def test_hierarchical_nuts_informative_groups(lib):
     mean, mcse = _mean_mcse(res)
     assert abs(mean[0] - mu_ex) <= 5 * mcse[0], (mean[0], mu_ex, mcse[0])
     assert abs(mean[1] - tau_ex) <= 5 * mcse[1], (mean[1], tau_ex, mcse[1])
+
+
+def _exact_gauss_moments(y, mu_loc=0.0, mu_scale=1.0, shape=2.0, rate=1.0):
+    """Posterior means of mu and s of the normal location/scale model on a fine
+    2-D grid over (mu, log s)."""
+    y = y.astype(np.float64)
+    n, ybar, sd = len(y), y.mean(), y.std()
+    mu = np.linspace(ybar - 8 * sd / np.sqrt(n) - 1, ybar + 8 * sd / np.sqrt(n) + 1, 1201)[:, None]
+    ls = np.linspace(np.log(sd) - 1.5, np.log(sd) + 1.5, 1201)[None, :]
+    s = np.exp(ls)
+    ss = n * (sd ** 2 + (ybar - mu) ** 2)   # sum_i (y_i - mu)^2
+    lp = -0.5 * ((mu - mu_loc) / mu_scale) ** 2 + (shape - 1) * ls - rate * s + ls - n * ls - 0.5 * ss / s ** 2
+    w = np.exp(lp - lp.max())
+    w /= w.sum()
+    return float((w * mu).sum()), float((w * s).sum())
+
+
+@pytest.mark.parametrize("strategy", ["persistent", "masked"])
+def test_gauss_nuts_matches_exact_posterior(lib, strategy):
+    """The normal location/scale family (the reference's gaussian scaling model)
+    under both device NUTS strategies: R-hat < 1.01 and posterior means of mu and
+    s within 5 Monte-Carlo standard errors of the grid-integrated posterior."""
+    y, _ = gauss_data(50, 13)
+    m = NormalLocationScale()
+    res = batched_nuts(m, (50,), {"y": y}, num_chains=512, num_samples=400, num_warmup=400,
+                       tree_strategy=strategy, rng=np.random.default_rng(3))
+    assert np.max(rhat(res)) < 1.01, rhat(res)
+    assert res.divergent.mean() < 0.01
+    mu_ex, s_ex = _exact_gauss_moments(y)
+    mean, mcse = _mean_mcse(res)
+    assert abs(mean[0] - mu_ex) <= 5 * mcse[0], (mean[0], mu_ex, mcse[0])
+    assert abs(mean[1] - s_ex) <= 5 * mcse[1], (mean[1], s_ex, mcse[1])
 
 
 def test_seed_reproducibility(lib):

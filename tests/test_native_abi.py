@@ -62,6 +62,13 @@ def test_lowering_report_flags_bad_descriptions(lib):
                         mu_scale=5.0, tau_scale=-1.0)
     assert lib.ut_lowering_report(ctypes.byref(hier), buf, len(buf)) == nat.UT_ERR_UNSUPPORTED
     assert b"tau prior scale" in buf.value
+    gauss = nat.PlanDesc(family=nat.UT_FAMILY_NORMAL_LOCATION_SCALE, num_params=2, num_obs=5, mu_scale=1.0,
+                         scale_shape=2.0, scale_rate=1.0)
+    assert lib.ut_lowering_report(ctypes.byref(gauss), buf, len(buf)) == nat.UT_OK
+    gauss.scale_rate = 0.0
+    gauss.num_params = 3
+    assert lib.ut_lowering_report(ctypes.byref(gauss), buf, len(buf)) == nat.UT_ERR_UNSUPPORTED
+    assert b"num_params must equal 2" in buf.value and b"gamma shape and rate" in buf.value
 
 
 def test_workspace_create_validates_before_touching_device(lib):

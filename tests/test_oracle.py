@@ -4,8 +4,8 @@ import numpy as np
 import pytest
 
 import oracle
-from uncertaintea_b200.models import (BernoulliLogitGLM, HierarchicalNormalNoncentered, hierarchical_data,
-                                      logistic_regression_data)
+from uncertaintea_b200.models import (BernoulliLogitGLM, HierarchicalNormalNoncentered, NormalLocationScale,
+                                      gauss_data, hierarchical_data, logistic_regression_data)
 
 
 def test_philox_kat_vectors(pins):
@@ -125,6 +125,57 @@ def test_hier_oracle_matches_direct_density():
     for j in range(5):
         ref += stats.norm(mu + tau * z[j], sig[j]).logpdf(y[starts[j]:starts[j] + sizes[j]].astype(np.float64)).sum()
     assert abs(t[0] - ref) < 1e-6 * abs(ref)
+
+
+# The reference's device-parity case for its gaussian model
+# (test/uncertaintea/core/device_lowering_parity.jl:131-134): five observations
+# and four chains of unconstrained (mu, log s).  The reference compares the
+# device value with its own CPU evaluator; here the oracle is pinned to the
+# closed-form density (scipy) in float64.
+GAUSS_YS = [0.4, -0.7, 1.1, 0.2, 0.9]
+GAUSS_PARAMS = [[0.5, 0.1], [-0.3, 0.7], [1.2, -0.2], [0.05, 0.4]]
+
+
+def test_gauss_oracle_on_the_reference_parity_case():
+    from scipy import stats
+    m = NormalLocationScale()
+    om = oracle.OracleModel(m.lower((5,), {"y": np.array(GAUSS_YS)}))
+    q = np.array(GAUSS_PARAMS)
+    t, g = om.logjoint_gradient_f64(q)
+    y = np.array(GAUSS_YS, dtype=np.float32).astype(np.float64)
+    for c, (mu, u) in enumerate(GAUSS_PARAMS):
+        s = np.exp(u)
+        ref = stats.norm(0, 1).logpdf(mu) + stats.gamma(2.0, scale=1.0).logpdf(s) + u + stats.norm(mu, s).logpdf(y).sum()
+        assert abs(t[c] - ref) <= 1e-12 * abs(ref)
+        # analytic gradient of the same closed form
+        gmu = -mu + np.sum(y - mu) / s ** 2
+        gu = 2.0 - s - 5 + np.sum((y - mu) ** 2) / s ** 2
+        assert abs(g[c, 0] - gmu) <= 1e-12 * max(1.0, abs(gmu))
+        assert abs(g[c, 1] - gu) <= 1e-12 * max(1.0, abs(gu))
+
+
+def test_gauss_oracle_finite_differences_and_support():
+    y, _ = gauss_data(40, 3)
+    m = NormalLocationScale(mu_loc=0.5, mu_scale=2.0, shape=3.0, rate=2.0)
+    om = oracle.OracleModel(m.lower((40,), {"y": y}))
+    q = np.random.default_rng(4).standard_normal((3, 2)) * 0.8
+    _, g = om.logjoint_gradient_f64(q)
+    h = 1e-6
+    for c in range(3):
+        for p in range(2):
+            qp, qm = q.copy(), q.copy()
+            qp[c, p] += h
+            qm[c, p] -= h
+            fd = (om.logjoint_gradient_f64(qp)[0][c] - om.logjoint_gradient_f64(qm)[0][c]) / (2 * h)
+            assert abs(fd - g[c, p]) <= 1e-5 * max(1.0, abs(g[c, p]))
+    # s = exp(u) below the smallest normal double: outside the gamma support
+    # (-Inf without observations; with observations the normal terms at s = 0
+    # make it NaN, as the reference's normal density does: math.jl:88-91)
+    empty = oracle.OracleModel(m.lower((0,), {"y": np.zeros(0)}))
+    t, _ = empty.logjoint_gradient_f64(np.array([[0.0, -800.0]]))
+    assert t[0] == -np.inf
+    t, _ = om.logjoint_gradient_f64(np.array([[0.0, -800.0]]))
+    assert not np.isfinite(t[0])
 
 
 def test_oracle_hmc_reversibility():

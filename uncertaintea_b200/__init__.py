@@ -7,8 +7,8 @@ ChEES-HMC, the Philox4x32-10 stream and the R-hat / ESS diagnostics; plus
 the learned gradient surrogate for ChEES-HMC and many-model batched NUTS
 (no reference counterparts).
 """
-from .models import (BernoulliLogitGLM, HierarchicalNormalNoncentered, TeaModelSpec, hierarchical_data,
-                     logistic_regression_data)
+from .models import (BernoulliLogitGLM, HierarchicalNormalNoncentered, NormalLocationScale, TeaModelSpec,
+                     gauss_data, hierarchical_data, logistic_regression_data)
 from .device import (DeviceBatchedWorkspace, device_batched_logjoint, device_batched_logjoint_,
                      device_batched_logjoint_gradient, device_batched_logjoint_gradient_, device_lowering_report)
 from .inference import HMCChains, batched_chees, batched_hmc, batched_nuts, posterior_array
@@ -18,7 +18,8 @@ from .multi import MultiChains, MultiModelBatch, batched_nuts_multi
 from . import rng
 
 __all__ = [
-    "BernoulliLogitGLM", "HierarchicalNormalNoncentered", "TeaModelSpec", "hierarchical_data",
+    "BernoulliLogitGLM", "HierarchicalNormalNoncentered", "NormalLocationScale", "TeaModelSpec", "gauss_data",
+    "hierarchical_data",
     "logistic_regression_data", "DeviceBatchedWorkspace", "device_batched_logjoint", "device_batched_logjoint_",
     "device_batched_logjoint_gradient", "device_batched_logjoint_gradient_", "device_lowering_report", "HMCChains",
     "batched_chees", "batched_hmc", "batched_nuts", "posterior_array", "ess", "min_ess_per_second", "rhat",

@@ -24,6 +24,7 @@ UT_ERR_DEVICE_TIMEOUT = 7
 
 UT_FAMILY_GLM_BERNOULLI_LOGIT = 1
 UT_FAMILY_HIER_NORMAL_NONCENTERED = 2
+UT_FAMILY_NORMAL_LOCATION_SCALE = 3
 
 
 class PlanDesc(ctypes.Structure):
@@ -41,6 +42,8 @@ class PlanDesc(ctypes.Structure):
         ("mu_loc", c_double),
         ("mu_scale", c_double),
         ("tau_scale", c_double),
+        ("scale_shape", c_double),
+        ("scale_rate", c_double),
     ]
 
 

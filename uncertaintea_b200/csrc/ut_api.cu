@@ -9,6 +9,7 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <cmath>
 
 #include "../../include/ut_b200.h"
 #include "ut_warp_kernels.cuh"
@@ -156,6 +157,11 @@ std::string plan_issues(const ut_plan_desc* p) {
         if (!(p->mu_scale > 0.0)) add("mu prior scale must be > 0");
         if (!(p->tau_scale > 0.0)) add("tau prior scale must be > 0");
         if (p->num_obs < 0) add("num_obs must be >= 0");
+    } else if (p->family == UT_FAMILY_NORMAL_LOCATION_SCALE) {
+        if (p->num_params != 2) add("num_params must equal 2 (mu, log s)");
+        if (!(p->mu_scale > 0.0)) add("mu prior scale must be > 0");
+        if (!(p->scale_shape > 0.0) || !(p->scale_rate > 0.0)) add("gamma shape and rate must be > 0");
+        if (p->num_obs < 0) add("num_obs must be >= 0");
     } else {
         char b[96];
         snprintf(b, sizeof(b), "unsupported kernel-description family %d", p->family);
@@ -182,6 +188,8 @@ int32_t need_device() {
             if ((ws)->K == 1 && (ws)->dmax == 16) { KERNEL(kFamGlm, 1, 16, __VA_ARGS__); }                   \
             else if ((ws)->K == 1) { KERNEL(kFamGlm, 1, 32, __VA_ARGS__); }                                  \
             else { KERNEL(kFamGlm, 2, 32, __VA_ARGS__); }                                                   \
+        } else if ((ws)->dm.family == kFamGauss) {                                                           \
+            KERNEL(kFamGauss, 1, 1, __VA_ARGS__);                                                            \
         } else {                                                                                             \
             switch ((ws)->K) {                                                                               \
                 case 1: KERNEL(kFamHier, 1, 1, __VA_ARGS__); break;                                          \
@@ -404,6 +412,10 @@ int32_t ut_workspace_create(const ut_plan_desc* plan, const float* observed, int
         if (observed_rows != want)
             return fail(UT_ERR_DIMENSION, "expected %lld staged observation rows (N*(D+1)), got %lld", (long long)want,
                         (long long)observed_rows);
+    } else if (plan->family == UT_FAMILY_NORMAL_LOCATION_SCALE) {
+        if (observed_rows != N)
+            return fail(UT_ERR_DIMENSION, "expected %d staged observation rows (N), got %lld", N,
+                        (long long)observed_rows);
     } else {
         int64_t want = (int64_t)N + plan->num_groups;
         if (observed_rows != want)
@@ -519,6 +531,18 @@ int32_t ut_workspace_create(const ut_plan_desc* plan, const float* observed, int
                 return bail(fail(UT_ERR_CUDA, "tensor-core GLM setup failed: %s", tc_glm_last_error()));
             }
         }
+    } else if (plan->family == UT_FAMILY_NORMAL_LOCATION_SCALE) {
+        dm.family = kFamGauss;
+        dm.gauss.N = N;
+        dm.gauss.mu_loc = (float)plan->mu_loc; dm.gauss.mu_scale = (float)plan->mu_scale;
+        dm.gauss.shape = (float)plan->scale_shape; dm.gauss.rate = (float)plan->scale_rate;
+        dm.gauss.lgc = (float)(plan->scale_shape * std::log(plan->scale_rate) - std::lgamma(plan->scale_shape));
+        if ((rc = dalloc(ws, &ws->d_y, std::max(N, 1)))) return bail(rc);
+        if (N > 0) UT_CUDA(cudaMemcpy(ws->d_y, observed, sizeof(float) * N, cudaMemcpyHostToDevice));
+        dm.gauss.y = ws->d_y;
+        ws->path = kPathWarp;
+        dm.stage = ((size_t)N * 4 + (size_t)kWarpsDensity * dm.Ppad * 4) <= kSmemBudget ? 1 : 0;
+        dm.staged_floats = dm.stage ? ((N + 3) / 4) * 4 : 0;
     } else {
         const int J = plan->num_groups;
         dm.family = kFamHier;

@@ -8,6 +8,8 @@
 // sums and control flow that depends on them stays warp-uniform).
 #pragma once
 
+#include <cfloat>
+
 #include "ut_common.cuh"
 
 namespace ut {
@@ -34,6 +36,16 @@ struct HierModel {
     const float* sig;      // J
     const int32_t* start;  // J
     const int32_t* count;  // J
+};
+
+// Normal location/scale with a gamma scale (reference gaussian device model:
+// Normal + Gamma(log transform) choice steps and a loop of normal observations,
+// logjoint_kernel.jl:105-111, 146-151; gamma density math.jl:103-107).
+// lgc = shape * log(rate) - loggamma(shape), a constant the host computes.
+struct GaussModel {
+    int N;
+    float mu_loc, mu_scale, shape, rate, lgc;
+    const float* y;  // N
 };
 
 // Parameters in per-warp shared memory so every lane can read any coefficient
@@ -162,6 +174,41 @@ __device__ __forceinline__ float hier_lj_grad(const HierModel& m, int P, const f
         }
     }
     return total;
+}
+
+// Two parameters: lane 0 holds mu, lane 1 holds u = log s.  The observation
+// loop accumulates sum (y - mu) and sum (y - mu)^2 over the warp's lanes:
+//   sum_i normal_logpdf(mu, s, y_i) = N (-log s - log(2 pi) / 2) - sq / (2 s^2),
+//   d/dmu = sum (y - mu) / s^2,   d/du = -N + sq / s^2 (chain rule ds/du = s);
+// the gamma prior on s with log|J| = u adds (shape - 1) u - rate s + u + lgc,
+// d/du = shape - rate s; -Inf when s is not a positive normal float (math.jl:66).
+template <int K>
+__device__ __forceinline__ float gauss_lj_grad(const GaussModel& m, const float (&q)[K], float (&g)[K],
+                                               bool want_grad) {
+    const int lane = threadIdx.x & 31;
+    const float mu = __shfl_sync(UT_FULL_MASK, q[0], 0);
+    const float u = __shfl_sync(UT_FULL_MASK, q[0], 1);
+    const float s = expf(u);
+    float sr = 0.0f, sq = 0.0f;
+    for (int i = lane; i < m.N; i += 32) {
+        const float r = m.y[i] - mu;
+        sr += r;
+        sq = fmaf(r, r, sq);
+    }
+    sr = warp_sum(sr);
+    sq = warp_sum(sq);
+    const float inv_s = 1.0f / s;
+    const float nf = (float)m.N;
+    float lj = nf * (-u - kHalfLog2Pi) - 0.5f * sq * inv_s * inv_s;
+    lj += normal_logpdf(m.mu_loc, m.mu_scale, mu);
+    lj += s >= FLT_MIN ? m.lgc + (m.shape - 1.0f) * u - m.rate * s + u : -INFINITY;
+    if (want_grad) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) g[k] = 0.0f;
+        if (lane == 0) g[0] = sr * inv_s * inv_s - (mu - m.mu_loc) / (m.mu_scale * m.mu_scale);
+        if (lane == 1) g[0] = -nf + sq * inv_s * inv_s + m.shape - m.rate * s;
+    }
+    return lj;
 }
 
 }  // namespace ut

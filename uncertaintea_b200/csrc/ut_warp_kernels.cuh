@@ -9,7 +9,7 @@
 
 namespace ut {
 
-enum Family : int { kFamGlm = 1, kFamHier = 2 };
+enum Family : int { kFamGlm = 1, kFamHier = 2, kFamGauss = 3 };
 
 struct DevModel {
     int family;
@@ -19,6 +19,7 @@ struct DevModel {
     int staged_floats;  // floats of staged data at the head of dynamic smem
     GlmModel glm;
     HierModel hier;
+    GaussModel gauss;
 };
 
 // Copies the model's observation data into shared memory (when dm.stage) and
@@ -38,6 +39,10 @@ __device__ __forceinline__ void stage_model(DevModel& dm, float* smem) {
         __syncthreads();
         dm.glm.XT = smem;
         dm.glm.y = ys;
+    } else if constexpr (FAM == kFamGauss) {
+        for (int i = threadIdx.x; i < dm.gauss.N; i += blockDim.x) smem[i] = dm.gauss.y[i];
+        __syncthreads();
+        dm.gauss.y = smem;
     } else {
         const int N = dm.hier.N, J = dm.hier.J;
         float* ys = smem;
@@ -62,6 +67,7 @@ template <int FAM, int K, int DMAX>
 __device__ __forceinline__ float eval_lj(const DevModel& dm, const float (&q)[K], float (&g)[K], float* qs,
                                          bool want_grad) {
     if constexpr (FAM == kFamGlm) return glm_lj_grad<K, DMAX>(dm.glm, dm.P, q, g, qs, want_grad);
+    else if constexpr (FAM == kFamGauss) return gauss_lj_grad<K>(dm.gauss, q, g, want_grad);
     else return hier_lj_grad<K>(dm.hier, dm.P, q, g, want_grad);
 }
 

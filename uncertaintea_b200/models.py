@@ -180,6 +180,59 @@ class HierarchicalNormalNoncentered(TeaModelSpec):
         return out
 
 
+@dataclass
+class NormalLocationScale(TeaModelSpec):
+    """``mu ~ normal(mu_loc, mu_scale)``, ``s ~ gamma(shape, rate)``,
+    ``y[i] ~ normal(mu, s)`` for i = 1..n -- the reference's device-lowerable
+    gaussian model (bench/crossppl/julia/models.jl:112-119,
+    test/uncertaintea/core/device_lowering_parity.jl:12-19: ``mu ~ normal(0, 1)``,
+    ``s ~ gamma(2, 1)``).
+
+    Unconstrained parameters: [mu, log(s)]; constrained: [mu, s].
+    args = (n,); constraints = {"y": y} with n observations.
+    """
+
+    mu_loc: float = 0.0
+    mu_scale: float = 1.0
+    shape: float = 2.0
+    rate: float = 1.0
+    name: str = "normal_location_scale"
+
+    def parameter_names(self, args=(), constraints=None):
+        return ["mu", "s"]
+
+    def lower(self, args=(), constraints=None) -> Lowered:
+        if len(args) != 1:
+            raise ValueError(f"{self.name} expects args=(n,), got {len(args)} argument(s)")
+        n = int(args[0])
+        if n < 0:
+            raise ValueError("n must be >= 0")
+        y = _observed_value(constraints, "y").astype(np.float32).reshape(-1)
+        if y.shape != (n,):
+            raise IndexError(f"expected {n} observations, got shape {y.shape}")
+        plan = nat.PlanDesc(
+            family=nat.UT_FAMILY_NORMAL_LOCATION_SCALE, num_params=2, num_obs=n, num_coefs=0, has_intercept=0,
+            num_groups=0, intercept_mu=0.0, intercept_sigma=1.0, coef_mu=0.0, coef_sigma=1.0,
+            mu_loc=self.mu_loc, mu_scale=self.mu_scale, tau_scale=1.0, scale_shape=self.shape,
+            scale_rate=self.rate)
+        empty = np.zeros(0, dtype=np.int32)
+        return Lowered(plan, np.ascontiguousarray(y), empty, empty, 2)
+
+    def constrain(self, unconstrained, args=(), constraints=None):
+        u = np.asarray(unconstrained)
+        out = np.array(u, dtype=np.float64, copy=True)
+        out[..., 1] = np.exp(u[..., 1])
+        return out
+
+    def initial_positions(self, rng, num_chains, args=(), constraints=None, init_strategy="prior"):
+        if init_strategy == "uniform":
+            return rng.uniform(-2.0, 2.0, size=(num_chains, 2))
+        out = np.empty((num_chains, 2))
+        out[:, 0] = rng.normal(self.mu_loc, self.mu_scale, size=num_chains)
+        out[:, 1] = np.log(np.maximum(rng.gamma(self.shape, 1.0 / self.rate, size=num_chains), 1e-30))
+        return out
+
+
 # ---- synthetic workloads (seeded stand-ins for the benchmark data sets) -----
 
 def logistic_regression_data(num_obs: int, num_coefs: int, seed: int, x_scale: float = 1.0):
@@ -203,3 +256,12 @@ def hierarchical_data(num_groups: int, group_sizes, seed: int, mu_loc=0.0, mu_sc
     theta = mu + tau * rng.standard_normal(num_groups)
     y = np.concatenate([rng.normal(theta[j], sigma[j], size=sizes[j]) for j in range(num_groups)]).astype(np.float32)
     return y, sigma, sizes, {"mu": mu, "tau": tau, "theta": theta}
+
+
+def gauss_data(num_obs: int, seed: int, mu_loc=0.0, mu_scale=1.0, shape=2.0, rate=1.0):
+    """mu ~ normal(mu_loc, mu_scale), s ~ gamma(shape, rate), y ~ normal(mu, s), seeded."""
+    rng = np.random.default_rng(seed)
+    mu = rng.normal(mu_loc, mu_scale)
+    s = rng.gamma(shape, 1.0 / rate)
+    y = rng.normal(mu, s, size=num_obs).astype(np.float32)
+    return y, {"mu": mu, "s": s}
