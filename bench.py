@@ -325,9 +325,30 @@ def hbm_sweep(chain_counts=(1, 4, 8, 16), steps=20, warmup=5):
             row[name] = {"ms": ms, "bytes": nbytes, "GB/s": gbs, "frac": gbs / hbm}
         out.append(row)
         ws.close()
+    # Yardsticks under the same flush + event method: a one-element fill (the
+    # launch + event floor of a single timed launch) and torch's own sum over a
+    # device copy of the same 40 MB design (a library read of the same bytes).
+    Xd = torch.from_numpy(np.ascontiguousarray(X)).cuda()
+    tiny = torch.empty(1, device="cuda")
+    yard = {}
+    for name, fn in (("launch_floor_one_element_fill", lambda: tiny.fill_(0.0)),
+                     ("torch_sum_of_X", lambda: Xd.sum())):
+        for _ in range(max(warmup, 3)):
+            flush.fill_(1.0)
+            fn()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for a, b in evs:
+            flush.fill_(1.0)
+            a.record(stream)
+            fn()
+            b.record(stream)
+        torch.cuda.synchronize()
+        ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
+        nbytes = 0 if name.startswith("launch") else N_OBS * N_COEF * 4
+        yard[name] = {"ms": ms, "GB/s": nbytes / (ms / 1000.0) / 1e9, "frac": nbytes / (ms / 1000.0) / 1e9 / hbm}
     return {"metric": "few-chain logjoint(+gradient) HBM roofline", "peak_GB/s": hbm,
             "peak_source": f"{kind} HBM copy bandwidth", "l2": "flushed before every timed evaluation",
-            "rows": out}
+            "rows": out, "yardsticks": yard}
 
 
 def sampler_configs():
