@@ -408,10 +408,14 @@ def surrogate_comparison(num_chains=4096, num_warmup=500, num_samples=500):
     steps, trajectory length and step size adapted in warmup).  The surrogate
     is trained on 2^20 (theta, gradient) pairs of the last 256 warmup
     iterations.  Min ESS over the 100 coefficients per second of sampling
-    (warmup, training and step-size re-tuning excluded, reported apart)."""
+    (warmup, training and step-size re-tuning excluded, reported apart).
+    Both arms adapt the trajectory length with the forward endpoint velocity
+    (an ascent on the ChEES criterion); the reference's own estimator descends
+    it and on this workload can collapse T to the step size."""
     from uncertaintea_b200 import batched_chees, batched_chees_surrogate, ess, rhat
     model, X, y, _ = _data()
-    kw = dict(num_chains=num_chains, num_samples=num_samples, num_warmup=num_warmup, num_leapfrog_steps=16, rng=1)
+    kw = dict(num_chains=num_chains, num_samples=num_samples, num_warmup=num_warmup, num_leapfrog_steps=16, rng=1,
+              trajectory_velocity="forward")
     out = {}
     runs = {"plain": batched_chees(model, (X,), {"y": y}, **kw),
             "surrogate": batched_chees_surrogate(model, (X,), {"y": y}, **kw)}

@@ -155,6 +155,27 @@ def test_gauss_nuts_matches_exact_posterior(lib, strategy):
     assert abs(mean[1] - s_ex) <= 5 * mcse[1], (mean[1], s_ex, mcse[1])
 
 
+def test_chees_forward_velocity_adapts_trajectory(lib):
+    """trajectory_velocity="forward" (the ChEES criterion's own derivative): T
+    settles to a finite value with a stable tail (the reference's gate on its
+    ChEES T trace, device_chees.jl:70-79) and the posterior agrees with NUTS."""
+    X, y, _ = logistic_regression_data(1000, 10, seed=1)
+    m = BernoulliLogitGLM(10)
+    trace = []
+    ch = batched_chees(m, (X,), {"y": y}, num_chains=256, num_samples=400, num_warmup=400,
+                       trajectory_velocity="forward", rng=np.random.default_rng(9), _trajectory_trace=trace)
+    assert len(trace) == 400 and np.all(np.isfinite(trace))
+    tail = np.asarray(trace[-150:])
+    assert tail.max() / tail.min() < 3.0
+    assert np.max(rhat(ch)) < 1.05
+    nuts = batched_nuts(m, (X,), {"y": y}, num_chains=256, num_samples=400, num_warmup=400,
+                        rng=np.random.default_rng(10))
+    (m1, s1), (m2, s2) = _mean_mcse(ch), _mean_mcse(nuts)
+    assert np.all(np.abs(m1 - m2) <= 5 * np.hypot(s1, s2))
+    with pytest.raises(ValueError, match="trajectory_velocity"):
+        batched_chees(m, (X,), {"y": y}, num_chains=4, num_samples=1, trajectory_velocity="backward")
+
+
 def test_seed_reproducibility(lib):
     X, y, _ = logistic_regression_data(200, 3, 4)
     m = BernoulliLogitGLM(3)

@@ -873,7 +873,21 @@ def batched_chees(model, args=(), constraints=None, *, num_chains, num_samples, 
                   init_strategy="prior", init_max_retries=100, target_accept=0.651, adapt_step_size=True,
                   adapt_mass_matrix=True, find_reasonable_step_size=False, divergence_threshold=1000.0,
                   mass_matrix_regularization=1e-3, mass_matrix_min_samples=10, callback=None, callback_every=10,
-                  backend="cuda", precision=None, rng=None, _trajectory_trace=None, _surrogate=None) -> HMCChains:
+                  backend="cuda", precision=None, rng=None, trajectory_velocity="reference", _trajectory_trace=None,
+                  _surrogate=None) -> HMCChains:
+    """ChEES-HMC (api_batched_chees.jl:314-347).
+
+    trajectory_velocity selects the endpoint velocity of the trajectory-length
+    gradient.  "reference" (default) is the reference's estimator: the endpoint
+    momentum after the reversible leapfrog's final negation
+    (chees_kernels.jl:392-396, integrator.jl:146-220) under an Adam ascent on
+    log T (api_batched_chees.jl:150-157), which makes its sign that of
+    -dChEES/dlog T.  "forward" uses the velocity the trajectory ends with
+    (the criterion's own derivative), so the ascent maximises ChEES as the
+    reference documents; it is the same reduction with the numerator negated.
+    """
+    if trajectory_velocity not in ("reference", "forward"):
+        raise ValueError(f"batched_chees trajectory_velocity must be 'reference' or 'forward', got {trajectory_velocity!r}")
     if not 0.0 <= jitter_amount <= 1.0:
         raise ValueError(f"batched_chees jitter_amount must be in [0, 1], got {jitter_amount}")
     if max_leapfrog_steps < 1:
@@ -955,6 +969,8 @@ def batched_chees(model, args=(), constraints=None, *, num_chains, num_samples, 
                                                   nat.ptr(run.divergent), nat.ptr(run.inverse_mass), out2,
                                                   _stream_handle()))
                 num, den = out2[0], out2[1]
+                if trajectory_velocity == "forward":
+                    num = -num
             weights = _mass_adaptation_weights(driver.variance.progress(), acc, ap, div)
             driver.warmup_update(it, _chees_harmonic_mean_accept(ap, div), run.position, weights, refind)
             if adapt_trajectory_length:
