@@ -222,6 +222,20 @@ int32_t ut_persistent_nuts_iteration(ut_workspace* ws, const ut_nuts_buffers* bu
 int32_t ut_lockstep_nuts_iteration(ut_workspace* ws, const ut_nuts_buffers* buf, int32_t max_tree_depth,
                                    float divergence_threshold, uint32_t iteration_coord, void* stream);
 
+/* One mean-field ADVI step over the workspace's batch of M particles
+ * (batch_size = M): draws eps[j, p] from the Philox stream at coordinate
+ * (particle j, iteration_coord, stream 5, parameter p), writes the particles
+ * location + scale * eps to d_particles (M x P), their logjoints to d_values (M)
+ * and gradients to d_gradients (M x P), and reduces
+ *   d_location_gradient[p] = mean_j grad[j, p],
+ *   d_scale_gradient[p]    = mean_j grad[j, p] * scale[p] * eps[j, p].
+ * Device pointers; queued on `stream`.  reference: the device ADVI inner loop
+ * _run_device_batched_advi (src/device/advi_kernels.jl:45-209) with its
+ * reduction _device_advi_reduce! (:15-38); the reference draws eps on the host. */
+int32_t ut_advi_step(ut_workspace* ws, const float* d_location, const float* d_scale, uint32_t iteration_coord,
+                     float* d_particles, float* d_values, float* d_gradients, float* d_location_gradient,
+                     float* d_scale_gradient, void* stream);
+
 /* ChEES cross-chain trajectory statistics, reduced on device.
  * reference: _chees_trajectory_update! (src/inference/api_batched_chees.jl:158-228),
  * device passes _device_chees_proposal_mean! / _device_chees_endpoint_terms!

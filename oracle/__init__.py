@@ -36,6 +36,8 @@ def load():
         "orc_logjoint_gradient_f32": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p,
                                                 c_void_p, c_int32]),
         "orc_max_threads": (c_int32, []),
+        "orc_advi_step_f32": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p, c_void_p, c_uint32,
+                                        c_void_p, c_void_p, c_void_p, c_void_p]),
         "orc_hmc_iteration_f32": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p, c_void_p,
                                             c_void_p, c_void_p, c_void_p, c_int32, c_uint32, c_float, c_void_p,
                                             c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32]),
@@ -125,6 +127,20 @@ class OracleModel:
         grads = np.empty_like(q) if want_grad else None
         load().orc_logjoint_gradient_f32(*self._common(), _p(q), C, _p(totals), _p(grads), threads)
         return totals, grads
+
+    def advi_step(self, location, scale, num_particles, coord):
+        """One mean-field ADVI step (orc_advi_step_f32): particles, values, mean
+        gradient and mean gradient * scale * eps."""
+        loc = np.ascontiguousarray(location, dtype=np.float32)
+        sc = np.ascontiguousarray(scale, dtype=np.float32)
+        M, P = int(num_particles), self.P
+        particles = np.empty((M, P), dtype=np.float32)
+        values = np.empty(M, dtype=np.float32)
+        lg = np.empty(P, dtype=np.float32)
+        sg = np.empty(P, dtype=np.float32)
+        load().orc_advi_step_f32(*self._common(), M, _p(loc), _p(sc), coord, _p(particles), _p(values), _p(lg),
+                                 _p(sg))
+        return {"particles": particles, "values": values, "location_gradient": lg, "scale_gradient": sg}
 
     def hmc_iteration(self, position, gradient, logjoint, inverse_mass, step, L, coord, thr=1000.0,
                       want_proposal=False, threads=0):

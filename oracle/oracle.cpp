@@ -603,6 +603,36 @@ int orc_logjoint_gradient_f32(const ut_plan_desc* plan, const float* observed, c
 
 int orc_max_threads(void) { return set_threads(0); }
 
+// One mean-field ADVI step (f32 arithmetic, the device step's Philox noise at
+// (particle j, coord, stream 5, parameter p)): particles, their logjoints, and
+// the per-parameter means of grad and grad * scale * eps over particles,
+// accumulated in double in particle order (advi_kernels.jl:15-38).
+int orc_advi_step_f32(const ut_plan_desc* plan, const float* observed, const int32_t* trip_counts,
+                      const int32_t* loop_starts, int32_t M, const float* location, const float* scale,
+                      uint32_t coord, float* particles, float* values, float* loc_grad, float* scale_grad) {
+    ModelData m = make_model(plan, observed, trip_counts, loop_starts);
+    const int P = plan->num_params;
+    std::vector<float> eps((size_t)M * P), g((size_t)M * P);
+    for (int j = 0; j < M; ++j)
+        for (int p = 0; p < P; ++p) {
+            const float e = rand_normal<float>((uint32_t)j, coord, 5u, (uint32_t)p);
+            eps[(size_t)j * P + p] = e;
+            particles[(size_t)j * P + p] = std::fma(scale[p], e, location[p]);
+        }
+    for (int j = 0; j < M; ++j)
+        values[j] = logjoint_grad<float, double>(m, particles + (size_t)j * P, g.data() + (size_t)j * P);
+    for (int p = 0; p < P; ++p) {
+        double a = 0.0, b = 0.0;
+        for (int j = 0; j < M; ++j) {
+            a += g[(size_t)j * P + p];
+            b += (double)g[(size_t)j * P + p] * scale[p] * eps[(size_t)j * P + p];
+        }
+        loc_grad[p] = (float)(a / M);
+        scale_grad[p] = (float)(b / M);
+    }
+    return 0;
+}
+
 // One HMC iteration (f32, Philox randomness).  position/gradient: C x P,
 // logjoint/step/outputs: C.  proposal/endpoint_momentum: optional C x P.
 int orc_hmc_iteration_f32(const ut_plan_desc* plan, const float* observed, const int32_t* trip_counts,

@@ -354,6 +354,39 @@ def test_persistent_nuts_iteration_vs_oracle(lib, case):
     ws.close()
 
 
+@pytest.mark.parametrize("case", ["glm", "gauss"])
+def test_advi_step_vs_oracle(lib, case):
+    """One device ADVI step (Philox particles, batched gradient, particle means)
+    against the oracle's restatement with the same noise coordinates."""
+    if case == "glm":
+        m, args, cons, _ = _glm_case(1000, 10, 64, False, 1)
+        loc = (0.3 * np.random.default_rng(2).standard_normal(10)).astype(np.float32)
+        sc = np.full(10, 0.1, dtype=np.float32)
+    else:
+        y, _ = gauss_data(200, 3)
+        m, args, cons = NormalLocationScale(), (200,), {"y": y}
+        loc = np.array([y.mean(), np.log(y.std())], dtype=np.float32)
+        sc = np.array([0.1, 0.05], dtype=np.float32)
+    M = 64
+    ws = _ws(m, args, cons, M)
+    P = loc.size
+    f = lambda *sh: torch.empty(sh, dtype=torch.float32, device="cuda")  # noqa: E731
+    loc_d, sc_d = torch.from_numpy(loc).cuda(), torch.from_numpy(sc).cuda()
+    parts, vals, grads, lg, sg = f(M, P), f(M), f(M, P), f(P), f(P)
+    for coord in (5, 6):   # two calls in a row, different noise
+        nat.check(lib.ut_advi_step(ws.handle, nat.ptr(loc_d), nat.ptr(sc_d), coord, nat.ptr(parts), nat.ptr(vals),
+                                   nat.ptr(grads), nat.ptr(lg), nat.ptr(sg), None))
+        torch.cuda.synchronize()
+        ref = oracle.OracleModel(ws.lowered).advi_step(loc, sc, M, coord)
+        np.testing.assert_allclose(parts.cpu().numpy(), ref["particles"], rtol=1e-6, atol=1e-6)
+        np.testing.assert_allclose(vals.cpu().numpy(), ref["values"], rtol=1e-5)
+        scale = max(np.abs(ref["location_gradient"]).max(), 1.0)
+        np.testing.assert_allclose(lg.cpu().numpy(), ref["location_gradient"], atol=1e-4 * scale)
+        scale = max(np.abs(ref["scale_gradient"]).max(), 1.0)
+        np.testing.assert_allclose(sg.cpu().numpy(), ref["scale_gradient"], atol=1e-4 * scale)
+    ws.close()
+
+
 def test_chees_reduce_vs_oracle(lib):
     C, P = 1000, 37
     r = np.random.default_rng(5)

@@ -12,9 +12,9 @@ instead, with the reason stated at the assertion."""
 import numpy as np
 import pytest
 
-from uncertaintea_b200 import (BernoulliLogitGLM, HierarchicalNormalNoncentered, NormalLocationScale, batched_chees,
-                               batched_hmc, batched_nuts, ess, gauss_data, hierarchical_data,
-                               logistic_regression_data, rhat)
+from uncertaintea_b200 import (BernoulliLogitGLM, HierarchicalNormalNoncentered, NormalLocationScale, batched_advi,
+                               batched_chees, batched_hmc, batched_nuts, ess, gauss_data, hierarchical_data,
+                               logistic_regression_data, rhat, variational_mean, variational_samples)
 
 pytestmark = pytest.mark.gpu
 
@@ -174,6 +174,41 @@ def test_chees_forward_velocity_adapts_trajectory(lib):
     assert np.all(np.abs(m1 - m2) <= 5 * np.hypot(s1, s2))
     with pytest.raises(ValueError, match="trajectory_velocity"):
         batched_chees(m, (X,), {"y": y}, num_chains=4, num_samples=1, trajectory_velocity="backward")
+
+
+def test_advi_on_the_gauss_model(lib):
+    """Device mean-field ADVI (the reference's device gate, device_hmc_advi.jl:130-147):
+    the fitted mean of mu matches the exact posterior mean, the ELBO's last quartile
+    beats its first, and the fitted scale of mu is near the posterior SD."""
+    y, _ = gauss_data(50, 13)
+    m = NormalLocationScale()
+    res = batched_advi(m, (50,), {"y": y}, num_iterations=600, num_particles=256, learning_rate=0.05,
+                       rng=np.random.default_rng(46))
+    assert np.all(np.isfinite(res.elbo_history)) and res.elbo_history.shape == (600,)
+    q = len(res.elbo_history) // 4
+    assert res.elbo_history[-q:].mean() > res.elbo_history[:q].mean()
+    mu_ex, s_ex = _exact_gauss_moments(y)
+    mean = variational_mean(res)
+    assert abs(mean[0] - mu_ex) < 0.05, (mean, mu_ex)
+    assert abs(mean[1] - s_ex) < 0.1 * s_ex, (mean, s_ex)
+    sd_mu = np.exp(res.best_log_scale[0])
+    assert 0.5 * s_ex / np.sqrt(50) < sd_mu < 2.0 * s_ex / np.sqrt(50)
+    draws = variational_samples(res, num_samples=2000, rng=np.random.default_rng(1))
+    assert draws.shape == (2, 2000) and np.all(draws[1] > 0)
+
+
+def test_advi_on_the_glm_matches_nuts_means(lib):
+    """On config 1's logistic regression (a near-Gaussian posterior) the mean-field
+    location matches the NUTS posterior means within 0.25 posterior SD."""
+    X, y, _ = logistic_regression_data(1000, 10, seed=1)
+    m = BernoulliLogitGLM(10)
+    res = batched_advi(m, (X,), {"y": y}, num_iterations=1500, num_particles=128, learning_rate=0.02,
+                       rng=np.random.default_rng(3))
+    nuts = batched_nuts(m, (X,), {"y": y}, num_chains=256, num_samples=300, num_warmup=300,
+                        rng=np.random.default_rng(4))
+    d = nuts.constrained.reshape(-1, 10)
+    loc = variational_mean(res)
+    assert np.all(np.abs(loc - d.mean(0)) < 0.25 * d.std(0)), (loc, d.mean(0), d.std(0))
 
 
 def test_seed_reproducibility(lib):

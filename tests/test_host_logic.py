@@ -149,3 +149,56 @@ def test_split_ess_matches_direct_sum():
         pair_sums[i] = min(pair_sums[i], pair_sums[i - 1])
     tau = max(-1 + 2 * sum(pair_sums), 1.0)
     assert dg._split_ess_of(split) == pytest.approx(min(M * S, M * S / tau), rel=1e-9)
+
+
+# ---- mean-field ADVI host logic (vi.jl:179-227, guides.jl:51-57) -----------
+def test_advi_entropy_clip_and_adam():
+    from uncertaintea_b200 import vi
+    ls = np.array([-1.0, 0.5, 2.0])
+    assert vi._gaussian_entropy(ls) == pytest.approx(1.5 * (1 + math.log(2 * math.pi)) + 1.5, abs=1e-14)
+    lg, sg = np.array([3.0, 0.0, 0.0]), np.array([0.0, 4.0, 0.0])
+    assert vi._clip_advi_gradients(lg, sg, math.inf) == pytest.approx(5.0)
+    assert vi._clip_advi_gradients(lg, sg, 1.0) == 1.0
+    np.testing.assert_allclose(lg, [0.6, 0, 0]) and np.testing.assert_allclose(sg, [0, 0.8, 0])
+    # Adam ascent, two steps against the scalar recursion
+    p, m1, m2 = np.array([0.5]), np.zeros(1), np.zeros(1)
+    ref, a, b = 0.5, 0.0, 0.0
+    for it, g in enumerate([2.0, -1.0], start=1):
+        vi._adam_ascent_step(p, m1, m2, np.array([g]), it, 0.05, 0.9, 0.999, 1e-8)
+        a = 0.9 * a + 0.1 * g
+        b = 0.999 * b + 0.001 * g * g
+        ref += 0.05 * (a / (1 - 0.9 ** it)) / (math.sqrt(b / (1 - 0.999 ** it)) + 1e-8)
+    assert p[0] == pytest.approx(ref, abs=1e-15)
+
+
+def test_advi_validation_before_any_device_work():
+    from uncertaintea_b200 import BernoulliLogitGLM, batched_advi
+    m = BernoulliLogitGLM(3)
+    X, y = np.zeros((4, 3)), np.zeros(4)
+    for kw, msg in [(dict(guide="fullrank"), "CPU-only"), (dict(elbo="iwae"), "CPU-only"),
+                    (dict(guide="bogus"), "guide must be"), (dict(num_iterations=0), "num_iterations > 0"),
+                    (dict(num_particles=0), "num_particles > 0"), (dict(beta1=1.0), "beta1"),
+                    (dict(gradient_clip=0.0), "gradient_clip > 0")]:
+        args = dict(num_iterations=5)
+        args.update(kw)
+        with pytest.raises(ValueError, match=msg):
+            batched_advi(m, (X,), {"y": y}, **args)
+
+
+def test_oracle_advi_step_consistency():
+    """The oracle's ADVI step equals its own pieces: Philox noise at stream 5,
+    particles location + scale * eps, means of the f64 gradients."""
+    import oracle
+    from uncertaintea_b200.models import NormalLocationScale, gauss_data
+    y, _ = gauss_data(30, 2)
+    om = oracle.OracleModel(NormalLocationScale().lower((30,), {"y": y}))
+    loc, sc = np.array([0.3, -0.2], dtype=np.float32), np.array([0.2, 0.5], dtype=np.float32)
+    r = om.advi_step(loc, sc, 16, 77)
+    eps = np.stack([oracle.rand_normal(j, 77, 5, 0, 2) for j in range(16)])
+    # one rounding (fused multiply-add): the f32 product is exact in f64
+    fused = (loc.astype(np.float64) + sc.astype(np.float64) * eps.astype(np.float64)).astype(np.float32)
+    np.testing.assert_array_equal(r["particles"], fused)
+    t, g = om.logjoint_gradient_f64(r["particles"].astype(np.float64))
+    np.testing.assert_allclose(r["values"], t, rtol=1e-5)
+    np.testing.assert_allclose(r["location_gradient"], g.mean(0), rtol=1e-4, atol=1e-4)
+    np.testing.assert_allclose(r["scale_gradient"], (g * sc * eps).mean(0), rtol=1e-4, atol=1e-4)

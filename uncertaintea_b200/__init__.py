@@ -3,7 +3,8 @@
 Public surface mirrors the reference's ``UncertainTea.Device`` and
 ``UncertainTea.Inference`` facades (src/UncertainTea.jl:101-200) for the
 device path: batched logjoint / gradient, batched HMC, persistent NUTS,
-ChEES-HMC, the Philox4x32-10 stream and the R-hat / ESS diagnostics; plus
+ChEES-HMC, mean-field ADVI, the Philox4x32-10 stream and the R-hat / ESS
+diagnostics; plus
 the learned gradient surrogate for ChEES-HMC and many-model batched NUTS
 (no reference counterparts).
 """
@@ -15,6 +16,7 @@ from .inference import HMCChains, batched_chees, batched_hmc, batched_nuts, post
 from .diagnostics import ess, min_ess_per_second, rhat, summarize
 from .surrogate import GradientSurrogate, batched_chees_surrogate
 from .multi import MultiChains, MultiModelBatch, batched_nuts_multi
+from .vi import ADVIResult, batched_advi, variational_mean, variational_samples
 from . import rng
 
 __all__ = [
@@ -24,5 +26,5 @@ __all__ = [
     "device_batched_logjoint_gradient", "device_batched_logjoint_gradient_", "device_lowering_report", "HMCChains",
     "batched_chees", "batched_hmc", "batched_nuts", "posterior_array", "ess", "min_ess_per_second", "rhat",
     "summarize", "rng", "GradientSurrogate", "batched_chees_surrogate", "MultiChains", "MultiModelBatch",
-    "batched_nuts_multi",
+    "batched_nuts_multi", "ADVIResult", "batched_advi", "variational_mean", "variational_samples",
 ]

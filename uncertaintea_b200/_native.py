@@ -131,6 +131,8 @@ SIGNATURES = [
      [c_void_p, POINTER(NutsBuffers), c_int32, c_float, c_uint32, c_void_p]),
     ("ut_lockstep_nuts_iteration", c_int32,
      [c_void_p, POINTER(NutsBuffers), c_int32, c_float, c_uint32, c_void_p]),
+    ("ut_advi_step", c_int32,
+     [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     ("ut_chees_reduce", c_int32,
      [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, POINTER(c_double), c_void_p]),
     ("ut_running_variance_update", c_int32,

@@ -18,6 +18,7 @@
 #include "ut_tc_glm.cuh"
 #include "ut_glm_stream.cuh"
 #include "ut_nuts_lockstep.cuh"
+#include "ut_advi.cuh"
 
 using namespace ut;
 
@@ -850,6 +851,28 @@ int32_t ut_persistent_nuts_iteration(ut_workspace* ws, const ut_nuts_buffers* bu
     a.thr = divergence_threshold;
     cudaStream_t st = (cudaStream_t)stream;
     UT_DISPATCH_WARP(ws, LAUNCH_NUTS, ws, a, st);
+    UT_LAUNCHED();
+    return UT_OK;
+}
+
+// ---- mean-field ADVI step ---------------------------------------------------
+int32_t ut_advi_step(ut_workspace* ws, const float* d_location, const float* d_scale, uint32_t iteration_coord,
+                     float* d_particles, float* d_values, float* d_gradients, float* d_location_gradient,
+                     float* d_scale_gradient, void* stream) {
+    int32_t rc = check_ws(ws);
+    if (rc) return rc;
+    if (!d_location || !d_scale || !d_particles || !d_values || !d_gradients || !d_location_gradient ||
+        !d_scale_gradient)
+        return fail(UT_ERR_ARGUMENT, "null ADVI buffer");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int P = ws->P, M = ws->C;
+    const long long n = (long long)P * M;
+    const unsigned grid = (unsigned)std::min<long long>((n + 255) / 256, 4096);
+    advi_particles_kernel<<<grid, 256, 0, st>>>(d_location, d_scale, iteration_coord, P, M, d_particles);
+    UT_LAUNCHED();
+    if ((rc = density(ws, d_particles, d_values, d_gradients, st))) return rc;
+    advi_reduce_kernel<<<P, 256, 0, st>>>(d_gradients, d_scale, iteration_coord, P, M, d_location_gradient,
+                                          d_scale_gradient);
     UT_LAUNCHED();
     return UT_OK;
 }
