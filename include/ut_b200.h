@@ -222,6 +222,39 @@ int32_t ut_persistent_nuts_iteration(ut_workspace* ws, const ut_nuts_buffers* bu
 int32_t ut_lockstep_nuts_iteration(ut_workspace* ws, const ut_nuts_buffers* buf, int32_t max_tree_depth,
                                    float divergence_threshold, uint32_t iteration_coord, void* stream);
 
+/* Per-iteration buffers of MEADS (device pointers). */
+typedef struct ut_meads_buffers {
+    float* position;            /* P x C in/out                                   */
+    float* gradient;            /* P x C in/out                                   */
+    float* logjoint;            /* C in/out                                       */
+    float* momentum;            /* P x C in/out: persistent whitened momentum     */
+    float* slice;               /* C in/out: persistent slice variable in [-1, 1) */
+    float* accept_prob;         /* C out (1 for the skipped fold)                 */
+    float* energy;              /* C out: -logjoint + |momentum|^2 / 2            */
+    float* energy_error;        /* C out (0 for the skipped fold)                 */
+    uint8_t* accepted;          /* C out                                          */
+    uint8_t* divergent;         /* C out                                          */
+    int32_t* integration_steps; /* C out: 1, or 0 for the skipped fold            */
+    float* fold_parameters;     /* optional K x 4 out: step, alpha, delta, 0      */
+} ut_meads_buffers;
+
+/* Initial MEADS state: momentum ~ N(0, I) from Philox stream 0 and slice
+ * u = 2 U - 1 from stream 4, at (chain, iteration_coord).
+ * reference: batched_meads (src/inference/api_batched_meads.jl:285-296). */
+int32_t ut_meads_init(ut_workspace* ws, const ut_meads_buffers* buf, uint32_t iteration_coord, void* stream);
+
+/* One MEADS iteration for every chain: per-fold ensemble statistics of the
+ * neighbour fold (mean, std, trace-ratio eigenvalue estimates of the whitened
+ * states and gradients) -> step size, damping, slice drift; partial momentum
+ * refresh (Philox stream 0), one leapfrog step with inverse mass std^2, the
+ * persistent-slice accept; the fold (iteration - 1) mod num_folds is left
+ * unchanged.  iteration >= 1; num_chains >= 2 * num_folds; P <= 544.
+ * reference: batched_meads (src/inference/api_batched_meads.jl:170-547),
+ * _meads_fold_parameters! (:89-153), _meads_max_eig (:48-78); the reference
+ * runs it on the host only. */
+int32_t ut_meads_iteration(ut_workspace* ws, const ut_meads_buffers* buf, int32_t num_folds, int32_t iteration,
+                           float divergence_threshold, uint32_t iteration_coord, void* stream);
+
 /* One mean-field ADVI step over the workspace's batch of M particles
  * (batch_size = M): draws eps[j, p] from the Philox stream at coordinate
  * (particle j, iteration_coord, stream 5, parameter p), writes the particles

@@ -36,6 +36,9 @@ def load():
         "orc_logjoint_gradient_f32": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p,
                                                 c_void_p, c_int32]),
         "orc_max_threads": (c_int32, []),
+        "orc_meads_max_eig": (c_double, [c_void_p, c_int32, c_int32]),
+        "orc_meads_iteration_f32": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32,
+                                              c_uint32, c_float] + [c_void_p] * 12),
         "orc_advi_step_f32": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p, c_void_p, c_uint32,
                                         c_void_p, c_void_p, c_void_p, c_void_p]),
         "orc_hmc_iteration_f32": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p, c_void_p,
@@ -94,6 +97,13 @@ def rand_normal(chain, iteration, stream, draw_start, n, dtype=np.float32):
     return out
 
 
+def meads_max_eig(columns):
+    """The MEADS trace-ratio largest-eigenvalue estimate of a P x N matrix whose
+    columns are the ensemble members (api_batched_meads.jl:48-78)."""
+    c = np.ascontiguousarray(np.asarray(columns, dtype=np.float64).T)   # N x P
+    return float(load().orc_meads_max_eig(_p(c), c.shape[1] if c.ndim == 2 else 0, c.shape[0]))
+
+
 class OracleModel:
     """Wraps a lowered kernel description for the oracle entry points."""
 
@@ -127,6 +137,25 @@ class OracleModel:
         grads = np.empty_like(q) if want_grad else None
         load().orc_logjoint_gradient_f32(*self._common(), _p(q), C, _p(totals), _p(grads), threads)
         return totals, grads
+
+    def meads_iteration(self, position, gradient, logjoint, momentum, slice_u, num_folds, iteration, coord,
+                        thr=1000.0):
+        """One MEADS iteration (orc_meads_iteration_f32) on copies of the state."""
+        st = {"position": np.array(position, dtype=np.float32), "gradient": np.array(gradient, dtype=np.float32),
+              "logjoint": np.array(logjoint, dtype=np.float32), "momentum": np.array(momentum, dtype=np.float32),
+              "slice": np.array(slice_u, dtype=np.float32)}
+        C = st["position"].shape[0]
+        out = {k: np.empty(C, dtype=np.float32) for k in ("accept_prob", "energy", "energy_error")}
+        out["accepted"] = np.empty(C, dtype=np.uint8)
+        out["divergent"] = np.empty(C, dtype=np.uint8)
+        out["integration_steps"] = np.empty(C, dtype=np.int32)
+        out["fold_parameters"] = np.empty((num_folds, 4), dtype=np.float32)
+        load().orc_meads_iteration_f32(*self._common(), C, num_folds, iteration, coord, thr,
+                                       *[_p(st[k]) for k in ("position", "gradient", "logjoint", "momentum", "slice")],
+                                       *[_p(out[k]) for k in ("accept_prob", "energy", "energy_error", "accepted",
+                                                              "divergent", "integration_steps", "fold_parameters")])
+        st.update(out)
+        return st
 
     def advi_step(self, location, scale, num_particles, coord):
         """One mean-field ADVI step (orc_advi_step_f32): particles, values, mean

@@ -603,6 +603,151 @@ int orc_logjoint_gradient_f32(const ut_plan_desc* plan, const float* observed, c
 
 int orc_max_threads(void) { return set_threads(0); }
 
+// ---------------------------------------------------------------------------
+// MEADS (api_batched_meads.jl): fold parameters in double, the literal
+// off-diagonal Gram sum of _meads_max_eig (:48-78); chain updates in float
+// with the device's Philox draws (refresh noise: stream 0 at (chain, coord, p)).
+// ---------------------------------------------------------------------------
+static double meads_max_eig(const std::vector<double>& cols, int P, int N) {  // cols: N x P
+    if (N < 2) return 0.0;
+    double tr = 0.0;
+    for (int n = 0; n < N; ++n)
+        for (int d = 0; d < P; ++d) tr += cols[(size_t)n * P + d] * cols[(size_t)n * P + d];
+    const double lam = tr / N;
+    if (!(lam > 0.0)) return 0.0;
+    double off = 0.0;
+    for (int a = 0; a < N; ++a)
+        for (int b = 0; b < N; ++b) {
+            if (a == b) continue;
+            double gram = 0.0;
+            for (int d = 0; d < P; ++d) gram += cols[(size_t)a * P + d] * cols[(size_t)b * P + d];
+            off += gram * gram;
+        }
+    return (off / ((double)N * (N - 1))) / lam;
+}
+
+// cols: N members x P (member-major)
+double orc_meads_max_eig(const double* cols, int32_t P, int32_t N) {
+    return meads_max_eig(std::vector<double>(cols, cols + (size_t)P * N), P, N);
+}
+
+int orc_meads_iteration_f32(const ut_plan_desc* plan, const float* observed, const int32_t* trip_counts,
+                            const int32_t* loop_starts, int32_t C, int32_t K, int32_t iteration, uint32_t coord,
+                            float thr, float* position, float* gradient, float* logjoint, float* momentum,
+                            float* slice, float* accept_prob, float* energy, float* energy_error,
+                            uint8_t* accepted, uint8_t* divergent, int32_t* steps, float* fold_params) {
+    ModelData m = make_model(plan, observed, trip_counts, loop_starts);
+    const int P = plan->num_params;
+    std::vector<int> start(K), size(K);
+    const int base = C / K, rem = C % K;
+    for (int f = 0, s0 = 0; f < K; ++f) {  // contiguous folds (:263-276)
+        size[f] = base + (f < rem ? 1 : 0);
+        start[f] = s0;
+        s0 += size[f];
+    }
+    std::vector<float> sdf((size_t)K * P), eps(K), alpha(K), delta(K);
+    for (int f = 0; f < K; ++f) {  // _meads_fold_parameters! (:89-153) from the neighbour's pre-update states
+        const int nb = f == 0 ? K - 1 : f - 1, s0 = start[nb], N = size[nb];
+        std::vector<double> wp((size_t)N * P), wg((size_t)N * P);
+        for (int d = 0; d < P; ++d) {
+            double mean = 0.0;
+            for (int i = 0; i < N; ++i) mean += position[(size_t)(s0 + i) * P + d];
+            mean /= N;
+            double var = 0.0;
+            for (int i = 0; i < N; ++i) {
+                const double x = position[(size_t)(s0 + i) * P + d] - mean;
+                var += x * x;
+            }
+            var /= N;
+            double sd = std::sqrt(var);
+            sd = sd > 1e-10 ? sd : 1e-10;
+            sdf[(size_t)f * P + d] = (float)sd;
+            for (int i = 0; i < N; ++i) {
+                wp[(size_t)i * P + d] = (position[(size_t)(s0 + i) * P + d] - mean) / sd;
+                wg[(size_t)i * P + d] = gradient[(size_t)(s0 + i) * P + d] * sd;
+            }
+        }
+        const double eg = meads_max_eig(wg, P, N), ep = meads_max_eig(wp, P, N);
+        const double e = std::min(1.0, 0.5 / std::sqrt(std::max(eg, 1e-12)));
+        const double gamma = std::max(1.0 / (iteration * e), 1.0 / std::sqrt(std::max(ep, 1e-12)));
+        double a = 1.0 - std::exp(-2.0 * e * gamma);
+        a = std::min(std::max(a, 0.0), 1.0);
+        eps[f] = (float)e;
+        alpha[f] = (float)a;
+        delta[f] = (float)(a / 2.0);
+        if (fold_params) {
+            fold_params[f * 4] = eps[f]; fold_params[f * 4 + 1] = alpha[f];
+            fold_params[f * 4 + 2] = delta[f]; fold_params[f * 4 + 3] = 0.0f;
+        }
+    }
+    const int skip = (iteration - 1) % K;
+    std::vector<float> q(P), g(P), p(P), mt(P);
+    for (int c = 0; c < C; ++c) {
+        int f = 0;
+        while (!(c >= start[f] && c < start[f] + size[f])) ++f;
+        float* mc = momentum + (size_t)c * P;
+        if (f == skip) {
+            double kin = 0.0;
+            for (int d = 0; d < P; ++d) kin += (double)mc[d] * mc[d];
+            accept_prob[c] = 1.0f; accepted[c] = 1; divergent[c] = 0; energy_error[c] = 0.0f; steps[c] = 0;
+            energy[c] = (float)(0.5 * kin - logjoint[c]);
+            continue;
+        }
+        const float* sd = &sdf[(size_t)f * P];
+        const float keep = std::sqrt(std::max(0.0f, 1.0f - alpha[f])), refresh = std::sqrt(std::max(0.0f, alpha[f]));
+        double kin0 = 0.0;
+        for (int d = 0; d < P; ++d) {
+            const float xi = rand_normal<float>((uint32_t)c, coord, kStreamMomentum, (uint32_t)d);
+            mt[d] = std::fma(keep, mc[d], refresh * xi);
+            p[d] = mt[d] / sd[d];
+            kin0 += (double)mt[d] * mt[d];
+            q[d] = position[(size_t)c * P + d];
+            g[d] = gradient[(size_t)c * P + d];
+        }
+        const float H0 = (float)(0.5 * kin0) - logjoint[c];
+        bool valid = all_finite(g.data(), P);
+        const float e = eps[f];
+        for (int d = 0; d < P; ++d) {
+            p[d] = std::fma(0.5f * e, g[d], p[d]);
+            q[d] = std::fma(e * sd[d] * sd[d], p[d], q[d]);
+        }
+        const float lj1 = logjoint_grad_f32(m, q.data(), g.data());
+        valid = valid && all_finite(g.data(), P) && all_finite(q.data(), P) && std::isfinite(lj1);
+        double kin1 = 0.0;
+        for (int d = 0; d < P; ++d) {
+            p[d] = -std::fma(0.5f * e, g[d], p[d]);
+            kin1 += (double)p[d] * p[d] * sd[d] * sd[d];
+        }
+        float lar = -std::numeric_limits<float>::infinity(), ee = std::numeric_limits<float>::infinity();
+        bool div = true;
+        if (valid) {
+            const float H1 = (float)(0.5 * kin1) - lj1;
+            lar = H0 - H1;
+            ee = H1 - H0;
+            div = !std::isfinite(ee) || ee > thr;
+        }
+        const float ap = std::isnan(lar) ? 0.0f : std::min(1.0f, std::exp(lar));
+        const float x = slice[c] + 1.0f + delta[f];
+        const float u = (x - 2.0f * std::floor(x * 0.5f)) - 1.0f;  // (:163) floored modulo
+        const bool acc = valid && std::log(std::fabs(u)) <= lar;
+        double km = 0.0;
+        for (int d = 0; d < P; ++d) {
+            mc[d] = acc ? -p[d] * sd[d] : -mt[d];
+            km += (double)mc[d] * mc[d];
+            if (acc) {
+                position[(size_t)c * P + d] = q[d];
+                gradient[(size_t)c * P + d] = g[d];
+            }
+        }
+        if (acc) logjoint[c] = lj1;
+        slice[c] = acc ? u * std::exp(ee) : u;
+        accept_prob[c] = ap; accepted[c] = acc ? 1 : 0; divergent[c] = div ? 1 : 0; energy_error[c] = ee;
+        steps[c] = 1;
+        energy[c] = (float)(0.5 * km) - logjoint[c];
+    }
+    return 0;
+}
+
 // One mean-field ADVI step (f32 arithmetic, the device step's Philox noise at
 // (particle j, coord, stream 5, parameter p)): particles, their logjoints, and
 // the per-parameter means of grad and grad * scale * eps over particles,

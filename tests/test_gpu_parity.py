@@ -387,6 +387,55 @@ def test_advi_step_vs_oracle(lib, case):
     ws.close()
 
 
+@pytest.mark.parametrize("case", ["glm", "gauss", "hier"])
+def test_meads_iterations_vs_oracle(lib, case):
+    """Two MEADS iterations (fold statistics in double, refresh, one leapfrog
+    step, persistent-slice accept) against the oracle's literal restatement,
+    from the same state and Philox coordinates."""
+    if case == "glm":
+        m, args, cons, q = _glm_case(1000, 10, 64, False, 1)
+        q *= 0.3
+    elif case == "gauss":
+        m, args, cons, q = _gauss_near_mode(200, 64, 4, 0.2)
+    else:
+        y, sig, sizes, _ = hierarchical_data(16, 10, 7)
+        m, args, cons = HierarchicalNormalNoncentered(16), (sig, sizes), {"y": y}
+        q = (np.random.default_rng(8).standard_normal((64, 18)) * 0.5).astype(np.float32)
+    C, P, K = q.shape[0], q.shape[1], 4
+    ws = _ws(m, args, cons, C)
+    qd, g, t = _state(ws, q)
+    f = lambda sh, dt=torch.float32: torch.zeros(sh, dtype=dt, device="cuda")  # noqa: E731
+    mom, sl = f((C, P)), f(C)
+    out = {"accept_prob": f(C), "energy": f(C), "energy_error": f(C), "accepted": f(C, torch.uint8),
+           "divergent": f(C, torch.uint8), "integration_steps": f(C, torch.int32), "fold_parameters": f((K, 4))}
+    buf = nat.MeadsBuffers(nat.ptr(qd), nat.ptr(g), nat.ptr(t), nat.ptr(mom), nat.ptr(sl),
+                           *[nat.ptr(out[k]) for k in ("accept_prob", "energy", "energy_error", "accepted",
+                                                       "divergent", "integration_steps", "fold_parameters")])
+    nat.check(lib.ut_meads_init(ws.handle, ctypes.byref(buf), 3, None))
+    torch.cuda.synchronize()
+    state = {"position": qd.cpu().numpy(), "gradient": g.cpu().numpy(), "logjoint": t.cpu().numpy(),
+             "momentum": mom.cpu().numpy(), "slice": sl.cpu().numpy()}
+    assert np.all(np.abs(state["slice"]) <= 1.0)
+    om = oracle.OracleModel(ws.lowered)
+    for it in (1, 2):
+        ref = om.meads_iteration(state["position"], state["gradient"], state["logjoint"], state["momentum"],
+                                 state["slice"], K, it, 100 + it)
+        nat.check(lib.ut_meads_iteration(ws.handle, ctypes.byref(buf), K, it, 1000.0, 100 + it, None))
+        torch.cuda.synchronize()
+        np.testing.assert_allclose(out["fold_parameters"].cpu().numpy(), ref["fold_parameters"], rtol=2e-5, atol=1e-7)
+        same = (out["accepted"].cpu().numpy() == ref["accepted"]) & (out["divergent"].cpu().numpy() == ref["divergent"])
+        assert same.mean() >= 0.95, same.mean()
+        assert np.array_equal(out["integration_steps"].cpu().numpy(), ref["integration_steps"])
+        pos = qd.cpu().numpy()
+        np.testing.assert_allclose(pos[same], ref["position"][same], rtol=1e-4, atol=1e-4)
+        np.testing.assert_allclose(mom.cpu().numpy()[same], ref["momentum"][same], rtol=1e-3, atol=1e-3)
+        np.testing.assert_allclose(out["accept_prob"].cpu().numpy()[same], ref["accept_prob"][same], atol=1e-3)
+        # carry the device state forward for the next iteration
+        state = {"position": pos, "gradient": g.cpu().numpy(), "logjoint": t.cpu().numpy(),
+                 "momentum": mom.cpu().numpy(), "slice": sl.cpu().numpy()}
+    ws.close()
+
+
 def test_chees_reduce_vs_oracle(lib):
     C, P = 1000, 37
     r = np.random.default_rng(5)

@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from uncertaintea_b200 import (BernoulliLogitGLM, HierarchicalNormalNoncentered, NormalLocationScale, batched_advi,
-                               batched_chees, batched_hmc, batched_nuts, ess, gauss_data, hierarchical_data,
+                               batched_chees, batched_hmc, batched_meads, batched_nuts, ess, gauss_data, hierarchical_data,
                                logistic_regression_data, rhat, variational_mean, variational_samples)
 
 pytestmark = pytest.mark.gpu
@@ -209,6 +209,39 @@ def test_advi_on_the_glm_matches_nuts_means(lib):
     d = nuts.constrained.reshape(-1, 10)
     loc = variational_mean(res)
     assert np.all(np.abs(loc - d.mean(0)) < 0.25 * d.std(0)), (loc, d.mean(0), d.std(0))
+
+
+def test_meads_on_the_gauss_model(lib):
+    """MEADS (no warmup adaptation; the reference's gate on its conjugate model,
+    batched_meads.jl:71-98): R-hat, the posterior means of mu and s within 5 MCSE
+    of the grid-integrated posterior, finite adaptation trace in range."""
+    y, _ = gauss_data(50, 13)
+    trace = []
+    res = batched_meads(NormalLocationScale(), (50,), {"y": y}, num_chains=256, num_samples=1500, num_warmup=500,
+                        rng=np.random.default_rng(11), _adapt_trace=trace)
+    assert len(trace) == 2000
+    assert all(0.0 < t["step"] <= 1.0 and 0.0 <= t["damping"] <= 1.0 for t in trace)
+    assert np.max(rhat(res)) < 1.02, rhat(res)
+    assert np.min(ess(res)) > 400
+    mu_ex, s_ex = _exact_gauss_moments(y)
+    mean, mcse = _mean_mcse(res)
+    assert abs(mean[0] - mu_ex) <= 5 * mcse[0], (mean[0], mu_ex, mcse[0])
+    assert abs(mean[1] - s_ex) <= 5 * mcse[1], (mean[1], s_ex, mcse[1])
+    ist = res.integration_steps
+    assert set(np.unique(ist)) <= {0, 1} and abs((ist == 0).mean() - 0.25) < 0.01
+
+
+def test_meads_on_the_glm_matches_nuts(lib):
+    X, y, _ = logistic_regression_data(1000, 10, seed=1)
+    m = BernoulliLogitGLM(10)
+    res = batched_meads(m, (X,), {"y": y}, num_chains=512, num_samples=1000, num_warmup=500,
+                        rng=np.random.default_rng(12))
+    assert np.max(rhat(res)) < 1.02
+    assert res.divergent.mean() < 0.01
+    nuts = batched_nuts(m, (X,), {"y": y}, num_chains=256, num_samples=400, num_warmup=400,
+                        rng=np.random.default_rng(13))
+    (m1, s1), (m2, s2) = _mean_mcse(res), _mean_mcse(nuts)
+    assert np.all(np.abs(m1 - m2) <= 5 * np.hypot(s1, s2))
 
 
 def test_seed_reproducibility(lib):

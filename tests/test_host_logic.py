@@ -202,3 +202,18 @@ def test_oracle_advi_step_consistency():
     np.testing.assert_allclose(r["values"], t, rtol=1e-5)
     np.testing.assert_allclose(r["location_gradient"], g.mean(0), rtol=1e-4, atol=1e-4)
     np.testing.assert_allclose(r["scale_gradient"], (g * sc * eps).mean(0), rtol=1e-4, atol=1e-4)
+
+
+def test_meads_validation_before_any_device_work():
+    """batched_meads argument errors (batched_meads.jl:59-69)."""
+    from uncertaintea_b200 import BernoulliLogitGLM, batched_meads
+    m = BernoulliLogitGLM(3)
+    X, y = np.zeros((4, 3)), np.zeros(4)
+    for kw, msg in [(dict(num_chains=4, num_folds=1), "num_folds must be >= 2"),
+                    (dict(num_chains=6, num_folds=4), "num_chains >= 2 \\* num_folds"),
+                    (dict(num_chains=8, num_samples=0), "num_samples must be > 0"),
+                    (dict(num_chains=8, init_strategy="bogus"), "init_strategy")]:
+        args = dict(num_chains=8, num_samples=10)
+        args.update(kw)
+        with pytest.raises(ValueError, match=msg):
+            batched_meads(m, (X,), {"y": y}, **args)

@@ -191,3 +191,21 @@ def test_oracle_hmc_reversibility():
     assert np.all(out["divergent"] == 0)
     assert np.all(np.isfinite(out["proposal"]))
     assert np.all((out["accept_prob"] >= 0) & (out["accept_prob"] <= 1))
+
+
+def test_meads_max_eig_pins():
+    """The reference's pins of its trace-ratio estimator (batched_meads.jl:32-48)."""
+    assert oracle.meads_max_eig(np.array([[1.0], [2.0]])) == 0.0          # one member
+    assert oracle.meads_max_eig(np.zeros((3, 0))) == 0.0                  # no members
+    v = np.array([3.0, 4.0])
+    assert abs(oracle.meads_max_eig(np.stack([v] * 4, axis=1)) - 25.0) < 1e-10
+    e1 = np.array([1.0, 0.0, 0.0])
+    big = np.stack([2 * e1, -2 * e1, 2 * e1, -2 * e1], axis=1)
+    assert abs(oracle.meads_max_eig(big) - 4.0) < 1e-10
+    # the P x P second-moment route the device uses gives the same value
+    x = np.random.default_rng(0).standard_normal((5, 40))
+    A = x @ x.T
+    n = x.shape[1]
+    sq = (x * x).sum(0)
+    alt = ((A * A).sum() - (sq ** 2).sum()) / (n * (n - 1)) / (sq.sum() / n)
+    assert abs(oracle.meads_max_eig(x) - alt) < 1e-10 * alt

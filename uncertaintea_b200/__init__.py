@@ -3,7 +3,7 @@
 Public surface mirrors the reference's ``UncertainTea.Device`` and
 ``UncertainTea.Inference`` facades (src/UncertainTea.jl:101-200) for the
 device path: batched logjoint / gradient, batched HMC, persistent NUTS,
-ChEES-HMC, mean-field ADVI, the Philox4x32-10 stream and the R-hat / ESS
+ChEES-HMC, MEADS, mean-field ADVI, the Philox4x32-10 stream and the R-hat / ESS
 diagnostics; plus
 the learned gradient surrogate for ChEES-HMC and many-model batched NUTS
 (no reference counterparts).
@@ -17,6 +17,7 @@ from .diagnostics import ess, min_ess_per_second, rhat, summarize
 from .surrogate import GradientSurrogate, batched_chees_surrogate
 from .multi import MultiChains, MultiModelBatch, batched_nuts_multi
 from .vi import ADVIResult, batched_advi, variational_mean, variational_samples
+from .meads import batched_meads
 from . import rng
 
 __all__ = [
@@ -27,4 +28,5 @@ __all__ = [
     "batched_chees", "batched_hmc", "batched_nuts", "posterior_array", "ess", "min_ess_per_second", "rhat",
     "summarize", "rng", "GradientSurrogate", "batched_chees_surrogate", "MultiChains", "MultiModelBatch",
     "batched_nuts_multi", "ADVIResult", "batched_advi", "variational_mean", "variational_samples",
+    "batched_meads",
 ]

@@ -47,6 +47,12 @@ class PlanDesc(ctypes.Structure):
     ]
 
 
+class MeadsBuffers(ctypes.Structure):
+    _fields_ = [(n, c_void_p) for n in ("position", "gradient", "logjoint", "momentum", "slice", "accept_prob",
+                                         "energy", "energy_error", "accepted", "divergent", "integration_steps",
+                                         "fold_parameters")]
+
+
 class HmcBuffers(ctypes.Structure):
     _fields_ = [
         ("position", c_void_p),
@@ -131,6 +137,8 @@ SIGNATURES = [
      [c_void_p, POINTER(NutsBuffers), c_int32, c_float, c_uint32, c_void_p]),
     ("ut_lockstep_nuts_iteration", c_int32,
      [c_void_p, POINTER(NutsBuffers), c_int32, c_float, c_uint32, c_void_p]),
+    ("ut_meads_init", c_int32, [c_void_p, POINTER(MeadsBuffers), c_uint32, c_void_p]),
+    ("ut_meads_iteration", c_int32, [c_void_p, POINTER(MeadsBuffers), c_int32, c_int32, c_float, c_uint32, c_void_p]),
     ("ut_advi_step", c_int32,
      [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     ("ut_chees_reduce", c_int32,

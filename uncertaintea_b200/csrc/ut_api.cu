@@ -19,6 +19,7 @@
 #include "ut_glm_stream.cuh"
 #include "ut_nuts_lockstep.cuh"
 #include "ut_advi.cuh"
+#include "ut_meads.cuh"
 
 using namespace ut;
 
@@ -113,6 +114,9 @@ struct ut_workspace {
     float* ls_cg = nullptr;
     float* ls_clj = nullptr;
     int ls_depth = -1;
+    // MEADS fold scratch
+    MeadsScratch meads = {};
+    int meads_k = 0;
     // ChEES scratch
     uint8_t* d_flags = nullptr;
     double* d_means = nullptr;
@@ -852,6 +856,98 @@ int32_t ut_persistent_nuts_iteration(ut_workspace* ws, const ut_nuts_buffers* bu
     cudaStream_t st = (cudaStream_t)stream;
     UT_DISPATCH_WARP(ws, LAUNCH_NUTS, ws, a, st);
     UT_LAUNCHED();
+    return UT_OK;
+}
+
+// ---- MEADS -------------------------------------------------------------------
+namespace {
+int meads_k_slots(int P) { return P <= 32 ? 1 : P <= 64 ? 2 : P <= 96 ? 3 : P <= 128 ? 4 : P <= 256 ? 8 : 17; }
+#define UT_MEADS_K_SWITCH(KV, ...)                                   \
+    switch (KV) {                                                    \
+        case 1: { constexpr int K = 1; __VA_ARGS__; } break;         \
+        case 2: { constexpr int K = 2; __VA_ARGS__; } break;         \
+        case 3: { constexpr int K = 3; __VA_ARGS__; } break;         \
+        case 4: { constexpr int K = 4; __VA_ARGS__; } break;         \
+        case 8: { constexpr int K = 8; __VA_ARGS__; } break;         \
+        default: { constexpr int K = 17; __VA_ARGS__; } break;       \
+    }
+
+int32_t meads_check(ut_workspace* ws, const ut_meads_buffers* buf) {
+    if (!buf || !buf->position || !buf->gradient || !buf->logjoint || !buf->momentum || !buf->slice ||
+        !buf->accept_prob || !buf->energy || !buf->energy_error || !buf->accepted || !buf->divergent ||
+        !buf->integration_steps)
+        return fail(UT_ERR_ARGUMENT, "null MEADS buffer");
+    if (ws->P > 544) return fail(UT_ERR_UNSUPPORTED, "MEADS supports up to 544 parameters");
+    return UT_OK;
+}
+
+MeadsArgs meads_args(ut_workspace* ws, const ut_meads_buffers* buf, uint32_t coord, float thr, int skip) {
+    MeadsArgs a;
+    a.position = buf->position; a.gradient = buf->gradient; a.logjoint = buf->logjoint;
+    a.momentum = buf->momentum; a.slice = buf->slice; a.accept_prob = buf->accept_prob; a.energy = buf->energy;
+    a.energy_error = buf->energy_error; a.accepted = buf->accepted; a.divergent = buf->divergent;
+    a.steps = buf->integration_steps;
+    a.C = ws->C; a.P = ws->P; a.skip = skip; a.coord = coord; a.thr = thr;
+    return a;
+}
+}  // namespace
+
+int32_t ut_meads_init(ut_workspace* ws, const ut_meads_buffers* buf, uint32_t iteration_coord, void* stream) {
+    int32_t rc = check_ws(ws);
+    if (rc) return rc;
+    if ((rc = meads_check(ws, buf))) return rc;
+    MeadsArgs a = meads_args(ws, buf, iteration_coord, 0.0f, -1);
+    const unsigned grid = (unsigned)((ws->C + 7) / 8);
+    UT_MEADS_K_SWITCH(meads_k_slots(ws->P), meads_init_kernel<K><<<grid, 256, 0, (cudaStream_t)stream>>>(a));
+    UT_LAUNCHED();
+    return UT_OK;
+}
+
+int32_t ut_meads_iteration(ut_workspace* ws, const ut_meads_buffers* buf, int32_t num_folds, int32_t iteration,
+                           float divergence_threshold, uint32_t iteration_coord, void* stream) {
+    int32_t rc = check_ws(ws);
+    if (rc) return rc;
+    if ((rc = meads_check(ws, buf))) return rc;
+    if (num_folds < 2 || num_folds > 32) return fail(UT_ERR_ARGUMENT, "num_folds must be in 2..32, got %d", (int)num_folds);
+    if (ws->C < 2 * num_folds)
+        return fail(UT_ERR_ARGUMENT, "MEADS needs num_chains >= 2 * num_folds; got num_chains=%d, num_folds=%d",
+                    (int)ws->C, (int)num_folds);
+    if (iteration < 1) return fail(UT_ERR_ARGUMENT, "iteration must be >= 1, got %d", (int)iteration);
+    if ((rc = ensure_lf(ws))) return rc;
+    const int P = ws->P, C = ws->C, K = num_folds;
+    const int tx = (P + kMeadsTile - 1) / kMeadsTile;
+    MeadsScratch& s = ws->meads;
+    if (ws->meads_k != K) {  // (re)allocate for this fold count; earlier buffers are freed with the workspace
+        s.ntiles = tx * tx;
+        if ((rc = dalloc(ws, &s.mean, (size_t)K * P))) return rc;
+        if ((rc = dalloc(ws, &s.sd, (size_t)K * P))) return rc;
+        if ((rc = dalloc(ws, &s.tiles, (size_t)K * 2 * s.ntiles))) return rc;
+        if ((rc = dalloc(ws, &s.norms, (size_t)K * 4))) return rc;
+        if ((rc = dalloc(ws, &s.sdf, (size_t)K * P))) return rc;
+        if ((rc = dalloc(ws, &s.fold, (size_t)K * 4))) return rc;
+        if (!s.refreshed && (rc = dalloc(ws, &s.refreshed, (size_t)C * P))) return rc;
+        ws->meads_k = K;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    MeadsFolds fo;
+    fo.C = C; fo.P = P; fo.K = K;
+    const int skip = (iteration - 1) % K;
+    meads_stats_kernel<<<dim3(P, K), 256, 0, st>>>(fo, buf->position, s);
+    meads_moment_kernel<<<dim3(tx, tx, 2 * K), dim3(kMeadsTile, kMeadsTile), 0, st>>>(fo, buf->position,
+                                                                                       buf->gradient, s);
+    meads_norm_kernel<<<2 * K, 256, 0, st>>>(fo, buf->position, buf->gradient, s);
+    meads_params_kernel<<<1, 32, 0, st>>>(fo, s, (int)iteration);
+    UT_LAUNCHED();
+    MeadsArgs a = meads_args(ws, buf, iteration_coord, divergence_threshold, skip);
+    const unsigned grid = (unsigned)((C + 7) / 8);
+    const int KS = meads_k_slots(P);
+    UT_MEADS_K_SWITCH(KS, meads_begin_kernel<K><<<grid, 256, 0, st>>>(a, fo, s, ws->lf));
+    UT_LAUNCHED();
+    if ((rc = density(ws, ws->lf.wq, ws->lf.wlj, ws->lf.wg, st))) return rc;
+    UT_MEADS_K_SWITCH(KS, meads_end_kernel<K><<<grid, 256, 0, st>>>(a, fo, s, ws->lf));
+    UT_LAUNCHED();
+    if (buf->fold_parameters)
+        UT_CUDA(cudaMemcpyAsync(buf->fold_parameters, s.fold, sizeof(float) * 4 * K, cudaMemcpyDeviceToDevice, st));
     return UT_OK;
 }
 
