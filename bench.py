@@ -12,7 +12,7 @@ shipped).
 At N=1 the line also carries `hbm_sweep`: the same design at 1, 4, 8 and 16
 chains, where an evaluation is bound by reading X from HBM (achieved GB/s
 against the measured HBM bandwidth), `samplers`: the config-1 HMC, config-2
-persistent-NUTS and config-3 masked-NUTS runs (min ESS/s, R-hat, gradient
+persistent-NUTS, config-3 masked-NUTS and config-3 MEADS runs (min ESS/s, R-hat, gradient
 evaluations/s; skipped with --no-samplers), `surrogate_chees`: the
 learned-gradient-surrogate workload on the same model (min ESS/s of
 surrogate-driven ChEES-HMC vs plain ChEES-HMC and vs the plain masked NUTS run,
@@ -252,6 +252,7 @@ def run_b200(args):
         if not args.no_samplers:
             samplers = sampler_configs()
             samplers["config3_nuts"] = config3_nuts()
+            samplers["config3_meads"] = config3_meads()
     if rank == 0 and world == 1 and not args.no_surrogate:
         sur = surrogate_comparison()
         if samplers is not None:
@@ -399,6 +400,25 @@ def config3_nuts(num_chains=4096, num_warmup=200, num_samples=200):
             "mean_tree_depth": float(ch.tree_depth.mean()), "max_tree_depth": int(ch.tree_depth.max()),
             "mean_leapfrog_steps": float(ch.integration_steps.mean()),
             "config": f"{num_chains} chains, masked NUTS depth 10, {num_warmup}+{num_samples}, GLM 100000x100"}
+
+
+def config3_meads(num_chains=4096, num_warmup=3000, num_samples=1000):
+    """MEADS on the large logistic regression (4096 chains, 4 folds): one
+    batched tensor-core gradient per iteration, every adaptation statistic on
+    the device, no warmup adaptation phase.  Started from prior draws (a
+    posterior ~15x narrower than the prior) the ensemble step size grows from
+    3e-4 to ~0.5 over ~2500 iterations as the folds contract, so the first 3000
+    draws are discarded."""
+    from uncertaintea_b200 import batched_meads, ess, rhat
+    model, X, y, _ = _data()
+    ch = batched_meads(model, (X,), {"y": y}, num_chains=num_chains, num_samples=num_samples,
+                       num_warmup=num_warmup, rng=1)
+    e, r = ess(ch, space="unconstrained"), rhat(ch, space="unconstrained")
+    return {"min_ess_per_s": float(np.min(e) / ch.sampling_seconds), "min_ess": float(np.min(e)),
+            "max_rhat": float(np.max(r)), "warmup_s": ch.warmup_seconds, "sampling_s": ch.sampling_seconds,
+            "ms_per_iteration": 1e3 * ch.sampling_seconds / num_samples,
+            "mean_accept": float(ch.accept_prob.mean()), "step_size": float(np.mean(ch.step_size)),
+            "config": f"{num_chains} chains, MEADS 4 folds, {num_warmup} discarded + {num_samples}, GLM 100000x100"}
 
 
 def surrogate_comparison(num_chains=4096, num_warmup=500, num_samples=500):
