@@ -58,13 +58,20 @@ extern "C" {
  * DeviceLoopStep of normal observations, src/device/plan/steps.jl:6-44,
  * 445-449; scored at src/device/logjoint_kernel.jl:105-111, 146-151). */
 #define UT_FAMILY_NORMAL_LOCATION_SCALE      3
+/* Bernoulli observations of a beta probability: p ~ beta(prob_alpha,
+ * prob_beta) (logit transform, log|J| = -|u| - 2 log1p(exp(-|u|))),
+ * z_i ~ bernoulli(p) for i = 1..N.  The reference's device-lowerable
+ * bernoulli model (DeviceBetaChoiceStep with the logit transform and a loop
+ * of Bernoulli observations; math.jl:161-165, 191-195, 1144-1159). */
+#define UT_FAMILY_BERNOULLI_BETA             4
 
 /* Fixed kernel description: what the host lowers a model's execution plan to
  * (reference: DeviceExecutionPlan, src/device/plan/steps.jl:482-489, produced
  * by _lower_device_plan, src/device/plan/lowering.jl:1360).  Parameter rows:
  *   GLM : [intercept (if has_intercept)] then num_coefs coefficients;
  *   HIER: [mu, log(tau), z_1 .. z_J];
- *   NLS : [mu, log(s)]. */
+ *   NLS : [mu, log(s)];
+ *   BB  : [logit(p)]. */
 typedef struct ut_plan_desc {
     int32_t family;          /* UT_FAMILY_*                                   */
     int32_t num_params;      /* P, unconstrained parameter count              */
@@ -81,6 +88,8 @@ typedef struct ut_plan_desc {
     double tau_scale;        /* HIER: tau ~ halfcauchy(tau_scale)             */
     double scale_shape;      /* NLS: s ~ gamma(scale_shape, scale_rate)       */
     double scale_rate;       /*      (mu uses mu_loc / mu_scale)              */
+    double prob_alpha;       /* BB: p ~ beta(prob_alpha, prob_beta)           */
+    double prob_beta;
 } ut_plan_desc;
 
 typedef struct ut_workspace ut_workspace;
@@ -108,7 +117,8 @@ int32_t ut_lowering_report(const ut_plan_desc* plan, char* issues, size_t len);
  *   HIER: observed_rows = N + J:  the N y values group after group, then the
  *         J fixed sigma_j; trip_counts[j] = n_j and loop_starts[j] = first row
  *         of group j (num_loops = J);
- *   NLS : observed_rows = N: the y values (no loops are passed).
+ *   NLS : observed_rows = N: the y values (no loops are passed);
+ *   BB  : observed_rows = N: the z values.
  * precision_bits must be 32 (Float32); anything else is UT_ERR_PRECISION. */
 int32_t ut_workspace_create(const ut_plan_desc* plan,
                             const float* observed, int64_t observed_rows, int64_t observed_cols,

@@ -152,7 +152,7 @@ ModelData make_model(const ut_plan_desc* plan, const float* observed, const int3
             for (int d = 0; d < D; ++d) m.X[(size_t)i * D + d] = observed[(size_t)i * (D + 1) + d];
             m.y[i] = observed[(size_t)i * (D + 1) + D];
         }
-    } else if (plan->family == UT_FAMILY_NORMAL_LOCATION_SCALE) {
+    } else if (plan->family == UT_FAMILY_NORMAL_LOCATION_SCALE || plan->family == UT_FAMILY_BERNOULLI_BETA) {
         m.y.assign(observed, observed + N);
     } else {
         const int J = plan->num_groups;
@@ -261,8 +261,35 @@ W gauss_logjoint_grad(const ModelData& m, const T* q, T* g) {
     return total;
 }
 
+// Bernoulli observations of a beta probability (steps: Beta with the logit
+// transform, math.jl:161-165, 1150-1155, then the loop of Bernoulli
+// observations, math.jl:191-195), every observation scored separately.
+template <class T, class W>
+W bern_logjoint_grad(const ModelData& m, const T* q, T* g) {
+    const ut_plan_desc& pl = m.plan;
+    const T u = q[0];
+    const T p = T(1) / (T(1) + std::exp(-u));
+    const T a = T(pl.prob_alpha), b = T(pl.prob_beta);
+    const T lbeta = (T)(std::lgamma(pl.prob_alpha) + std::lgamma(pl.prob_beta) -
+                        std::lgamma(pl.prob_alpha + pl.prob_beta));
+    const T au = std::fabs(u);
+    W total = (p > T(0) && p < T(1)) ? (W)((a - T(1)) * std::log(p) + (b - T(1)) * std::log1p(-p) - lbeta)
+                                     : -std::numeric_limits<W>::infinity();
+    total += (W)(-au - T(2) * std::log1p(std::exp(-au)));
+    W gu = (W)(a - T(1)) * (W(1) - (W)p) - (W)(b - T(1)) * (W)p + W(1) - W(2) * (W)p;
+    for (size_t i = 0; i < m.y.size(); ++i) {
+        const T z = (T)m.y[i];
+        const bool in_support = z == T(0) || z == T(1);
+        total += in_support ? (W)(z > T(0.5) ? std::log(p) : std::log1p(-p)) : -std::numeric_limits<W>::infinity();
+        gu += z > T(0.5) ? W(1) - (W)p : -(W)p;
+    }
+    if (g) g[0] = (T)gu;
+    return total;
+}
+
 template <class T, class W>
 W logjoint_grad(const ModelData& m, const T* q, T* g) {
+    if (m.plan.family == UT_FAMILY_BERNOULLI_BETA) return bern_logjoint_grad<T, W>(m, q, g);
     if (m.plan.family == UT_FAMILY_GLM_BERNOULLI_LOGIT) return glm_logjoint_grad<T, W>(m, q, g);
     if (m.plan.family == UT_FAMILY_NORMAL_LOCATION_SCALE) return gauss_logjoint_grad<T, W>(m, q, g);
     return hier_logjoint_grad<T, W>(m, q, g);

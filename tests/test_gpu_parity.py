@@ -19,8 +19,8 @@ import pytest
 
 import oracle
 from uncertaintea_b200 import _native as nat
-from uncertaintea_b200.models import (BernoulliLogitGLM, HierarchicalNormalNoncentered, NormalLocationScale,
-                                      gauss_data, hierarchical_data, logistic_regression_data)
+from uncertaintea_b200.models import (BernoulliBeta, BernoulliLogitGLM, HierarchicalNormalNoncentered,
+                                      NormalLocationScale, gauss_data, hierarchical_data, logistic_regression_data)
 
 pytestmark = pytest.mark.gpu
 
@@ -140,6 +140,24 @@ def test_gauss_density_vs_fp64_oracle(lib, n, C):
     m = NormalLocationScale()
     ws = _ws(m, (n,), {"y": y}, C)
     assert ws.kernel_path() == "warp"
+    t, g = ws.logjoint_gradient(q.T)
+    t64, g64 = oracle.OracleModel(ws.lowered).logjoint_gradient_f64(q.astype(np.float64))
+    assert _lj_err(t, t64) <= 1e-5
+    assert _grad_err(np.asarray(g.T), g64) <= 1e-5
+    ws.close()
+
+
+@pytest.mark.parametrize("n,C", [(4, 3), (1000, 64), (0, 4)])
+def test_bernoulli_beta_density_vs_fp64_oracle(lib, n, C):
+    """The Bernoulli-beta family; n = 4, C = 3 is the reference's own parity case
+    (device_lowering_parity.jl:150-158)."""
+    if n == 4:
+        z = np.array([1.0, 0.0, 1.0, 1.0], dtype=np.float32)
+        q = np.array([[0.3], [-0.8], [1.5]], dtype=np.float32)
+    else:
+        z = (np.random.default_rng(3).random(n) < 0.3).astype(np.float32)
+        q = (np.random.default_rng(4).standard_normal((C, 1)) * 2).astype(np.float32)
+    ws = _ws(BernoulliBeta(), (n,), {"z": z}, C)
     t, g = ws.logjoint_gradient(q.T)
     t64, g64 = oracle.OracleModel(ws.lowered).logjoint_gradient_f64(q.astype(np.float64))
     assert _lj_err(t, t64) <= 1e-5
@@ -323,9 +341,14 @@ def _nuts_gpu(ws, qd, g, t, im, step, depth, coord):
     return res
 
 
-@pytest.mark.parametrize("case", ["hier", "glm", "gauss"])
+@pytest.mark.parametrize("case", ["hier", "glm", "gauss", "bern"])
 def test_persistent_nuts_iteration_vs_oracle(lib, case):
-    if case == "gauss":
+    if case == "bern":
+        z = (np.random.default_rng(3).random(300) < 0.3).astype(np.float32)
+        m, args, cons = BernoulliBeta(), (300,), {"z": z}
+        q = (np.log(0.3 / 0.7) + 0.2 * np.random.default_rng(5).standard_normal((128, 1))).astype(np.float32)
+        step = 0.3
+    elif case == "gauss":
         m, args, cons, q = _gauss_near_mode(200, 128, 8, 0.1)
         step = 0.1
     elif case == "hier":

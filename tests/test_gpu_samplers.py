@@ -12,7 +12,8 @@ instead, with the reason stated at the assertion."""
 import numpy as np
 import pytest
 
-from uncertaintea_b200 import (BernoulliLogitGLM, HierarchicalNormalNoncentered, NormalLocationScale, batched_advi,
+from uncertaintea_b200 import (BernoulliBeta, BernoulliLogitGLM, HierarchicalNormalNoncentered, NormalLocationScale,
+                               batched_advi,
                                batched_chees, batched_hmc, batched_meads, batched_nuts, ess, gauss_data, hierarchical_data,
                                logistic_regression_data, rhat, variational_mean, variational_samples)
 
@@ -242,6 +243,24 @@ def test_meads_on_the_glm_matches_nuts(lib):
                         rng=np.random.default_rng(13))
     (m1, s1), (m2, s2) = _mean_mcse(res), _mean_mcse(nuts)
     assert np.all(np.abs(m1 - m2) <= 5 * np.hypot(s1, s2))
+
+
+def test_bernoulli_beta_nuts_matches_the_conjugate_posterior(lib):
+    """Beta(2, 3) prior, Bernoulli data: the posterior is Beta(2 + S, 3 + n - S);
+    NUTS mean of p within 5 MCSE of it, and MEADS agrees too."""
+    z = (np.random.default_rng(17).random(200) < 0.35).astype(np.float32)
+    S, n = float(z.sum()), 200
+    exact = (2 + S) / (5 + n)
+    m = BernoulliBeta()
+    res = batched_nuts(m, (n,), {"z": z}, num_chains=512, num_samples=400, num_warmup=400,
+                       rng=np.random.default_rng(18))
+    assert np.max(rhat(res)) < 1.01
+    mean, mcse = _mean_mcse(res)
+    assert abs(mean[0] - exact) <= 5 * mcse[0], (mean[0], exact, mcse[0])
+    med = batched_meads(m, (n,), {"z": z}, num_chains=256, num_samples=800, num_warmup=400,
+                        rng=np.random.default_rng(19))
+    mean2, mcse2 = _mean_mcse(med)
+    assert abs(mean2[0] - exact) <= 5 * mcse2[0], (mean2[0], exact, mcse2[0])
 
 
 def test_seed_reproducibility(lib):

@@ -4,8 +4,8 @@ import numpy as np
 import pytest
 
 import oracle
-from uncertaintea_b200.models import (BernoulliLogitGLM, HierarchicalNormalNoncentered, NormalLocationScale,
-                                      gauss_data, hierarchical_data, logistic_regression_data)
+from uncertaintea_b200.models import (BernoulliBeta, BernoulliLogitGLM, HierarchicalNormalNoncentered,
+                                      NormalLocationScale, gauss_data, hierarchical_data, logistic_regression_data)
 
 
 def test_philox_kat_vectors(pins):
@@ -209,3 +209,21 @@ def test_meads_max_eig_pins():
     sq = (x * x).sum(0)
     alt = ((A * A).sum() - (sq ** 2).sum()) / (n * (n - 1)) / (sq.sum() / n)
     assert abs(oracle.meads_max_eig(x) - alt) < 1e-10 * alt
+
+
+def test_bernoulli_beta_oracle_on_the_reference_parity_case():
+    """The reference's bernoulli parity case (device_lowering_parity.jl:150-158):
+    z = [1, 0, 1, 1], three chains of u = logit p, against the closed form."""
+    from scipy import stats
+    z = np.array([1.0, 0.0, 1.0, 1.0])
+    om = oracle.OracleModel(BernoulliBeta().lower((4,), {"z": z}))
+    u = np.array([[0.3], [-0.8], [1.5]])
+    t, g = om.logjoint_gradient_f64(u)
+    for c in range(3):
+        p = 1 / (1 + np.exp(-u[c, 0]))
+        ref = stats.beta(2, 3).logpdf(p) + np.log(p) + np.log1p(-p) + stats.bernoulli(p).logpmf(z).sum()
+        assert abs(t[c] - ref) <= 1e-12 * abs(ref)
+        assert abs(g[c, 0] - (3 + 2 - (4 + 5) * p)) <= 1e-12
+    # a value outside {0, 1} is outside the support
+    bad = oracle.OracleModel(BernoulliBeta().lower((2,), {"z": np.array([1.0, 0.5])}))
+    assert bad.logjoint_gradient_f64(u)[0][0] == -np.inf

@@ -25,6 +25,7 @@ UT_ERR_DEVICE_TIMEOUT = 7
 UT_FAMILY_GLM_BERNOULLI_LOGIT = 1
 UT_FAMILY_HIER_NORMAL_NONCENTERED = 2
 UT_FAMILY_NORMAL_LOCATION_SCALE = 3
+UT_FAMILY_BERNOULLI_BETA = 4
 
 
 class PlanDesc(ctypes.Structure):
@@ -44,6 +45,8 @@ class PlanDesc(ctypes.Structure):
         ("tau_scale", c_double),
         ("scale_shape", c_double),
         ("scale_rate", c_double),
+        ("prob_alpha", c_double),
+        ("prob_beta", c_double),
     ]
 
 

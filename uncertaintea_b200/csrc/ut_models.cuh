@@ -48,6 +48,16 @@ struct GaussModel {
     const float* y;  // N
 };
 
+// Bernoulli observations of a beta probability (reference device steps: Beta
+// with the logit transform, math.jl:161-165, 1150-1155; a loop of Bernoulli
+// observations, math.jl:191-195).  lbeta = loggamma(a) + loggamma(b) -
+// loggamma(a + b), a constant the host computes.
+struct BernModel {
+    int N;
+    float a, b, lbeta;
+    const float* z;  // N
+};
+
 // Parameters in per-warp shared memory so every lane can read any coefficient
 // with a broadcast load.  `qs` has room for P floats.
 template <int K, int DMAX>
@@ -207,6 +217,42 @@ __device__ __forceinline__ float gauss_lj_grad(const GaussModel& m, const float 
         for (int k = 0; k < K; ++k) g[k] = 0.0f;
         if (lane == 0) g[0] = sr * inv_s * inv_s - (mu - m.mu_loc) / (m.mu_scale * m.mu_scale);
         if (lane == 1) g[0] = -nf + sq * inv_s * inv_s + m.shape - m.rate * s;
+    }
+    return lj;
+}
+
+// One parameter u = logit p in lane 0.  The observation loop counts ones,
+// zeros and values outside {0, 1} (which score -Inf):
+//   sum_i bernoulli(p, z_i) = S log p + (n - S) log1p(-p),
+//   d/du = S - n p;  beta prior (a-1) log p + (b-1) log1p(-p) - lbeta,
+//   d/du = (a-1)(1-p) - (b-1) p;  log|J| = -|u| - 2 log1p(exp(-|u|)),
+//   d/du = 1 - 2p.  -Inf when p is not strictly inside (0, 1).
+template <int K>
+__device__ __forceinline__ float bern_lj_grad(const BernModel& m, const float (&q)[K], float (&g)[K],
+                                              bool want_grad) {
+    const int lane = threadIdx.x & 31;
+    const float u = __shfl_sync(UT_FULL_MASK, q[0], 0);
+    float ones = 0.0f, zeros = 0.0f, bad = 0.0f;
+    for (int i = lane; i < m.N; i += 32) {
+        const float zv = m.z[i];
+        ones += zv == 1.0f ? 1.0f : 0.0f;
+        zeros += zv == 0.0f ? 1.0f : 0.0f;
+        bad += (zv == 0.0f || zv == 1.0f) ? 0.0f : 1.0f;
+    }
+    ones = warp_sum(ones);
+    zeros = warp_sum(zeros);
+    bad = warp_sum(bad);
+    const float p = 1.0f / (1.0f + expf(-u));
+    const float lp = logf(p), l1p = log1pf(-p);
+    const float au = fabsf(u);
+    float lj = ones * lp + zeros * l1p;
+    lj += (p > 0.0f && p < 1.0f) ? (m.a - 1.0f) * lp + (m.b - 1.0f) * l1p - m.lbeta : -INFINITY;
+    lj += -au - 2.0f * log1pf(expf(-au));
+    if (bad > 0.0f) lj = -INFINITY;
+    if (want_grad) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) g[k] = 0.0f;
+        if (lane == 0) g[0] = ones + m.a - (ones + zeros + m.a + m.b) * p;
     }
     return lj;
 }

@@ -233,6 +233,51 @@ class NormalLocationScale(TeaModelSpec):
         return out
 
 
+@dataclass
+class BernoulliBeta(TeaModelSpec):
+    """``p ~ beta(alpha, beta)``, ``z[i] ~ bernoulli(p)`` for i = 1..n -- the
+    reference's device-lowerable bernoulli model
+    (test/uncertaintea/core/device_lowering_parity.jl:30-37: ``p ~ beta(2, 3)``).
+
+    Unconstrained parameter: [logit(p)]; constrained: [p].
+    args = (n,); constraints = {"z": z} with z in {0, 1}.
+    """
+
+    alpha: float = 2.0
+    beta: float = 3.0
+    name: str = "bernoulli_beta"
+
+    def parameter_names(self, args=(), constraints=None):
+        return ["p"]
+
+    def lower(self, args=(), constraints=None) -> Lowered:
+        if len(args) != 1:
+            raise ValueError(f"{self.name} expects args=(n,), got {len(args)} argument(s)")
+        n = int(args[0])
+        if n < 0:
+            raise ValueError("n must be >= 0")
+        z = _observed_value(constraints, "z").astype(np.float32).reshape(-1)
+        if z.shape != (n,):
+            raise IndexError(f"expected {n} observations, got shape {z.shape}")
+        plan = nat.PlanDesc(
+            family=nat.UT_FAMILY_BERNOULLI_BETA, num_params=1, num_obs=n, num_coefs=0, has_intercept=0,
+            num_groups=0, intercept_mu=0.0, intercept_sigma=1.0, coef_mu=0.0, coef_sigma=1.0, mu_loc=0.0,
+            mu_scale=1.0, tau_scale=1.0, scale_shape=1.0, scale_rate=1.0, prob_alpha=self.alpha,
+            prob_beta=self.beta)
+        empty = np.zeros(0, dtype=np.int32)
+        return Lowered(plan, np.ascontiguousarray(z), empty, empty, 1)
+
+    def constrain(self, unconstrained, args=(), constraints=None):
+        u = np.asarray(unconstrained, dtype=np.float64)
+        return 1.0 / (1.0 + np.exp(-u))
+
+    def initial_positions(self, rng, num_chains, args=(), constraints=None, init_strategy="prior"):
+        if init_strategy == "uniform":
+            return rng.uniform(-2.0, 2.0, size=(num_chains, 1))
+        p = np.clip(rng.beta(self.alpha, self.beta, size=(num_chains, 1)), 1e-12, 1 - 1e-12)
+        return np.log(p) - np.log1p(-p)
+
+
 # ---- synthetic workloads (seeded stand-ins for the benchmark data sets) -----
 
 def logistic_regression_data(num_obs: int, num_coefs: int, seed: int, x_scale: float = 1.0):
