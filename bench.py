@@ -324,6 +324,29 @@ def hbm_sweep(chain_counts=(1, 4, 8, 16), steps=20, warmup=5):
             nbytes = N_OBS * N_COEF * 4 + N_OBS * 4 + (2 if grad else 1) * C * N_COEF * 4 + C * 4
             gbs = nbytes / (ms / 1000.0) / 1e9
             row[name] = {"ms": ms, "bytes": nbytes, "GB/s": gbs, "frac": gbs / hbm}
+        # sustained: evaluations back to back over 6 workspaces holding their own
+        # copies of X (240 MB > the 126 MB L2, visited cyclically, so every
+        # evaluation reads its design from HBM), one event pair around them all
+        extra = [DeviceBatchedWorkspace(model, C, args=(X,), constraints={"y": y}) for _ in range(5)]
+        ring = [ws] + extra
+        reps = 10 * len(ring)
+        for _ in range(2):
+            for w in ring:
+                w.logjoint_gradient_device(qd, totals, grads)
+        a_ev, b_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a_ev.record(stream)
+        for r in range(reps):
+            ring[r % len(ring)].logjoint_gradient_device(qd, totals, grads)
+        b_ev.record(stream)
+        torch.cuda.synchronize()
+        ms = a_ev.elapsed_time(b_ev) / reps
+        nbytes = N_OBS * N_COEF * 4 + N_OBS * 4 + 2 * C * N_COEF * 4 + C * 4
+        row["sustained_logjoint_gradient"] = {"ms": ms, "GB/s": nbytes / (ms / 1000.0) / 1e9,
+                                              "frac": nbytes / (ms / 1000.0) / 1e9 / hbm,
+                                              "method": "back-to-back over 6 copies of X (240 MB > L2), no flush"}
+        for w in extra:
+            w.close()
         out.append(row)
         ws.close()
     # Yardsticks under the same flush + event method: a one-element fill (the
