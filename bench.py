@@ -110,6 +110,22 @@ def _dist():
     return world, rank, local
 
 
+def _max_over_ranks(x, dist=None, device="cuda"):
+    """Max of x over all ranks (the slowest replica's clock); x itself at N = 1."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _replica_value(units_per_rank, world, seconds_max):
+    """Whole-job throughput of `world` independent replicas: all ranks' units over
+    the max-over-ranks time."""
+    return world * units_per_rank / seconds_max
+
+
 def _data():
     from uncertaintea_b200.models import BernoulliLogitGLM, logistic_regression_data
     X, y, _ = logistic_regression_data(N_OBS, N_COEF, seed=3, x_scale=1.0 / np.sqrt(N_COEF))
@@ -197,13 +213,9 @@ def run_b200(args):
         dist.barrier()
     step_ms = [s.elapsed_time(e) for s, e in evs]
     total_ms = float(sum(step_ms))
-    t_max = total_ms
-    if dist:
-        tt = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
+    t_max = _max_over_ranks(total_ms, dist)
     clk = clocks.stop()
-    value = world * N_CHAINS * args.steps / (t_max / 1000.0)
+    value = _replica_value(N_CHAINS * args.steps, world, t_max / 1000.0)
 
     # end to end through the public host-array API: pinned host params in,
     # host totals + gradients out, every step.
@@ -218,12 +230,8 @@ def run_b200(args):
     e2e_steps = max(3, args.steps // 2)
     for _ in range(e2e_steps):
         vals, g = ws.logjoint_gradient(pt)
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        tt = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
-    e2e_value = world * N_CHAINS * e2e_steps / e2e_s
+    e2e_s = _max_over_ranks(time.perf_counter() - t0, dist)
+    e2e_value = _replica_value(N_CHAINS * e2e_steps, world, e2e_s)
 
     hbm, bf16, peak_kind = _peaks()
     tc = bool(getattr(ws, "tensor_core_path", lambda: False)())
