@@ -226,7 +226,7 @@ int32_t ut_persistent_nuts_iteration(ut_workspace* ws, const ut_nuts_buffers* bu
  * whose gradient is a batched all-chains kernel (the large GLM): every chain's
  * tree is advanced one leaf per step between batched gradient evaluations, with
  * the tree decisions and Philox draws of ut_persistent_nuts_iteration (so the
- * two give the same trees where both apply).  Synchronises `stream` every 4
+ * two give the same trees where both apply).  Synchronises `stream` every 16
  * leaves to stop once every tree is complete.  P <= 256, max_tree_depth <= 16.
  * reference: the masked lockstep device tree (src/device/nuts_kernels.jl:61-600). */
 int32_t ut_lockstep_nuts_iteration(ut_workspace* ws, const ut_nuts_buffers* buf, int32_t max_tree_depth,

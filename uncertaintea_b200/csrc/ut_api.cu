@@ -993,6 +993,10 @@ int32_t ut_advi_step(ut_workspace* ws, const float* d_location, const float* d_s
 }
 
 // ---- lockstep (masked) NUTS ------------------------------------------------
+// Leaves between the host's checks of the live-chain count: a check drains the
+// stream, while a step with no live chain costs only its kernels' early exits.
+constexpr int kLsCheckEvery = 16;
+
 int32_t ut_lockstep_nuts_iteration(ut_workspace* ws, const ut_nuts_buffers* buf, int32_t max_tree_depth,
                                    float divergence_threshold, uint32_t iteration_coord, void* stream) {
     int32_t rc = check_ws(ws);
@@ -1050,7 +1054,7 @@ int32_t ut_lockstep_nuts_iteration(ut_workspace* ws, const ut_nuts_buffers* buf,
     const unsigned grid = (unsigned)((C + 3) / 4);
     UT_K_SWITCH(K, ls_init_kernel<K><<<grid, 128, 0, st>>>(a));
     UT_LAUNCHED();
-    // at most 2^max_depth - 1 leaves per tree; every 4 leaves the host stops once no
+    // at most 2^max_depth - 1 leaves per tree; every kLsCheckEvery leaves the host stops once no
     // chain is still growing
     const int max_steps = (1 << max_tree_depth) - 1;
     const bool compact = ws->tc.enabled;
@@ -1058,7 +1062,7 @@ int32_t ut_lockstep_nuts_iteration(ut_workspace* ws, const ut_nuts_buffers* buf,
     for (int step = 0; step < max_steps; ++step) {
         ls_compact_kernel<<<1, 1024, 0, st>>>(ws->ls_act, (int)C, ws->ls_idx, ws->ls_active);
         UT_LAUNCHED();
-        if (step > 0 && (step & 3) == 0) {
+        if (step > 0 && step % kLsCheckEvery == 0) {
             UT_CUDA(cudaMemcpyAsync(ws->h_active, ws->ls_active, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
             UT_CUDA(cudaStreamSynchronize(st));
             if (*ws->h_active == 0) break;
