@@ -81,6 +81,8 @@ def _glm_case(N, D, C, intercept, seed, scale=1.0):
     (777, 5, 33, True, 1.0),          # ragged sizes, intercept
     (20000, 100, 200, True, 0.1),     # tiled path
     (3000, 40, 64, False, 1.0),       # tiled path, D just above the warp path
+    (5000, 256, 40, False, 0.1),      # the largest GLM (256 parameters), tiled path
+    (3000, 255, 20, True, 0.1),       # 255 covariates + intercept = 256 parameters
 ])
 def test_glm_density_vs_fp64_oracle(lib, N, D, C, intercept, scale):
     m, args, cons, q = _glm_case(N, D, C, intercept, 11, scale)
@@ -113,7 +115,7 @@ def test_glm_density_full_config3_subset(lib):
     ws.close()
 
 
-@pytest.mark.parametrize("J,n,C", [(64, 20, 512), (8, 5, 3), (150, 7, 40)])
+@pytest.mark.parametrize("J,n,C", [(64, 20, 512), (8, 5, 3), (150, 7, 40), (542, 2, 8)])  # 542: 544 params, the max
 def test_hier_density_vs_fp64_oracle(lib, J, n, C):
     y, sig, sizes, _ = hierarchical_data(J, n, 7)
     m = HierarchicalNormalNoncentered(J)

@@ -62,6 +62,19 @@ def test_lowering_report_flags_bad_descriptions(lib):
                         mu_scale=5.0, tau_scale=-1.0)
     assert lib.ut_lowering_report(ctypes.byref(hier), buf, len(buf)) == nat.UT_ERR_UNSUPPORTED
     assert b"tau prior scale" in buf.value
+    # one past the largest supported sizes
+    wide = nat.PlanDesc(family=nat.UT_FAMILY_GLM_BERNOULLI_LOGIT, num_params=257, num_obs=10, num_coefs=257,
+                        has_intercept=0, coef_sigma=1.0)
+    assert lib.ut_lowering_report(ctypes.byref(wide), buf, len(buf)) == nat.UT_ERR_UNSUPPORTED
+    assert b"more than 256" in buf.value
+    wide.num_params = wide.num_coefs = 256
+    assert lib.ut_lowering_report(ctypes.byref(wide), buf, len(buf)) == nat.UT_OK
+    big = nat.PlanDesc(family=nat.UT_FAMILY_HIER_NORMAL_NONCENTERED, num_params=545, num_obs=10, num_groups=543,
+                       mu_scale=5.0, tau_scale=2.5)
+    assert lib.ut_lowering_report(ctypes.byref(big), buf, len(buf)) == nat.UT_ERR_UNSUPPORTED
+    assert b"more than 544" in buf.value
+    big.num_params, big.num_groups = 544, 542
+    assert lib.ut_lowering_report(ctypes.byref(big), buf, len(buf)) == nat.UT_OK
     gauss = nat.PlanDesc(family=nat.UT_FAMILY_NORMAL_LOCATION_SCALE, num_params=2, num_obs=5, mu_scale=1.0,
                          scale_shape=2.0, scale_rate=1.0)
     assert lib.ut_lowering_report(ctypes.byref(gauss), buf, len(buf)) == nat.UT_OK
