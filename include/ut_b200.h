@@ -64,6 +64,12 @@ extern "C" {
  * bernoulli model (DeviceBetaChoiceStep with the logit transform and a loop
  * of Bernoulli observations; math.jl:161-165, 191-195, 1144-1159). */
 #define UT_FAMILY_BERNOULLI_BETA             4
+/* Normal observations with a lognormal log-scale and a gamma location:
+ * a ~ lognormal(mu_loc, mu_scale), b ~ gamma(scale_shape, scale_rate) (both
+ * log transform), y_i ~ normal(b, exp(a)) for i = 1..N.  The reference's
+ * device-lowerable lognormal/gamma model (math.jl:93-97, 103-107; an
+ * exp-derived scale argument). */
+#define UT_FAMILY_LOGNORMAL_GAMMA_NORMAL     5
 
 /* Fixed kernel description: what the host lowers a model's execution plan to
  * (reference: DeviceExecutionPlan, src/device/plan/steps.jl:482-489, produced
@@ -71,7 +77,8 @@ extern "C" {
  *   GLM : [intercept (if has_intercept)] then num_coefs coefficients;
  *   HIER: [mu, log(tau), z_1 .. z_J];
  *   NLS : [mu, log(s)];
- *   BB  : [logit(p)]. */
+ *   BB  : [logit(p)];
+ *   LGN : [log(a), log(b)]. */
 typedef struct ut_plan_desc {
     int32_t family;          /* UT_FAMILY_*                                   */
     int32_t num_params;      /* P, unconstrained parameter count              */
@@ -118,7 +125,8 @@ int32_t ut_lowering_report(const ut_plan_desc* plan, char* issues, size_t len);
  *         J fixed sigma_j; trip_counts[j] = n_j and loop_starts[j] = first row
  *         of group j (num_loops = J);
  *   NLS : observed_rows = N: the y values (no loops are passed);
- *   BB  : observed_rows = N: the z values.
+ *   BB  : observed_rows = N: the z values;
+ *   LGN : observed_rows = N: the y values.
  * precision_bits must be 32 (Float32); anything else is UT_ERR_PRECISION. */
 int32_t ut_workspace_create(const ut_plan_desc* plan,
                             const float* observed, int64_t observed_rows, int64_t observed_cols,

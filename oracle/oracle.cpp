@@ -152,7 +152,8 @@ ModelData make_model(const ut_plan_desc* plan, const float* observed, const int3
             for (int d = 0; d < D; ++d) m.X[(size_t)i * D + d] = observed[(size_t)i * (D + 1) + d];
             m.y[i] = observed[(size_t)i * (D + 1) + D];
         }
-    } else if (plan->family == UT_FAMILY_NORMAL_LOCATION_SCALE || plan->family == UT_FAMILY_BERNOULLI_BETA) {
+    } else if (plan->family == UT_FAMILY_NORMAL_LOCATION_SCALE || plan->family == UT_FAMILY_BERNOULLI_BETA ||
+               plan->family == UT_FAMILY_LOGNORMAL_GAMMA_NORMAL) {
         m.y.assign(observed, observed + N);
     } else {
         const int J = plan->num_groups;
@@ -287,8 +288,38 @@ W bern_logjoint_grad(const ModelData& m, const T* q, T* g) {
     return total;
 }
 
+// Lognormal log-scale and gamma location (steps: LogNormal on a and Gamma on b,
+// both with the log transform, lad = u; math.jl:93-97, 103-107; then the loop
+// of Normal(b, exp(a)) observations), every observation scored separately.
+template <class T, class W>
+W lgn_logjoint_grad(const ModelData& m, const T* q, T* g) {
+    const ut_plan_desc& p = m.plan;
+    const T ua = q[0], ub = q[1];
+    const T a = std::exp(ua), b = std::exp(ub), s = std::exp(a);
+    const T lx = std::log(a);
+    const T z = (lx - T(p.mu_loc)) / T(p.mu_scale);
+    W total = a >= std::numeric_limits<T>::min()
+                  ? (W)(-std::log(T(p.mu_scale)) - T(0.9189385332046727) - z * z / T(2) - lx)
+                  : -std::numeric_limits<W>::infinity();
+    total += (W)ua;
+    total += (W)gamma_logpdf<T>(T(p.scale_shape), T(p.scale_rate), b) + (W)ub;
+    W ga = -(W)(ua - T(p.mu_loc)) / ((W)p.mu_scale * (W)p.mu_scale);
+    W gb = (W)p.scale_shape - (W)p.scale_rate * (W)b;
+    const W inv_s2 = W(1) / ((W)s * (W)s);
+    for (size_t i = 0; i < m.y.size(); ++i) {
+        const T yv = (T)m.y[i];
+        total += (W)normal_logpdf<T>(b, s, yv);
+        const W r = (W)yv - (W)b;
+        ga += (W)a * (-W(1) + r * r * inv_s2);
+        gb += (W)b * r * inv_s2;
+    }
+    if (g) { g[0] = (T)ga; g[1] = (T)gb; }
+    return total;
+}
+
 template <class T, class W>
 W logjoint_grad(const ModelData& m, const T* q, T* g) {
+    if (m.plan.family == UT_FAMILY_LOGNORMAL_GAMMA_NORMAL) return lgn_logjoint_grad<T, W>(m, q, g);
     if (m.plan.family == UT_FAMILY_BERNOULLI_BETA) return bern_logjoint_grad<T, W>(m, q, g);
     if (m.plan.family == UT_FAMILY_GLM_BERNOULLI_LOGIT) return glm_logjoint_grad<T, W>(m, q, g);
     if (m.plan.family == UT_FAMILY_NORMAL_LOCATION_SCALE) return gauss_logjoint_grad<T, W>(m, q, g);

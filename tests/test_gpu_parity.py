@@ -20,7 +20,8 @@ import pytest
 import oracle
 from uncertaintea_b200 import _native as nat
 from uncertaintea_b200.models import (BernoulliBeta, BernoulliLogitGLM, HierarchicalNormalNoncentered,
-                                      NormalLocationScale, gauss_data, hierarchical_data, logistic_regression_data)
+                                      LognormalGammaNormal, NormalLocationScale, gauss_data, hierarchical_data,
+                                      logistic_regression_data)
 
 pytestmark = pytest.mark.gpu
 
@@ -160,6 +161,24 @@ def test_bernoulli_beta_density_vs_fp64_oracle(lib, n, C):
         z = (np.random.default_rng(3).random(n) < 0.3).astype(np.float32)
         q = (np.random.default_rng(4).standard_normal((C, 1)) * 2).astype(np.float32)
     ws = _ws(BernoulliBeta(), (n,), {"z": z}, C)
+    t, g = ws.logjoint_gradient(q.T)
+    t64, g64 = oracle.OracleModel(ws.lowered).logjoint_gradient_f64(q.astype(np.float64))
+    assert _lj_err(t, t64) <= 1e-5
+    assert _grad_err(np.asarray(g.T), g64) <= 1e-5
+    ws.close()
+
+
+@pytest.mark.parametrize("n,C", [(3, 3), (2000, 64)])
+def test_lognormal_gamma_density_vs_fp64_oracle(lib, n, C):
+    """The lognormal/gamma family; n = 3, C = 3 is the reference's parity case
+    (device_lowering_parity.jl:140-148)."""
+    if n == 3:
+        y = np.array([0.4, 1.1, -0.7], dtype=np.float32)
+        q = np.array([[0.5, 0.1], [-0.3, 0.7], [0.9, -0.2]], dtype=np.float32)
+    else:
+        y = (1.5 + 2.0 * np.random.default_rng(3).standard_normal(n)).astype(np.float32)
+        q = (np.array([0.0, 0.4]) + 0.3 * np.random.default_rng(4).standard_normal((C, 2))).astype(np.float32)
+    ws = _ws(LognormalGammaNormal(), (n,), {"y": y}, C)
     t, g = ws.logjoint_gradient(q.T)
     t64, g64 = oracle.OracleModel(ws.lowered).logjoint_gradient_f64(q.astype(np.float64))
     assert _lj_err(t, t64) <= 1e-5

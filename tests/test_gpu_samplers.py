@@ -12,8 +12,8 @@ instead, with the reason stated at the assertion."""
 import numpy as np
 import pytest
 
-from uncertaintea_b200 import (BernoulliBeta, BernoulliLogitGLM, HierarchicalNormalNoncentered, NormalLocationScale,
-                               batched_advi,
+from uncertaintea_b200 import (BernoulliBeta, BernoulliLogitGLM, HierarchicalNormalNoncentered, LognormalGammaNormal,
+                               NormalLocationScale, batched_advi,
                                batched_chees, batched_hmc, batched_meads, batched_nuts, ess, gauss_data, hierarchical_data,
                                logistic_regression_data, rhat, variational_mean, variational_samples)
 
@@ -261,6 +261,30 @@ def test_bernoulli_beta_nuts_matches_the_conjugate_posterior(lib):
                         rng=np.random.default_rng(19))
     mean2, mcse2 = _mean_mcse(med)
     assert abs(mean2[0] - exact) <= 5 * mcse2[0], (mean2[0], exact, mcse2[0])
+
+
+def test_lognormal_gamma_nuts_matches_grid_posterior(lib):
+    """The lognormal/gamma family under NUTS: posterior means of a and b within 5
+    MCSE of a fine grid over (log a, log b)."""
+    from scipy import stats
+    y = (1.5 + 2.0 * np.random.default_rng(21).standard_normal(40)).astype(np.float32).astype(np.float64)
+    m = LognormalGammaNormal()
+    res = batched_nuts(m, (40,), {"y": y}, num_chains=512, num_samples=400, num_warmup=400,
+                       rng=np.random.default_rng(22))
+    assert np.max(rhat(res)) < 1.01
+    ua = np.linspace(-2.5, 1.5, 801)[:, None]
+    ub = np.linspace(-2.0, 1.8, 801)[None, :]
+    a, b = np.exp(ua), np.exp(ub)
+    s = np.exp(a)
+    ss = ((y[None, None, :] - b[..., None]) ** 2).sum(-1)
+    lp = (stats.norm(0, 1).logpdf(ua) + stats.gamma(3.0, scale=0.5).logpdf(b) + ub
+          - len(y) * a - 0.5 * ss / s ** 2)
+    w = np.exp(lp - lp.max())
+    w /= w.sum()
+    ea, eb = float((w * a).sum()), float((w * b).sum())
+    mean, mcse = _mean_mcse(res)
+    assert abs(mean[0] - ea) <= 5 * mcse[0], (mean[0], ea, mcse[0])
+    assert abs(mean[1] - eb) <= 5 * mcse[1], (mean[1], eb, mcse[1])
 
 
 def test_seed_reproducibility(lib):

@@ -5,7 +5,8 @@ import pytest
 
 import oracle
 from uncertaintea_b200.models import (BernoulliBeta, BernoulliLogitGLM, HierarchicalNormalNoncentered,
-                                      NormalLocationScale, gauss_data, hierarchical_data, logistic_regression_data)
+                                      LognormalGammaNormal, NormalLocationScale, gauss_data, hierarchical_data,
+                                      logistic_regression_data)
 
 
 def test_philox_kat_vectors(pins):
@@ -227,3 +228,28 @@ def test_bernoulli_beta_oracle_on_the_reference_parity_case():
     # a value outside {0, 1} is outside the support
     bad = oracle.OracleModel(BernoulliBeta().lower((2,), {"z": np.array([1.0, 0.5])}))
     assert bad.logjoint_gradient_f64(u)[0][0] == -np.inf
+
+
+def test_lognormal_gamma_oracle_on_the_reference_parity_case():
+    """The reference's lognormal/gamma parity case (device_lowering_parity.jl:140-148):
+    y = [0.4, 1.1, -0.7], three chains of (log a, log b), against the closed form;
+    the gradient against central finite differences."""
+    from scipy import stats
+    y = np.array([0.4, 1.1, -0.7])
+    om = oracle.OracleModel(LognormalGammaNormal().lower((3,), {"y": y}))
+    q = np.array([[0.5, 0.1], [-0.3, 0.7], [0.9, -0.2]])
+    t, g = om.logjoint_gradient_f64(q)
+    yf = y.astype(np.float32).astype(np.float64)
+    for c, (ua, ub) in enumerate(q):
+        a, b = np.exp(ua), np.exp(ub)
+        ref = (stats.lognorm(s=1.0, scale=1.0).logpdf(a) + ua + stats.gamma(3.0, scale=0.5).logpdf(b) + ub
+               + stats.norm(b, np.exp(a)).logpdf(yf).sum())
+        assert abs(t[c] - ref) <= 1e-12 * abs(ref)
+    h = 1e-6
+    for c in range(3):
+        for k in range(2):
+            qp, qm = q.copy(), q.copy()
+            qp[c, k] += h
+            qm[c, k] -= h
+            fd = (om.logjoint_gradient_f64(qp)[0][c] - om.logjoint_gradient_f64(qm)[0][c]) / (2 * h)
+            assert abs(fd - g[c, k]) <= 1e-6 * max(1.0, abs(g[c, k]))

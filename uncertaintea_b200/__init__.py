@@ -8,8 +8,8 @@ diagnostics; plus
 the learned gradient surrogate for ChEES-HMC and many-model batched NUTS
 (no reference counterparts).
 """
-from .models import (BernoulliBeta, BernoulliLogitGLM, HierarchicalNormalNoncentered, NormalLocationScale,
-                     TeaModelSpec, gauss_data, hierarchical_data, logistic_regression_data)
+from .models import (BernoulliBeta, BernoulliLogitGLM, HierarchicalNormalNoncentered, LognormalGammaNormal,
+                     NormalLocationScale, TeaModelSpec, gauss_data, hierarchical_data, logistic_regression_data)
 from .device import (DeviceBatchedWorkspace, device_batched_logjoint, device_batched_logjoint_,
                      device_batched_logjoint_gradient, device_batched_logjoint_gradient_, device_lowering_report)
 from .inference import HMCChains, batched_chees, batched_hmc, batched_nuts, posterior_array
@@ -21,7 +21,8 @@ from .meads import batched_meads
 from . import rng
 
 __all__ = [
-    "BernoulliBeta", "BernoulliLogitGLM", "HierarchicalNormalNoncentered", "NormalLocationScale", "TeaModelSpec",
+    "BernoulliBeta", "BernoulliLogitGLM", "HierarchicalNormalNoncentered", "LognormalGammaNormal",
+    "NormalLocationScale", "TeaModelSpec",
     "gauss_data",
     "hierarchical_data",
     "logistic_regression_data", "DeviceBatchedWorkspace", "device_batched_logjoint", "device_batched_logjoint_",

@@ -26,6 +26,7 @@ UT_FAMILY_GLM_BERNOULLI_LOGIT = 1
 UT_FAMILY_HIER_NORMAL_NONCENTERED = 2
 UT_FAMILY_NORMAL_LOCATION_SCALE = 3
 UT_FAMILY_BERNOULLI_BETA = 4
+UT_FAMILY_LOGNORMAL_GAMMA_NORMAL = 5
 
 
 class PlanDesc(ctypes.Structure):

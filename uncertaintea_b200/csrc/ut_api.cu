@@ -167,6 +167,11 @@ std::string plan_issues(const ut_plan_desc* p) {
         if (!(p->mu_scale > 0.0)) add("mu prior scale must be > 0");
         if (!(p->scale_shape > 0.0) || !(p->scale_rate > 0.0)) add("gamma shape and rate must be > 0");
         if (p->num_obs < 0) add("num_obs must be >= 0");
+    } else if (p->family == UT_FAMILY_LOGNORMAL_GAMMA_NORMAL) {
+        if (p->num_params != 2) add("num_params must equal 2 (log a, log b)");
+        if (!(p->mu_scale > 0.0)) add("lognormal scale must be > 0");
+        if (!(p->scale_shape > 0.0) || !(p->scale_rate > 0.0)) add("gamma shape and rate must be > 0");
+        if (p->num_obs < 0) add("num_obs must be >= 0");
     } else if (p->family == UT_FAMILY_BERNOULLI_BETA) {
         if (p->num_params != 1) add("num_params must equal 1 (logit p)");
         if (!(p->prob_alpha > 0.0) || !(p->prob_beta > 0.0)) add("beta prior parameters must be > 0");
@@ -201,6 +206,8 @@ int32_t need_device() {
             KERNEL(kFamGauss, 1, 1, __VA_ARGS__);                                                            \
         } else if ((ws)->dm.family == kFamBern) {                                                            \
             KERNEL(kFamBern, 1, 1, __VA_ARGS__);                                                             \
+        } else if ((ws)->dm.family == kFamLgn) {                                                             \
+            KERNEL(kFamLgn, 1, 1, __VA_ARGS__);                                                              \
         } else {                                                                                             \
             switch ((ws)->K) {                                                                               \
                 case 1: KERNEL(kFamHier, 1, 1, __VA_ARGS__); break;                                          \
@@ -423,7 +430,8 @@ int32_t ut_workspace_create(const ut_plan_desc* plan, const float* observed, int
         if (observed_rows != want)
             return fail(UT_ERR_DIMENSION, "expected %lld staged observation rows (N*(D+1)), got %lld", (long long)want,
                         (long long)observed_rows);
-    } else if (plan->family == UT_FAMILY_NORMAL_LOCATION_SCALE || plan->family == UT_FAMILY_BERNOULLI_BETA) {
+    } else if (plan->family == UT_FAMILY_NORMAL_LOCATION_SCALE || plan->family == UT_FAMILY_BERNOULLI_BETA ||
+               plan->family == UT_FAMILY_LOGNORMAL_GAMMA_NORMAL) {
         if (observed_rows != N)
             return fail(UT_ERR_DIMENSION, "expected %d staged observation rows (N), got %lld", N,
                         (long long)observed_rows);
@@ -551,6 +559,18 @@ int32_t ut_workspace_create(const ut_plan_desc* plan, const float* observed, int
         if ((rc = dalloc(ws, &ws->d_y, std::max(N, 1)))) return bail(rc);
         if (N > 0) UT_CUDA(cudaMemcpy(ws->d_y, observed, sizeof(float) * N, cudaMemcpyHostToDevice));
         dm.gauss.y = ws->d_y;
+        ws->path = kPathWarp;
+        dm.stage = ((size_t)N * 4 + (size_t)kWarpsDensity * dm.Ppad * 4) <= kSmemBudget ? 1 : 0;
+        dm.staged_floats = dm.stage ? ((N + 3) / 4) * 4 : 0;
+    } else if (plan->family == UT_FAMILY_LOGNORMAL_GAMMA_NORMAL) {
+        dm.family = kFamLgn;
+        dm.lgn.N = N;
+        dm.lgn.mu = (float)plan->mu_loc; dm.lgn.sigma = (float)plan->mu_scale;
+        dm.lgn.shape = (float)plan->scale_shape; dm.lgn.rate = (float)plan->scale_rate;
+        dm.lgn.lgc = (float)(plan->scale_shape * std::log(plan->scale_rate) - std::lgamma(plan->scale_shape));
+        if ((rc = dalloc(ws, &ws->d_y, std::max(N, 1)))) return bail(rc);
+        if (N > 0) UT_CUDA(cudaMemcpy(ws->d_y, observed, sizeof(float) * N, cudaMemcpyHostToDevice));
+        dm.lgn.y = ws->d_y;
         ws->path = kPathWarp;
         dm.stage = ((size_t)N * 4 + (size_t)kWarpsDensity * dm.Ppad * 4) <= kSmemBudget ? 1 : 0;
         dm.staged_floats = dm.stage ? ((N + 3) / 4) * 4 : 0;

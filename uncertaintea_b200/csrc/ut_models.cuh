@@ -58,6 +58,16 @@ struct BernModel {
     const float* z;  // N
 };
 
+// Normal observations with a lognormal log-scale and a gamma location (the
+// reference's lognormal/gamma device model: LogNormal and Gamma choice steps
+// with the log transform, math.jl:93-97, 103-107, and a loop of Normal
+// observations whose scale is exp(a)).  lgc = shape log(rate) - loggamma(shape).
+struct LgnModel {
+    int N;
+    float mu, sigma, shape, rate, lgc;
+    const float* y;  // N
+};
+
 // Parameters in per-warp shared memory so every lane can read any coefficient
 // with a broadcast load.  `qs` has room for P floats.
 template <int K, int DMAX>
@@ -253,6 +263,41 @@ __device__ __forceinline__ float bern_lj_grad(const BernModel& m, const float (&
 #pragma unroll
         for (int k = 0; k < K; ++k) g[k] = 0.0f;
         if (lane == 0) g[0] = ones + m.a - (ones + zeros + m.a + m.b) * p;
+    }
+    return lj;
+}
+
+// Lane 0 holds ua = log a, lane 1 ub = log b; s = exp(a), log s = a:
+//   sum_i normal_logpdf(b, s, y_i) = N (-a - log(2 pi) / 2) - sq / (2 s^2),
+//   d/dua = a (-N + sq / s^2) - (ua - mu) / sigma^2   (lognormal + log|J| = ua),
+//   d/dub = b sr / s^2 + shape - rate b               (gamma + log|J| = ub).
+template <int K>
+__device__ __forceinline__ float lgn_lj_grad(const LgnModel& m, const float (&q)[K], float (&g)[K],
+                                             bool want_grad) {
+    const int lane = threadIdx.x & 31;
+    const float ua = __shfl_sync(UT_FULL_MASK, q[0], 0);
+    const float ub = __shfl_sync(UT_FULL_MASK, q[0], 1);
+    const float a = expf(ua), b = expf(ub);
+    const float s = expf(a);
+    float sr = 0.0f, sq = 0.0f;
+    for (int i = lane; i < m.N; i += 32) {
+        const float r = m.y[i] - b;
+        sr += r;
+        sq = fmaf(r, r, sq);
+    }
+    sr = warp_sum(sr);
+    sq = warp_sum(sq);
+    const float inv_s2 = 1.0f / (s * s);
+    const float nf = (float)m.N;
+    float lj = nf * (-a - kHalfLog2Pi) - 0.5f * sq * inv_s2;
+    const float z = (ua - m.mu) / m.sigma;
+    lj += a >= FLT_MIN ? -logf(m.sigma) - kHalfLog2Pi - 0.5f * z * z : -INFINITY;  // lognormal - log a + log|J|
+    lj += b >= FLT_MIN ? m.lgc + (m.shape - 1.0f) * ub - m.rate * b + ub : -INFINITY;
+    if (want_grad) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) g[k] = 0.0f;
+        if (lane == 0) g[0] = a * (-nf + sq * inv_s2) - z / m.sigma;
+        if (lane == 1) g[0] = b * sr * inv_s2 + m.shape - m.rate * b;
     }
     return lj;
 }

@@ -9,7 +9,7 @@
 
 namespace ut {
 
-enum Family : int { kFamGlm = 1, kFamHier = 2, kFamGauss = 3, kFamBern = 4 };
+enum Family : int { kFamGlm = 1, kFamHier = 2, kFamGauss = 3, kFamBern = 4, kFamLgn = 5 };
 
 struct DevModel {
     int family;
@@ -21,6 +21,7 @@ struct DevModel {
     HierModel hier;
     GaussModel gauss;
     BernModel bern;
+    LgnModel lgn;
 };
 
 // Copies the model's observation data into shared memory (when dm.stage) and
@@ -44,6 +45,10 @@ __device__ __forceinline__ void stage_model(DevModel& dm, float* smem) {
         for (int i = threadIdx.x; i < dm.gauss.N; i += blockDim.x) smem[i] = dm.gauss.y[i];
         __syncthreads();
         dm.gauss.y = smem;
+    } else if constexpr (FAM == kFamLgn) {
+        for (int i = threadIdx.x; i < dm.lgn.N; i += blockDim.x) smem[i] = dm.lgn.y[i];
+        __syncthreads();
+        dm.lgn.y = smem;
     } else if constexpr (FAM == kFamBern) {
         for (int i = threadIdx.x; i < dm.bern.N; i += blockDim.x) smem[i] = dm.bern.z[i];
         __syncthreads();
@@ -74,6 +79,7 @@ __device__ __forceinline__ float eval_lj(const DevModel& dm, const float (&q)[K]
     if constexpr (FAM == kFamGlm) return glm_lj_grad<K, DMAX>(dm.glm, dm.P, q, g, qs, want_grad);
     else if constexpr (FAM == kFamGauss) return gauss_lj_grad<K>(dm.gauss, q, g, want_grad);
     else if constexpr (FAM == kFamBern) return bern_lj_grad<K>(dm.bern, q, g, want_grad);
+    else if constexpr (FAM == kFamLgn) return lgn_lj_grad<K>(dm.lgn, q, g, want_grad);
     else return hier_lj_grad<K>(dm.hier, dm.P, q, g, want_grad);
 }
 

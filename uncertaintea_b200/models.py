@@ -278,6 +278,54 @@ class BernoulliBeta(TeaModelSpec):
         return np.log(p) - np.log1p(-p)
 
 
+@dataclass
+class LognormalGammaNormal(TeaModelSpec):
+    """``a ~ lognormal(mu, sigma)``, ``b ~ gamma(shape, rate)``, ``scale = exp(a)``,
+    ``y[i] ~ normal(b, scale)`` -- the reference's device-lowerable lognormal/gamma
+    model (test/uncertaintea/core/device_lowering_parity.jl:21-28:
+    ``a ~ lognormal(0, 1)``, ``b ~ gamma(3, 2)``).
+
+    Unconstrained parameters: [log(a), log(b)]; constrained: [a, b].
+    args = (n,); constraints = {"y": y}.
+    """
+
+    mu: float = 0.0
+    sigma: float = 1.0
+    shape: float = 3.0
+    rate: float = 2.0
+    name: str = "lognormal_gamma_normal"
+
+    def parameter_names(self, args=(), constraints=None):
+        return ["a", "b"]
+
+    def lower(self, args=(), constraints=None) -> Lowered:
+        if len(args) != 1:
+            raise ValueError(f"{self.name} expects args=(n,), got {len(args)} argument(s)")
+        n = int(args[0])
+        if n < 0:
+            raise ValueError("n must be >= 0")
+        y = _observed_value(constraints, "y").astype(np.float32).reshape(-1)
+        if y.shape != (n,):
+            raise IndexError(f"expected {n} observations, got shape {y.shape}")
+        plan = nat.PlanDesc(
+            family=nat.UT_FAMILY_LOGNORMAL_GAMMA_NORMAL, num_params=2, num_obs=n, num_coefs=0, has_intercept=0,
+            num_groups=0, intercept_mu=0.0, intercept_sigma=1.0, coef_mu=0.0, coef_sigma=1.0,
+            mu_loc=self.mu, mu_scale=self.sigma, tau_scale=1.0, scale_shape=self.shape, scale_rate=self.rate)
+        empty = np.zeros(0, dtype=np.int32)
+        return Lowered(plan, np.ascontiguousarray(y), empty, empty, 2)
+
+    def constrain(self, unconstrained, args=(), constraints=None):
+        return np.exp(np.asarray(unconstrained, dtype=np.float64))
+
+    def initial_positions(self, rng, num_chains, args=(), constraints=None, init_strategy="prior"):
+        if init_strategy == "uniform":
+            return rng.uniform(-2.0, 2.0, size=(num_chains, 2))
+        out = np.empty((num_chains, 2))
+        out[:, 0] = rng.normal(self.mu, self.sigma, size=num_chains)
+        out[:, 1] = np.log(np.maximum(rng.gamma(self.shape, 1.0 / self.rate, size=num_chains), 1e-30))
+        return out
+
+
 # ---- synthetic workloads (seeded stand-ins for the benchmark data sets) -----
 
 def logistic_regression_data(num_obs: int, num_coefs: int, seed: int, x_scale: float = 1.0):
