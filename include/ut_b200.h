@@ -70,6 +70,12 @@ extern "C" {
  * device-lowerable lognormal/gamma model (math.jl:93-97, 103-107; an
  * exp-derived scale argument). */
 #define UT_FAMILY_LOGNORMAL_GAMMA_NORMAL     5
+/* Heavy-tailed location with two scales: loc ~ studentt(nu_prior, mu_loc,
+ * mu_scale) (identity), s ~ inversegamma(scale_shape, scale_rate) and
+ * w ~ weibull(weibull_shape, weibull_scale) (both log transform),
+ * y_i ~ studentt(nu_obs, loc, s + w).  The reference's device-lowerable
+ * heavy-tail model (math.jl:167-186). */
+#define UT_FAMILY_STUDENTT_HEAVY_TAIL        6
 
 /* Fixed kernel description: what the host lowers a model's execution plan to
  * (reference: DeviceExecutionPlan, src/device/plan/steps.jl:482-489, produced
@@ -78,7 +84,8 @@ extern "C" {
  *   HIER: [mu, log(tau), z_1 .. z_J];
  *   NLS : [mu, log(s)];
  *   BB  : [logit(p)];
- *   LGN : [log(a), log(b)]. */
+ *   LGN : [log(a), log(b)];
+ *   HT  : [loc, log(s), log(w)]. */
 typedef struct ut_plan_desc {
     int32_t family;          /* UT_FAMILY_*                                   */
     int32_t num_params;      /* P, unconstrained parameter count              */
@@ -97,6 +104,10 @@ typedef struct ut_plan_desc {
     double scale_rate;       /*      (mu uses mu_loc / mu_scale)              */
     double prob_alpha;       /* BB: p ~ beta(prob_alpha, prob_beta)           */
     double prob_beta;
+    double nu_prior;         /* HT: loc ~ studentt(nu_prior, mu_loc, mu_scale) */
+    double nu_obs;           /*     y ~ studentt(nu_obs, loc, s + w)          */
+    double weibull_shape;    /*     w ~ weibull(weibull_shape, weibull_scale) */
+    double weibull_scale;    /*     (s uses scale_shape / scale_rate)         */
 } ut_plan_desc;
 
 typedef struct ut_workspace ut_workspace;
@@ -126,7 +137,8 @@ int32_t ut_lowering_report(const ut_plan_desc* plan, char* issues, size_t len);
  *         of group j (num_loops = J);
  *   NLS : observed_rows = N: the y values (no loops are passed);
  *   BB  : observed_rows = N: the z values;
- *   LGN : observed_rows = N: the y values.
+ *   LGN : observed_rows = N: the y values;
+ *   HT  : observed_rows = N: the y values.
  * precision_bits must be 32 (Float32); anything else is UT_ERR_PRECISION. */
 int32_t ut_workspace_create(const ut_plan_desc* plan,
                             const float* observed, int64_t observed_rows, int64_t observed_cols,

@@ -153,7 +153,7 @@ ModelData make_model(const ut_plan_desc* plan, const float* observed, const int3
             m.y[i] = observed[(size_t)i * (D + 1) + D];
         }
     } else if (plan->family == UT_FAMILY_NORMAL_LOCATION_SCALE || plan->family == UT_FAMILY_BERNOULLI_BETA ||
-               plan->family == UT_FAMILY_LOGNORMAL_GAMMA_NORMAL) {
+               plan->family == UT_FAMILY_LOGNORMAL_GAMMA_NORMAL || plan->family == UT_FAMILY_STUDENTT_HEAVY_TAIL) {
         m.y.assign(observed, observed + N);
     } else {
         const int J = plan->num_groups;
@@ -317,8 +317,51 @@ W lgn_logjoint_grad(const ModelData& m, const T* q, T* g) {
     return total;
 }
 
+// Heavy-tailed location with two scales (steps: StudentT identity, InverseGamma
+// and Weibull with the log transform, then the loop of StudentT observations with
+// scale s + w; densities as math.jl:167-186, loggamma ratio by the C library in
+// double), every observation scored separately.
+template <class T>
+inline T studentt_logpdf(T nu, T mu, T sigma, T x) {
+    const T z = (x - mu) / sigma;
+    const T c = (T)(std::lgamma(((double)nu + 1.0) / 2.0) - std::lgamma((double)nu / 2.0));
+    return c - (std::log(nu) + T(1.1447298858494002)) / T(2) - std::log(sigma) - (nu + T(1)) * std::log1p(z * z / nu) / T(2);
+}
+
+template <class T, class W>
+W ht_logjoint_grad(const ModelData& m, const T* q, T* g) {
+    const ut_plan_desc& p = m.plan;
+    const T loc = q[0], us = q[1], uw = q[2];
+    const T s = std::exp(us), w = std::exp(uw), sig = s + w;
+    const T nu0 = T(p.nu_prior), mu0 = T(p.mu_loc), s0 = T(p.mu_scale), nu1 = T(p.nu_obs);
+    const T a = T(p.scale_shape), b = T(p.scale_rate), k = T(p.weibull_shape), lam = T(p.weibull_scale);
+    W total = (W)studentt_logpdf<T>(nu0, mu0, s0, loc);
+    const T ig = a * std::log(b) - (T)std::lgamma((double)a) - (a + T(1)) * std::log(s) - b / s;  // math.jl:175-179
+    total += (s >= std::numeric_limits<T>::min() ? (W)ig : -std::numeric_limits<W>::infinity()) + (W)us;
+    const T wb = std::log(k) + (k - T(1)) * std::log(w) - k * std::log(lam) - std::exp(k * (std::log(w) - std::log(lam)));
+    total += (w >= std::numeric_limits<T>::min() ? (W)wb : -std::numeric_limits<W>::infinity()) + (W)uw;
+    const W d0 = (W)loc - (W)mu0;
+    W gl = -((W)nu0 + 1) * d0 / ((W)nu0 * (W)s0 * (W)s0 + d0 * d0);
+    W dsig = 0;
+    const W ns2 = (W)nu1 * (W)sig * (W)sig;
+    for (size_t i = 0; i < m.y.size(); ++i) {
+        const T yv = (T)m.y[i];
+        total += (W)studentt_logpdf<T>(nu1, loc, sig, yv);
+        const W r = (W)yv - (W)loc, t = r * r;
+        gl += ((W)nu1 + 1) * r / (ns2 + t);
+        dsig += -W(1) / (W)sig + ((W)nu1 + 1) * t / ((W)sig * (ns2 + t));
+    }
+    if (g) {
+        g[0] = (T)gl;
+        g[1] = (T)(-(W)a + (W)b / (W)s + (W)s * dsig);
+        g[2] = (T)((W)k - (W)k * std::pow((W)w / (W)lam, (W)k) + (W)w * dsig);
+    }
+    return total;
+}
+
 template <class T, class W>
 W logjoint_grad(const ModelData& m, const T* q, T* g) {
+    if (m.plan.family == UT_FAMILY_STUDENTT_HEAVY_TAIL) return ht_logjoint_grad<T, W>(m, q, g);
     if (m.plan.family == UT_FAMILY_LOGNORMAL_GAMMA_NORMAL) return lgn_logjoint_grad<T, W>(m, q, g);
     if (m.plan.family == UT_FAMILY_BERNOULLI_BETA) return bern_logjoint_grad<T, W>(m, q, g);
     if (m.plan.family == UT_FAMILY_GLM_BERNOULLI_LOGIT) return glm_logjoint_grad<T, W>(m, q, g);

@@ -20,8 +20,8 @@ import pytest
 import oracle
 from uncertaintea_b200 import _native as nat
 from uncertaintea_b200.models import (BernoulliBeta, BernoulliLogitGLM, HierarchicalNormalNoncentered,
-                                      LognormalGammaNormal, NormalLocationScale, gauss_data, hierarchical_data,
-                                      logistic_regression_data)
+                                      LognormalGammaNormal, NormalLocationScale, StudentTHeavyTail, gauss_data,
+                                      hierarchical_data, logistic_regression_data)
 
 pytestmark = pytest.mark.gpu
 
@@ -179,6 +179,24 @@ def test_lognormal_gamma_density_vs_fp64_oracle(lib, n, C):
         y = (1.5 + 2.0 * np.random.default_rng(3).standard_normal(n)).astype(np.float32)
         q = (np.array([0.0, 0.4]) + 0.3 * np.random.default_rng(4).standard_normal((C, 2))).astype(np.float32)
     ws = _ws(LognormalGammaNormal(), (n,), {"y": y}, C)
+    t, g = ws.logjoint_gradient(q.T)
+    t64, g64 = oracle.OracleModel(ws.lowered).logjoint_gradient_f64(q.astype(np.float64))
+    assert _lj_err(t, t64) <= 1e-5
+    assert _grad_err(np.asarray(g.T), g64) <= 1e-5
+    ws.close()
+
+
+@pytest.mark.parametrize("n,C", [(5, 3), (3000, 64)])
+def test_heavy_tail_density_vs_fp64_oracle(lib, n, C):
+    """The Student-t heavy-tail family; n = 5, C = 3 is the reference's parity case
+    (device_lowering_parity.jl:170-176)."""
+    if n == 5:
+        y = np.array([0.4, -0.7, 1.1, 0.2, 0.9], dtype=np.float32)
+        q = np.array([[0.5, 0.1, -0.4], [-0.3, 0.7, 0.2], [1.2, -0.2, 0.6]], dtype=np.float32)
+    else:
+        y = (0.5 + np.random.default_rng(3).standard_t(5, size=n)).astype(np.float32)
+        q = (np.array([0.5, -0.3, 0.0]) + 0.3 * np.random.default_rng(4).standard_normal((C, 3))).astype(np.float32)
+    ws = _ws(StudentTHeavyTail(), (n,), {"y": y}, C)
     t, g = ws.logjoint_gradient(q.T)
     t64, g64 = oracle.OracleModel(ws.lowered).logjoint_gradient_f64(q.astype(np.float64))
     assert _lj_err(t, t64) <= 1e-5
@@ -362,9 +380,14 @@ def _nuts_gpu(ws, qd, g, t, im, step, depth, coord):
     return res
 
 
-@pytest.mark.parametrize("case", ["hier", "glm", "gauss", "bern"])
+@pytest.mark.parametrize("case", ["hier", "glm", "gauss", "bern", "ht"])
 def test_persistent_nuts_iteration_vs_oracle(lib, case):
-    if case == "bern":
+    if case == "ht":
+        y = (0.5 + np.random.default_rng(3).standard_t(5, size=200)).astype(np.float32)
+        m, args, cons = StudentTHeavyTail(), (200,), {"y": y}
+        q = (np.array([0.5, -0.3, 0.0]) + 0.2 * np.random.default_rng(6).standard_normal((128, 3))).astype(np.float32)
+        step = 0.1
+    elif case == "bern":
         z = (np.random.default_rng(3).random(300) < 0.3).astype(np.float32)
         m, args, cons = BernoulliBeta(), (300,), {"z": z}
         q = (np.log(0.3 / 0.7) + 0.2 * np.random.default_rng(5).standard_normal((128, 1))).astype(np.float32)

@@ -5,7 +5,8 @@ import pytest
 
 import oracle
 from uncertaintea_b200.models import (BernoulliBeta, BernoulliLogitGLM, HierarchicalNormalNoncentered,
-                                      LognormalGammaNormal, NormalLocationScale, gauss_data, hierarchical_data,
+                                      LognormalGammaNormal, NormalLocationScale, StudentTHeavyTail, gauss_data,
+                                      hierarchical_data,
                                       logistic_regression_data)
 
 
@@ -248,6 +249,31 @@ def test_lognormal_gamma_oracle_on_the_reference_parity_case():
     h = 1e-6
     for c in range(3):
         for k in range(2):
+            qp, qm = q.copy(), q.copy()
+            qp[c, k] += h
+            qm[c, k] -= h
+            fd = (om.logjoint_gradient_f64(qp)[0][c] - om.logjoint_gradient_f64(qm)[0][c]) / (2 * h)
+            assert abs(fd - g[c, k]) <= 1e-6 * max(1.0, abs(g[c, k]))
+
+
+def test_heavy_tail_oracle_on_the_reference_parity_case():
+    """The reference's heavy-tail parity case (device_lowering_parity.jl:170-176):
+    y = [0.4, -0.7, 1.1, 0.2, 0.9], three chains of (loc, log s, log w), against
+    the closed form; the gradient against central finite differences."""
+    from scipy import stats
+    y = np.array([0.4, -0.7, 1.1, 0.2, 0.9])
+    om = oracle.OracleModel(StudentTHeavyTail().lower((5,), {"y": y}))
+    q = np.array([[0.5, 0.1, -0.4], [-0.3, 0.7, 0.2], [1.2, -0.2, 0.6]])
+    t, g = om.logjoint_gradient_f64(q)
+    yf = y.astype(np.float32).astype(np.float64)
+    for c, (loc, us, uw) in enumerate(q):
+        s, w = np.exp(us), np.exp(uw)
+        ref = (stats.t(4).logpdf(loc) + stats.invgamma(3.0, scale=2.0).logpdf(s) + us
+               + stats.weibull_min(2.0, scale=1.5).logpdf(w) + uw + stats.t(5, loc, s + w).logpdf(yf).sum())
+        assert abs(t[c] - ref) <= 1e-12 * abs(ref)
+    h = 1e-6
+    for c in range(3):
+        for k in range(3):
             qp, qm = q.copy(), q.copy()
             qp[c, k] += h
             qm[c, k] -= h

@@ -27,6 +27,7 @@ UT_FAMILY_HIER_NORMAL_NONCENTERED = 2
 UT_FAMILY_NORMAL_LOCATION_SCALE = 3
 UT_FAMILY_BERNOULLI_BETA = 4
 UT_FAMILY_LOGNORMAL_GAMMA_NORMAL = 5
+UT_FAMILY_STUDENTT_HEAVY_TAIL = 6
 
 
 class PlanDesc(ctypes.Structure):
@@ -48,6 +49,10 @@ class PlanDesc(ctypes.Structure):
         ("scale_rate", c_double),
         ("prob_alpha", c_double),
         ("prob_beta", c_double),
+        ("nu_prior", c_double),
+        ("nu_obs", c_double),
+        ("weibull_shape", c_double),
+        ("weibull_scale", c_double),
     ]
 
 

@@ -167,6 +167,13 @@ std::string plan_issues(const ut_plan_desc* p) {
         if (!(p->mu_scale > 0.0)) add("mu prior scale must be > 0");
         if (!(p->scale_shape > 0.0) || !(p->scale_rate > 0.0)) add("gamma shape and rate must be > 0");
         if (p->num_obs < 0) add("num_obs must be >= 0");
+    } else if (p->family == UT_FAMILY_STUDENTT_HEAVY_TAIL) {
+        if (p->num_params != 3) add("num_params must equal 3 (loc, log s, log w)");
+        if (!(p->nu_prior > 0.0) || !(p->nu_obs > 0.0)) add("Student-t degrees of freedom must be > 0");
+        if (!(p->mu_scale > 0.0)) add("Student-t prior scale must be > 0");
+        if (!(p->scale_shape > 0.0) || !(p->scale_rate > 0.0)) add("inverse-gamma shape and scale must be > 0");
+        if (!(p->weibull_shape > 0.0) || !(p->weibull_scale > 0.0)) add("Weibull shape and scale must be > 0");
+        if (p->num_obs < 0) add("num_obs must be >= 0");
     } else if (p->family == UT_FAMILY_LOGNORMAL_GAMMA_NORMAL) {
         if (p->num_params != 2) add("num_params must equal 2 (log a, log b)");
         if (!(p->mu_scale > 0.0)) add("lognormal scale must be > 0");
@@ -208,6 +215,8 @@ int32_t need_device() {
             KERNEL(kFamBern, 1, 1, __VA_ARGS__);                                                             \
         } else if ((ws)->dm.family == kFamLgn) {                                                             \
             KERNEL(kFamLgn, 1, 1, __VA_ARGS__);                                                              \
+        } else if ((ws)->dm.family == kFamHt) {                                                              \
+            KERNEL(kFamHt, 1, 1, __VA_ARGS__);                                                               \
         } else {                                                                                             \
             switch ((ws)->K) {                                                                               \
                 case 1: KERNEL(kFamHier, 1, 1, __VA_ARGS__); break;                                          \
@@ -431,7 +440,7 @@ int32_t ut_workspace_create(const ut_plan_desc* plan, const float* observed, int
             return fail(UT_ERR_DIMENSION, "expected %lld staged observation rows (N*(D+1)), got %lld", (long long)want,
                         (long long)observed_rows);
     } else if (plan->family == UT_FAMILY_NORMAL_LOCATION_SCALE || plan->family == UT_FAMILY_BERNOULLI_BETA ||
-               plan->family == UT_FAMILY_LOGNORMAL_GAMMA_NORMAL) {
+               plan->family == UT_FAMILY_LOGNORMAL_GAMMA_NORMAL || plan->family == UT_FAMILY_STUDENTT_HEAVY_TAIL) {
         if (observed_rows != N)
             return fail(UT_ERR_DIMENSION, "expected %d staged observation rows (N), got %lld", N,
                         (long long)observed_rows);
@@ -559,6 +568,27 @@ int32_t ut_workspace_create(const ut_plan_desc* plan, const float* observed, int
         if ((rc = dalloc(ws, &ws->d_y, std::max(N, 1)))) return bail(rc);
         if (N > 0) UT_CUDA(cudaMemcpy(ws->d_y, observed, sizeof(float) * N, cudaMemcpyHostToDevice));
         dm.gauss.y = ws->d_y;
+        ws->path = kPathWarp;
+        dm.stage = ((size_t)N * 4 + (size_t)kWarpsDensity * dm.Ppad * 4) <= kSmemBudget ? 1 : 0;
+        dm.staged_floats = dm.stage ? ((N + 3) / 4) * 4 : 0;
+    } else if (plan->family == UT_FAMILY_STUDENTT_HEAVY_TAIL) {
+        dm.family = kFamHt;
+        HtModel& h = dm.ht;
+        h.N = N;
+        h.nu0 = (float)plan->nu_prior; h.mu0 = (float)plan->mu_loc; h.sigma0 = (float)plan->mu_scale;
+        h.nu1 = (float)plan->nu_obs;
+        h.ig_a = (float)plan->scale_shape; h.ig_b = (float)plan->scale_rate;
+        h.wb_k = (float)plan->weibull_shape; h.wb_l = (float)plan->weibull_scale;
+        auto tconst = [](double nu) {
+            return std::lgamma((nu + 1.0) / 2.0) - std::lgamma(nu / 2.0) - 0.5 * (std::log(nu) + std::log(3.141592653589793));
+        };
+        h.c_prior = (float)(tconst(plan->nu_prior) - std::log(plan->mu_scale));
+        h.c_obs = (float)tconst(plan->nu_obs);
+        h.c_ig = (float)(plan->scale_shape * std::log(plan->scale_rate) - std::lgamma(plan->scale_shape));
+        h.c_wb = (float)(std::log(plan->weibull_shape) - plan->weibull_shape * std::log(plan->weibull_scale));
+        if ((rc = dalloc(ws, &ws->d_y, std::max(N, 1)))) return bail(rc);
+        if (N > 0) UT_CUDA(cudaMemcpy(ws->d_y, observed, sizeof(float) * N, cudaMemcpyHostToDevice));
+        h.y = ws->d_y;
         ws->path = kPathWarp;
         dm.stage = ((size_t)N * 4 + (size_t)kWarpsDensity * dm.Ppad * 4) <= kSmemBudget ? 1 : 0;
         dm.staged_floats = dm.stage ? ((N + 3) / 4) * 4 : 0;

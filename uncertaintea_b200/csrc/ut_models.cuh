@@ -68,6 +68,19 @@ struct LgnModel {
     const float* y;  // N
 };
 
+// Heavy-tailed location with two scales (the reference's heavy-tail device
+// model: StudentT (identity), InverseGamma and Weibull (log transform) choice
+// steps and a loop of StudentT observations with scale s + w; math.jl:167-186).
+// Host constants: c_prior = loggamma((nu0+1)/2) - loggamma(nu0/2)
+// - log(nu0 pi)/2 - log(sigma0), c_obs likewise for nu1 without the scale,
+// c_ig = a log b - loggamma(a), c_wb = log k - k log lambda.
+struct HtModel {
+    int N;
+    float nu0, mu0, sigma0, nu1, ig_a, ig_b, wb_k, wb_l;
+    float c_prior, c_obs, c_ig, c_wb;
+    const float* y;  // N
+};
+
 // Parameters in per-warp shared memory so every lane can read any coefficient
 // with a broadcast load.  `qs` has room for P floats.
 template <int K, int DMAX>
@@ -298,6 +311,53 @@ __device__ __forceinline__ float lgn_lj_grad(const LgnModel& m, const float (&q)
         for (int k = 0; k < K; ++k) g[k] = 0.0f;
         if (lane == 0) g[0] = a * (-nf + sq * inv_s2) - z / m.sigma;
         if (lane == 1) g[0] = b * sr * inv_s2 + m.shape - m.rate * b;
+    }
+    return lj;
+}
+
+// Lanes 0, 1, 2 hold loc, us = log s, uw = log w; sigma = s + w.  Per
+// observation r = y - loc, t = r^2:
+//   sum_i studentt = N (c_obs - log sigma) - (nu1+1)/2 sum log1p(t / (nu1 sigma^2)),
+//   d/dloc = (nu1+1) sum r / (nu1 sigma^2 + t),
+//   d/dsigma = -N / sigma + (nu1+1) / sigma sum t / (nu1 sigma^2 + t);
+// priors with log|J|: d/dloc of studentt = -(nu0+1)(loc-mu0)/(nu0 sigma0^2 + (loc-mu0)^2),
+// inverse gamma + us: d/dus = -a + b / s, weibull + uw: d/duw = k - k (w/lambda)^k.
+template <int K>
+__device__ __forceinline__ float ht_lj_grad(const HtModel& m, const float (&q)[K], float (&g)[K],
+                                            bool want_grad) {
+    const int lane = threadIdx.x & 31;
+    const float loc = __shfl_sync(UT_FULL_MASK, q[0], 0);
+    const float us = __shfl_sync(UT_FULL_MASK, q[0], 1);
+    const float uw = __shfl_sync(UT_FULL_MASK, q[0], 2);
+    const float s = expf(us), w = expf(uw);
+    const float sig = s + w;
+    const float ns2 = m.nu1 * sig * sig;
+    float a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
+    for (int i = lane; i < m.N; i += 32) {
+        const float r = m.y[i] - loc;
+        const float t = r * r;
+        const float den = 1.0f / (ns2 + t);
+        a1 += log1pf(t / ns2);
+        a2 += r * den;
+        a3 += t * den;
+    }
+    a1 = warp_sum(a1);
+    a2 = warp_sum(a2);
+    a3 = warp_sum(a3);
+    const float nf = (float)m.N;
+    float lj = nf * (m.c_obs - logf(sig)) - 0.5f * (m.nu1 + 1.0f) * a1;
+    const float d0 = loc - m.mu0, z = d0 / m.sigma0;
+    lj += m.c_prior - 0.5f * (m.nu0 + 1.0f) * log1pf(z * z / m.nu0);
+    lj += s >= FLT_MIN ? m.c_ig - (m.ig_a + 1.0f) * us - m.ig_b / s + us : -INFINITY;
+    const float wl = expf(m.wb_k * (uw - logf(m.wb_l)));  // (w / lambda)^k
+    lj += w >= FLT_MIN ? m.c_wb + (m.wb_k - 1.0f) * uw - wl + uw : -INFINITY;
+    if (want_grad) {
+        const float dsig = -nf / sig + (m.nu1 + 1.0f) * a3 / sig;
+#pragma unroll
+        for (int k = 0; k < K; ++k) g[k] = 0.0f;
+        if (lane == 0) g[0] = (m.nu1 + 1.0f) * a2 - (m.nu0 + 1.0f) * d0 / (m.nu0 * m.sigma0 * m.sigma0 + d0 * d0);
+        if (lane == 1) g[0] = -m.ig_a + m.ig_b / s + s * dsig;
+        if (lane == 2) g[0] = m.wb_k - m.wb_k * wl + w * dsig;
     }
     return lj;
 }

@@ -9,7 +9,7 @@
 
 namespace ut {
 
-enum Family : int { kFamGlm = 1, kFamHier = 2, kFamGauss = 3, kFamBern = 4, kFamLgn = 5 };
+enum Family : int { kFamGlm = 1, kFamHier = 2, kFamGauss = 3, kFamBern = 4, kFamLgn = 5, kFamHt = 6 };
 
 struct DevModel {
     int family;
@@ -22,6 +22,7 @@ struct DevModel {
     GaussModel gauss;
     BernModel bern;
     LgnModel lgn;
+    HtModel ht;
 };
 
 // Copies the model's observation data into shared memory (when dm.stage) and
@@ -45,6 +46,10 @@ __device__ __forceinline__ void stage_model(DevModel& dm, float* smem) {
         for (int i = threadIdx.x; i < dm.gauss.N; i += blockDim.x) smem[i] = dm.gauss.y[i];
         __syncthreads();
         dm.gauss.y = smem;
+    } else if constexpr (FAM == kFamHt) {
+        for (int i = threadIdx.x; i < dm.ht.N; i += blockDim.x) smem[i] = dm.ht.y[i];
+        __syncthreads();
+        dm.ht.y = smem;
     } else if constexpr (FAM == kFamLgn) {
         for (int i = threadIdx.x; i < dm.lgn.N; i += blockDim.x) smem[i] = dm.lgn.y[i];
         __syncthreads();
@@ -80,6 +85,7 @@ __device__ __forceinline__ float eval_lj(const DevModel& dm, const float (&q)[K]
     else if constexpr (FAM == kFamGauss) return gauss_lj_grad<K>(dm.gauss, q, g, want_grad);
     else if constexpr (FAM == kFamBern) return bern_lj_grad<K>(dm.bern, q, g, want_grad);
     else if constexpr (FAM == kFamLgn) return lgn_lj_grad<K>(dm.lgn, q, g, want_grad);
+    else if constexpr (FAM == kFamHt) return ht_lj_grad<K>(dm.ht, q, g, want_grad);
     else return hier_lj_grad<K>(dm.hier, dm.P, q, g, want_grad);
 }
 

@@ -326,6 +326,65 @@ class LognormalGammaNormal(TeaModelSpec):
         return out
 
 
+@dataclass
+class StudentTHeavyTail(TeaModelSpec):
+    """``loc ~ studentt(nu_prior, mu, sigma)``, ``s ~ inversegamma(shape, scale)``,
+    ``w ~ weibull(k, lambda)``, ``y[i] ~ studentt(nu_obs, loc, s + w)`` -- the
+    reference's device-lowerable heavy-tail model
+    (test/uncertaintea/core/device_lowering_parity.jl:51-60: studentt(4, 0, 1),
+    inversegamma(3, 2), weibull(2, 1.5), studentt(5, loc, s + w)).
+
+    Unconstrained parameters: [loc, log(s), log(w)]; constrained: [loc, s, w].
+    args = (n,); constraints = {"y": y}.
+    """
+
+    nu_prior: float = 4.0
+    mu: float = 0.0
+    sigma: float = 1.0
+    ig_shape: float = 3.0
+    ig_scale: float = 2.0
+    wb_shape: float = 2.0
+    wb_scale: float = 1.5
+    nu_obs: float = 5.0
+    name: str = "studentt_heavy_tail"
+
+    def parameter_names(self, args=(), constraints=None):
+        return ["loc", "s", "w"]
+
+    def lower(self, args=(), constraints=None) -> Lowered:
+        if len(args) != 1:
+            raise ValueError(f"{self.name} expects args=(n,), got {len(args)} argument(s)")
+        n = int(args[0])
+        if n < 0:
+            raise ValueError("n must be >= 0")
+        y = _observed_value(constraints, "y").astype(np.float32).reshape(-1)
+        if y.shape != (n,):
+            raise IndexError(f"expected {n} observations, got shape {y.shape}")
+        plan = nat.PlanDesc(
+            family=nat.UT_FAMILY_STUDENTT_HEAVY_TAIL, num_params=3, num_obs=n, num_coefs=0, has_intercept=0,
+            num_groups=0, intercept_mu=0.0, intercept_sigma=1.0, coef_mu=0.0, coef_sigma=1.0, mu_loc=self.mu,
+            mu_scale=self.sigma, tau_scale=1.0, scale_shape=self.ig_shape, scale_rate=self.ig_scale,
+            prob_alpha=1.0, prob_beta=1.0, nu_prior=self.nu_prior, nu_obs=self.nu_obs, weibull_shape=self.wb_shape,
+            weibull_scale=self.wb_scale)
+        empty = np.zeros(0, dtype=np.int32)
+        return Lowered(plan, np.ascontiguousarray(y), empty, empty, 3)
+
+    def constrain(self, unconstrained, args=(), constraints=None):
+        u = np.asarray(unconstrained, dtype=np.float64)
+        out = u.copy()
+        out[..., 1:] = np.exp(u[..., 1:])
+        return out
+
+    def initial_positions(self, rng, num_chains, args=(), constraints=None, init_strategy="prior"):
+        if init_strategy == "uniform":
+            return rng.uniform(-2.0, 2.0, size=(num_chains, 3))
+        out = np.empty((num_chains, 3))
+        out[:, 0] = self.mu + self.sigma * rng.standard_t(self.nu_prior, size=num_chains)
+        out[:, 1] = np.log(self.ig_scale / np.maximum(rng.gamma(self.ig_shape, 1.0, size=num_chains), 1e-30))
+        out[:, 2] = np.log(np.maximum(self.wb_scale * rng.weibull(self.wb_shape, size=num_chains), 1e-30))
+        return out
+
+
 # ---- synthetic workloads (seeded stand-ins for the benchmark data sets) -----
 
 def logistic_regression_data(num_obs: int, num_coefs: int, seed: int, x_scale: float = 1.0):
