@@ -421,11 +421,15 @@ def test_persistent_nuts_iteration_vs_oracle(lib, case):
     ws.close()
 
 
-@pytest.mark.parametrize("case", ["glm", "gauss"])
+@pytest.mark.parametrize("case", ["glm", "gauss", "glm_tc"])
 def test_advi_step_vs_oracle(lib, case):
     """One device ADVI step (Philox particles, batched gradient, particle means)
     against the oracle's restatement with the same noise coordinates."""
-    if case == "glm":
+    if case == "glm_tc":
+        m, args, cons, _ = _glm_case(3000, 100, 128, False, 5, 0.1)
+        loc = (0.1 * np.random.default_rng(2).standard_normal(100)).astype(np.float32)
+        sc = np.full(100, 0.05, dtype=np.float32)
+    elif case == "glm":
         m, args, cons, _ = _glm_case(1000, 10, 64, False, 1)
         loc = (0.3 * np.random.default_rng(2).standard_normal(10)).astype(np.float32)
         sc = np.full(10, 0.1, dtype=np.float32)
@@ -434,8 +438,10 @@ def test_advi_step_vs_oracle(lib, case):
         m, args, cons = NormalLocationScale(), (200,), {"y": y}
         loc = np.array([y.mean(), np.log(y.std())], dtype=np.float32)
         sc = np.array([0.1, 0.05], dtype=np.float32)
-    M = 64
+    M = 128 if case == "glm_tc" else 64
     ws = _ws(m, args, cons, M)
+    if case == "glm_tc":
+        assert ws.kernel_path() == "tensor_core"
     P = loc.size
     f = lambda *sh: torch.empty(sh, dtype=torch.float32, device="cuda")  # noqa: E731
     loc_d, sc_d = torch.from_numpy(loc).cuda(), torch.from_numpy(sc).cuda()
@@ -454,12 +460,16 @@ def test_advi_step_vs_oracle(lib, case):
     ws.close()
 
 
-@pytest.mark.parametrize("case", ["glm", "gauss", "hier"])
+@pytest.mark.parametrize("case", ["glm", "gauss", "hier", "glm_tc"])
 def test_meads_iterations_vs_oracle(lib, case):
     """Two MEADS iterations (fold statistics in double, refresh, one leapfrog
     step, persistent-slice accept) against the oracle's literal restatement,
-    from the same state and Philox coordinates."""
-    if case == "glm":
+    from the same state and Philox coordinates; glm_tc runs the gradient on the
+    tensor-core kernel."""
+    if case == "glm_tc":
+        m, args, cons, q = _glm_case(3000, 100, 64, False, 5, 0.1)
+        q *= 0.1
+    elif case == "glm":
         m, args, cons, q = _glm_case(1000, 10, 64, False, 1)
         q *= 0.3
     elif case == "gauss":
@@ -470,6 +480,8 @@ def test_meads_iterations_vs_oracle(lib, case):
         q = (np.random.default_rng(8).standard_normal((64, 18)) * 0.5).astype(np.float32)
     C, P, K = q.shape[0], q.shape[1], 4
     ws = _ws(m, args, cons, C)
+    if case == "glm_tc":
+        assert ws.kernel_path() == "tensor_core"
     qd, g, t = _state(ws, q)
     f = lambda sh, dt=torch.float32: torch.zeros(sh, dtype=dt, device="cuda")  # noqa: E731
     mom, sl = f((C, P)), f(C)
