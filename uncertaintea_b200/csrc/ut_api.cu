@@ -339,6 +339,59 @@ int32_t launch_stream(ut_workspace* ws, const float* params, float* totals, floa
     return UT_OK;
 }
 
+// The streaming kernel over the first n (<= 16) rows of `params` of a GLM
+// workspace that normally uses another path (the lockstep tail): buffers for 16
+// chains are made on first use, the stage plan follows the chain bucket.
+int32_t launch_stream_rows(ut_workspace* ws, const float* params, float* totals, float* grads, int n,
+                           cudaStream_t st) {
+    const int F = ws->P;
+    int32_t rc;
+    if (!ws->d_spart) {
+        int dev_sms = 148;
+        cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, ws->device);
+        ws->stream_splits = dev_sms;
+        const int chunks = (ws->N + kStreamRows - 1) / kStreamRows;
+        const size_t ypad = (size_t)chunks * kStreamRows;
+        const int groups = glm_stream_groups(dev_sms);
+        if ((rc = dalloc(ws, &ws->d_ypad, ypad))) return rc;
+        UT_CUDA(cudaMemset(ws->d_ypad, 0, ypad * sizeof(float)));
+        UT_CUDA(cudaMemcpy(ws->d_ypad, ws->d_y, (size_t)ws->N * sizeof(float), cudaMemcpyDeviceToDevice));
+        if ((rc = dalloc(ws, &ws->d_spart, (size_t)dev_sms * kStreamMaxC * (F + 1)))) return rc;
+        if ((rc = dalloc(ws, &ws->d_sgpart, (size_t)groups * kStreamMaxC * (F + 1)))) return rc;
+        if ((rc = dalloc(ws, &ws->d_stickets, (size_t)groups + 1))) return rc;
+        if ((rc = dalloc(ws, &ws->d_serr, 1))) return rc;
+        UT_CUDA(cudaMemset(ws->d_stickets, 0, ((size_t)groups + 1) * sizeof(unsigned)));
+        UT_CUDA(cudaMemset(ws->d_serr, 0, sizeof(int)));
+    }
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ws->device);
+    const int CB = n <= 1 ? 1 : n <= 2 ? 2 : n <= 4 ? 4 : n <= 8 ? 8 : 16;
+    int stages = 0, slots = 0;
+    if (!glm_stream_plan(CB, F, (size_t)std::max(0, optin - 1024), &stages, &slots))
+        return fail(UT_ERR_UNSUPPORTED, "streaming kernel: shared memory too small");
+    GlmStreamArgs a;
+    a.Xa = ws->d_Xa; a.ypad = ws->d_ypad; a.params = params;
+    a.part = ws->d_spart; a.gpart = ws->d_sgpart; a.tickets = ws->d_stickets; a.err = ws->d_serr;
+    a.totals = totals; a.grads = grads;
+    a.N = ws->N; a.F = F; a.C = n; a.stages = stages; a.slots = slots; a.off = ws->plan.has_intercept;
+    a.icpt_mu = (float)ws->plan.intercept_mu; a.icpt_sigma = (float)ws->plan.intercept_sigma;
+    a.coef_mu = (float)ws->plan.coef_mu; a.coef_sigma = (float)ws->plan.coef_sigma;
+    const size_t smem = glm_stream_smem(CB, F, stages);
+#define STREAM_CASE(CBV)                                                                            \
+    case CBV: {                                                                                     \
+        auto kern = grads ? glm_stream_kernel<CBV, true> : glm_stream_kernel<CBV, false>;          \
+        UT_CUDA(launch_dyn(kern, 0, 0, smem, st));                                                  \
+        kern<<<ws->stream_splits, kStreamThreads, smem, st>>>(a);                                   \
+    } break;
+    switch (CB) {
+        STREAM_CASE(1) STREAM_CASE(2) STREAM_CASE(4) STREAM_CASE(8)
+        default: STREAM_CASE(16)
+    }
+#undef STREAM_CASE
+    UT_LAUNCHED();
+    return UT_OK;
+}
+
 // Batched density on device buffers, whichever path the workspace uses.
 int32_t density(ut_workspace* ws, const float* params, float* totals, float* grads, cudaStream_t st) {
     if (ws->streaming) return launch_stream(ws, params, totals, grads, st);
@@ -1108,6 +1161,12 @@ int32_t ut_lockstep_nuts_iteration(ut_workspace* ws, const ut_nuts_buffers* buf,
     // chain is still growing
     const int max_steps = (1 << max_tree_depth) - 1;
     const bool compact = ws->tc.enabled;
+    // once at most 16 trees still grow (known at a check; the count only falls
+    // within an iteration), the remaining leaves are evaluated by the few-chain
+    // streaming kernel over that many compacted rows
+    const char* no_stream = getenv("UT_DISABLE_STREAM_KERNEL");
+    const bool can_stream = compact && P % 4 == 0 && P <= (size_t)kStreamMaxF && !(no_stream && no_stream[0] == '1');
+    int tail_rows = 0;
     const unsigned rows_grid = (unsigned)std::min<size_t>((C * P + 255) / 256, 4096);
     for (int step = 0; step < max_steps; ++step) {
         ls_compact_kernel<<<1, 1024, 0, st>>>(ws->ls_act, (int)C, ws->ls_idx, ws->ls_active);
@@ -1116,11 +1175,14 @@ int32_t ut_lockstep_nuts_iteration(ut_workspace* ws, const ut_nuts_buffers* buf,
             UT_CUDA(cudaMemcpyAsync(ws->h_active, ws->ls_active, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
             UT_CUDA(cudaStreamSynchronize(st));
             if (*ws->h_active == 0) break;
+            if (can_stream && *ws->h_active <= kStreamMaxC) tail_rows = *ws->h_active;
         }
         if (compact) {
             ls_gather_kernel<<<rows_grid, 256, 0, st>>>(ws->lf.wq, ws->ls_idx, ws->ls_active, (int)P, ws->ls_cq);
             UT_LAUNCHED();
-            if (tc_glm_launch(ws->tc, ws->ls_cq, ws->ls_clj, ws->ls_cg, st, ws->ls_active) != cudaSuccess)
+            if (tail_rows) {
+                if ((rc = launch_stream_rows(ws, ws->ls_cq, ws->ls_clj, ws->ls_cg, tail_rows, st))) return rc;
+            } else if (tc_glm_launch(ws->tc, ws->ls_cq, ws->ls_clj, ws->ls_cg, st, ws->ls_active) != cudaSuccess)
                 return fail(UT_ERR_CUDA, "tensor-core GLM launch failed: %s", cudaGetErrorString(cudaGetLastError()));
             ls_scatter_kernel<<<rows_grid, 256, 0, st>>>(ws->ls_cg, ws->ls_clj, ws->ls_idx, ws->ls_active, (int)P,
                                                          ws->lf.wg, ws->lf.wlj);
