@@ -11,8 +11,8 @@ shipped).
 
 At N=1 the line also carries `hbm_sweep`: the same design at 1, 4, 8 and 16
 chains, where an evaluation is bound by reading X from HBM (achieved GB/s
-against the measured HBM bandwidth), `samplers`: the config-1 HMC, config-2
-persistent-NUTS, config-3 masked-NUTS and config-3 MEADS runs (min ESS/s, R-hat, gradient
+against the measured HBM bandwidth), `samplers`: the 1000x10 GLM HMC, the
+hierarchical (J=64) persistent-NUTS, and the 100000x100 GLM masked-NUTS and MEADS runs (min ESS/s, R-hat, gradient
 evaluations/s; skipped with --no-samplers), `surrogate_chees`: the
 learned-gradient-surrogate workload on the same model (min ESS/s of
 surrogate-driven ChEES-HMC vs plain ChEES-HMC and vs the plain masked NUTS run,
@@ -45,7 +45,7 @@ N_OBS, N_COEF, N_CHAINS = 100_000, 100, 4096
 FLOP_FP32 = 4.0 * N_OBS * N_COEF * N_CHAINS            # two N x D x C contractions (x, +)
 METRIC = "grad evals/s"
 UNIT = "chain-gradient evaluations/s"
-WORKLOAD = ("config-3 logistic regression: batched logjoint+gradient, N=100000 obs, D=100, "
+WORKLOAD = ("logistic regression: batched logjoint+gradient, N=100000 obs, D=100, "
             "4096 chains, FP32 (3xTF32 tensor-core contraction when available)")
 
 
@@ -259,13 +259,13 @@ def run_b200(args):
         sweep = hbm_sweep()
         if not args.no_samplers:
             samplers = sampler_configs()
-            samplers["config3_nuts"] = config3_nuts()
-            samplers["config3_meads"] = config3_meads()
+            samplers["glm100000x100_nuts"] = glm_large_nuts()
+            samplers["glm100000x100_meads"] = glm_large_meads()
     if rank == 0 and world == 1 and not args.no_surrogate:
         sur = surrogate_comparison()
         if samplers is not None:
             # the headline comparison: surrogate-driven trajectories vs plain NUTS on the same model
-            nuts = samplers["config3_nuts"]
+            nuts = samplers["glm100000x100_nuts"]
             sur["plain_nuts"] = {k: nuts[k] for k in ("min_ess_per_s", "min_ess", "max_rhat", "sampling_s")}
             sur["ratio_vs_plain_nuts"] = sur["surrogate"]["min_ess_per_s"] / nuts["min_ess_per_s"]
     if rank == 0 and world == 1 and not args.no_uneven:
@@ -384,12 +384,12 @@ def hbm_sweep(chain_counts=(1, 4, 8, 16), steps=20, warmup=5):
 
 
 def sampler_configs():
-    """The two sampler workloads of the small models, timed end to end: config 1
-    (batched HMC on the 1000 x 10 logistic regression, 256 chains, 8 leapfrog
-    steps, step 0.05 without step adaptation, 1000 warmup + 1000 draws, seed 1) and
-    config 2 (batched persistent NUTS on the non-centred hierarchical model with
-    J = 64 groups x 20 observations, sigma_j ~ U(0.5, 2), y from the prior at seed 7;
-    4096 chains, max tree depth 10, 1000 warmup + 1000 draws).  Min bulk ESS over
+    """The two sampler workloads of the small models, timed end to end: batched
+    HMC on the 1000 x 10 logistic regression (256 chains, 8 leapfrog steps, step
+    0.05 without step adaptation, 1000 warmup + 1000 draws, seed 1) and batched
+    persistent NUTS on the non-centred hierarchical model with J = 64 groups x 20
+    observations (sigma_j ~ U(0.5, 2), y from the prior at seed 7; 4096 chains, max
+    tree depth 10, 1000 warmup + 1000 draws).  Min bulk ESS over
     parameters per second of sampling, max split R-hat, gradient evaluations/s."""
     from uncertaintea_b200 import (BernoulliLogitGLM, HierarchicalNormalNoncentered, batched_hmc, batched_nuts, ess,
                                    hierarchical_data, logistic_regression_data, rhat)
@@ -400,22 +400,22 @@ def sampler_configs():
     yh, sig, sizes, _ = hierarchical_data(64, 20, 7)
     c2 = batched_nuts(HierarchicalNormalNoncentered(64), (sig, sizes), {"y": yh}, num_chains=4096, num_samples=1000,
                       num_warmup=1000, max_tree_depth=10, rng=7)
-    for name, ch, cfg in (("config1_hmc", c1, "256 chains, L=8, step 0.05, 1000+1000, GLM 1000x10"),
-                          ("config2_nuts", c2, "4096 chains, depth 10, 1000+1000, hierarchical J=64 x 20")):
+    for name, ch, cfg in (("glm1000x10_hmc", c1, "256 chains, L=8, step 0.05, 1000+1000, GLM 1000x10"),
+                          ("hier64x20_nuts", c2, "4096 chains, depth 10, 1000+1000, hierarchical J=64 x 20")):
         e, r = ess(ch, space="unconstrained"), rhat(ch, space="unconstrained")
         total_s = ch.warmup_seconds + ch.sampling_seconds
         out[name] = {"min_ess_per_s": float(np.min(e) / ch.sampling_seconds), "min_ess": float(np.min(e)),
                      "max_rhat": float(np.max(r)), "warmup_s": ch.warmup_seconds, "sampling_s": ch.sampling_seconds,
                      "grad_evals_per_s": ch.gradient_evaluations / total_s, "mean_accept": float(ch.accept_prob.mean()),
                      "config": cfg}
-    out["config2_nuts"]["mean_tree_depth"] = float(c2.tree_depth.mean())
+    out["hier64x20_nuts"]["mean_tree_depth"] = float(c2.tree_depth.mean())
     return out
 
 
-def config3_nuts(num_chains=4096, num_warmup=200, num_samples=200):
+def glm_large_nuts(num_chains=4096, num_warmup=200, num_samples=200):
     """Masked (lockstep) NUTS on the large logistic regression, 4096 chains, max
     tree depth 10: every leaf is one batched tensor-core gradient over the chains
-    whose trees are still growing (compacted).  Fewer iterations than configs 1-2
+    whose trees are still growing (compacted).  Fewer iterations than the small-model runs
     (200 + 200) keep the bench within minutes; the draws are still nearly
     independent (min ESS at the draw count)."""
     from uncertaintea_b200 import batched_nuts, ess, rhat
@@ -433,7 +433,7 @@ def config3_nuts(num_chains=4096, num_warmup=200, num_samples=200):
             "config": f"{num_chains} chains, masked NUTS depth 10, {num_warmup}+{num_samples}, GLM 100000x100"}
 
 
-def config3_meads(num_chains=4096, num_warmup=3000, num_samples=1000):
+def glm_large_meads(num_chains=4096, num_warmup=3000, num_samples=1000):
     """MEADS on the large logistic regression (4096 chains, 4 folds): one
     batched tensor-core gradient per iteration, every adaptation statistic on
     the device, no warmup adaptation phase.  Started from prior draws (a
@@ -486,7 +486,7 @@ def surrogate_comparison(num_chains=4096, num_warmup=500, num_samples=500):
     out["ratio"] = out["surrogate"]["min_ess_per_s"] / out["plain"]["min_ess_per_s"]
     out["metric"] = "min ESS/s (R-hat<1.01), surrogate ChEES-HMC vs plain ChEES-HMC"
     out["unit"] = "effective samples/s"
-    out["config"] = (f"config-4: learned gradient surrogate on the config-3 model, {num_chains} chains, "
+    out["config"] = (f"learned gradient surrogate on the 100000x100 logistic regression, {num_chains} chains, "
                      f"{num_warmup} warmup + {num_samples} sampling iterations")
     return out
 
@@ -533,7 +533,7 @@ def uneven_batch(num_models=512, chains=64, num_warmup=500, num_samples=500):
            "classes": {"slots": cls["slots"].tolist(), "models": cls["models"].tolist(),
                        "chains_per_block": cls["chains_per_block"].tolist(),
                        "stage_limit_bytes": cls["stage_limit_bytes"].tolist()},
-           "config": (f"config-5: {num_models} non-centred hierarchical models, J~U[8,512], obs/group~U[5,100], "
+           "config": (f"uneven batch: {num_models} non-centred hierarchical models, J~U[8,512], obs/group~U[5,100], "
                       f"{chains} chains each, max tree depth 10, {num_warmup} warmup + {num_samples} draws, "
                       "CUDA graph replay, autotuned launch shapes")}
     res.batch.close()
@@ -568,7 +568,7 @@ def main():
     ap.add_argument("--no-surrogate", action="store_true",
                     help="skip the learned-surrogate ChEES comparison (about a minute) in the output line")
     ap.add_argument("--no-samplers", action="store_true",
-                    help="skip the config-1 HMC and config-2 NUTS sampler runs in the output line")
+                    help="skip the small-model HMC and NUTS sampler runs in the output line")
     ap.add_argument("--no-uneven", action="store_true",
                     help="skip the uneven-batch run (512 hierarchical models, about two minutes)")
     args = ap.parse_args()

@@ -1,7 +1,7 @@
 """CPU oracle of the batched density + sampler hot path.
 
 TEST INFRASTRUCTURE: only the tests, ``__graft_entry__.smoke`` and the CPU
-baseline leg of ``bench.py`` use this package, as the checker.  The product
+baseline leg of ``bench.py`` use this package, as the test oracle.  The product
 library never calls it.  See oracle.cpp for what each function restates and
 how far parity is pinned (Philox and the ChEES scalar helpers by the
 reference's own known-answer tests; the densities and samplers by closed

@@ -1,6 +1,6 @@
 // oracle.cpp -- CPU restatement of UncertainTea's batched density + sampler
 // hot path.  TEST INFRASTRUCTURE ONLY: the parity tests, the smoke check and
-// the CPU-baseline leg of bench.py load it as the checker.  The product
+// the CPU-baseline leg of bench.py load it as the test oracle.  The product
 // library (uncertaintea_b200/csrc) never links, loads or calls it.
 //
 // Parity pinning: Philox4x32-10 is pinned by the Random123 known-answer
@@ -9,8 +9,10 @@
 // (test/uncertaintea/core/batched_chees_adaptation.jl:29-72).  The reference is
 // Julia, which is not installed here, so its density/gradient/sampler code
 // cannot be run: those functions are restated from the cited source lines and
-// checked against closed forms and central finite differences instead
-// (parity for them is unpinned by reference outputs).
+// checked against closed forms and central finite differences instead, on
+// the reference's own parity-case inputs where it has them
+// (test/uncertaintea/core/device_lowering_parity.jl:131-176); parity for them
+// is unpinned by reference outputs.
 //
 // Everything is templated on the arithmetic type T (float / double), like the
 // reference's precision-generic kernels (Float32 on Metal, Float64 on CPU()).
@@ -643,7 +645,7 @@ int set_threads(int threads) {
 }  // namespace
 
 // ===========================================================================
-// C entry points (checker side)
+// C entry points (test side)
 // ===========================================================================
 extern "C" {
 

@@ -1,6 +1,6 @@
 // oracle_mlp.cpp -- CPU restatement of the project's learned gradient
 // surrogate.  TEST INFRASTRUCTURE ONLY: the parity tests load it as the
-// checker of the device MLP kernels; the product library never links it.
+// test oracle of the device MLP kernels; the product library never links it.
 //
 // No reference counterpart (the surrogate is this project's addition), so
 // parity is anchored on the mathematics: the FP64 mode is checked against

@@ -78,7 +78,7 @@ def _glm_case(N, D, C, intercept, seed, scale=1.0):
 
 
 @pytest.mark.parametrize("N,D,C,intercept,scale", [
-    (1000, 10, 256, False, 1.0),      # config 1 shape, warp path (data staged in shared memory)
+    (1000, 10, 256, False, 1.0),      # 1000x10 GLM, warp path (data staged in shared memory)
     (777, 5, 33, True, 1.0),          # ragged sizes, intercept
     (20000, 100, 200, True, 0.1),     # tiled path
     (3000, 40, 64, False, 1.0),       # tiled path, D just above the warp path
@@ -98,8 +98,8 @@ def test_glm_density_vs_fp64_oracle(lib, N, D, C, intercept, scale):
     ws.close()
 
 
-def test_glm_density_full_config3_subset(lib):
-    """Full config-3 size (N=100000, D=100, C=4096): every chain computed on the
+def test_glm_density_full_size_subset(lib):
+    """Full size (N=100000, D=100, C=4096): every chain computed on the
     GPU, 12 chains checked against the FP64 oracle."""
     m, args, cons, q = _glm_case(100000, 100, 4096, False, 3, 0.1)
     ws = _ws(m, args, cons, 4096)
@@ -571,7 +571,7 @@ def test_running_variance_vs_sequential(lib):
 
 
 @pytest.mark.parametrize("N,D,C,intercept", [
-    (100000, 100, 4096, False),   # config 3
+    (100000, 100, 4096, False),   # full-size design, 4096 chains
     (5003, 100, 200, True),       # ragged obs tile and chain tile, F=101 -> 104 padded features
     (777, 64, 128, False),
     (70, 3, 5, True),             # tiny: one observation tile, one partial chain tile
@@ -603,8 +603,8 @@ def test_tensor_core_path_vs_cuda_core_and_oracle(lib, N, D, C, intercept, monke
 
 
 @pytest.mark.parametrize("N,D,C,intercept", [
-    (100000, 100, 1, False),      # config-3 design, one chain
-    (100000, 100, 16, False),     # config-3 design, 16 chains
+    (100000, 100, 1, False),      # 100000x100 design, one chain
+    (100000, 100, 16, False),     # 100000x100 design, 16 chains
     (5003, 99, 8, True),          # F = 100, ragged last chunk (5003 = 78 x 64 + 11)
     (1000, 63, 3, True),          # F = 64, chains padded to 4
     (130, 35, 5, True),           # F = 36, three chunks

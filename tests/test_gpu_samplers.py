@@ -103,7 +103,7 @@ def _exact_mu_tau_moments(y, sig, sizes, mu_scale=5.0, tau_scale=2.5):
 
 
 def test_hierarchical_nuts_informative_groups(lib):
-    """Config-2 data shape (64 groups x 20 observations, y from the prior at
+    """Hierarchical data shape (64 groups x 20 observations, y from the prior at
     seed 7).  The group effects are pinned by the data; mu and tau move slowly
     along the non-centred ridge, so the check is against the exact marginal
     posterior means of mu and tau, within 5 Monte-Carlo standard errors."""
@@ -199,7 +199,7 @@ def test_advi_on_the_gauss_model(lib):
 
 
 def test_advi_on_the_glm_matches_nuts_means(lib):
-    """On config 1's logistic regression (a near-Gaussian posterior) the mean-field
+    """On the 1000x10 logistic regression (a near-Gaussian posterior) the mean-field
     location matches the NUTS posterior means within 0.25 posterior SD."""
     X, y, _ = logistic_regression_data(1000, 10, seed=1)
     m = BernoulliLogitGLM(10)
@@ -309,7 +309,7 @@ def test_argument_validation(lib):
 
 
 def test_masked_nuts_on_the_large_glm(lib):
-    """Lockstep NUTS over the tensor-core batched gradient on the config-3 design
+    """Lockstep NUTS over the tensor-core batched gradient on the 100000x100 design
     (100000 x 100, 256 chains): R-hat < 1.01 and posterior means within 5 MCSE of
     a ChEES run on the same model."""
     X, y, _ = logistic_regression_data(100000, 100, 3, x_scale=0.1)
