@@ -108,6 +108,7 @@ struct ut_workspace {
     float* ls_ckpt = nullptr;
     int32_t* ls_active = nullptr;  // live-chain count (device)
     int32_t* h_active = nullptr;   // pinned host copy of the live-chain count
+    int32_t* h_err = nullptr;      // pinned host copies of the tensor-core / streaming error flags
     uint8_t* ls_act = nullptr;     // per-chain live flags
     int32_t* ls_idx = nullptr;     // compacted live chains
     float* ls_cq = nullptr;        // compacted positions / gradients / logjoints
@@ -427,6 +428,35 @@ int32_t ensure_host_buffers(ut_workspace* ws) {
     if ((rc = dalloc(ws, &ws->d_params, pc))) return rc;
     if ((rc = dalloc(ws, &ws->d_totals, ws->C))) return rc;
     if ((rc = dalloc(ws, &ws->d_grads, pc))) return rc;
+    void* hp = nullptr;
+    UT_CUDA(cudaMallocHost(&hp, 2 * sizeof(int32_t)));
+    ws->h_err = static_cast<int32_t*>(hp);
+    return UT_OK;
+}
+
+// Enqueue the reads of the kernels' error flags on `st` (into pinned host words),
+// so the host-array entry points need one stream synchronisation in all.
+int32_t enqueue_error_reads(ut_workspace* ws, cudaStream_t st) {
+    ws->h_err[0] = ws->h_err[1] = 0;
+    if (ws->tc.err)
+        UT_CUDA(cudaMemcpyAsync(&ws->h_err[0], ws->tc.err, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    if (ws->d_serr)
+        UT_CUDA(cudaMemcpyAsync(&ws->h_err[1], ws->d_serr, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    return UT_OK;
+}
+
+// After the synchronisation: report (and clear) a flag the kernels raised.
+int32_t error_reads_status(ut_workspace* ws) {
+    if (ws->h_err[0]) {
+        UT_CUDA(cudaMemset(ws->tc.err, 0, sizeof(int)));
+        return fail(UT_ERR_DEVICE_TIMEOUT, "a bounded wait inside the tensor-core GLM kernel gave up; "
+                                           "its results are invalid");
+    }
+    if (ws->h_err[1]) {
+        UT_CUDA(cudaMemset(ws->d_serr, 0, sizeof(int)));
+        return fail(UT_ERR_DEVICE_TIMEOUT, "a bounded wait inside the streaming GLM kernel gave up; "
+                                           "its results are invalid");
+    }
     return UT_OK;
 }
 
@@ -699,6 +729,7 @@ int32_t ut_workspace_destroy(ut_workspace* ws) {
     if (!ws) return UT_OK;
     for (void* p : ws->allocations) cudaFree(p);
     if (ws->h_active) cudaFreeHost(ws->h_active);
+    if (ws->h_err) cudaFreeHost(ws->h_err);
     if (ws->stream) cudaStreamDestroy(ws->stream);
     delete ws;
     return UT_OK;
@@ -769,8 +800,9 @@ int32_t ut_logjoint(ut_workspace* ws, const float* params, float* totals) {
     UT_CUDA(cudaMemcpyAsync(ws->d_params, params, pc * sizeof(float), cudaMemcpyHostToDevice, ws->stream));
     if ((rc = density(ws, ws->d_params, ws->d_totals, nullptr, ws->stream))) return rc;
     UT_CUDA(cudaMemcpyAsync(totals, ws->d_totals, ws->C * sizeof(float), cudaMemcpyDeviceToHost, ws->stream));
+    if ((rc = enqueue_error_reads(ws, ws->stream))) return rc;
     UT_CUDA(cudaStreamSynchronize(ws->stream));
-    return ut_workspace_check(ws, ws->stream);
+    return error_reads_status(ws);
 }
 
 int32_t ut_logjoint_gradient(ut_workspace* ws, const float* params, float* totals, float* gradients) {
@@ -783,8 +815,9 @@ int32_t ut_logjoint_gradient(ut_workspace* ws, const float* params, float* total
     if ((rc = density(ws, ws->d_params, ws->d_totals, ws->d_grads, ws->stream))) return rc;
     UT_CUDA(cudaMemcpyAsync(totals, ws->d_totals, ws->C * sizeof(float), cudaMemcpyDeviceToHost, ws->stream));
     UT_CUDA(cudaMemcpyAsync(gradients, ws->d_grads, pc * sizeof(float), cudaMemcpyDeviceToHost, ws->stream));
+    if ((rc = enqueue_error_reads(ws, ws->stream))) return rc;
     UT_CUDA(cudaStreamSynchronize(ws->stream));
-    return ut_workspace_check(ws, ws->stream);
+    return error_reads_status(ws);
 }
 
 // ---- Philox ---------------------------------------------------------------

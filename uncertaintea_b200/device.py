@@ -56,6 +56,20 @@ def _stream_handle():
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
+def _host_output(shape):
+    """A fresh float32 host array in page-locked memory for a device->host result.
+
+    Drawn from torch's caching pinned-host allocator: after the first call a block
+    of the same size is reused without registering pages again, and the copy runs
+    at DMA speed without first-touch page faults or a staging bounce.  The array
+    owns its block (through the tensor it views) until it is dropped, so each call
+    returns independent arrays, as the reference's allocating copies do
+    (src/device/api.jl:103-106).  The library's own copy is synchronised before
+    the entry point returns, so a block freed later has no copy in flight."""
+    torch = _torch()
+    return torch.empty(shape, dtype=torch.float32, pin_memory=True).numpy()
+
+
 def device_lowering_report(model: TeaModelSpec, args=(), constraints=None):
     """(supported, issues) for a model's kernel description (workspace.jl:24-35)."""
     lib = nat.load()
@@ -159,15 +173,15 @@ class DeviceBatchedWorkspace:
     def logjoint(self, params) -> np.ndarray:
         """device_batched_logjoint!(ws, params) -> Vector (C,)."""
         q = self._check_host_params(params)
-        totals = np.empty(self.batch_size, dtype=np.float32)
+        totals = _host_output(self.batch_size)
         nat.check(self.lib.ut_logjoint(self.handle, nat.ptr(q), nat.ptr(totals)))
         return totals
 
     def logjoint_gradient(self, params):
         """device_batched_logjoint_gradient!(ws, params) -> (values (C,), gradients (P, C))."""
         q = self._check_host_params(params)
-        totals = np.empty(self.batch_size, dtype=np.float32)
-        grads = np.empty((self.batch_size, self.parameter_count), dtype=np.float32)
+        totals = _host_output(self.batch_size)
+        grads = _host_output((self.batch_size, self.parameter_count))
         nat.check(self.lib.ut_logjoint_gradient(self.handle, nat.ptr(q), nat.ptr(totals), nat.ptr(grads)))
         return totals, grads.T
 
