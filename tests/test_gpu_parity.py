@@ -116,6 +116,26 @@ def test_glm_density_full_size_subset(lib):
     ws.close()
 
 
+def test_host_arrays_are_independent_and_any_layout(lib):
+    """The host-array entry points return fresh arrays on every call (the
+    reference's allocating copies, api.jl:103-106), in page-locked memory; a
+    float64 or row-major P x C input gives the same values as the chain-major
+    float32 one (bitwise: the same float32 parameters reach the device)."""
+    m, args, cons, q = _glm_case(20000, 100, 200, True, 5, 0.1)
+    ws = _ws(m, args, cons, 200)
+    t1, g1 = ws.logjoint_gradient(q.T)
+    t1c, g1c = t1.copy(), np.array(g1)
+    t2, g2 = ws.logjoint_gradient((q * 0.5).T)
+    assert np.array_equal(t1, t1c) and np.array_equal(g1, g1c)   # the first results were not overwritten
+    assert not np.array_equal(t1, t2)
+    assert torch.from_numpy(t1).is_pinned() and torch.from_numpy(np.ascontiguousarray(g1.T)).is_pinned()
+    for alt in (q.T.astype(np.float64), np.ascontiguousarray(q.T), np.asfortranarray(q.T.astype(np.float64))):
+        ta, ga = ws.logjoint_gradient(alt)
+        assert np.array_equal(ta, t1) and np.array_equal(ga, g1)
+        assert np.array_equal(ws.logjoint(alt), ws.logjoint(q.T))
+    ws.close()
+
+
 @pytest.mark.parametrize("J,n,C", [(64, 20, 512), (8, 5, 3), (150, 7, 40), (542, 2, 8)])  # 542: 544 params, the max
 def test_hier_density_vs_fp64_oracle(lib, J, n, C):
     y, sig, sizes, _ = hierarchical_data(J, n, 7)

@@ -155,8 +155,15 @@ class DeviceBatchedWorkspace:
                              f"{params.shape[0] if params.ndim == 2 else params.shape}")
         if params.shape[1] != self.batch_size:
             raise IndexError(f"expected {self.batch_size} batch elements, got {params.shape[1]}")
-        # P x C (reference layout) -> chain-major contiguous float32
-        return np.ascontiguousarray(params.T, dtype=np.float32)
+        # P x C (reference layout) -> chain-major contiguous float32.  A P x C view of
+        # chain-major float32 memory is passed as it is; otherwise the converted copy
+        # is written into page-locked memory, so the upload needs no staging bounce.
+        qt = params.T
+        if qt.dtype == np.float32 and qt.flags.c_contiguous:
+            return qt
+        q = _host_output(qt.shape)
+        np.copyto(q, qt, casting="unsafe")
+        return q
 
     def _check_device_params(self, params):
         torch = _torch()
