@@ -76,6 +76,13 @@ extern "C" {
  * y_i ~ studentt(nu_obs, loc, s + w).  The reference's device-lowerable
  * heavy-tail model (math.jl:167-186). */
 #define UT_FAMILY_STUDENTT_HEAVY_TAIL        6
+/* Normal location with a known observation scale: mu ~ normal(mu_loc,
+ * mu_scale) (identity), y_i ~ normal(mu, obs_scale) for i = 1..N.  The
+ * reference's conjugate gaussian gate model (a DeviceNormalChoiceStep and
+ * normal observations with a constant scale argument; the persistent-NUTS and
+ * ChEES device tests, test/uncertaintea/core/device_persistent_nuts.jl:33-38,
+ * device_chees.jl:26-32). */
+#define UT_FAMILY_NORMAL_KNOWN_SCALE         7
 
 /* Fixed kernel description: what the host lowers a model's execution plan to
  * (reference: DeviceExecutionPlan, src/device/plan/steps.jl:482-489, produced
@@ -85,7 +92,8 @@ extern "C" {
  *   NLS : [mu, log(s)];
  *   BB  : [logit(p)];
  *   LGN : [log(a), log(b)];
- *   HT  : [loc, log(s), log(w)]. */
+ *   HT  : [loc, log(s), log(w)];
+ *   NKS : [mu]. */
 typedef struct ut_plan_desc {
     int32_t family;          /* UT_FAMILY_*                                   */
     int32_t num_params;      /* P, unconstrained parameter count              */
@@ -108,6 +116,7 @@ typedef struct ut_plan_desc {
     double nu_obs;           /*     y ~ studentt(nu_obs, loc, s + w)          */
     double weibull_shape;    /*     w ~ weibull(weibull_shape, weibull_scale) */
     double weibull_scale;    /*     (s uses scale_shape / scale_rate)         */
+    double obs_scale;        /* NKS: y ~ normal(mu, obs_scale)                */
 } ut_plan_desc;
 
 typedef struct ut_workspace ut_workspace;

@@ -155,7 +155,8 @@ ModelData make_model(const ut_plan_desc* plan, const float* observed, const int3
             m.y[i] = observed[(size_t)i * (D + 1) + D];
         }
     } else if (plan->family == UT_FAMILY_NORMAL_LOCATION_SCALE || plan->family == UT_FAMILY_BERNOULLI_BETA ||
-               plan->family == UT_FAMILY_LOGNORMAL_GAMMA_NORMAL || plan->family == UT_FAMILY_STUDENTT_HEAVY_TAIL) {
+               plan->family == UT_FAMILY_LOGNORMAL_GAMMA_NORMAL || plan->family == UT_FAMILY_STUDENTT_HEAVY_TAIL ||
+               plan->family == UT_FAMILY_NORMAL_KNOWN_SCALE) {
         m.y.assign(observed, observed + N);
     } else {
         const int J = plan->num_groups;
@@ -264,6 +265,25 @@ W gauss_logjoint_grad(const ModelData& m, const T* q, T* g) {
     return total;
 }
 
+// Normal location with a known observation scale (steps: Normal on mu, then
+// the loop of normal observations with a constant scale argument;
+// logjoint_kernel.jl:105-111, the reference's conjugate gate model
+// test/uncertaintea/core/device_persistent_nuts.jl:33-38).
+template <class T, class W>
+W nks_logjoint_grad(const ModelData& m, const T* q, T* g) {
+    const ut_plan_desc& p = m.plan;
+    const T mu = q[0], sigma = T(p.obs_scale);
+    W total = (W)normal_logpdf<T>(T(p.mu_loc), T(p.mu_scale), mu);
+    W gmu = -(W)(mu - T(p.mu_loc)) / ((W)p.mu_scale * (W)p.mu_scale);
+    for (int i = 0; i < p.num_obs; ++i) {
+        const T yv = (T)m.y[i];
+        total += (W)normal_logpdf<T>(mu, sigma, yv);
+        gmu += ((W)yv - (W)mu) / ((W)sigma * (W)sigma);
+    }
+    if (g) g[0] = (T)gmu;
+    return total;
+}
+
 // Bernoulli observations of a beta probability (steps: Beta with the logit
 // transform, math.jl:161-165, 1150-1155, then the loop of Bernoulli
 // observations, math.jl:191-195), every observation scored separately.
@@ -368,6 +388,7 @@ W logjoint_grad(const ModelData& m, const T* q, T* g) {
     if (m.plan.family == UT_FAMILY_BERNOULLI_BETA) return bern_logjoint_grad<T, W>(m, q, g);
     if (m.plan.family == UT_FAMILY_GLM_BERNOULLI_LOGIT) return glm_logjoint_grad<T, W>(m, q, g);
     if (m.plan.family == UT_FAMILY_NORMAL_LOCATION_SCALE) return gauss_logjoint_grad<T, W>(m, q, g);
+    if (m.plan.family == UT_FAMILY_NORMAL_KNOWN_SCALE) return nks_logjoint_grad<T, W>(m, q, g);
     return hier_logjoint_grad<T, W>(m, q, g);
 }
 

@@ -20,7 +20,8 @@ import pytest
 import oracle
 from uncertaintea_b200 import _native as nat
 from uncertaintea_b200.models import (BernoulliBeta, BernoulliLogitGLM, HierarchicalNormalNoncentered,
-                                      LognormalGammaNormal, NormalLocationScale, StudentTHeavyTail, gauss_data,
+                                      LognormalGammaNormal, NormalKnownScale, NormalLocationScale, StudentTHeavyTail,
+                                      gauss_data,
                                       hierarchical_data, logistic_regression_data)
 
 pytestmark = pytest.mark.gpu
@@ -400,9 +401,32 @@ def _nuts_gpu(ws, qd, g, t, im, step, depth, coord):
     return res
 
 
-@pytest.mark.parametrize("case", ["hier", "glm", "gauss", "bern", "ht"])
+@pytest.mark.parametrize("n,C", [(1, 4), (500, 100), (0, 8)])
+def test_known_scale_density_vs_fp64_oracle(lib, n, C):
+    """The normal known-scale family (the reference's conjugate gate model,
+    device_persistent_nuts.jl:33-38: y = 0.3 with n = 1), an empty loop, and a
+    larger one with another prior and scale."""
+    if n == 1:
+        m, y = NormalKnownScale(), np.array([0.3], dtype=np.float32)
+    else:
+        m, y = NormalKnownScale(mu_loc=0.5, mu_scale=2.0, sigma=0.7), gauss_data(n, 4)[0] if n else np.zeros(0)
+    q = (np.random.default_rng(6).standard_normal((C, 1)) * 1.5).astype(np.float32)
+    ws = _ws(m, (n,), {"y": y}, C)
+    assert ws.kernel_path() == "warp"
+    t, g = ws.logjoint_gradient(q.T)
+    t64, g64 = oracle.OracleModel(ws.lowered).logjoint_gradient_f64(q.astype(np.float64))
+    assert _lj_err(t, t64) <= 1e-5
+    assert _grad_err(np.asarray(g.T), g64) <= 1e-5
+    ws.close()
+
+
+@pytest.mark.parametrize("case", ["hier", "glm", "gauss", "bern", "ht", "nks"])
 def test_persistent_nuts_iteration_vs_oracle(lib, case):
-    if case == "ht":
+    if case == "nks":
+        m, args, cons = NormalKnownScale(), (1,), {"y": np.array([0.3])}
+        q = (0.15 + 0.7 * np.random.default_rng(4).standard_normal((128, 1))).astype(np.float32)
+        step = 0.5
+    elif case == "ht":
         y = (0.5 + np.random.default_rng(3).standard_t(5, size=200)).astype(np.float32)
         m, args, cons = StudentTHeavyTail(), (200,), {"y": y}
         q = (np.array([0.5, -0.3, 0.0]) + 0.2 * np.random.default_rng(6).standard_normal((128, 3))).astype(np.float32)

@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from uncertaintea_b200 import (BernoulliBeta, BernoulliLogitGLM, HierarchicalNormalNoncentered, LognormalGammaNormal,
-                               NormalLocationScale, batched_advi,
+                               NormalKnownScale, NormalLocationScale, batched_advi,
                                batched_chees, batched_hmc, batched_meads, batched_nuts, ess, gauss_data, hierarchical_data,
                                logistic_regression_data, rhat, variational_mean, variational_samples)
 
@@ -154,6 +154,47 @@ def test_gauss_nuts_matches_exact_posterior(lib, strategy):
     mean, mcse = _mean_mcse(res)
     assert abs(mean[0] - mu_ex) <= 5 * mcse[0], (mean[0], mu_ex, mcse[0])
     assert abs(mean[1] - s_ex) <= 5 * mcse[1], (mean[1], s_ex, mcse[1])
+
+
+# The reference's conjugate gate (device_persistent_nuts.jl:33-38, device_chees.jl:26-32):
+# mu ~ normal(0, 1), y ~ normal(mu, 1) observed at y = 0.3; posterior normal(0.15, sqrt(0.5)).
+CONJ_MEAN, CONJ_SD = 0.15, np.sqrt(0.5)
+
+
+@pytest.mark.parametrize("strategy", ["persistent", "masked"])
+def test_conjugate_gauss_nuts_gate(lib, strategy):
+    """The reference's persistent-NUTS gate (device_persistent_nuts.jl:58-72; 64
+    chains, 1000 draws after 500 warmup): mean and sd within 0.03 of the exact
+    posterior, R-hat < 1.01, no divergences -- for both device tree strategies
+    (its persistent-vs-masked check, :74-100, compares the same moments)."""
+    res = batched_nuts(NormalKnownScale(), (1,), {"y": np.array([0.3])}, num_chains=64, num_samples=1000,
+                       num_warmup=500, tree_strategy=strategy, rng=np.random.default_rng(511))
+    d = res.constrained[..., 0]
+    assert np.all(np.isfinite(d))
+    assert abs(d.mean() - CONJ_MEAN) <= 0.03, d.mean()
+    assert abs(d.std() - CONJ_SD) <= 0.03, d.std()
+    assert np.max(rhat(res)) < 1.01, rhat(res)
+    assert res.divergent.sum() == 0
+
+
+def test_conjugate_gauss_chees_gate(lib):
+    """The reference's device ChEES gate (device_chees.jl:45-79; 16 chains, 2000
+    draws after 600 warmup, the default trajectory-gradient estimator): mean
+    within 0.05 and sd within 0.08 of the exact posterior, R-hat < 1.05, and the
+    trajectory length T finite, in (0.5, 200) at the end of warmup, with a tail
+    (last 150 warmup iterations) whose max/min ratio is below 3."""
+    trace = []
+    res = batched_chees(NormalKnownScale(), (1,), {"y": np.array([0.3])}, num_chains=16, num_samples=2000,
+                        num_warmup=600, rng=np.random.default_rng(161), _trajectory_trace=trace)
+    d = res.constrained[..., 0]
+    assert np.all(np.isfinite(d))
+    assert abs(d.mean() - CONJ_MEAN) <= 0.05, d.mean()
+    assert abs(d.std() - CONJ_SD) <= 0.08, d.std()
+    assert np.max(rhat(res)) < 1.05, rhat(res)
+    assert len(trace) == 600 and np.all(np.isfinite(trace))
+    assert 0.5 < trace[-1] < 200.0, trace[-1]
+    tail = np.asarray(trace[-150:])
+    assert tail.max() / tail.min() < 3.0
 
 
 def test_chees_forward_velocity_adapts_trajectory(lib):

@@ -82,6 +82,14 @@ def test_lowering_report_flags_bad_descriptions(lib):
     gauss.num_params = 3
     assert lib.ut_lowering_report(ctypes.byref(gauss), buf, len(buf)) == nat.UT_ERR_UNSUPPORTED
     assert b"num_params must equal 2" in buf.value and b"gamma shape and rate" in buf.value
+    nks = nat.PlanDesc(family=nat.UT_FAMILY_NORMAL_KNOWN_SCALE, num_params=1, num_obs=1, mu_scale=1.0, obs_scale=1.0)
+    assert lib.ut_lowering_report(ctypes.byref(nks), buf, len(buf)) == nat.UT_OK
+    nks.obs_scale = 0.0
+    nks.num_params = 2
+    assert lib.ut_lowering_report(ctypes.byref(nks), buf, len(buf)) == nat.UT_ERR_UNSUPPORTED
+    assert b"num_params must equal 1 (mu)" in buf.value and b"observation scale" in buf.value
+    nks.num_params, nks.obs_scale = 1, float("inf")
+    assert lib.ut_lowering_report(ctypes.byref(nks), buf, len(buf)) == nat.UT_ERR_UNSUPPORTED
 
 
 def test_workspace_create_validates_before_touching_device(lib):

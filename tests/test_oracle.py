@@ -5,8 +5,8 @@ import pytest
 
 import oracle
 from uncertaintea_b200.models import (BernoulliBeta, BernoulliLogitGLM, HierarchicalNormalNoncentered,
-                                      LognormalGammaNormal, NormalLocationScale, StudentTHeavyTail, gauss_data,
-                                      hierarchical_data,
+                                      LognormalGammaNormal, NormalKnownScale, NormalLocationScale, StudentTHeavyTail,
+                                      gauss_data, hierarchical_data,
                                       logistic_regression_data)
 
 
@@ -211,6 +211,36 @@ def test_meads_max_eig_pins():
     sq = (x * x).sum(0)
     alt = ((A * A).sum() - (sq ** 2).sum()) / (n * (n - 1)) / (sq.sum() / n)
     assert abs(oracle.meads_max_eig(x) - alt) < 1e-10 * alt
+
+
+def test_known_scale_oracle_on_the_reference_gate_model():
+    """The reference's conjugate gate model (device_persistent_nuts.jl:33-38):
+    mu ~ normal(0, 1), y ~ normal(mu, 1) at y = 0.3.  The logjoint is the closed
+    form, the gradient is 0.3 - 2 mu (zero at the posterior mean 0.15), and the
+    logjoint minus its maximum is the posterior normal(0.15, sqrt(0.5)) kernel."""
+    from scipy import stats
+    y = np.float32(0.3).astype(np.float64)
+    om = oracle.OracleModel(NormalKnownScale().lower((1,), {"y": np.array([0.3])}))
+    mu = np.linspace(-3.0, 3.0, 13)[:, None]
+    t, g = om.logjoint_gradient_f64(mu)
+    ref = stats.norm(0, 1).logpdf(mu[:, 0]) + stats.norm(mu[:, 0], 1).logpdf(y)
+    assert np.max(np.abs(t - ref)) <= 1e-12 * np.max(np.abs(ref))
+    assert np.max(np.abs(g[:, 0] - (y - 2 * mu[:, 0]))) <= 1e-12
+    post = stats.norm(y / 2, np.sqrt(0.5)).logpdf(mu[:, 0])
+    assert np.ptp((t - post)) <= 1e-12
+    # several observations and another known scale: the precision-weighted sum
+    ys = np.array([0.4, -0.7, 1.1, 0.2, 0.9])
+    m = NormalKnownScale(mu_loc=0.5, mu_scale=2.0, sigma=0.7)
+    om = oracle.OracleModel(m.lower((5,), {"y": ys}))
+    t, g = om.logjoint_gradient_f64(mu)
+    yf = ys.astype(np.float32).astype(np.float64)
+    for c in range(len(mu)):
+        r = stats.norm(0.5, 2.0).logpdf(mu[c, 0]) + stats.norm(mu[c, 0], 0.7).logpdf(yf).sum()
+        assert abs(t[c] - r) <= 1e-12 * abs(r)
+    # an empty observation loop leaves the prior
+    empty = oracle.OracleModel(m.lower((0,), {"y": np.zeros(0)}))
+    t, _ = empty.logjoint_gradient_f64(mu)
+    assert np.max(np.abs(t - stats.norm(0.5, 2.0).logpdf(mu[:, 0]))) <= 1e-12
 
 
 def test_bernoulli_beta_oracle_on_the_reference_parity_case():

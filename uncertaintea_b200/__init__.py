@@ -9,7 +9,7 @@ the learned gradient surrogate for ChEES-HMC and many-model batched NUTS
 (no reference counterparts).
 """
 from .models import (BernoulliBeta, BernoulliLogitGLM, HierarchicalNormalNoncentered, LognormalGammaNormal,
-                     NormalLocationScale, StudentTHeavyTail, TeaModelSpec, gauss_data, hierarchical_data, logistic_regression_data)
+                     NormalKnownScale, NormalLocationScale, StudentTHeavyTail, TeaModelSpec, gauss_data, hierarchical_data, logistic_regression_data)
 from .device import (DeviceBatchedWorkspace, device_batched_logjoint, device_batched_logjoint_,
                      device_batched_logjoint_gradient, device_batched_logjoint_gradient_, device_lowering_report)
 from .inference import HMCChains, batched_chees, batched_hmc, batched_nuts, posterior_array
@@ -22,7 +22,7 @@ from . import rng
 
 __all__ = [
     "BernoulliBeta", "BernoulliLogitGLM", "HierarchicalNormalNoncentered", "LognormalGammaNormal",
-    "NormalLocationScale", "StudentTHeavyTail", "TeaModelSpec",
+    "NormalKnownScale", "NormalLocationScale", "StudentTHeavyTail", "TeaModelSpec",
     "gauss_data",
     "hierarchical_data",
     "logistic_regression_data", "DeviceBatchedWorkspace", "device_batched_logjoint", "device_batched_logjoint_",

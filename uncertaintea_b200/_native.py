@@ -28,6 +28,7 @@ UT_FAMILY_NORMAL_LOCATION_SCALE = 3
 UT_FAMILY_BERNOULLI_BETA = 4
 UT_FAMILY_LOGNORMAL_GAMMA_NORMAL = 5
 UT_FAMILY_STUDENTT_HEAVY_TAIL = 6
+UT_FAMILY_NORMAL_KNOWN_SCALE = 7
 
 
 class PlanDesc(ctypes.Structure):
@@ -53,6 +54,7 @@ class PlanDesc(ctypes.Structure):
         ("nu_obs", c_double),
         ("weibull_shape", c_double),
         ("weibull_scale", c_double),
+        ("obs_scale", c_double),
     ]
 
 

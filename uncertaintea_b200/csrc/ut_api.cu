@@ -168,6 +168,11 @@ std::string plan_issues(const ut_plan_desc* p) {
         if (!(p->mu_scale > 0.0)) add("mu prior scale must be > 0");
         if (!(p->scale_shape > 0.0) || !(p->scale_rate > 0.0)) add("gamma shape and rate must be > 0");
         if (p->num_obs < 0) add("num_obs must be >= 0");
+    } else if (p->family == UT_FAMILY_NORMAL_KNOWN_SCALE) {
+        if (p->num_params != 1) add("num_params must equal 1 (mu)");
+        if (!(p->mu_scale > 0.0)) add("mu prior scale must be > 0");
+        if (!(p->obs_scale > 0.0) || !std::isfinite(p->obs_scale)) add("observation scale must be finite and > 0");
+        if (p->num_obs < 0) add("num_obs must be >= 0");
     } else if (p->family == UT_FAMILY_STUDENTT_HEAVY_TAIL) {
         if (p->num_params != 3) add("num_params must equal 3 (loc, log s, log w)");
         if (!(p->nu_prior > 0.0) || !(p->nu_obs > 0.0)) add("Student-t degrees of freedom must be > 0");
@@ -523,7 +528,8 @@ int32_t ut_workspace_create(const ut_plan_desc* plan, const float* observed, int
             return fail(UT_ERR_DIMENSION, "expected %lld staged observation rows (N*(D+1)), got %lld", (long long)want,
                         (long long)observed_rows);
     } else if (plan->family == UT_FAMILY_NORMAL_LOCATION_SCALE || plan->family == UT_FAMILY_BERNOULLI_BETA ||
-               plan->family == UT_FAMILY_LOGNORMAL_GAMMA_NORMAL || plan->family == UT_FAMILY_STUDENTT_HEAVY_TAIL) {
+               plan->family == UT_FAMILY_LOGNORMAL_GAMMA_NORMAL || plan->family == UT_FAMILY_STUDENTT_HEAVY_TAIL ||
+               plan->family == UT_FAMILY_NORMAL_KNOWN_SCALE) {
         if (observed_rows != N)
             return fail(UT_ERR_DIMENSION, "expected %d staged observation rows (N), got %lld", N,
                         (long long)observed_rows);
@@ -642,12 +648,21 @@ int32_t ut_workspace_create(const ut_plan_desc* plan, const float* observed, int
                 return bail(fail(UT_ERR_CUDA, "tensor-core GLM setup failed: %s", tc_glm_last_error()));
             }
         }
-    } else if (plan->family == UT_FAMILY_NORMAL_LOCATION_SCALE) {
+    } else if (plan->family == UT_FAMILY_NORMAL_LOCATION_SCALE || plan->family == UT_FAMILY_NORMAL_KNOWN_SCALE) {
         dm.family = kFamGauss;
         dm.gauss.N = N;
         dm.gauss.mu_loc = (float)plan->mu_loc; dm.gauss.mu_scale = (float)plan->mu_scale;
-        dm.gauss.shape = (float)plan->scale_shape; dm.gauss.rate = (float)plan->scale_rate;
-        dm.gauss.lgc = (float)(plan->scale_shape * std::log(plan->scale_rate) - std::lgamma(plan->scale_shape));
+        if (plan->family == UT_FAMILY_NORMAL_KNOWN_SCALE) {
+            dm.gauss.known = 1;
+            dm.gauss.sigma = (float)plan->obs_scale;
+            dm.gauss.log_sigma = std::log((float)plan->obs_scale);
+            dm.gauss.shape = dm.gauss.rate = 1.0f;
+            dm.gauss.lgc = 0.0f;
+        } else {
+            dm.gauss.known = 0;
+            dm.gauss.shape = (float)plan->scale_shape; dm.gauss.rate = (float)plan->scale_rate;
+            dm.gauss.lgc = (float)(plan->scale_shape * std::log(plan->scale_rate) - std::lgamma(plan->scale_shape));
+        }
         if ((rc = dalloc(ws, &ws->d_y, std::max(N, 1)))) return bail(rc);
         if (N > 0) UT_CUDA(cudaMemcpy(ws->d_y, observed, sizeof(float) * N, cudaMemcpyHostToDevice));
         dm.gauss.y = ws->d_y;

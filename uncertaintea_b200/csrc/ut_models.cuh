@@ -42,9 +42,14 @@ struct HierModel {
 // Normal + Gamma(log transform) choice steps and a loop of normal observations,
 // logjoint_kernel.jl:105-111, 146-151; gamma density math.jl:103-107).
 // lgc = shape * log(rate) - loggamma(shape), a constant the host computes.
+// known = 1: the observation scale is the constant sigma and mu is the only
+// parameter (the reference's conjugate gate model, normal observations with a
+// constant scale argument); log_sigma = log(sigma), computed by the host.
 struct GaussModel {
     int N;
     float mu_loc, mu_scale, shape, rate, lgc;
+    int known;
+    float sigma, log_sigma;
     const float* y;  // N
 };
 
@@ -220,8 +225,8 @@ __device__ __forceinline__ float gauss_lj_grad(const GaussModel& m, const float 
                                                bool want_grad) {
     const int lane = threadIdx.x & 31;
     const float mu = __shfl_sync(UT_FULL_MASK, q[0], 0);
-    const float u = __shfl_sync(UT_FULL_MASK, q[0], 1);
-    const float s = expf(u);
+    const float u = m.known ? m.log_sigma : __shfl_sync(UT_FULL_MASK, q[0], 1);
+    const float s = m.known ? m.sigma : expf(u);
     float sr = 0.0f, sq = 0.0f;
     for (int i = lane; i < m.N; i += 32) {
         const float r = m.y[i] - mu;
@@ -234,12 +239,12 @@ __device__ __forceinline__ float gauss_lj_grad(const GaussModel& m, const float 
     const float nf = (float)m.N;
     float lj = nf * (-u - kHalfLog2Pi) - 0.5f * sq * inv_s * inv_s;
     lj += normal_logpdf(m.mu_loc, m.mu_scale, mu);
-    lj += s >= FLT_MIN ? m.lgc + (m.shape - 1.0f) * u - m.rate * s + u : -INFINITY;
+    if (!m.known) lj += s >= FLT_MIN ? m.lgc + (m.shape - 1.0f) * u - m.rate * s + u : -INFINITY;
     if (want_grad) {
 #pragma unroll
         for (int k = 0; k < K; ++k) g[k] = 0.0f;
         if (lane == 0) g[0] = sr * inv_s * inv_s - (mu - m.mu_loc) / (m.mu_scale * m.mu_scale);
-        if (lane == 1) g[0] = -nf + sq * inv_s * inv_s + m.shape - m.rate * s;
+        if (lane == 1 && !m.known) g[0] = -nf + sq * inv_s * inv_s + m.shape - m.rate * s;
     }
     return lj;
 }

@@ -234,6 +234,51 @@ class NormalLocationScale(TeaModelSpec):
 
 
 @dataclass
+class NormalKnownScale(TeaModelSpec):
+    """``mu ~ normal(mu_loc, mu_scale)``, ``y[i] ~ normal(mu, sigma)`` for i = 1..n
+    with sigma known -- the reference's conjugate gaussian gate model
+    (test/uncertaintea/core/device_persistent_nuts.jl:33-38, device_chees.jl:26-32:
+    ``mu ~ normal(0, 1)``, ``{:y} ~ normal(mu, 1)`` observed at y = 0.3, posterior
+    normal(0.15, sqrt(0.5))).
+
+    Unconstrained parameter: [mu] (identity transform).
+    args = (n,); constraints = {"y": y} with n observations.
+    """
+
+    mu_loc: float = 0.0
+    mu_scale: float = 1.0
+    sigma: float = 1.0
+    name: str = "normal_known_scale"
+
+    def parameter_names(self, args=(), constraints=None):
+        return ["mu"]
+
+    def lower(self, args=(), constraints=None) -> Lowered:
+        if len(args) != 1:
+            raise ValueError(f"{self.name} expects args=(n,), got {len(args)} argument(s)")
+        n = int(args[0])
+        if n < 0:
+            raise ValueError("n must be >= 0")
+        y = _observed_value(constraints, "y").astype(np.float32).reshape(-1)
+        if y.shape != (n,):
+            raise IndexError(f"expected {n} observations, got shape {y.shape}")
+        plan = nat.PlanDesc(
+            family=nat.UT_FAMILY_NORMAL_KNOWN_SCALE, num_params=1, num_obs=n, num_coefs=0, has_intercept=0,
+            num_groups=0, intercept_mu=0.0, intercept_sigma=1.0, coef_mu=0.0, coef_sigma=1.0,
+            mu_loc=self.mu_loc, mu_scale=self.mu_scale, tau_scale=1.0, obs_scale=self.sigma)
+        empty = np.zeros(0, dtype=np.int32)
+        return Lowered(plan, np.ascontiguousarray(y), empty, empty, 1)
+
+    def constrain(self, unconstrained, args=(), constraints=None):
+        return np.array(unconstrained, dtype=np.float64, copy=True)
+
+    def initial_positions(self, rng, num_chains, args=(), constraints=None, init_strategy="prior"):
+        if init_strategy == "uniform":
+            return rng.uniform(-2.0, 2.0, size=(num_chains, 1))
+        return rng.normal(self.mu_loc, self.mu_scale, size=(num_chains, 1))
+
+
+@dataclass
 class BernoulliBeta(TeaModelSpec):
     """``p ~ beta(alpha, beta)``, ``z[i] ~ bernoulli(p)`` for i = 1..n -- the
     reference's device-lowerable bernoulli model
