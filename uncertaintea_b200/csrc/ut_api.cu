@@ -352,7 +352,7 @@ int32_t launch_stream_rows(ut_workspace* ws, const float* params, float* totals,
                            cudaStream_t st) {
     const int F = ws->P;
     int32_t rc;
-    if (!ws->d_spart) {
+    if (!ws->d_serr) {  // keyed on the last buffer made, so a failed attempt is redone
         int dev_sms = 148;
         cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, ws->device);
         ws->stream_splits = dev_sms;
@@ -413,8 +413,12 @@ int32_t density(ut_workspace* ws, const float* params, float* totals, float* gra
     return grads ? launch_tiled_t<true>(ws, params, totals, grads, st) : launch_tiled_t<false>(ws, params, totals, nullptr, st);
 }
 
+// Lazily made buffer sets are keyed on the last buffer each makes: after a
+// failed attempt (out of device memory) the next call makes the whole set again
+// instead of finding it half made.  Buffers of a failed attempt stay in the
+// workspace's allocation list and are freed with it.
 int32_t ensure_lf(ut_workspace* ws) {
-    if (ws->lf.wq) return UT_OK;
+    if (ws->lf.valid) return UT_OK;
     size_t pc = (size_t)ws->P * ws->C;
     int32_t rc;
     if ((rc = dalloc(ws, &ws->lf.wq, pc))) return rc;
@@ -427,7 +431,7 @@ int32_t ensure_lf(ut_workspace* ws) {
 }
 
 int32_t ensure_host_buffers(ut_workspace* ws) {
-    if (ws->d_params) return UT_OK;
+    if (ws->h_err) return UT_OK;
     size_t pc = (size_t)ws->P * ws->C;
     int32_t rc;
     if ((rc = dalloc(ws, &ws->d_params, pc))) return rc;
@@ -1163,7 +1167,7 @@ int32_t ut_lockstep_nuts_iteration(ut_workspace* ws, const ut_nuts_buffers* buf,
     if ((rc = ensure_lf(ws))) return rc;
     const size_t C = ws->C, P = ws->P;
     const int K = ws->P <= 32 ? 1 : ws->P <= 64 ? 2 : ws->P <= 96 ? 3 : ws->P <= 128 ? 4 : 8;
-    if (!ws->ls_vec) {
+    if (!ws->h_active) {  // keyed on the last buffer made
         if ((rc = dalloc(ws, &ws->ls_vec, (size_t)kLsNumVec * C * P))) return rc;
         if ((rc = dalloc(ws, &ws->ls_f, (size_t)kLsNumF * C))) return rc;
         if ((rc = dalloc(ws, &ws->ls_i, (size_t)kLsNumI * C))) return rc;
@@ -1252,7 +1256,7 @@ int32_t ut_chees_reduce(ut_workspace* ws, const float* d_initials, const float* 
     if (rc) return rc;
     if (!d_initials || !d_proposals || !d_endpoint_momentum || !d_accept_prob || !d_divergent || !d_inverse_mass || !out)
         return fail(UT_ERR_ARGUMENT, "null ChEES buffer");
-    if (!ws->d_flags) {
+    if (!ws->d_out) {  // keyed on the last buffer made
         if ((rc = dalloc(ws, &ws->d_flags, ws->C))) return rc;
         if ((rc = dalloc(ws, &ws->d_means, 2 * (size_t)ws->P))) return rc;
         if ((rc = dalloc(ws, &ws->d_terms, 2 * (size_t)ws->C))) return rc;
