@@ -151,6 +151,125 @@ def test_split_ess_matches_direct_sum():
     assert dg._split_ess_of(split) == pytest.approx(min(M * S, M * S / tau), rel=1e-9)
 
 
+def test_summarize_matches_the_reference_formulas():
+    """summarize (diagnostics.jl:662-712, summaries.jl:1-76) restated with direct
+    loops: quantiles at position 1 + (n - 1) p, MCSE of the mean sd / sqrt(ess),
+    tail ESS from the 5% / 95% indicators, order-statistic MCSE of the
+    quantiles, per-chain means and SDs, quantile validation."""
+    rng = np.random.default_rng(7)
+    x = np.cumsum(rng.standard_normal((4, 301, 2)), axis=1) * 0.05 + rng.standard_normal((4, 301, 2))
+
+    class Fake:
+        constrained = x
+        unconstrained = x
+        accept_prob = rng.random((4, 301))
+        divergent = rng.random((4, 301)) < 0.01
+        step_size = np.array([0.1, 0.2, 0.3, 0.4])
+        energy = rng.standard_normal((4, 301))
+        tree_depth = np.zeros((4, 301), dtype=np.int32)
+
+        @staticmethod
+        def parameter_names():
+            return ["a", "b"]
+
+    out = dg.summarize(Fake, quantiles=(0.1, 0.5, 0.9), per_chain=True)
+
+    def quant(sv, q):  # diagnostics.jl:486-497, 1-based
+        n = len(sv)
+        pos = 1 + (n - 1) * q
+        lo, hi = int(np.floor(pos)), int(np.ceil(pos))
+        return sv[lo - 1] if lo == hi else (1 - (pos - lo)) * sv[lo - 1] + (pos - lo) * sv[hi - 1]
+
+    for p, row in enumerate(out["parameters"]):
+        pooled = np.concatenate([x[c, :, p] for c in range(4)])
+        sv = np.sort(pooled)
+        n = pooled.size
+        mean = sum(pooled) / n
+        sd = np.sqrt(sum((v - mean) ** 2 for v in pooled) / (n - 1))
+        assert row["parameter"] == "ab"[p]
+        assert row["mean"] == pytest.approx(mean, rel=1e-12) and row["sd"] == pytest.approx(sd, rel=1e-12)
+        assert row["quantiles"] == pytest.approx([quant(sv, q) for q in (0.1, 0.5, 0.9)], rel=1e-12)
+        split = dg._split_chain_draws(x[:, :, p])
+        ess_bulk = dg._split_ess_of(split)
+        assert row["ess_bulk"] == pytest.approx(ess_bulk, rel=1e-12)
+        assert row["mcse_mean"] == pytest.approx(sd * np.sqrt(1 / ess_bulk), rel=1e-12)
+        ind = lambda t: dg._split_ess_of((split <= t).astype(float))  # noqa: E731
+        assert row["ess_tail"] == pytest.approx(min(ind(quant(sv, 0.05)), ind(quant(sv, 0.95))), rel=1e-12)
+        for q, th, m in zip((0.1, 0.5, 0.9), row["quantiles"], row["mcse_quantiles"]):
+            e = ind(th)
+            spread = np.sqrt(q * (1 - q) / e)
+            ref = (quant(sv, min(q + spread, 1.0)) - quant(sv, max(q - spread, 0.0))) / 2
+            assert m == pytest.approx(ref, rel=1e-12)
+        for c in range(4):
+            cm = sum(x[c, :, p]) / 301
+            assert row["per_chain_means"][c] == pytest.approx(cm, rel=1e-12)
+            assert row["per_chain_sds"][c] == pytest.approx(np.sqrt(sum((x[c, :, p] - cm) ** 2) / 300), rel=1e-12)
+    dgn = out["diagnostics"]
+    assert dgn["acceptance_rate"] == pytest.approx(Fake.accept_prob.mean())
+    assert dgn["divergence_rate"] == pytest.approx(Fake.divergent.mean())
+    assert dgn["mean_step_size"] == pytest.approx(0.25)
+    assert dg.summarize(Fake)["parameters"][0]["per_chain_means"] is None
+    # a parameter on one side of the tail threshold has NaN tail ESS (a constant indicator)
+    class Const(Fake):
+        constrained = np.ones((4, 301, 2))
+        unconstrained = constrained
+    assert np.isnan(dg.summarize(Const)["parameters"][0]["ess_tail"])
+    for bad, msg in [((), "non-empty"), ((0.5, 1.5), r"lie in \[0, 1\]")]:
+        with pytest.raises(ValueError, match=msg):
+            dg.summarize(Fake, quantiles=bad)
+
+
+def test_check_diagnostics_matches_the_reference_rules():
+    """check_diagnostics / has_warnings (warnings.jl:7-86): per-chain divergence
+    counts, E-BFMI, treedepth hits at the depth limit, high-R-hat and low-ESS
+    parameters (non-finite values count), none of the latter below 4 draws."""
+    rng = np.random.default_rng(2)
+    C, S = 3, 200
+
+    class Fake:
+        constrained = rng.standard_normal((C, S, 2))
+        unconstrained = constrained
+        divergent = np.zeros((C, S), dtype=bool)
+        energy = rng.standard_normal((C, S))
+        tree_depth = np.full((C, S), 3)
+        max_tree_depth = 10
+        accept_prob = np.full((C, S), 0.8)
+        step_size = np.full(C, 0.1)
+
+        @staticmethod
+        def parameter_names():
+            return ["a", "b"]
+
+    w = dg.check_diagnostics(Fake)
+    ref = [np.sum(np.diff(e) ** 2) / np.sum((e - e.mean()) ** 2) for e in Fake.energy]
+    assert w.ebfmi == pytest.approx(ref, rel=1e-12)
+    assert not dg.has_warnings(w) and w.low_ess_parameters == [] and w.high_rhat_parameters == []
+
+    class Bad(Fake):
+        constrained = np.concatenate([rng.standard_normal((C, S, 1)),
+                                      rng.standard_normal((C, S, 1)) + np.arange(C)[:, None, None] * 3], axis=2)
+        unconstrained = constrained
+        divergent = np.zeros((C, S), dtype=bool)
+        divergent[1, :5] = True
+        tree_depth = np.full((C, S), 10)
+        energy = np.cumsum(rng.standard_normal((C, S)), axis=1)   # random walk: E-BFMI far below 0.3
+
+    w = dg.check_diagnostics(Bad)
+    assert list(w.num_divergent) == [0, 5, 0] and list(w.treedepth_hits) == [S, S, S]
+    assert np.all(w.ebfmi < 0.3) and w.high_rhat_parameters == ["b"] and "b" in w.low_ess_parameters
+    assert dg.has_warnings(w)
+    assert dg.check_diagnostics(Bad, ess_threshold=0.0).low_ess_parameters == []
+
+    class Short(Fake):
+        constrained = np.ones((C, 3, 2))
+        unconstrained = constrained
+        energy = np.ones((C, 3))
+
+    w = dg.check_diagnostics(Short)
+    assert w.high_rhat_parameters == [] and np.all(np.isnan(w.ebfmi))
+    assert isinstance(dg.summarize(Fake)["warnings"], dg.SamplerWarnings)
+
+
 # ---- mean-field ADVI host logic (vi.jl:179-227, guides.jl:51-57) -----------
 def test_advi_entropy_clip_and_adam():
     from uncertaintea_b200 import vi
@@ -178,11 +297,31 @@ def test_advi_validation_before_any_device_work():
     for kw, msg in [(dict(guide="fullrank"), "CPU-only"), (dict(elbo="iwae"), "CPU-only"),
                     (dict(guide="bogus"), "guide must be"), (dict(num_iterations=0), "num_iterations > 0"),
                     (dict(num_particles=0), "num_particles > 0"), (dict(beta1=1.0), "beta1"),
-                    (dict(gradient_clip=0.0), "gradient_clip > 0")]:
+                    (dict(gradient_clip=0.0), "gradient_clip > 0"), (dict(adtype="bogus"), "adtype must be"),
+                    (dict(adtype="reverse"), "host-only path")]:
         args = dict(num_iterations=5)
         args.update(kw)
         with pytest.raises(ValueError, match=msg):
             batched_advi(m, (X,), {"y": y}, **args)
+
+
+def test_nuts_validation_before_any_device_work():
+    """batched_nuts rejects what the reference rejects (api_batched_nuts.jl:60-63,
+    99-102) with its messages, before any device work."""
+    from uncertaintea_b200 import BernoulliLogitGLM, batched_nuts
+    m = BernoulliLogitGLM(3)
+    X, y = np.zeros((4, 3)), np.zeros(4)
+    for kw, msg in [(dict(adtype="bogus"), "adtype must be :auto, :forward, or :reverse"),
+                    (dict(adtype="reverse"), "adtype=:reverse is a host-only path"),
+                    (dict(tree_strategy="hybrid"), "requires tree_strategy=:masked or :persistent"),
+                    (dict(tree_strategy="bogus"), "tree_strategy must be"),
+                    (dict(persistent_gradient="bogus"), "persistent_gradient must be"),
+                    (dict(max_tree_depth=0), "max_tree_depth must be >= 1"),
+                    (dict(num_chains=0), "num_chains must be >= 1")]:
+        args = dict(num_chains=4, num_samples=5, device_sync_per_leaf=True)
+        args.update(kw)
+        with pytest.raises(ValueError, match=msg):
+            batched_nuts(m, (X,), {"y": y}, **args)
 
 
 def test_oracle_advi_step_consistency():

@@ -13,7 +13,7 @@ from .models import (BernoulliBeta, BernoulliLogitGLM, HierarchicalNormalNoncent
 from .device import (DeviceBatchedWorkspace, device_batched_logjoint, device_batched_logjoint_,
                      device_batched_logjoint_gradient, device_batched_logjoint_gradient_, device_lowering_report)
 from .inference import HMCChains, batched_chees, batched_hmc, batched_nuts, posterior_array
-from .diagnostics import ess, min_ess_per_second, rhat, summarize
+from .diagnostics import SamplerWarnings, check_diagnostics, ess, has_warnings, min_ess_per_second, rhat, summarize
 from .surrogate import GradientSurrogate, batched_chees_surrogate
 from .multi import MultiChains, MultiModelBatch, batched_nuts_multi
 from .vi import ADVIResult, batched_advi, variational_mean, variational_samples
@@ -28,7 +28,7 @@ __all__ = [
     "logistic_regression_data", "DeviceBatchedWorkspace", "device_batched_logjoint", "device_batched_logjoint_",
     "device_batched_logjoint_gradient", "device_batched_logjoint_gradient_", "device_lowering_report", "HMCChains",
     "batched_chees", "batched_hmc", "batched_nuts", "posterior_array", "ess", "min_ess_per_second", "rhat",
-    "summarize", "rng", "GradientSurrogate", "batched_chees_surrogate", "MultiChains", "MultiModelBatch",
+    "summarize", "check_diagnostics", "has_warnings", "SamplerWarnings", "rng", "GradientSurrogate", "batched_chees_surrogate", "MultiChains", "MultiModelBatch",
     "batched_nuts_multi", "ADVIResult", "batched_advi", "variational_mean", "variational_samples",
     "batched_meads",
 ]

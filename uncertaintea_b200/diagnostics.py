@@ -8,6 +8,8 @@ Autocovariances are computed with an FFT; they are the same biased estimates
 """
 from __future__ import annotations
 
+from dataclasses import dataclass
+
 import numpy as np
 from scipy.special import ndtri
 
@@ -120,15 +122,155 @@ def min_ess_per_second(chains, space: str = "constrained") -> float:
     return float(np.nanmin(ess(chains, space)) / max(chains.sampling_seconds, 1e-12))
 
 
-def summarize(chains, space: str = "constrained", quantiles=(0.05, 0.5, 0.95)):
+def _quantile_sorted(sorted_values: np.ndarray, probability: float) -> float:
+    """diagnostics.jl:486-497: linear interpolation at position 1 + (n - 1) p."""
+    n = sorted_values.size
+    if n == 0:
+        raise ValueError("quantile requires at least one value")
+    if n == 1:
+        return float(sorted_values[0])
+    position = (n - 1) * probability
+    lower, upper = int(np.floor(position)), int(np.ceil(position))
+    if lower == upper:
+        return float(sorted_values[lower])
+    weight = position - lower
+    return float((1 - weight) * sorted_values[lower] + weight * sorted_values[upper])
+
+
+def _indicator_split_ess(split: np.ndarray, threshold: float) -> float:
+    """Split ESS of I(x <= threshold); NaN when the indicator is constant
+    (summaries.jl:16-21)."""
+    indicator = split <= threshold
+    if indicator.all() or not indicator.any():
+        return float("nan")
+    return _split_ess_of(indicator.astype(np.float64))
+
+
+def _nan_min(a: float, b: float) -> float:
+    """Julia's min: NaN when either argument is NaN."""
+    return float("nan") if (np.isnan(a) or np.isnan(b)) else min(a, b)
+
+
+EBFMI_WARNING_THRESHOLD = 0.3  # warnings.jl:27
+
+
+@dataclass
+class SamplerWarnings:
+    """SamplerWarnings (data_types.jl:147): per-chain divergence counts, E-BFMI and
+    treedepth-saturation counts, and the parameters with low ESS / high R-hat."""
+    num_divergent: np.ndarray
+    ebfmi: np.ndarray
+    treedepth_hits: np.ndarray
+    low_ess_parameters: list
+    high_rhat_parameters: list
+    ebfmi_threshold: float = EBFMI_WARNING_THRESHOLD
+
+
+def _ebfmi(energies: np.ndarray) -> float:
+    """warnings.jl:7-18: sum of squared successive energy differences / sum of
+    squared deviations from the mean energy; NaN with fewer than 2 draws or
+    constant energy."""
+    e = np.asarray(energies, dtype=np.float64)
+    if e.size < 2:
+        return float("nan")
+    den = float(np.sum((e - e.mean()) ** 2))
+    if den == 0:
+        return float("nan")
+    return float(np.sum(np.diff(e) ** 2) / den)
+
+
+def check_diagnostics(chains, space: str = "constrained", rhat_threshold: float = 1.01, ess_threshold: float = 100.0,
+                      ebfmi_threshold: float = EBFMI_WARNING_THRESHOLD) -> SamplerWarnings:
+    """``check_diagnostics(chains; space, rhat_threshold, ess_threshold,
+    ebfmi_threshold)`` (warnings.jl:20-24, 38-77): divergences, E-BFMI and treedepth
+    saturation per chain; parameters whose R-hat exceeds the threshold (or is not
+    finite) and whose ESS is below the threshold (or not finite), checked when
+    there are at least 4 draws per chain."""
+    divergent = np.asarray(chains.divergent).astype(bool)
+    energy = np.asarray(chains.energy, dtype=np.float64)
+    num_divergent = divergent.sum(axis=1).astype(np.int64)
+    ebfmi = np.array([_ebfmi(energy[c]) for c in range(energy.shape[0])])
+    depth_limit = int(getattr(chains, "max_tree_depth", 0) or 0)
+    if depth_limit > 0:
+        treedepth_hits = (np.asarray(chains.tree_depth) == depth_limit).sum(axis=1).astype(np.int64)
+    else:
+        treedepth_hits = np.zeros(divergent.shape[0], dtype=np.int64)
+    low_ess, high_rhat = [], []
     d = _draws(chains, space)
-    names = chains.parameter_names() if hasattr(chains, "parameter_names") else [str(i) for i in range(d.shape[2])]
+    if d.shape[0] >= 1 and d.shape[1] >= 4:
+        rh, es = rhat(chains, space), ess(chains, space)
+        names = chains.parameter_names() if hasattr(chains, "parameter_names") else [str(i) for i in range(d.shape[2])]
+        for p, name in enumerate(names):
+            if not np.isfinite(rh[p]) or rh[p] > rhat_threshold:
+                high_rhat.append(name)
+            if not np.isfinite(es[p]) or es[p] < ess_threshold:
+                low_ess.append(name)
+    return SamplerWarnings(num_divergent, ebfmi, treedepth_hits, low_ess, high_rhat, float(ebfmi_threshold))
+
+
+def has_warnings(warnings: SamplerWarnings) -> bool:
+    """warnings.jl:79-86."""
+    return bool(np.any(warnings.num_divergent > 0)
+                or np.any(np.isfinite(warnings.ebfmi) & (warnings.ebfmi < warnings.ebfmi_threshold))
+                or np.any(warnings.treedepth_hits > 0) or warnings.low_ess_parameters
+                or warnings.high_rhat_parameters)
+
+
+def summarize(chains, space: str = "constrained", quantiles=(0.05, 0.5, 0.95), per_chain: bool = False):
+    """``summarize(chains; space, quantiles, per_chain)`` (diagnostics.jl:662-712,
+    summaries.jl:1-76): per parameter the pooled mean and sample SD, the requested
+    quantiles, split R-hat, bulk ESS, the MCSE of the mean (sd / sqrt(ess)), the
+    tail ESS (the smaller split ESS of the indicators at the pooled 5% / 95%
+    quantiles), the MCSE of each quantile (half the spread of the order
+    statistics at q -+ sqrt(q (1 - q) / ess_q)), and with per_chain the per-chain
+    means and SDs; plus the run's acceptance and divergence rates and the
+    per-chain step sizes."""
+    quantiles = list(quantiles)
+    if not quantiles:
+        raise ValueError("summary quantiles must be non-empty")
+    probs = [float(q) for q in quantiles]
+    if not all(0.0 <= q <= 1.0 for q in probs):
+        raise ValueError("summary quantiles must lie in [0, 1]")
+    d = _draws(chains, space)
+    C, S, P = d.shape
+    names = chains.parameter_names() if hasattr(chains, "parameter_names") else [str(i) for i in range(P)]
     rh, es = rhat(chains, space), ess(chains, space)
     rows = []
-    for p in range(d.shape[2]):
-        flat = d[:, :, p].reshape(-1).astype(np.float64)
-        rows.append({"parameter": names[p], "mean": float(flat.mean()), "sd": float(flat.std(ddof=1)),
-                     "quantiles": [float(np.quantile(flat, q)) for q in quantiles], "rhat": float(rh[p]),
-                     "ess": float(es[p])})
-    return {"parameters": rows, "acceptance_rate": float(np.mean(chains.accept_prob)),
-            "divergence_rate": float(np.mean(chains.divergent))}
+    for p in range(P):
+        x = d[:, :, p].astype(np.float64)
+        pooled = x.reshape(-1)                       # chain after chain (diagnostics.jl:474-484)
+        sorted_draws = np.sort(pooled)
+        mean = float(pooled.mean())
+        sd = float(np.sqrt(max(pooled.var(ddof=1), 0.0))) if pooled.size > 1 else 0.0
+        ess_bulk = float(es[p])
+        qvals = [_quantile_sorted(sorted_draws, q) for q in probs]
+        split = _split_chain_draws(x)
+        mcse_mean = sd * np.sqrt(1.0 / ess_bulk) if (np.isfinite(ess_bulk) and ess_bulk > 0) else float("nan")
+        q05, q95 = _quantile_sorted(sorted_draws, 0.05), _quantile_sorted(sorted_draws, 0.95)
+        ess_tail = _nan_min(_indicator_split_ess(split, q05), _indicator_split_ess(split, q95))
+        mcse_q = []
+        for q, theta in zip(probs, qvals):
+            ess_q = _indicator_split_ess(split, theta)
+            if not (np.isfinite(ess_q) and ess_q > 0):
+                mcse_q.append(float("nan"))
+                continue
+            spread = np.sqrt(q * (1 - q) / ess_q)
+            lo = _quantile_sorted(sorted_draws, min(max(q - spread, 0.0), 1.0))
+            hi = _quantile_sorted(sorted_draws, min(max(q + spread, 0.0), 1.0))
+            mcse_q.append((hi - lo) / 2)
+        row = {"index": p, "parameter": names[p], "mean": mean, "sd": sd, "quantiles": qvals,
+               "rhat": float(rh[p]), "ess": ess_bulk, "ess_bulk": ess_bulk, "mcse_mean": float(mcse_mean),
+               "ess_tail": ess_tail, "mcse_quantiles": mcse_q, "per_chain_means": None, "per_chain_sds": None}
+        if per_chain:
+            row["per_chain_means"] = x.mean(axis=1)
+            row["per_chain_sds"] = x.std(axis=1, ddof=1) if S > 1 else np.zeros(C)
+        rows.append(row)
+    accept = np.asarray(chains.accept_prob, dtype=np.float64)
+    divergent = np.asarray(chains.divergent)
+    steps = np.broadcast_to(np.asarray(chains.step_size, dtype=np.float64), (C,)).copy()
+    diagnostics = {"acceptance_rate": float(accept.mean()) if accept.size else 0.0,
+                   "divergence_rate": float(np.count_nonzero(divergent) / divergent.size) if divergent.size else 0.0,
+                   "step_sizes": steps, "mean_step_size": float(steps.mean()) if steps.size else 0.0}
+    return {"space": space, "quantiles": probs, "diagnostics": diagnostics, "parameters": rows,
+            "warnings": check_diagnostics(chains, space),
+            "acceptance_rate": diagnostics["acceptance_rate"], "divergence_rate": diagnostics["divergence_rate"]}

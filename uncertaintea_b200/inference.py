@@ -433,6 +433,7 @@ class HMCChains:
     trajectory_length: float = float("nan")
     gradient_evaluations: int = 0
     surrogate: object = None  # report of the learned gradient surrogate, when one drove the run
+    max_tree_depth: int = 0   # NUTS: the depth limit (treedepth-saturation diagnostics); 0 otherwise
 
     @property
     def num_chains(self):
@@ -614,6 +615,17 @@ class _DeviceRun:
         return np.clip(steps, lo, hi)
 
 
+def _validate_adtype(name, adtype, backend):
+    """The reference's gradient-backend keyword (api_batched_nuts.jl:60-63,
+    vi.jl:339-342): one of :auto, :forward, :reverse, and :reverse is host-only.
+    Every path here is a device path with analytic gradients (the work of the
+    reference's forward-mode duals), so :auto and :forward select it."""
+    if adtype not in ("auto", "forward", "reverse"):
+        raise ValueError(f"{name} adtype must be :auto, :forward, or :reverse, got {adtype!r}")
+    if adtype == "reverse" and backend is not None:
+        raise ValueError(f"{name} adtype=:reverse is a host-only path and cannot be combined with a device `backend`")
+
+
 def _validate_common(num_chains, num_samples, num_warmup, step_size, target_accept, divergence_threshold,
                      mass_matrix_regularization, mass_matrix_min_samples):
     if num_chains < 1:
@@ -783,7 +795,17 @@ def batched_nuts(model, args=(), constraints=None, *, num_chains, num_samples, n
                  target_accept=0.8, adapt_step_size=True, adapt_mass_matrix=True, per_chain_adaptation=None,
                  find_reasonable_step_size=False, divergence_threshold=1000.0, mass_matrix_regularization=1e-3,
                  mass_matrix_min_samples=10, callback=None, callback_every=10, tree_strategy="persistent",
-                 backend="cuda", precision=None, persistent_gradient="auto", rng=None) -> HMCChains:
+                 backend="cuda", precision=None, persistent_gradient="auto", device_sync_per_leaf=False,
+                 adtype="auto", rng=None) -> HMCChains:
+    """Batched multinomial NUTS on the device (api_batched_nuts.jl:22-51).
+
+    tree_strategy "persistent" runs a whole iteration per chain in one launch;
+    "masked" grows every chain's tree in lockstep, one leaf per batched
+    gradient evaluation.  device_sync_per_leaf is accepted for the reference's
+    masked-path debugging switch (a host synchronisation after every leaf); it
+    changes no result, and the lockstep driver here reads the live-chain count
+    every 16 leaves either way."""
+    _validate_adtype("batched_nuts", adtype, backend)
     if tree_strategy not in ("hybrid", "masked", "persistent"):
         raise ValueError(f"batched_nuts tree_strategy must be :hybrid, :masked, or :persistent, got {tree_strategy!r}")
     if tree_strategy == "hybrid":  # api_batched_nuts.jl:99-102
@@ -859,6 +881,7 @@ def batched_nuts(model, args=(), constraints=None, *, num_chains, num_samples, n
     windows = driver.mass.mass_adaptation_windows if per_chain else driver.mass_adaptation_windows
     out = _finish("nuts", run, draws, steps, driver.inverse_mass_matrix, windows, t_sample - t0, t1 - t_sample,
                   grad_evals=int(grad_evals.item()))
+    out.max_tree_depth = int(max_tree_depth)
     run.ws.close()
     return out
 

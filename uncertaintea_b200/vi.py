@@ -82,11 +82,17 @@ def _resolve_scale_vector(name, scale, parameter_total):
 
 
 def batched_advi(model, args=(), constraints=None, *, num_iterations, num_particles=32, learning_rate=0.05,
-                 initial_params=None, initial_log_scale=-1.0, guide="meanfield", elbo="standard", iwae_samples=0,
-                 beta1=0.9, beta2=0.999, adam_epsilon=1e-8, gradient_clip=math.inf, callback=None, callback_every=10,
-                 backend="cuda", precision=None, rng=None) -> ADVIResult:
+                 initial_params=None, initial_log_scale=-1.0, guide="meanfield", lowrank_rank=1, num_flow_layers=4,
+                 elbo="standard", iwae_samples=0, beta1=0.9, beta2=0.999, adam_epsilon=1e-8, gradient_clip=math.inf,
+                 callback=None, callback_every=10, backend="cuda", precision=None, adtype="auto",
+                 rng=None) -> ADVIResult:
     """Mean-field ADVI with ``num_particles`` particles per Adam step, run for
-    ``num_iterations`` steps on the device (vi.jl:314; advi_kernels.jl:45)."""
+    ``num_iterations`` steps on the device (vi.jl:314; advi_kernels.jl:45).
+    lowrank_rank and num_flow_layers belong to the reference's host-only
+    :lowrank and :flow guides; like the reference's mean-field path, this one
+    accepts and ignores them."""
+    from .inference import _validate_adtype
+    _validate_adtype("batched_advi", adtype, backend)
     if guide not in ("meanfield", "fullrank", "lowrank", "flow"):
         raise ValueError(f"batched_advi guide must be :meanfield, :fullrank, :lowrank, or :flow, got {guide}")
     if elbo not in ("standard", "iwae"):
