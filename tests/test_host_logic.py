@@ -268,6 +268,14 @@ def test_check_diagnostics_matches_the_reference_rules():
     w = dg.check_diagnostics(Short)
     assert w.high_rhat_parameters == [] and np.all(np.isnan(w.ebfmi))
     assert isinstance(dg.summarize(Fake)["warnings"], dg.SamplerWarnings)
+    # the reference's diagnostics checks (diagnostics.jl:332-340, 384-402)
+    with pytest.raises(ValueError, match="at least 4 samples"):
+        dg.rhat(Short)
+    with pytest.raises(ValueError, match="at least 4 samples"):
+        dg.summarize(Short)
+    with pytest.raises(ValueError, match="diagnostic space"):
+        dg.ess(Fake, space="bogus")
+    assert dg.rhat(Fake, space="unconstrained").shape == (2,)
 
 
 # ---- mean-field ADVI host logic (vi.jl:179-227, guides.jl:51-57) -----------

@@ -88,14 +88,31 @@ def _rank_normal(draws: np.ndarray) -> np.ndarray:
 
 
 def _draws(chains, space):
-    arr = chains.constrained if space == "constrained" else chains.unconstrained
+    """(C, S, P) draws of one space (diagnostics.jl:332-340)."""
+    if space == "constrained":
+        arr = chains.constrained
+    elif space == "unconstrained":
+        arr = chains.unconstrained
+    else:
+        raise ValueError("diagnostic space must be :constrained or :unconstrained")
     return np.asarray(arr)
+
+
+def _validated_draws(chains, space):
+    """diagnostics.jl:384-402: at least one chain and 4 draws per chain (one
+    chain still gives two split halves)."""
+    d = _draws(chains, space)
+    if d.ndim != 3 or d.shape[0] < 1:
+        raise ValueError("chain diagnostics require at least 1 chain")
+    if d.shape[1] < 4:
+        raise ValueError("chain diagnostics require at least 4 samples per chain")
+    return d
 
 
 def rhat(chains, space: str = "constrained", method: str = "split") -> np.ndarray:
     if method not in ("split", "rank"):
         raise ValueError(f"rhat method must be :split or :rank, got {method!r}")
-    d = _draws(chains, space)
+    d = _validated_draws(chains, space)
     out = np.empty(d.shape[2])
     for p in range(d.shape[2]):
         split = _split_chain_draws(d[:, :, p].astype(np.float64))
@@ -110,7 +127,7 @@ def rhat(chains, space: str = "constrained", method: str = "split") -> np.ndarra
 
 
 def ess(chains, space: str = "constrained") -> np.ndarray:
-    d = _draws(chains, space)
+    d = _validated_draws(chains, space)
     out = np.empty(d.shape[2])
     for p in range(d.shape[2]):
         out[p] = _split_ess_of(_split_chain_draws(d[:, :, p].astype(np.float64)))
@@ -231,7 +248,7 @@ def summarize(chains, space: str = "constrained", quantiles=(0.05, 0.5, 0.95), p
     probs = [float(q) for q in quantiles]
     if not all(0.0 <= q <= 1.0 for q in probs):
         raise ValueError("summary quantiles must lie in [0, 1]")
-    d = _draws(chains, space)
+    d = _validated_draws(chains, space)
     C, S, P = d.shape
     names = chains.parameter_names() if hasattr(chains, "parameter_names") else [str(i) for i in range(P)]
     rh, es = rhat(chains, space), ess(chains, space)
