@@ -197,6 +197,53 @@ def test_conjugate_gauss_chees_gate(lib):
     assert tail.max() / tail.min() < 3.0
 
 
+def test_gauss_masked_nuts_stranding_gate(lib):
+    """The reference's per-chain stranding gate (device_perchain_stranding.jl):
+    normal location/scale with 400 observations (mu 0.3, s 1.2), masked NUTS
+    from prior draws with per-chain step sizes and a pooled mass, 64 chains,
+    200 warmup + 500 draws: aggregate divergence < 1%, no chain more than 50%
+    divergent, posterior mean of s within 0.25 of 1.2, R-hat < 1.2."""
+    ys = 0.3 + 1.2 * np.random.default_rng(137).standard_normal(400)
+    res = batched_nuts(NormalLocationScale(), (400,), {"y": ys}, num_chains=64, num_samples=500, num_warmup=200,
+                       tree_strategy="masked", rng=np.random.default_rng(2024))
+    div = np.asarray(res.divergent, dtype=bool)
+    assert div.mean() < 0.01, div.mean()
+    assert div.mean(axis=1).max() < 0.5
+    d = res.constrained
+    assert np.all(np.isfinite(d))
+    assert abs(d[:, :, 1].mean() - 1.2) <= 0.25, d[:, :, 1].mean()
+    assert np.all(rhat(res) < 1.2), rhat(res)
+
+
+def test_summary_and_warnings_on_device_hmc(lib):
+    """The reference's diagnostics test (mcmc_diagnostics_ess_mcse.jl:1-80) on
+    device HMC: mu ~ normal(0, 1), y ~ normal(mu, 1) at y = 0.4, 4 chains of
+    300 + 300.  MCSE of the mean is sd / sqrt(ess); tail ESS and quantile MCSEs
+    are finite; per-chain statistics are opt-in and average to the mean; the
+    clean run has no warnings; a step of 16 without adaptation diverges and
+    raises them."""
+    from uncertaintea_b200 import check_diagnostics, has_warnings, summarize
+    m, cons = NormalKnownScale(), {"y": np.array([0.4])}
+    ch = batched_hmc(m, (1,), cons, num_chains=4, num_samples=300, num_warmup=300, rng=np.random.default_rng(2024))
+    sm = summarize(ch)
+    p = sm["parameters"][0]
+    assert abs(p["mcse_mean"] - p["sd"] * np.sqrt(1 / p["ess"])) <= 1e-12
+    assert np.isfinite(p["mcse_mean"]) and np.isfinite(p["ess_tail"]) and p["ess_tail"] > 0
+    assert len(p["mcse_quantiles"]) == len(sm["quantiles"])
+    assert all(np.isfinite(v) and v >= 0 for v in p["mcse_quantiles"])
+    assert p["per_chain_means"] is None and p["per_chain_sds"] is None
+    pc = summarize(ch, per_chain=True)["parameters"][0]
+    assert len(pc["per_chain_means"]) == 4 and len(pc["per_chain_sds"]) == 4
+    assert abs(np.mean(pc["per_chain_means"]) - pc["mean"]) <= 1e-8
+    w = check_diagnostics(ch)
+    assert len(w.num_divergent) == 4 and len(w.ebfmi) == 4 and list(w.treedepth_hits) == [0, 0, 0, 0]
+    assert w.high_rhat_parameters == [] and w.low_ess_parameters == [] and not has_warnings(w)
+    bad = batched_hmc(m, (1,), cons, num_chains=4, num_samples=200, num_warmup=0, step_size=16.0,
+                      adapt_step_size=False, adapt_mass_matrix=False, rng=np.random.default_rng(7))
+    ws = summarize(bad)["warnings"]
+    assert np.any(ws.num_divergent > 0) and has_warnings(ws)
+
+
 def test_chees_forward_velocity_adapts_trajectory(lib):
     """trajectory_velocity="forward" (the ChEES criterion's own derivative): T
     settles to a finite value with a stable tail (the reference's gate on its

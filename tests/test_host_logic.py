@@ -240,6 +240,9 @@ def test_check_diagnostics_matches_the_reference_rules():
         def parameter_names():
             return ["a", "b"]
 
+    # the reference's hand-computed E-BFMI pins (mcmc_diagnostics_ess_mcse.jl:52-56)
+    assert dg._ebfmi(np.array([1.0, 3.0, 2.0])) == pytest.approx(2.5, abs=1e-12)
+    assert np.isnan(dg._ebfmi(np.array([1.0]))) and np.isnan(dg._ebfmi(np.array([5.0, 5.0, 5.0])))
     w = dg.check_diagnostics(Fake)
     ref = [np.sum(np.diff(e) ** 2) / np.sum((e - e.mean()) ** 2) for e in Fake.energy]
     assert w.ebfmi == pytest.approx(ref, rel=1e-12)
