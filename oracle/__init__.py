@@ -55,6 +55,9 @@ def load():
                                                    c_void_p, c_void_p, c_void_p, c_int32]),
         "orc_chees_reduce": (None, [c_int32, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                     c_void_p]),
+        "orc_is_turning_f64": (c_int32, [c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+        "orc_store_tree_checkpoint_f64": (None, [c_int32, c_void_p, c_int32, c_void_p, c_void_p]),
+        "orc_dyadic_turning_f64": (c_int32, [c_int32, c_void_p, c_int32, c_void_p, c_void_p, c_int32, c_void_p]),
         "orc_mlp_num_weights": (c_int64, [c_int32]),
         "orc_mlp_forward": (None, [c_void_p, c_void_p, c_int32, c_void_p, c_int64, c_void_p, c_int32]),
         "orc_mlp_loss_gradient": (None, [c_void_p, c_void_p, c_int32, c_void_p, c_void_p, c_int64, c_void_p, c_int32,
@@ -102,6 +105,37 @@ def meads_max_eig(columns):
     columns are the ensemble members (api_batched_meads.jl:48-78)."""
     c = np.ascontiguousarray(np.asarray(columns, dtype=np.float64).T)   # N x P
     return float(load().orc_meads_max_eig(_p(c), c.shape[1] if c.ndim == 2 else 0, c.shape[0]))
+
+
+def _vec(x):
+    return np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1))
+
+
+def is_turning(q_left, q_right, p_left, p_right, inverse_mass=None):
+    """Metric-aware U-turn criterion (state_init.jl:296-350): turning when
+    (q_right - q_left) . M^-1 p is <= 0 at either end."""
+    ql, qr, pl, pr = _vec(q_left), _vec(q_right), _vec(p_left), _vec(p_right)
+    im = np.ones_like(ql) if inverse_mass is None else _vec(inverse_mass)
+    return bool(load().orc_is_turning_f64(ql.size, _p(ql), _p(qr), _p(pl), _p(pr), _p(im)))
+
+
+def new_checkpoints(P, max_depth):
+    """Checkpoint storage of one subtree: [slots][position, momentum][P]."""
+    return np.zeros((max_depth + 1, 2, P), dtype=np.float64)
+
+
+def store_tree_checkpoint(ckpt, leaf_index, q, p):
+    """Even leaf into slot popcount(leaf_index) (tree_expand.jl:64-76)."""
+    qv, pv = _vec(q), _vec(p)
+    load().orc_store_tree_checkpoint_f64(qv.size, _p(ckpt), int(leaf_index), _p(qv), _p(pv))
+
+
+def dyadic_turning(ckpt, leaf_index, q, p, direction, inverse_mass=None):
+    """Odd-leaf dyadic U-turn test against the block checkpoints (tree_expand.jl:82-102)."""
+    qv, pv = _vec(q), _vec(p)
+    im = np.ones_like(qv) if inverse_mass is None else _vec(inverse_mass)
+    return bool(load().orc_dyadic_turning_f64(qv.size, _p(ckpt), int(leaf_index), _p(qv), _p(pv), int(direction),
+                                              _p(im)))
 
 
 class OracleModel:

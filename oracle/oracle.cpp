@@ -457,6 +457,51 @@ inline float logaddexp(float x, float y) {  // persistent_nuts.jl:83-92
     return hi + std::log1p(std::exp(std::min(x, y) - hi));
 }
 
+// ---------------------------------------------------------------------------
+// U-turn criterion and dyadic checkpoints (src/inference/nuts/state_init.jl:296-350,
+// src/inference/nuts/tree_expand.jl:57-102; device form persistent_nuts.jl:109-155).
+// Velocities are metric-aware: M^-1 p with the diagonal inverse mass `im`.
+// ---------------------------------------------------------------------------
+template <class T>
+bool is_turning(int P, const T* qL, const T* qR, const T* pL, const T* pR, const T* im) {
+    T ld = T(0), rd = T(0);
+    for (int k = 0; k < P; ++k) {
+        const T delta = qR[k] - qL[k];
+        ld += delta * im[k] * pL[k];
+        rd += delta * im[k] * pR[k];
+    }
+    return ld <= T(0) || rd <= T(0);
+}
+
+// Even leaf: (position, momentum) into checkpoint slot popcount(leaf_index)
+// (0-based; the reference's count_ones(leaf_index) + 1).  ckpt holds
+// [slot][0 = position, 1 = momentum][P].
+template <class T>
+void store_tree_checkpoint(int P, T* ckpt, int leaf_index, const T* q, const T* p) {
+    const int slot = __builtin_popcount((unsigned)leaf_index);
+    for (int k = 0; k < P; ++k) {
+        ckpt[((size_t)slot * 2 + 0) * P + k] = q[k];
+        ckpt[((size_t)slot * 2 + 1) * P + k] = p[k];
+    }
+}
+
+// Odd leaf: every dyadic block ending at leaf_index (one per trailing one)
+// tested from its start checkpoint to the current endpoint, oriented by the
+// direction of the subtree.
+template <class T>
+bool dyadic_turning(int P, const T* ckpt, int leaf_index, const T* q, const T* p, bool forward, const T* im) {
+    const int nt = __builtin_ctz(~(unsigned)leaf_index);  // trailing ones
+    for (int kk = 1; kk <= nt; ++kk) {
+        const int block_start = leaf_index - (1 << kk) + 1;
+        const int slot = __builtin_popcount((unsigned)block_start);
+        const T* cq = ckpt + ((size_t)slot * 2 + 0) * P;
+        const T* cp = ckpt + ((size_t)slot * 2 + 1) * P;
+        const bool turned = forward ? is_turning(P, cq, q, cp, p, im) : is_turning(P, q, cq, p, cp, im);
+        if (turned) return true;
+    }
+    return false;
+}
+
 struct NutsOut {
     float accept, energy, error;
     int32_t depth, steps;
@@ -486,13 +531,7 @@ NutsOut nuts_chain(const ModelData& m, int P, uint32_t chain, uint32_t iter, flo
     lj3[0] = lj0; lj3[1] = lj0;
     float prop_lj = lj0;
     auto is_turning_lr = [&]() {  // :109-119
-        float ld = 0.0f, rd = 0.0f;
-        for (int k = 0; k < P; ++k) {
-            float delta = R[k] - L[k];
-            ld += delta * im[k] * L[P + k];
-            rd += delta * im[k] * R[P + k];
-        }
-        return ld <= 0.0f || rd <= 0.0f;
+        return is_turning<float>(P, L.data(), R.data(), L.data() + P, R.data() + P, im);
     };
     float cont_w = -H0, accept_sum = 0.0f;
     int accept_count = 0, depth = 1, isteps = 0;
@@ -580,34 +619,10 @@ NutsOut nuts_chain(const ModelData& m, int P, uint32_t chain, uint32_t iter, flo
             leaf_counter += 1;
             int leaf_index = sub_int - 1;
             if ((leaf_index & 1) == 0) {  // even leaf: checkpoint (:412-417)
-                int slot = __builtin_popcount((unsigned)leaf_index);
-                for (int k = 0; k < P; ++k) {
-                    ckpt[((size_t)slot * 2 + 0) * P + k] = q[k];
-                    ckpt[((size_t)slot * 2 + 1) * P + k] = p[k];
-                }
-            } else {  // odd leaf: dyadic U-turn (:126-155)
-                int nt = __builtin_ctz(~(unsigned)leaf_index);  // trailing ones
-                bool turned = false;
-                for (int kk = 1; kk <= nt && !turned; ++kk) {
-                    int block_start = leaf_index - (1 << kk) + 1;
-                    int slot = __builtin_popcount((unsigned)block_start);
-                    float ld = 0.0f, rd = 0.0f;
-                    for (int k = 0; k < P; ++k) {
-                        float cp = ckpt[((size_t)slot * 2 + 0) * P + k];
-                        float cm = ckpt[((size_t)slot * 2 + 1) * P + k];
-                        if (forward) {
-                            float delta2 = q[k] - cp;
-                            ld += delta2 * im[k] * cm;
-                            rd += delta2 * im[k] * p[k];
-                        } else {
-                            float delta2 = cp - q[k];
-                            ld += delta2 * im[k] * p[k];
-                            rd += delta2 * im[k] * cm;
-                        }
-                    }
-                    if (ld <= 0.0f || rd <= 0.0f) turned = true;
-                }
-                if (turned) { sub_turn = true; break; }
+                store_tree_checkpoint<float>(P, ckpt.data(), leaf_index, q, p.data());
+            } else if (dyadic_turning<float>(P, ckpt.data(), leaf_index, q, p.data(), forward, im)) {
+                sub_turn = true;  // odd leaf: dyadic U-turn (:126-155)
+                break;
             }
         }
         depth += 1;
@@ -1048,6 +1063,21 @@ int orc_nuts_iteration_keyed_f32(const ut_plan_desc* plan, const float* observed
                                  int32_t max_depth, float thr, uint32_t coord, float* accept_prob, float* energy,
                                  float* energy_error, int32_t* tree_depth, int32_t* integration_steps,
                                  uint8_t* divergent, uint8_t* moved, int32_t threads);
+
+// The U-turn helpers in double, for their unit pins.  ckpt: [slots][2][P].
+int orc_is_turning_f64(int32_t P, const double* qL, const double* qR, const double* pL, const double* pR,
+                       const double* im) {
+    return is_turning<double>(P, qL, qR, pL, pR, im) ? 1 : 0;
+}
+
+void orc_store_tree_checkpoint_f64(int32_t P, double* ckpt, int32_t leaf_index, const double* q, const double* p) {
+    store_tree_checkpoint<double>(P, ckpt, leaf_index, q, p);
+}
+
+int orc_dyadic_turning_f64(int32_t P, const double* ckpt, int32_t leaf_index, const double* q, const double* p,
+                           int32_t direction, const double* im) {
+    return dyadic_turning<double>(P, ckpt, leaf_index, q, p, direction > 0, im) ? 1 : 0;
+}
 
 int orc_nuts_iteration_f32(const ut_plan_desc* plan, const float* observed, const int32_t* trip_counts,
                            const int32_t* loop_starts, int32_t C, float* position, float* gradient,

@@ -180,6 +180,41 @@ def test_gauss_oracle_finite_differences_and_support():
     assert not np.isfinite(t[0])
 
 
+def test_uturn_criterion_pins():
+    """The reference's U-turn unit pins (test/uncertaintea/core/nuts_uturn_turning.jl:204-380):
+    checkpoint slots, the dyadic test in both orientations, and the metric-aware
+    velocity M^-1 p flipping the verdict of the raw-momentum criterion."""
+    ck = oracle.new_checkpoints(2, 2)
+    oracle.store_tree_checkpoint(ck, 0, [0.0, 0.0], [1.0, 0.0])
+    assert list(ck[0, 0]) == [0.0, 0.0] and list(ck[0, 1]) == [1.0, 0.0]
+    backward = oracle.dyadic_turning(ck, 1, [-1.0, 0.0], [1.0, 0.0], 1, [1.0, 1.0])
+    assert backward and backward == oracle.is_turning([0.0, 0.0], [-1.0, 0.0], [1.0, 0.0], [1.0, 0.0])
+    assert not oracle.dyadic_turning(ck, 1, [1.0, 0.0], [1.0, 0.0], 1, [1.0, 1.0])
+    ql, qr, p, imm = [0.0, 0.0], [1.0, 1.0], [1.0, -0.5], [0.1, 10.0]
+    assert not oracle.is_turning(ql, qr, p, p)            # raw dot 0.5
+    assert oracle.is_turning(ql, qr, p, p, imm)           # metric dot -4.9
+    pm = [-1.0, 0.5]
+    assert oracle.is_turning(ql, qr, pm, pm)              # raw dot -0.5
+    assert not oracle.is_turning(ql, qr, pm, pm, imm)     # metric dot 4.9
+    for case in ([1.0, -0.5], [-1.0, 0.5], [1.0, 1.0], [-0.2, -0.1]):
+        assert oracle.is_turning(ql, qr, case, case, [1.0, 1.0]) == oracle.is_turning(ql, qr, case, case)
+    ck = oracle.new_checkpoints(2, 2)
+    oracle.store_tree_checkpoint(ck, 0, ql, p)
+    assert not oracle.dyadic_turning(ck, 1, qr, p, 1, [1.0, 1.0])
+    assert oracle.dyadic_turning(ck, 1, qr, p, 1, imm)
+    # a backward subtree swaps the orientation: the checkpoint is the right end
+    assert oracle.dyadic_turning(ck, 1, qr, p, -1, [1.0, 1.0]) == oracle.is_turning(qr, ql, p, p)
+    # deeper leaves: leaf 3 tests the blocks starting at leaves 2 (slot 1) and 0 (slot 0)
+    ck = oracle.new_checkpoints(1, 3)
+    oracle.store_tree_checkpoint(ck, 0, [0.0], [1.0])
+    oracle.store_tree_checkpoint(ck, 2, [2.0], [-1.0])   # popcount(2) = 1
+    assert ck[1, 0, 0] == 2.0 and ck[1, 1, 0] == -1.0
+    assert oracle.dyadic_turning(ck, 3, [3.0], [1.0], 1)           # block [2, 3]: left velocity -1
+    oracle.store_tree_checkpoint(ck, 2, [2.0], [1.0])
+    assert not oracle.dyadic_turning(ck, 3, [3.0], [1.0], 1)
+    assert not oracle.dyadic_turning(ck, 2, [3.0], [-1.0], 1)      # even leaf: no trailing ones, no test
+
+
 def test_oracle_hmc_reversibility():
     """A trajectory followed by the same trajectory from the (flipped) end
     returns to the start: leapfrog is reversible and the final flip is applied."""
