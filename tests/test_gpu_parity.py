@@ -401,6 +401,25 @@ def _nuts_gpu(ws, qd, g, t, im, step, depth, coord):
     return res
 
 
+def test_bernoulli_beta_float32_logit_cliff(lib):
+    """The reference's device Float32 logit cliff (device_float32_saturation.jl,
+    "device_f32_logit_cliff"; p ~ beta(2, 2), y = 1): -Inf with a finite
+    gradient where float32 p rounds to 1 (logit 18, 20, 30), finite and within
+    4 eps(f32) e^theta + 1e-5 of float64 at 13, 15, 16, within 1e-5 at -1.5, 0.3, 2."""
+    m = BernoulliBeta(alpha=2.0, beta=2.0)
+    q = np.array([[18.0], [20.0], [30.0], [13.0], [15.0], [16.0], [-1.5], [0.3], [2.0]], dtype=np.float32)
+    ws = _ws(m, (1,), {"z": np.array([1.0])}, len(q))
+    t, g = ws.logjoint_gradient(q.T)
+    g = np.asarray(g.T)[:, 0]
+    t64, g64 = oracle.OracleModel(ws.lowered).logjoint_gradient_f64(q.astype(np.float64))
+    assert np.all(t[:3] == -np.inf) and not np.any(np.isnan(g[:3]))
+    tol = 4 * np.finfo(np.float32).eps * np.exp(q[3:6, 0].astype(np.float64)) + 1e-5
+    assert np.all(np.isfinite(t[3:6])) and np.all(np.abs(t[3:6] - t64[3:6]) <= tol)
+    assert np.all(np.abs(g[3:6] - g64[3:6, 0]) <= tol)
+    assert np.all(np.abs(t[6:] - t64[6:]) <= 1e-5) and np.all(np.abs(g[6:] - g64[6:, 0]) <= 1e-5)
+    ws.close()
+
+
 @pytest.mark.parametrize("n,C", [(1, 4), (500, 100), (0, 8)])
 def test_known_scale_density_vs_fp64_oracle(lib, n, C):
     """The normal known-scale family (the reference's conjugate gate model,

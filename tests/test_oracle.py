@@ -296,6 +296,28 @@ def test_bernoulli_beta_oracle_on_the_reference_parity_case():
     assert bad.logjoint_gradient_f64(u)[0][0] == -np.inf
 
 
+def test_bernoulli_beta_float32_logit_cliff():
+    """The reference's Float32 logit cliff (device_float32_saturation.jl,
+    "device_f32_logit_cliff"; p ~ beta(2, 2), y = 1): at logit p = 18, 20, 30 the
+    float32 p rounds to 1 and the logjoint is -Inf with a finite gradient; at
+    13, 15, 16 it is finite and within 4 eps(f32) e^theta + 1e-5 of float64; at
+    -1.5, 0.3, 2 within 1e-5."""
+    om = oracle.OracleModel(BernoulliBeta(alpha=2.0, beta=2.0).lower((1,), {"z": np.array([1.0])}))
+    cliff = np.array([[18.0], [20.0], [30.0]])
+    t, g = om.logjoint_gradient_f32(cliff)
+    assert np.all(t == -np.inf) and not np.any(np.isnan(g))
+    near = np.array([[13.0], [15.0], [16.0]])
+    t, g = om.logjoint_gradient_f32(near)
+    t64, g64 = om.logjoint_gradient_f64(near)
+    tol = 4 * np.finfo(np.float32).eps * np.exp(near[:, 0]) + 1e-5
+    assert np.all(np.isfinite(t)) and np.all(np.abs(t - t64) <= tol)
+    assert np.all(np.isfinite(g)) and np.all(np.abs(g[:, 0] - g64[:, 0]) <= tol)
+    mid = np.array([[-1.5], [0.3], [2.0]])
+    t, g = om.logjoint_gradient_f32(mid)
+    t64, g64 = om.logjoint_gradient_f64(mid)
+    assert np.all(np.abs(t - t64) <= 1e-5) and np.all(np.abs(g - g64) <= 1e-5)
+
+
 def test_lognormal_gamma_oracle_on_the_reference_parity_case():
     """The reference's lognormal/gamma parity case (device_lowering_parity.jl:140-148):
     y = [0.4, 1.1, -0.7], three chains of (log a, log b), against the closed form;

@@ -273,7 +273,10 @@ __device__ __forceinline__ float bern_lj_grad(const BernModel& m, const float (&
     const float p = 1.0f / (1.0f + expf(-u));
     const float lp = logf(p), l1p = log1pf(-p);
     const float au = fabsf(u);
-    float lj = ones * lp + zeros * l1p;
+    // A count of zero contributes nothing, even where its log is -inf: at the
+    // float32 logit cliff (|u| >= ~17, p rounds to 0 or 1) 0 * -inf would be
+    // NaN; the value there is the prior's -inf, as the reference scores it.
+    float lj = (ones > 0.0f ? ones * lp : 0.0f) + (zeros > 0.0f ? zeros * l1p : 0.0f);
     lj += (p > 0.0f && p < 1.0f) ? (m.a - 1.0f) * lp + (m.b - 1.0f) * l1p - m.lbeta : -INFINITY;
     lj += -au - 2.0f * log1pf(expf(-au));
     if (bad > 0.0f) lj = -INFINITY;
