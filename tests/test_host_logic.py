@@ -281,6 +281,73 @@ def test_check_diagnostics_matches_the_reference_rules():
     assert dg.rhat(Fake, space="unconstrained").shape == (2,)
 
 
+class _OracleProbeRun:
+    """The step-size searches of the device runner, driven by the oracle's
+    leapfrog probe (the same log accept ratio the device probe returns) with
+    one fixed momentum coordinate."""
+
+    def __init__(self, C=2, P=4, seed=1):
+        import oracle
+        from uncertaintea_b200.models import BernoulliLogitGLM, logistic_regression_data
+        X, y, _ = logistic_regression_data(200, P, seed)
+        self.om = oracle.OracleModel(BernoulliLogitGLM(P).lower((X,), {"y": y}))
+        self.C = C
+        self.q = np.random.default_rng(seed).standard_normal((C, P)).astype(np.float32)
+        self.lj, self.g = self.om.logjoint_gradient_f32(self.q)
+        self.probes = []
+
+    def next_probe_coord(self):
+        return 12345
+
+    def probe(self, trial_steps, inverse_mass, coord):
+        ts = np.broadcast_to(np.asarray(trial_steps, dtype=np.float32), (self.C,)).copy()
+        self.probes.append(ts)
+        return self.om.leapfrog_probe(self.q.copy(), self.g.copy(), self.lj.copy(), np.asarray(inverse_mass), ts,
+                                      coord).astype(np.float64)
+
+
+def test_shared_step_search_stops_at_the_first_crossing():
+    """The reference's shared step-search regression (warmup_driver_regression.jl:67-137):
+    searches started from s0 and 2 s0 with the same momentum land on the same
+    step, on the halving (or doubling) grid of their start, and the downward
+    and upward searches bracket each other within a factor 4."""
+    from uncertaintea_b200.inference import _DeviceRun
+    run = _OracleProbeRun()
+    search = lambda s0: _DeviceRun.find_reasonable_step_size(run, s0, np.ones(4), 1000.0)  # noqa: E731
+    down, down2 = search(10.0), search(20.0)
+    assert down == down2 and down < 10.0
+    assert float(np.log2(10.0 / down)).is_integer() and float(np.log2(20.0 / down2)).is_integer()
+    up, up2 = search(1e-4), search(2e-4)
+    assert up == up2 and up > 1e-4 and float(np.log2(up / 1e-4)).is_integer()
+    assert up / 4 <= down <= up * 4
+
+
+def test_per_chain_step_search_equals_independent_searches():
+    """The reference's vectorised per-chain search (warmup_driver_regression.jl:139-221)
+    reproduces independent per-chain searches: each chain's step is the first
+    crossing of log(0.5) along its own halving / doubling sequence."""
+    import math
+    from uncertaintea_b200.inference import _DeviceRun
+    run = _OracleProbeRun(C=6, seed=3)
+    starts = np.array([10.0, 1e-4, 0.5, 2.0, 1e-3, 40.0])
+    got = _DeviceRun.find_reasonable_step_size_per_chain(run, starts, np.ones(4))
+    for c in range(6):
+        def lar(step):
+            ts = np.full(6, step, dtype=np.float32)
+            return float(run.om.leapfrog_probe(run.q.copy(), run.g.copy(), run.lj.copy(), np.ones(4), ts, 12345)[c])
+        s = float(starts[c])
+        d = 1.0 if lar(s) > math.log(0.5) else -1.0
+        for _ in range(20):
+            nxt = s * 2.0 ** d
+            if nxt < 1e-8 or nxt > 1e3:
+                break
+            s = nxt
+            v = lar(s)
+            if (d > 0 and v <= math.log(0.5)) or (d < 0 and v >= math.log(0.5)):
+                break
+        assert got[c] == pytest.approx(s, rel=1e-12), c
+
+
 # ---- mean-field ADVI host logic (vi.jl:179-227, guides.jl:51-57) -----------
 def test_advi_entropy_clip_and_adam():
     from uncertaintea_b200 import vi
