@@ -56,6 +56,7 @@ def load():
         "orc_chees_reduce": (None, [c_int32, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                     c_void_p]),
         "orc_is_turning_f64": (c_int32, [c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+        "orc_meads_slice_drift_f64": (c_double, [c_double, c_double]),
         "orc_store_tree_checkpoint_f64": (None, [c_int32, c_void_p, c_int32, c_void_p, c_void_p]),
         "orc_dyadic_turning_f64": (c_int32, [c_int32, c_void_p, c_int32, c_void_p, c_void_p, c_int32, c_void_p]),
         "orc_mlp_num_weights": (c_int64, [c_int32]),
@@ -105,6 +106,11 @@ def meads_max_eig(columns):
     columns are the ensemble members (api_batched_meads.jl:48-78)."""
     c = np.ascontiguousarray(np.asarray(columns, dtype=np.float64).T)   # N x P
     return float(load().orc_meads_max_eig(_p(c), c.shape[1] if c.ndim == 2 else 0, c.shape[0]))
+
+
+def meads_slice_drift(u, delta):
+    """MEADS persistent-slice drift ((u + 1 + delta) mod 2) - 1 (api_batched_meads.jl:140)."""
+    return float(load().orc_meads_slice_drift_f64(float(u), float(delta)))
 
 
 def _vec(x):

@@ -502,6 +502,14 @@ bool dyadic_turning(int P, const T* ckpt, int leaf_index, const T* q, const T* p
     return false;
 }
 
+// MEADS persistent-slice drift (api_batched_meads.jl:140): ((u + 1 + delta) mod 2) - 1
+// with the floored modulo, so the result stays in [-1, 1).
+template <class T>
+T meads_slice_drift(T u, T delta) {
+    const T x = u + T(1) + delta;
+    return (x - T(2) * std::floor(x * T(0.5))) - T(1);
+}
+
 struct NutsOut {
     float accept, energy, error;
     int32_t depth, steps;
@@ -866,8 +874,7 @@ int orc_meads_iteration_f32(const ut_plan_desc* plan, const float* observed, con
             div = !std::isfinite(ee) || ee > thr;
         }
         const float ap = std::isnan(lar) ? 0.0f : std::min(1.0f, std::exp(lar));
-        const float x = slice[c] + 1.0f + delta[f];
-        const float u = (x - 2.0f * std::floor(x * 0.5f)) - 1.0f;  // (:163) floored modulo
+        const float u = meads_slice_drift<float>(slice[c], delta[f]);  // (:163) floored modulo
         const bool acc = valid && std::log(std::fabs(u)) <= lar;
         double km = 0.0;
         for (int d = 0; d < P; ++d) {
@@ -1063,6 +1070,8 @@ int orc_nuts_iteration_keyed_f32(const ut_plan_desc* plan, const float* observed
                                  int32_t max_depth, float thr, uint32_t coord, float* accept_prob, float* energy,
                                  float* energy_error, int32_t* tree_depth, int32_t* integration_steps,
                                  uint8_t* divergent, uint8_t* moved, int32_t threads);
+
+double orc_meads_slice_drift_f64(double u, double delta) { return meads_slice_drift<double>(u, delta); }
 
 // The U-turn helpers in double, for their unit pins.  ckpt: [slots][2][P].
 int orc_is_turning_f64(int32_t P, const double* qL, const double* qR, const double* pL, const double* pR,

@@ -278,6 +278,17 @@ def test_known_scale_oracle_on_the_reference_gate_model():
     assert np.max(np.abs(t - stats.norm(0.5, 2.0).logpdf(mu[:, 0]))) <= 1e-12
 
 
+def test_meads_slice_drift_pins():
+    """The reference's persistent-slice drift pins (batched_meads.jl:50-57)."""
+    assert oracle.meads_slice_drift(0.9, 0.2) == pytest.approx(-0.9, abs=1e-12)
+    assert oracle.meads_slice_drift(-0.9, 0.0) == pytest.approx(-0.9, abs=1e-12)
+    for u in (-0.99, -0.5, 0.0, 0.4, 0.999):
+        for d in (0.0, 0.1, 0.5, 0.9):
+            v = oracle.meads_slice_drift(u, d)
+            assert -1.0 <= v < 1.0
+            assert v == pytest.approx(((u + 1.0 + d) % 2.0) - 1.0, abs=1e-12)   # floored modulo
+
+
 def test_bernoulli_beta_oracle_on_the_reference_parity_case():
     """The reference's bernoulli parity case (device_lowering_parity.jl:150-158):
     z = [1, 0, 1, 1], three chains of u = logit p, against the closed form."""
