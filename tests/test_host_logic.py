@@ -395,11 +395,26 @@ def test_nuts_validation_before_any_device_work():
                     (dict(tree_strategy="bogus"), "tree_strategy must be"),
                     (dict(persistent_gradient="bogus"), "persistent_gradient must be"),
                     (dict(max_tree_depth=0), "max_tree_depth must be >= 1"),
-                    (dict(num_chains=0), "num_chains must be >= 1")]:
+                    (dict(num_chains=0), "num_chains must be >= 1"),
+                    (dict(init_strategy="bogus"), "init_strategy must be :prior or :uniform, got :bogus"),
+                    (dict(init_max_retries=-1), "init_max_retries must be >= 0, got -1")]:
         args = dict(num_chains=4, num_samples=5, device_sync_per_leaf=True)
         args.update(kw)
         with pytest.raises(ValueError, match=msg):
             batched_nuts(m, (X,), {"y": y}, **args)
+
+
+def test_init_validation_before_any_device_work():
+    """init_robustness_batched.jl:62-69: a bad init_strategy or a negative retry
+    budget is rejected up front by every sampler."""
+    from uncertaintea_b200 import BernoulliLogitGLM, batched_chees, batched_hmc
+    m = BernoulliLogitGLM(3)
+    X, y = np.zeros((4, 3)), np.zeros(4)
+    for fn, name in ((batched_hmc, "batched_hmc"), (batched_chees, "batched_chees")):
+        with pytest.raises(ValueError, match=f"{name} init_strategy must be"):
+            fn(m, (X,), {"y": y}, num_chains=2, num_samples=2, init_strategy="bogus")
+        with pytest.raises(ValueError, match=f"{name} init_max_retries must be >= 0"):
+            fn(m, (X,), {"y": y}, num_chains=2, num_samples=2, init_max_retries=-1)
 
 
 def test_oracle_advi_step_consistency():

@@ -615,6 +615,16 @@ class _DeviceRun:
         return np.clip(steps, lo, hi)
 
 
+def _validate_init(name, init_strategy, init_max_retries):
+    """api_batched_nuts.jl:68-71, api_batched_chees.jl:348-351: checked before any
+    device work."""
+    if init_strategy not in ("prior", "uniform"):
+        shown = f":{init_strategy}" if isinstance(init_strategy, str) else repr(init_strategy)
+        raise ValueError(f"{name} init_strategy must be :prior or :uniform, got {shown}")
+    if init_max_retries < 0:
+        raise ValueError(f"{name} init_max_retries must be >= 0, got {init_max_retries}")
+
+
 def _validate_adtype(name, adtype, backend):
     """The reference's gradient-backend keyword (api_batched_nuts.jl:60-63,
     vi.jl:339-342): one of :auto, :forward, :reverse, and :reverse is host-only.
@@ -714,6 +724,7 @@ def batched_hmc(model, args=(), constraints=None, *, num_chains, num_samples, nu
                 divergence_threshold=1000.0, mass_matrix_regularization=1e-3, mass_matrix_min_samples=10,
                 callback=None, callback_every=10, backend="cuda", precision=None, rng=None,
                 init_strategy="prior", init_max_retries=100) -> HMCChains:
+    _validate_init("batched_hmc", init_strategy, init_max_retries)
     _validate_common(num_chains, num_samples, num_warmup, step_size, target_accept, divergence_threshold,
                      mass_matrix_regularization, mass_matrix_min_samples)
     if num_leapfrog_steps < 1:
@@ -806,6 +817,7 @@ def batched_nuts(model, args=(), constraints=None, *, num_chains, num_samples, n
     changes no result, and the lockstep driver here reads the live-chain count
     every 16 leaves either way."""
     _validate_adtype("batched_nuts", adtype, backend)
+    _validate_init("batched_nuts", init_strategy, init_max_retries)
     if tree_strategy not in ("hybrid", "masked", "persistent"):
         raise ValueError(f"batched_nuts tree_strategy must be :hybrid, :masked, or :persistent, got {tree_strategy!r}")
     if tree_strategy == "hybrid":  # api_batched_nuts.jl:99-102
@@ -909,6 +921,7 @@ def batched_chees(model, args=(), constraints=None, *, num_chains, num_samples, 
     (the criterion's own derivative), so the ascent maximises ChEES as the
     reference documents; it is the same reduction with the numerator negated.
     """
+    _validate_init("batched_chees", init_strategy, init_max_retries)
     if trajectory_velocity not in ("reference", "forward"):
         raise ValueError(f"batched_chees trajectory_velocity must be 'reference' or 'forward', got {trajectory_velocity!r}")
     if not 0.0 <= jitter_amount <= 1.0:
