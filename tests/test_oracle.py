@@ -215,6 +215,40 @@ def test_uturn_criterion_pins():
     assert not oracle.dyadic_turning(ck, 2, [3.0], [-1.0], 1)      # even leaf: no trailing ones, no test
 
 
+def _family_cases():
+    X, y, _ = logistic_regression_data(300, 5, 2)
+    yh, sig, sizes, _ = hierarchical_data(6, 9, 3)
+    yg, _ = gauss_data(40, 5)
+    z = (np.random.default_rng(1).random(30) < 0.4).astype(np.float64)
+    return [
+        (BernoulliLogitGLM(5), (X,), {"y": y}),
+        (HierarchicalNormalNoncentered(6), (sig, sizes), {"y": yh}),
+        (NormalLocationScale(), (40,), {"y": yg}),
+        (BernoulliBeta(), (30,), {"z": z}),
+        (LognormalGammaNormal(), (40,), {"y": yg}),
+        (StudentTHeavyTail(), (40,), {"y": yg}),
+        (NormalKnownScale(), (40,), {"y": yg}),
+    ]
+
+
+@pytest.mark.parametrize("case", range(7))
+def test_initial_positions_every_family(case):
+    """init_strategy=:uniform draws every unconstrained coordinate from U[-2, 2)
+    (init_robustness_batched.jl:40-48, the Stan / NumPyro protocol); :prior
+    draws give finite logjoints and gradients for almost every chain, and
+    both have the (chains, parameters) shape of the lowered description."""
+    m, args, cons = _family_cases()[case]
+    low = m.lower(args, cons)
+    P, C = low.num_params, 64
+    u = m.initial_positions(np.random.default_rng(3), C, args, cons, "uniform")
+    assert u.shape == (C, P) and np.all((u >= -2.0) & (u < 2.0)) and np.unique(u).size > 1
+    pr = m.initial_positions(np.random.default_rng(4), C, args, cons, "prior")
+    assert pr.shape == (C, P) and np.all(np.isfinite(pr))
+    t, g = oracle.OracleModel(low).logjoint_gradient_f64(pr)
+    ok = np.isfinite(t) & np.all(np.isfinite(g), axis=1)
+    assert ok.mean() >= 0.95, ok.mean()
+
+
 def test_oracle_hmc_reversibility():
     """A trajectory followed by the same trajectory from the (flipped) end
     returns to the start: leapfrog is reversible and the final flip is applied."""
