@@ -109,6 +109,65 @@ def test_workspace_create_validates_before_touching_device(lib):
                                        ctypes.byref(h)) == nat.UT_ERR_NO_DEVICE
 
 
+_HANDLE_ENTRY_POINTS = [
+    "ut_hmc_iteration", "ut_surrogate_hmc_iteration", "ut_leapfrog_probe", "ut_persistent_nuts_iteration",
+    "ut_meads_init", "ut_meads_iteration", "ut_advi_step", "ut_lockstep_nuts_iteration", "ut_chees_reduce",
+    "ut_workspace_check", "ut_workspace_info", "ut_logjoint", "ut_logjoint_gradient", "ut_logjoint_device",
+    "ut_logjoint_gradient_device", "ut_surrogate_num_weights", "ut_surrogate_get_weights",
+    "ut_surrogate_set_weights", "ut_surrogate_get_normalization", "ut_surrogate_set_normalization",
+    "ut_surrogate_fit_normalization", "ut_surrogate_train", "ut_surrogate_loss_gradient", "ut_surrogate_gradient",
+    "ut_surrogate_check", "ut_multi_layout", "ut_multi_class_info", "ut_multi_configure", "ut_multi_set_positions",
+    "ut_multi_begin", "ut_multi_run", "ut_multi_autotune", "ut_multi_split_rhat", "ut_multi_buffers",
+]
+
+
+def _null_args(fn):
+    import ctypes as ct
+    out = []
+    for t in fn.argtypes:
+        if t in (ct.c_float, ct.c_double):
+            out.append(0.0)
+        elif t in (ct.c_int8, ct.c_uint8, ct.c_int16, ct.c_int32, ct.c_uint32, ct.c_int64, ct.c_uint64):
+            out.append(0)
+        else:
+            out.append(None)
+    return out
+
+
+def test_entry_points_reject_null_handles_and_buffers(lib):
+    """Every entry point that takes a workspace, surrogate or multi-model handle
+    returns UT_ERR_ARGUMENT (never a crash) for a null handle, the no-allocation
+    gradient for null buffers, and the destroy calls accept null; the message
+    names the problem."""
+    from uncertaintea_b200 import _native as nat
+    for name in _HANDLE_ENTRY_POINTS:
+        fn = getattr(lib, name)
+        assert fn(*_null_args(fn)) == nat.UT_ERR_ARGUMENT, name
+        assert b"null" in nat.last_error().encode() or b"handle" in nat.last_error().encode(), name
+    fn = lib.ut_glm_logjoint_gradient_noalloc
+    assert fn(*_null_args(fn)) == nat.UT_ERR_ARGUMENT
+    for name in ("ut_workspace_destroy", "ut_surrogate_destroy", "ut_multi_destroy"):
+        assert getattr(lib, name)(None) == nat.UT_OK
+
+
+@pytest.mark.skipif(HAS_GPU, reason="checks the no-device error path")
+def test_handle_free_entry_points_report_no_device(lib):
+    """Without a device the compute entry points that need no handle return
+    UT_ERR_NO_DEVICE: there is no CPU fallback behind the C ABI."""
+    import ctypes as ct
+    from uncertaintea_b200 import _native as nat
+    keys = np.zeros(2, dtype=np.uint32)
+    ctrs = np.zeros(4, dtype=np.uint32)
+    out = np.zeros(4, dtype=np.uint32)
+    assert lib.ut_philox4x32(keys.ctypes.data, ctrs.ctypes.data, 1, out.ctypes.data) == nat.UT_ERR_NO_DEVICE
+    u = np.zeros(8, dtype=np.float32)
+    assert lib.ut_rand_uniform(0, 0, 0, 0, 8, u.ctypes.data) == nat.UT_ERR_NO_DEVICE
+    assert lib.ut_rand_normal(0, 0, 0, 0, 8, u.ctypes.data) == nat.UT_ERR_NO_DEVICE
+    h = ct.c_void_p()
+    assert lib.ut_surrogate_create(4, 1, ct.byref(h)) == nat.UT_ERR_NO_DEVICE and not h.value
+    assert lib.ut_device_count() == 0
+
+
 @pytest.mark.skipif(HAS_GPU, reason="checks the no-device error path")
 def test_no_cpu_fallback_without_device():
     from uncertaintea_b200 import BernoulliLogitGLM, device_batched_logjoint, logistic_regression_data
