@@ -150,6 +150,35 @@ def test_entry_points_reject_null_handles_and_buffers(lib):
         assert getattr(lib, name)(None) == nat.UT_OK
 
 
+def _tc_split(lib, N, C, sms):
+    fn = lib.ut_internal_tc_split_plan
+    fn.restype = ctypes.c_int32
+    fn.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]
+    S, tps = ctypes.c_int32(), ctypes.c_int32()
+    assert fn(N, C, sms, ctypes.addressof(S), ctypes.addressof(tps)) == 0
+    return S.value, tps.value
+
+
+def test_tensor_core_split_minimises_the_wave_model(lib):
+    """The tensor-core grid's observation split (host planning, no GPU): the
+    100000 x 100 design with 4096 chains on 148 SMs gets S = 9 (288 CTAs in two
+    waves, 348 tiles each); for every shape the chosen split covers the tiles
+    exactly once, keeps >= 8 tiles per CTA when it can, and no other split has a
+    lower ceil(CTAs / SMs) x (11 + tiles per CTA) cost."""
+    import math
+    assert _tc_split(lib, 100000, 4096, 148) == (9, 348)
+    for N, C, sms in [(100000, 4096, 148), (20000, 128, 148), (3000, 64, 148), (5000, 300, 148), (100000, 1024, 148),
+                      (31, 128, 148), (100, 4096, 132), (777, 33, 148), (1_000_000, 8192, 148)]:
+        S, tps = _tc_split(lib, N, C, sms)
+        nt, ct = (N + 31) // 32, (C + 127) // 128
+        assert S * tps >= nt and (S - 1) * tps < nt
+        assert tps >= 8 or S == 1
+        cost = lambda s_: math.ceil(ct * s_ / sms) * (11 + (nt + s_ - 1) // s_)  # noqa: E731
+        best = min(cost((nt + ((nt + s_ - 1) // s_) - 1) // ((nt + s_ - 1) // s_)) for s_ in range(1, max(1, nt // 8) + 1))
+        assert cost(S) == best, (N, C, S)
+    assert lib.ut_internal_tc_split_plan(0, 4096, 148, None, None) != 0
+
+
 @pytest.mark.skipif(HAS_GPU, reason="checks the no-device error path")
 def test_handle_free_entry_points_report_no_device(lib):
     """Without a device the compute entry points that need no handle return

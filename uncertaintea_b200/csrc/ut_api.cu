@@ -795,6 +795,18 @@ int32_t ut_workspace_check(ut_workspace* ws, void* stream) {
     return UT_OK;
 }
 
+// Test hook (not part of the C ABI in ut_b200.h): the tensor-core grid's
+// observation split for num_obs observations, num_chains chains and sms SMs.
+extern "C" int32_t ut_internal_tc_split_plan(int32_t num_obs, int32_t num_chains, int32_t sms, int32_t* splits,
+                                             int32_t* tiles_per_split) {
+    if (num_obs < 1 || num_chains < 1 || sms < 1 || !splits || !tiles_per_split) return UT_ERR_ARGUMENT;
+    int S = 0, tps = 0;
+    tc_choose_split((num_obs + kTcObs - 1) / kTcObs, (num_chains + kTcChains - 1) / kTcChains, sms, &S, &tps);
+    *splits = S;
+    *tiles_per_split = tps;
+    return UT_OK;
+}
+
 int32_t ut_logjoint_device(ut_workspace* ws, const float* d_params, float* d_totals, void* stream) {
     int32_t rc = check_ws(ws);
     if (rc) return rc;

@@ -623,6 +623,28 @@ __global__ void tc_split_x_kernel(const float* __restrict__ Xa, float* __restric
     lo[i] = __uint_as_float(tf32_bits(x - __uint_as_float(h)));
 }
 
+// Observation split count S of the (chain tile, split) grid, one CTA per SM:
+// the S that minimises ceil(ctiles * S / sms) waves x (per-CTA set-up + tiles per
+// CTA).  A grid whose last wave is nearly empty costs a whole wave, and every
+// extra wave repeats the set-up.  S is at most num_tiles / 8 (at least 8 tiles a
+// CTA) and is rounded to the split count its tiles-per-split gives.
+inline void tc_choose_split(int num_tiles, int ctiles, int sms, int* S_out, int* tiles_per_split_out) {
+    int best = 1;
+    double best_cost = 1e300;
+    for (int s_try = 1; s_try <= std::max(1, num_tiles / 8); ++s_try) {
+        const int tps = (num_tiles + s_try - 1) / s_try;
+        const int s_eff = (num_tiles + tps - 1) / tps;
+        const double waves = std::ceil((double)ctiles * s_eff / sms);
+        const double cost = waves * (double)(kTcCtaOverheadTiles + tps);
+        if (cost < best_cost - 1e-9) {
+            best_cost = cost;
+            best = s_eff;
+        }
+    }
+    *tiles_per_split_out = (num_tiles + best - 1) / best;
+    *S_out = (num_tiles + *tiles_per_split_out - 1) / *tiles_per_split_out;
+}
+
 inline int tc_glm_setup(TcGlmPlan& t, const float* d_Xa, const float* d_y, int N, int F, int C, int off,
                         float icpt_mu, float icpt_sigma, float coef_mu, float coef_sigma, int sms,
                         std::vector<void*>* allocs) {
@@ -638,26 +660,7 @@ inline int tc_glm_setup(TcGlmPlan& t, const float* d_Xa, const float* d_y, int N
     t.icpt_mu = icpt_mu; t.icpt_sigma = icpt_sigma; t.coef_mu = coef_mu; t.coef_sigma = coef_sigma;
     t.num_tiles = (N + kTcObs - 1) / kTcObs;
     const int ctiles = (C + kTcChains - 1) / kTcChains;
-    // One CTA per SM (shared memory).  The observation split count S minimises the
-    // modelled time: ceil(ctiles * S / sms) waves x (per-CTA set-up + tiles per CTA);
-    // a grid whose last wave is nearly empty costs a whole wave, and every extra
-    // wave repeats the set-up.
-    {
-        int best = 1;
-        double best_cost = 1e300;
-        for (int s_try = 1; s_try <= std::max(1, t.num_tiles / 8); ++s_try) {
-            const int tps = (t.num_tiles + s_try - 1) / s_try;
-            const int s_eff = (t.num_tiles + tps - 1) / tps;
-            const double waves = std::ceil((double)ctiles * s_eff / sms);
-            const double cost = waves * (double)(kTcCtaOverheadTiles + tps);
-            if (cost < best_cost - 1e-9) {
-                best_cost = cost;
-                best = s_eff;
-            }
-        }
-        t.tiles_per_split = (t.num_tiles + best - 1) / best;
-        t.S = (t.num_tiles + t.tiles_per_split - 1) / t.tiles_per_split;
-    }
+    tc_choose_split(t.num_tiles, ctiles, sms, &t.S, &t.tiles_per_split);
     t.ctiles = ctiles;
     t.sms = sms;
     // partial rows for every split plan tc_split can pick: at most ctiles * S CTAs of 128 chains
