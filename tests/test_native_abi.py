@@ -179,6 +179,38 @@ def test_tensor_core_split_minimises_the_wave_model(lib):
     assert lib.ut_internal_tc_split_plan(0, 4096, 148, None, None) != 0
 
 
+def test_streaming_stage_plan_stays_in_shared_memory(lib):
+    """The streaming kernel's stage plan for every chain bucket and feature count
+    it serves, under the 227 KB a CTA can opt into (less the 1 KB the launch
+    keeps): the whole layout fits; stages are a whole multiple of the chunk slots
+    (each stage belongs to one slot, so its mbarrier phase is never ambiguous);
+    there are at least 4 stages and at most 48 (the mbarrier header's size); the
+    ring can hold the warps' partials after the stream, 16 x (chains per warp) x
+    (F + 1) floats; and too small a budget is refused, not overrun."""
+    fn = lib.ut_internal_stream_plan
+    fn.restype = ctypes.c_int32
+    fn.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    limit = 227 * 1024 - 1024
+    for CB in (1, 2, 4, 8, 16):
+        cg = 2 if CB >= 2 else 1
+        ch = CB // cg
+        for F in range(4, 129, 4):
+            st, sl, sm = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64()
+            rc = fn(CB, F, limit, ctypes.addressof(st), ctypes.addressof(sl), ctypes.addressof(sm))
+            assert rc == 0, (CB, F)
+            stages, slots = st.value, sl.value
+            assert sm.value <= limit, (CB, F, sm.value)
+            assert 4 <= stages <= 48 and stages % slots == 0 and 1 <= slots <= 16 // cg, (CB, F, stages, slots)
+            assert 16 * ch * (F + 1) <= stages * 32 * (F + 1)
+            fixed = 1024 + 4 * (CB * F + 16 * 32 * ch)
+            assert sm.value == fixed + 4 * stages * (32 * F + 32)
+    st, sl, sm = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64()
+    from uncertaintea_b200 import _native as nat
+    refs = (ctypes.addressof(st), ctypes.addressof(sl), ctypes.addressof(sm))
+    assert fn(16, 128, 40 * 1024, *refs) == nat.UT_ERR_UNSUPPORTED
+    assert fn(17, 128, limit, *refs) == nat.UT_ERR_ARGUMENT
+
+
 @pytest.mark.skipif(HAS_GPU, reason="checks the no-device error path")
 def test_handle_free_entry_points_report_no_device(lib):
     """Without a device the compute entry points that need no handle return

@@ -807,6 +807,21 @@ extern "C" int32_t ut_internal_tc_split_plan(int32_t num_obs, int32_t num_chains
     return UT_OK;
 }
 
+// Test hook (not part of the C ABI in ut_b200.h): the streaming kernel's stage
+// plan for a chain bucket CB and F features under smem_limit bytes; returns
+// UT_ERR_UNSUPPORTED when fewer than 4 stages fit.
+extern "C" int32_t ut_internal_stream_plan(int32_t CB, int32_t F, int64_t smem_limit, int32_t* stages,
+                                           int32_t* slots, int64_t* smem_bytes) {
+    if (CB < 1 || CB > kStreamMaxC || F < 1 || smem_limit < 0 || !stages || !slots || !smem_bytes)
+        return UT_ERR_ARGUMENT;
+    int st = 0, sl = 0;
+    if (!glm_stream_plan(CB, F, (size_t)smem_limit, &st, &sl)) return UT_ERR_UNSUPPORTED;
+    *stages = st;
+    *slots = sl;
+    *smem_bytes = (int64_t)glm_stream_smem(CB, F, st);
+    return UT_OK;
+}
+
 int32_t ut_logjoint_device(ut_workspace* ws, const float* d_params, float* d_totals, void* stream) {
     int32_t rc = check_ws(ws);
     if (rc) return rc;
