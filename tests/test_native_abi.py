@@ -179,6 +179,34 @@ def test_tensor_core_split_minimises_the_wave_model(lib):
     assert lib.ut_internal_tc_split_plan(0, 4096, 148, None, None) != 0
 
 
+def test_tensor_core_live_split_fits_the_launched_grid(lib):
+    """The lockstep tree's live-chain split (tc_split with a live count) for
+    every live count of several shapes: the live work (chain tiles x splits)
+    never exceeds the launched grid, so the partial rows sized for the full
+    plan hold it; the splits cover every observation tile once with no empty
+    split; few live tiles are re-split to fill the SMs; without a live count
+    the full plan comes back unchanged."""
+    fn = lib.ut_internal_tc_live_split
+    fn.restype = ctypes.c_int32
+    fn.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]
+    out = (ctypes.c_int32 * 4)()
+    for N, C, sms in [(100000, 4096, 148), (20000, 512, 148), (3000, 300, 148), (100, 4096, 132)]:
+        S_full, tps_full = _tc_split(lib, N, C, sms)
+        nt_tiles, ctiles = (N + 31) // 32, (C + 127) // 128
+        assert fn(N, C, sms, -1, out) == 0
+        assert list(out) == [ctiles, S_full, tps_full, C]
+        for live in sorted({0, 1, 2, 127, 128, 129, 255, 256, C // 2, C - 1, C} | set(range(0, C + 1, 97))):
+            assert fn(N, C, sms, live, out) == 0
+            nt, S, tps, Cl = list(out)
+            assert nt == max(1, (live + 127) // 128) and Cl == nt * 128 and nt <= ctiles
+            assert nt * S <= ctiles * S_full, (N, C, live)
+            assert S * tps >= nt_tiles and (S - 1) * tps < nt_tiles
+            assert S >= S_full
+            if nt * S_full < min(ctiles * S_full, sms):
+                assert nt * S >= min(ctiles * S_full, sms, nt * nt_tiles) // 2, (N, C, live, nt, S)
+    assert fn(100, 10, 148, 11, out) != 0
+
+
 def test_streaming_stage_plan_stays_in_shared_memory(lib):
     """The streaming kernel's stage plan for every chain bucket and feature count
     it serves, under the 227 KB a CTA can opt into (less the 1 KB the launch

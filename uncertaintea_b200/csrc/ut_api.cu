@@ -822,6 +822,26 @@ extern "C" int32_t ut_internal_stream_plan(int32_t CB, int32_t F, int64_t smem_l
     return UT_OK;
 }
 
+// Test hook (not part of the C ABI in ut_b200.h): the tensor-core work split
+// when only `live` chains are live (live < 0: no live count), as the kernels
+// compute it; out = {chain tiles, splits, tiles per split, partial-row chains}.
+extern "C" int32_t ut_internal_tc_live_split(int32_t num_obs, int32_t num_chains, int32_t sms, int32_t live,
+                                             int32_t* out) {
+    if (num_obs < 1 || num_chains < 1 || sms < 1 || !out || live > num_chains) return UT_ERR_ARGUMENT;
+    TcGlmParams p = {};
+    p.N = num_obs;
+    p.C = num_chains;
+    p.num_tiles = (num_obs + kTcObs - 1) / kTcObs;
+    p.ctiles = (num_chains + kTcChains - 1) / kTcChains;
+    p.sms = sms;
+    tc_choose_split(p.num_tiles, p.ctiles, sms, &p.S, &p.tiles_per_split);
+    int n = live;
+    p.nact = live >= 0 ? &n : nullptr;
+    const TcSplit r = tc_split(p);
+    out[0] = r.nt; out[1] = r.S; out[2] = r.tps; out[3] = r.Cl;
+    return UT_OK;
+}
+
 int32_t ut_logjoint_device(ut_workspace* ws, const float* d_params, float* d_totals, void* stream) {
     int32_t rc = check_ws(ws);
     if (rc) return rc;

@@ -72,7 +72,7 @@ struct TcSplit {
     int nt, S, tps, Cl;
 };
 
-__device__ __forceinline__ TcSplit tc_split(const TcGlmParams& p) {
+__host__ __device__ __forceinline__ TcSplit tc_split(const TcGlmParams& p) {
     TcSplit r;
     if (!p.nact) {
         r.nt = p.ctiles; r.S = p.S; r.tps = p.tiles_per_split; r.Cl = p.C;
