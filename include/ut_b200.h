@@ -219,6 +219,14 @@ typedef struct ut_hmc_buffers {
 int32_t ut_hmc_iteration(ut_workspace* ws, const ut_hmc_buffers* buf, int32_t num_leapfrog_steps,
                          uint32_t iteration_coord, float divergence_threshold, void* stream);
 
+/* One ChEES-HMC iteration: ut_hmc_iteration with this iteration's jittered
+ * step count, keeping the proposal position and the negated endpoint momentum
+ * on the device for ut_chees_reduce; both optional outputs of `buf` are
+ * required.  reference: the per-iteration device body of
+ * _run_device_batched_chees (src/device/chees_kernels.jl:375-474). */
+int32_t ut_chees_iteration(ut_workspace* ws, const ut_hmc_buffers* buf, int32_t num_leapfrog_steps,
+                           uint32_t iteration_coord, float divergence_threshold, void* stream);
+
 /* One-step leapfrog probe used by the reasonable-step-size search: from the
  * current state, with momentum drawn at `iteration_coord`, integrate one step
  * of size trial_step[c] and write log_accept_ratio[c] = H0 - H1 (-Inf when

@@ -268,7 +268,7 @@ def _state(ws, q):
     return qd, g, t
 
 
-def _hmc_gpu(ws, qd, g, t, im, step, L, coord, want=False):
+def _hmc_gpu(ws, qd, g, t, im, step, L, coord, want=False, entry="ut_hmc_iteration"):
     C, P = qd.shape
     f = lambda: torch.zeros(C, dtype=torch.float32, device="cuda")  # noqa: E731
     out = {"accept_prob": f(), "energy": f(), "energy_error": f(),
@@ -281,7 +281,7 @@ def _hmc_gpu(ws, qd, g, t, im, step, L, coord, want=False):
     buf = nat.HmcBuffers(nat.ptr(qd), nat.ptr(g), nat.ptr(t), nat.ptr(imd), nat.ptr(sd), nat.ptr(out["accept_prob"]),
                          nat.ptr(out["energy"]), nat.ptr(out["energy_error"]), nat.ptr(out["accepted"]),
                          nat.ptr(out["divergent"]), nat.ptr(prop), nat.ptr(mom))
-    nat.check(nat.load().ut_hmc_iteration(ws.handle, ctypes.byref(buf), L, coord, 1000.0, None))
+    nat.check(getattr(nat.load(), entry)(ws.handle, ctypes.byref(buf), L, coord, 1000.0, None))
     torch.cuda.synchronize()
     res = {k: v.cpu().numpy() for k, v in out.items()}
     res["position"], res["gradient"], res["logjoint"] = qd.cpu().numpy(), g.cpu().numpy(), t.cpu().numpy()
@@ -309,6 +309,23 @@ def _gauss_near_mode(n, C, seed, spread):
     q[:, 0] = y.mean() + spread * r.standard_normal(C)
     q[:, 1] = np.log(y.std()) + spread * r.standard_normal(C)
     return NormalLocationScale(), (n,), {"y": y}, q
+
+
+def test_chees_iteration_is_the_hmc_iteration_with_its_outputs(lib):
+    """ut_chees_iteration (the reference's ChEES device iteration) is
+    ut_hmc_iteration with the proposal and endpoint momentum kept: bitwise the
+    same state and outputs, and it refuses buffers without them."""
+    m, args, cons, q = _glm_case(1000, 10, 64, False, 2)
+    q *= 0.3
+    ws = _ws(m, args, cons, 64)
+    im, step = np.ones(10), np.full(64, 0.05)
+    a = _hmc_gpu(ws, *_state(ws, q), im, step, 7, 99, want=True)
+    b = _hmc_gpu(ws, *_state(ws, q), im, step, 7, 99, want=True, entry="ut_chees_iteration")
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+    with pytest.raises(Exception, match="endpoint-momentum"):
+        _hmc_gpu(ws, *_state(ws, q), im, step, 7, 99, want=False, entry="ut_chees_iteration")
+    ws.close()
 
 
 @pytest.mark.parametrize("case", ["glm_c1", "glm_tiled", "hier", "gauss"])

@@ -110,7 +110,7 @@ def test_workspace_create_validates_before_touching_device(lib):
 
 
 _HANDLE_ENTRY_POINTS = [
-    "ut_hmc_iteration", "ut_surrogate_hmc_iteration", "ut_leapfrog_probe", "ut_persistent_nuts_iteration",
+    "ut_hmc_iteration", "ut_chees_iteration", "ut_surrogate_hmc_iteration", "ut_leapfrog_probe", "ut_persistent_nuts_iteration",
     "ut_meads_init", "ut_meads_iteration", "ut_advi_step", "ut_lockstep_nuts_iteration", "ut_chees_reduce",
     "ut_workspace_check", "ut_workspace_info", "ut_logjoint", "ut_logjoint_gradient", "ut_logjoint_device",
     "ut_logjoint_gradient_device", "ut_surrogate_num_weights", "ut_surrogate_get_weights",

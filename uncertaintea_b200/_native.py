@@ -142,6 +142,7 @@ SIGNATURES = [
     ("ut_rand_uniform", c_int32, [c_uint32, c_uint32, c_uint32, c_uint32, c_int64, c_void_p]),
     ("ut_rand_normal", c_int32, [c_uint32, c_uint32, c_uint32, c_uint32, c_int64, c_void_p]),
     ("ut_hmc_iteration", c_int32, [c_void_p, POINTER(HmcBuffers), c_int32, c_uint32, c_float, c_void_p]),
+    ("ut_chees_iteration", c_int32, [c_void_p, POINTER(HmcBuffers), c_int32, c_uint32, c_float, c_void_p]),
     ("ut_leapfrog_probe", c_int32,
      [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_uint32, c_void_p, c_void_p]),
     ("ut_persistent_nuts_iteration", c_int32,

@@ -964,6 +964,15 @@ int32_t ut_hmc_iteration(ut_workspace* ws, const ut_hmc_buffers* buf, int32_t nu
     return UT_OK;
 }
 
+int32_t ut_chees_iteration(ut_workspace* ws, const ut_hmc_buffers* buf, int32_t num_leapfrog_steps,
+                           uint32_t iteration_coord, float divergence_threshold, void* stream) {
+    int32_t rc = check_ws(ws);
+    if (rc) return rc;
+    if (!buf || !buf->proposal || !buf->endpoint_momentum)
+        return fail(UT_ERR_ARGUMENT, "a ChEES iteration needs non-null proposal and endpoint-momentum buffers");
+    return ut_hmc_iteration(ws, buf, num_leapfrog_steps, iteration_coord, divergence_threshold, stream);
+}
+
 // Defined in ut_surrogate.cu (C++ linkage: not part of the exported C ABI).
 extern "C++" int ut_internal_surrogate_num_params(const ut_surrogate* s);
 extern "C++" int32_t ut_internal_surrogate_forward(const ut_surrogate* s, const float* x, int64_t n, float* out,
