@@ -46,6 +46,32 @@ def test_version_and_last_error(lib):
     lib.ut_last_error(buf, len(buf))
 
 
+def test_last_error_is_per_thread_and_truncates(lib):
+    """ut_last_error copies this thread's message, truncated and NUL-terminated
+    to the buffer, and returns its full length; another thread's failure does
+    not overwrite it (the header's contract)."""
+    import threading
+    from uncertaintea_b200 import _native as nat
+    assert lib.ut_workspace_info(None, None, None) == nat.UT_ERR_ARGUMENT
+    full = nat.last_error()
+    assert "null workspace handle" in full
+    small = ctypes.create_string_buffer(5)
+    assert lib.ut_last_error(small, 5) == len(full) and small.value == full[:4].encode()
+    assert lib.ut_last_error(None, 0) == len(full)
+    seen = {}
+
+    def other():
+        seen["before"] = nat.last_error()
+        lib.ut_chees_reduce(None, None, None, None, None, None, None, None, None)
+        seen["after"] = nat.last_error()
+
+    t = threading.Thread(target=other)
+    t.start()
+    t.join()
+    assert seen["before"] == "" and "null workspace handle" in seen["after"]
+    assert nat.last_error() == full
+
+
 def test_lowering_report_flags_bad_descriptions(lib):
     from uncertaintea_b200 import _native as nat
     bad = nat.PlanDesc(family=99)
