@@ -40,6 +40,21 @@ def test_header_compiles_as_c(tmp_path):
                     "-o", str(tmp_path / "t.o")], check=True)
 
 
+def test_plain_c_host_binds_the_library(tmp_path, lib):
+    """A C program bound through include/ut_b200.h alone (tests/c_host/c_caller.c)
+    links the shared library and holds the boundary's contract from C: lowering
+    report, validation, errors, the no-device path (and, with a device, a closed
+    form logjoint and gradient)."""
+    exe = tmp_path / "c_caller"
+    libdir = os.path.join(ROOT, "uncertaintea_b200")
+    subprocess.run(["gcc", "-std=gnu11", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "c_host", "c_caller.c"), "-L", libdir, "-lut_b200",
+                    f"-Wl,-rpath,{libdir}", "-lm", "-o", str(exe)], check=True)
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert run.returncode == 0, run.stderr
+    assert "all checks passed" in run.stdout
+
+
 def test_version_and_last_error(lib):
     assert b"sm_100a" in lib.ut_version()
     buf = ctypes.create_string_buffer(64)
