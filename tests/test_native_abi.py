@@ -55,6 +55,51 @@ def test_plain_c_host_binds_the_library(tmp_path, lib):
     assert "all checks passed" in run.stdout
 
 
+def test_julia_shim_struct_matches_the_c_struct():
+    """The Julia mirror of ut_plan_desc in INTEGRATION.md has the C struct's
+    fields in the same order with the same widths (a ccall passes it by
+    reference, so any drift would shift every later field)."""
+    import ctypes as ct
+    from uncertaintea_b200 import _native as nat
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    body = text[text.index("struct UtPlanDesc"):]
+    body = body[body.index("\n") + 1:body.index("\nend")]
+    fields = []
+    for line in body.splitlines():
+        line = line.split("#")[0]
+        fields += re.findall(r"([a-z_]+)::(Int32|Float64)", line)
+    widths = {"Int32": ct.c_int32, "Float64": ct.c_double}
+    assert [(n, widths[t]) for n, t in fields] == [(n, t) for n, t in nat.PlanDesc._fields_]
+    header = open(HEADER).read()
+    c_body = header[header.index("typedef struct ut_plan_desc"):header.index("} ut_plan_desc;")]
+    c_fields = re.findall(r"(int32_t|double)\s+([a-z_]+);", c_body)
+    assert [n for _, n in c_fields] == [n for n, _ in nat.PlanDesc._fields_]
+
+
+def _header_struct_fields(name):
+    header = open(HEADER).read()
+    body = header[header.index(f"typedef struct {name} {{"):header.index(f"}} {name};")]
+    return re.findall(r"^\s*(?:const\s+)?[a-z0-9_]+\s*\*?\s*([a-z_]+);", body, re.M)
+
+
+def test_buffer_struct_mirrors_match_the_header():
+    """The Python (ctypes) and Julia mirrors of the sampler
+    buffer structs list the header's fields in its order."""
+    from uncertaintea_b200 import _native as nat
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    for c_name, py, jl in [("ut_hmc_buffers", nat.HmcBuffers, "UtHmcBuffers"),
+                           ("ut_nuts_buffers", nat.NutsBuffers, "UtNutsBuffers"),
+                           ("ut_meads_buffers", nat.MeadsBuffers, "UtMeadsBuffers"),
+                           ("ut_multi_view", nat.MultiView, None)]:
+        fields = _header_struct_fields(c_name)
+        assert fields and fields == [n for n, _ in py._fields_], c_name
+        if jl:
+            body = text[text.index(f"struct {jl}"):]
+            body = body[body.index("\n") + 1:body.index("\nend")]
+            jl_fields = [n for line in body.splitlines() for n in re.findall(r"([a-z_]+)::", line.split("#")[0])]
+            assert jl_fields == fields, jl
+
+
 def test_version_and_last_error(lib):
     assert b"sm_100a" in lib.ut_version()
     buf = ctypes.create_string_buffer(64)
