@@ -12,8 +12,6 @@ the workspace entry point (ut_logjoint_gradient_device) on the same inputs,
 within the density tests' tolerances (logjoint 1e-5 relative, gradient 1e-5 of
 the chain's max |g|), and a batch larger than the fixed scratch is rejected.
 """
-import ctypes
-
 import numpy as np
 import pytest
 

@@ -27,7 +27,7 @@ from __future__ import annotations
 import ctypes
 import math
 import time
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 
 import numpy as np
 

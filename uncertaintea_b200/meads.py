@@ -18,8 +18,6 @@ from __future__ import annotations
 
 import time
 
-import numpy as np
-
 from . import _native as nat
 from .device import _stream_handle
 from .inference import _DeviceRun, _DrawBuffer, _finish, _invoke_callback

@@ -14,7 +14,7 @@ Calls mirror the reference: ``args`` carries the model's data arguments and
 """
 from __future__ import annotations
 
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 
 import numpy as np
 

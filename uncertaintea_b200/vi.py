@@ -13,7 +13,6 @@ workspace before any step.
 """
 from __future__ import annotations
 
-import ctypes
 import math
 from dataclasses import dataclass
 
