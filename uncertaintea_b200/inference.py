@@ -575,12 +575,10 @@ class _DeviceRun:
         direction = 0.0
         for trial in range(21):
             lar = self.probe(step, inverse_mass, coord)
-            valid = np.isfinite(lar) | (lar == -np.inf)
             ee = np.where(lar == -np.inf, np.inf, -lar)
             div = ~np.isfinite(ee) | (ee > divergence_threshold)
             ap = np.where(~np.isfinite(lar), 0.0, np.where(lar >= 0, 1.0, np.exp(np.minimum(lar, 0.0))))
             mean_ap = _mean_batched_adaptation_probability(ap, div)
-            del valid
             if trial == 0:
                 direction = 1.0 if mean_ap > target else -1.0
             elif (direction > 0 and mean_ap <= target) or (direction < 0 and mean_ap >= target):
