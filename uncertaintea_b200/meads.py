@@ -43,7 +43,7 @@ def batched_meads(model, args=(), constraints=None, *, num_chains, num_samples, 
     run = _DeviceRun(model, args, constraints, num_chains, backend, precision, rng, initial_params, init_strategy,
                      init_max_retries, "batched MEADS")
     torch = run.torch
-    C, P, K = run.C, run.P, int(num_folds)
+    C, K = run.C, int(num_folds)
     momentum = torch.empty_like(run.position)
     slice_u = torch.empty(C, dtype=torch.float32, device=run.device)
     steps = torch.zeros(C, dtype=torch.int32, device=run.device)
