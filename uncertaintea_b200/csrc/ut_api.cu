@@ -235,9 +235,9 @@ int32_t need_device() {
         }                                                                                                    \
     } while (0)
 
+// Lets `kern` take `smem` bytes of dynamic shared memory (needed above 48 KB).
 template <class Kern>
-cudaError_t launch_dyn(Kern kern, dim3 grid, dim3 block, size_t smem, cudaStream_t st) {
-    (void)st;
+cudaError_t allow_dynamic_smem(Kern kern, size_t smem) {
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
@@ -249,7 +249,7 @@ cudaError_t launch_dyn(Kern kern, dim3 grid, dim3 block, size_t smem, cudaStream
     {                                                                                                      \
         auto kern = density_warp_kernel<FAM, K, DM>;                                                        \
         size_t smem = warp_smem_bytes(ws, kWarpsDensity);                                                   \
-        UT_CUDA(launch_dyn(kern, 0, 0, smem, st));                                                          \
+        UT_CUDA(allow_dynamic_smem(kern, smem));                                                          \
         kern<<<((ws)->C + kWarpsDensity - 1) / kWarpsDensity, 32 * kWarpsDensity, smem, st>>>((ws)->dm, params, totals, grads, (ws)->C); \
     }
 
@@ -257,7 +257,7 @@ cudaError_t launch_dyn(Kern kern, dim3 grid, dim3 block, size_t smem, cudaStream
     {                                                                                                      \
         auto kern = hmc_warp_kernel<FAM, K, DM>;                                                            \
         size_t smem = warp_smem_bytes(ws, kWarpsDensity);                                                   \
-        UT_CUDA(launch_dyn(kern, 0, 0, smem, st));                                                          \
+        UT_CUDA(allow_dynamic_smem(kern, smem));                                                          \
         kern<<<((ws)->C + kWarpsDensity - 1) / kWarpsDensity, 32 * kWarpsDensity, smem, st>>>((ws)->dm, args); \
     }
 
@@ -265,7 +265,7 @@ cudaError_t launch_dyn(Kern kern, dim3 grid, dim3 block, size_t smem, cudaStream
     {                                                                                                      \
         auto kern = probe_warp_kernel<FAM, K, DM>;                                                          \
         size_t smem = warp_smem_bytes(ws, kWarpsDensity);                                                   \
-        UT_CUDA(launch_dyn(kern, 0, 0, smem, st));                                                          \
+        UT_CUDA(allow_dynamic_smem(kern, smem));                                                          \
         kern<<<((ws)->C + kWarpsDensity - 1) / kWarpsDensity, 32 * kWarpsDensity, smem, st>>>((ws)->dm, args); \
     }
 
@@ -273,7 +273,7 @@ cudaError_t launch_dyn(Kern kern, dim3 grid, dim3 block, size_t smem, cudaStream
     {                                                                                                      \
         auto kern = nuts_warp_kernel<FAM, K, DM>;                                                           \
         size_t smem = warp_smem_bytes(ws, kWarpsNuts);                                                      \
-        UT_CUDA(launch_dyn(kern, 0, 0, smem, st));                                                          \
+        UT_CUDA(allow_dynamic_smem(kern, smem));                                                          \
         kern<<<((ws)->C + kWarpsNuts - 1) / kWarpsNuts, 32 * kWarpsNuts, smem, st>>>((ws)->dm, args);     \
     }
 
@@ -301,7 +301,7 @@ int32_t launch_tiled_t(ut_workspace* ws, const float* params, float* totals, flo
 #define TILED_CASE(FPTV)                                                                  \
     case FPTV: {                                                                          \
         auto kern = glm_tiled_kernel<GRAD, FPTV>;                                         \
-        UT_CUDA(launch_dyn(kern, 0, 0, smem, st));                                        \
+        UT_CUDA(allow_dynamic_smem(kern, smem));                                        \
         kern<<<grid, 256, smem, st>>>(a);                                                 \
     } break;
     switch (ws->fpt) {
@@ -333,7 +333,7 @@ int32_t launch_stream(ut_workspace* ws, const float* params, float* totals, floa
 #define STREAM_CASE(CBV)                                                                            \
     case CBV: {                                                                                     \
         auto kern = grads ? glm_stream_kernel<CBV, true> : glm_stream_kernel<CBV, false>;          \
-        UT_CUDA(launch_dyn(kern, 0, 0, smem, st));                                                  \
+        UT_CUDA(allow_dynamic_smem(kern, smem));                                                  \
         kern<<<ws->stream_splits, kStreamThreads, smem, st>>>(a);                                   \
     } break;
     switch (ws->stream_cb) {
@@ -386,7 +386,7 @@ int32_t launch_stream_rows(ut_workspace* ws, const float* params, float* totals,
 #define STREAM_CASE(CBV)                                                                            \
     case CBV: {                                                                                     \
         auto kern = grads ? glm_stream_kernel<CBV, true> : glm_stream_kernel<CBV, false>;          \
-        UT_CUDA(launch_dyn(kern, 0, 0, smem, st));                                                  \
+        UT_CUDA(allow_dynamic_smem(kern, smem));                                                  \
         kern<<<ws->stream_splits, kStreamThreads, smem, st>>>(a);                                   \
     } break;
     switch (CB) {
@@ -1345,7 +1345,7 @@ int32_t ut_running_variance_update(const float* d_positions, const double* d_wei
     if (num_chains == 0) return UT_OK;
     int threads = ((num_params + 31) / 32) * 32;
     size_t smem = (size_t)32 * num_params * sizeof(float);
-    UT_CUDA(launch_dyn(running_variance_kernel, 0, 0, smem, nullptr));
+    UT_CUDA(allow_dynamic_smem(running_variance_kernel, smem));
     running_variance_kernel<<<1, threads, smem, (cudaStream_t)stream>>>(d_positions, d_weights, num_params, num_chains,
                                                                       d_state, window_length);
     UT_LAUNCHED();
