@@ -271,6 +271,11 @@ def test_check_diagnostics_matches_the_reference_rules():
     w = dg.check_diagnostics(Short)
     assert w.high_rhat_parameters == [] and np.all(np.isnan(w.ebfmi))
     assert isinstance(dg.summarize(Fake)["warnings"], dg.SamplerWarnings)
+    text = str(dg.summarize(Fake))
+    assert "parameter" in text and "rhat" in text and "warnings" not in text
+    assert any(line.split()[0] == "a" for line in text.splitlines()[2:4])
+    bad_text = str(dg.summarize(Bad))
+    assert "warnings:" in bad_text and "divergences: 5 total" in bad_text and "high Rhat parameters: ['b']" in bad_text
     # the reference's diagnostics checks (diagnostics.jl:332-340, 384-402)
     with pytest.raises(ValueError, match="at least 4 samples"):
         dg.rhat(Short)

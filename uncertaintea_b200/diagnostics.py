@@ -233,6 +233,42 @@ def has_warnings(warnings: SamplerWarnings) -> bool:
                 or warnings.high_rhat_parameters)
 
 
+class Summary(dict):
+    """The result of ``summarize``: a dict (space, quantiles, diagnostics,
+    parameters, warnings) whose text form is a per-parameter table followed by
+    the run diagnostics and, when there are any, the sampler warnings."""
+
+    def __str__(self):
+        qs = self["quantiles"]
+        head = ["parameter", "mean", "sd", "mcse"] + [f"q{100 * q:g}" for q in qs] + ["rhat", "ess_bulk", "ess_tail"]
+        rows = []
+        for p in self["parameters"]:
+            rows.append([str(p["parameter"])] + [f"{v:.4g}" for v in (p["mean"], p["sd"], p["mcse_mean"])]
+                        + [f"{v:.4g}" for v in p["quantiles"]]
+                        + [f"{p['rhat']:.4f}", f"{p['ess_bulk']:.1f}", f"{p['ess_tail']:.1f}"])
+        widths = [max(len(h), *(len(r[i]) for r in rows)) if rows else len(h) for i, h in enumerate(head)]
+        fmt = lambda cells: "  ".join(c.rjust(w) for c, w in zip(cells, widths))  # noqa: E731
+        d = self["diagnostics"]
+        lines = [f"summary ({self['space']} space)", fmt(head)] + [fmt(r) for r in rows]
+        lines.append(f"acceptance rate {d['acceptance_rate']:.4f}, divergence rate {d['divergence_rate']:.4f}, "
+                     f"mean step size {d['mean_step_size']:.4g}")
+        w = self.get("warnings")
+        if w is not None and has_warnings(w):
+            lines.append("warnings:")
+            if int(np.sum(w.num_divergent)) > 0:
+                lines.append(f"  divergences: {int(np.sum(w.num_divergent))} total {list(map(int, w.num_divergent))}")
+            low = np.isfinite(w.ebfmi) & (w.ebfmi < w.ebfmi_threshold)
+            if np.any(low):
+                lines.append(f"  low E-BFMI (< {w.ebfmi_threshold}): {np.round(w.ebfmi, 3).tolist()}")
+            if int(np.sum(w.treedepth_hits)) > 0:
+                lines.append(f"  treedepth saturation: {int(np.sum(w.treedepth_hits))} total")
+            if w.low_ess_parameters:
+                lines.append(f"  low ESS parameters: {w.low_ess_parameters}")
+            if w.high_rhat_parameters:
+                lines.append(f"  high Rhat parameters: {w.high_rhat_parameters}")
+        return "\n".join(lines)
+
+
 def summarize(chains, space: str = "constrained", quantiles=(0.05, 0.5, 0.95), per_chain: bool = False):
     """``summarize(chains; space, quantiles, per_chain)`` (diagnostics.jl:662-712,
     summaries.jl:1-76): per parameter the pooled mean and sample SD, the requested
@@ -288,6 +324,6 @@ def summarize(chains, space: str = "constrained", quantiles=(0.05, 0.5, 0.95), p
     diagnostics = {"acceptance_rate": float(accept.mean()) if accept.size else 0.0,
                    "divergence_rate": float(np.count_nonzero(divergent) / divergent.size) if divergent.size else 0.0,
                    "step_sizes": steps, "mean_step_size": float(steps.mean()) if steps.size else 0.0}
-    return {"space": space, "quantiles": probs, "diagnostics": diagnostics, "parameters": rows,
-            "warnings": check_diagnostics(chains, space),
-            "acceptance_rate": diagnostics["acceptance_rate"], "divergence_rate": diagnostics["divergence_rate"]}
+    return Summary(space=space, quantiles=probs, diagnostics=diagnostics, parameters=rows,
+                   warnings=check_diagnostics(chains, space), acceptance_rate=diagnostics["acceptance_rate"],
+                   divergence_rate=diagnostics["divergence_rate"])
