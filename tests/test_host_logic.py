@@ -95,6 +95,62 @@ def test_dual_averaging_matches_scalar_recursion():
     assert math.isclose(da.final()[0], math.exp(avg), rel_tol=1e-12)
 
 
+def test_mass_window_summaries_follow_the_reference(monkeypatch):
+    """The warmup driver records one summary per slow window with the reference's
+    fields (adaptation.jl:143-170) and summarize groups them (diagnostics.jl:411-448).
+    The device running-variance update is replaced by a host weighted Welford
+    update of the same state layout, so the driver runs on the CPU."""
+    P, C, W = 3, 8, 300
+
+    def host_update(self, positions, weights):
+        st = self.state.numpy()
+        x = np.asarray(positions, dtype=np.float64)
+        for c in range(x.shape[0]):
+            w = float(weights[c])
+            if w <= 0:
+                continue
+            st[2 * P + 1] += w
+            st[2 * P + 2] += w * w
+            d = x[c] - st[:P]
+            st[:P] += (w / st[2 * P + 1]) * d
+            st[P:2 * P] += w * d * (x[c] - st[:P])
+        self.count += int(np.count_nonzero(np.asarray(weights) > 0))
+
+    monkeypatch.setattr(inf.DeviceRunningVariance, "update", host_update)
+    drv = inf.WarmupDriver(None, P, W, 0.1, 0.8, adapt_step_size=False, adapt_mass_matrix=True,
+                           mass_matrix_regularization=1e-3, mass_matrix_min_samples=10, device="cpu")
+    rng = np.random.default_rng(0)
+    scale = np.array([0.5, 1.0, 3.0])
+    for it in range(1, W + 1):
+        weights = np.where(np.arange(C) == it % C, 0.5, 1.0)
+        drv.warmup_update(it, 0.8, rng.standard_normal((C, P)) * scale, weights, None)
+    sched = drv.schedule
+    wins = drv.mass_adaptation_windows
+    assert [w["window"] for w in wins] == list(range(1, len(sched.slow_window_ends) + 1))
+    for i, w in enumerate(wins, start=1):
+        start = sched.initial_buffer + 1 if i == 1 else sched.slow_window_ends[i - 2] + 1
+        length = sched.slow_window_ends[i - 1] - start + 1
+        assert (w["start"], w["end"], w["window_length"]) == (start, sched.slow_window_ends[i - 1], length)
+        assert w["samples"] == C * length
+        assert w["weight_sum"] == pytest.approx(C * length - 0.5 * length)
+        assert w["effective_count"] == pytest.approx(w["weight_sum"] ** 2 / ((C - 1) * length + 0.25 * length))
+        assert w["mean_weight"] == pytest.approx(w["weight_sum"] / w["samples"])
+        assert w["clip_scale_start"] == 8.0 and w["updated"]
+        assert w["mass_min"] <= w["mass_mean"] <= w["mass_max"]
+    last = wins[-1]
+    mass = 1.0 / drv.inverse_mass_matrix   # the mass the last window left
+    assert (last["mass_min"], last["mass_mean"], last["mass_max"]) == pytest.approx(
+        (mass.min(), mass.mean(), mass.max()))
+    assert np.argmin(drv.inverse_mass_matrix) == 0 and np.argmax(drv.inverse_mass_matrix) == 2   # variances learned
+
+    class Fake:
+        mass_adaptation_windows = wins
+    groups = dg._mass_adaptation_diagnostics(Fake.mass_adaptation_windows, 4)
+    assert [g["window_index"] for g in groups] == [w["window"] for w in wins]
+    assert all(g["chains"] == 4 and g["updated_chains"] == 4 for g in groups)
+    assert groups[0]["mean_effective_count"] == pytest.approx(wins[0]["effective_count"])
+
+
 def test_mass_adaptation_weights():
     w = inf._mass_adaptation_weights(0.5, [True, False, False, False], [0.3, 0.3, np.nan, 0.9], [False, False, False, True])
     assert w[0] == 1.0 and w[2] == 0.0 and w[3] == 0.0

@@ -269,6 +269,24 @@ class Summary(dict):
         return "\n".join(lines)
 
 
+def _mass_adaptation_diagnostics(windows, num_chains):
+    """Per slow window, the reference's summary over chains (diagnostics.jl:411-448).
+    The mass here is pooled, so every chain shares one record per window: chains
+    = num_chains, updated chains = num_chains or 0, and min = mean = max."""
+    out = []
+    for w in windows or []:
+        if "weight_sum" not in w:
+            continue
+        out.append({"window_index": w["window"], "iteration_start": w["start"], "iteration_end": w["end"],
+                    "window_length": w["window_length"], "chains": num_chains,
+                    "updated_chains": num_chains if w["updated"] else 0, "mean_pooled_samples": float(w["samples"]),
+                    "mean_weight_sum": w["weight_sum"], "mean_effective_count": w["effective_count"],
+                    "min_effective_count": w["effective_count"], "max_effective_count": w["effective_count"],
+                    "mean_weight": w["mean_weight"], "mean_clip_scale_end": w["clip_scale_end"],
+                    "mass_mean": w["mass_mean"], "mass_min": w["mass_min"], "mass_max": w["mass_max"]})
+    return sorted(out, key=lambda r: (r["window_index"], r["iteration_start"], r["iteration_end"]))
+
+
 def summarize(chains, space: str = "constrained", quantiles=(0.05, 0.5, 0.95), per_chain: bool = False):
     """``summarize(chains; space, quantiles, per_chain)`` (diagnostics.jl:662-712,
     summaries.jl:1-76): per parameter the pooled mean and sample SD, the requested
@@ -323,7 +341,9 @@ def summarize(chains, space: str = "constrained", quantiles=(0.05, 0.5, 0.95), p
     steps = np.broadcast_to(np.asarray(chains.step_size, dtype=np.float64), (C,)).copy()
     diagnostics = {"acceptance_rate": float(accept.mean()) if accept.size else 0.0,
                    "divergence_rate": float(np.count_nonzero(divergent) / divergent.size) if divergent.size else 0.0,
-                   "step_sizes": steps, "mean_step_size": float(steps.mean()) if steps.size else 0.0}
+                   "step_sizes": steps, "mean_step_size": float(steps.mean()) if steps.size else 0.0,
+                   "mass_adaptation": _mass_adaptation_diagnostics(getattr(chains, "mass_adaptation_windows", None),
+                                                                   C)}
     return Summary(space=space, quantiles=probs, diagnostics=diagnostics, parameters=rows,
                    warnings=check_diagnostics(chains, space), acceptance_rate=diagnostics["acceptance_rate"],
                    divergence_rate=diagnostics["divergence_rate"])

@@ -95,6 +95,11 @@ def _warmup_window_length(schedule: WarmupSchedule, window_index: int) -> int:
     return schedule.slow_window_ends[window_index - 1] - start + 1
 
 
+def _warmup_window_start(schedule: WarmupSchedule, window_index: int) -> int:
+    """First iteration of a slow window, 1-based window index (adaptation.jl:50-54)."""
+    return schedule.initial_buffer + 1 if window_index == 1 else schedule.slow_window_ends[window_index - 2] + 1
+
+
 def _window_progress(count: int, window_length: int) -> float:  # adaptation.jl:56-65
     if window_length <= _RUNNING_VARIANCE_CLIP_START:
         return 1.0
@@ -187,6 +192,23 @@ class DeviceRunningVariance:
         return np.maximum(shrink * variance + (1.0 - shrink), regularization)
 
 
+def _mass_adaptation_window_summary(schedule, window_index, variance, inverse_mass, updated) -> dict:
+    """One slow window's record at its end (adaptation.jl:143-170): its span, the
+    pooled samples, weight sum, effective count and mean weight of the running
+    variance, the clip scale at its start and end, whether the mass was updated,
+    and the mean / min / max of the diagonal mass (1 / inverse mass) it left."""
+    _, _, _, ws, wss = variance.host_state()
+    pooled = int(variance.count)
+    mass = 1.0 / np.asarray(inverse_mass, dtype=np.float64)
+    return {"window": window_index, "start": _warmup_window_start(schedule, window_index),
+            "end": schedule.slow_window_ends[window_index - 1], "window_length": int(variance.window_length),
+            "samples": pooled, "weight_sum": float(ws), "effective_count": 0.0 if wss <= 0 else float(ws * ws / wss),
+            "mean_weight": 0.0 if pooled == 0 else float(ws) / pooled,
+            "clip_scale_start": _RUNNING_VARIANCE_CLIP_SCALE_EARLY, "clip_scale_end": float(variance.clip_scale()),
+            "updated": bool(updated), "mass_mean": float(mass.mean()), "mass_min": float(mass.min()),
+            "mass_max": float(mass.max())}
+
+
 def _mass_adaptation_weights(progress: float, accepted, accept_prob, divergent) -> np.ndarray:
     """adaptation.jl:225-260, vectorised."""
     ap = np.asarray(accept_prob, dtype=np.float64)
@@ -250,9 +272,8 @@ class WarmupDriver:
                 if self.variance.effective_count() >= self.min_samples:
                     self.inverse_mass_matrix = self.variance.inverse_mass(self.regularization)
                     updated = True
-                self.mass_adaptation_windows.append({
-                    "window": self.mass_window_index, "end": iteration, "updated": updated,
-                    "samples": self.variance.count})
+                self.mass_adaptation_windows.append(_mass_adaptation_window_summary(
+                    s, self.mass_window_index, self.variance, self.inverse_mass_matrix, updated))
                 self.mass_window_index += 1
                 if self.mass_window_index <= len(s.slow_window_ends):
                     self.variance = DeviceRunningVariance(
