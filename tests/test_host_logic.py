@@ -151,6 +151,49 @@ def test_mass_window_summaries_follow_the_reference(monkeypatch):
     assert groups[0]["mean_effective_count"] == pytest.approx(wins[0]["effective_count"])
 
 
+def test_per_chain_step_driver_restarts_at_window_ends(monkeypatch):
+    """Shared pooled mass + per-chain dual-averaged steps (warmup.jl:362-473):
+    each chain's step follows its own dual-averaging recursion on its own
+    acceptance; at every slow-window end before the last warmup iteration the
+    step search is re-run with the new mass, and dual averaging restarts from
+    the steps it returns; finalisation gives each chain's averaged step."""
+    P, C, W = 2, 5, 150
+
+    def host_update(self, positions, weights):
+        st = self.state.numpy()
+        for c in range(len(weights)):
+            st[2 * P + 1] += float(weights[c])
+            st[2 * P + 2] += float(weights[c]) ** 2
+        st[P:2 * P] += 1.0
+        self.count += int(np.count_nonzero(np.asarray(weights) > 0))
+
+    monkeypatch.setattr(inf.DeviceRunningVariance, "update", host_update)
+    steps0 = np.array([0.05, 0.1, 0.2, 0.4, 0.8])
+    drv = inf.PooledMassPerChainStepDriver(None, P, W, steps0, 0.8, adapt_step_size=True, adapt_mass_matrix=True,
+                                           mass_matrix_regularization=1e-3, mass_matrix_min_samples=10,
+                                           device="cpu")
+    calls = []
+
+    def refind(steps, inverse_mass):
+        calls.append(np.array(inverse_mass))
+        return np.asarray(steps) * 0.5
+
+    refs = [inf.DualAveraging(np.array([s]), 0.8) for s in steps0]
+    ends = set(drv.mass.schedule.slow_window_ends)
+    rng = np.random.default_rng(1)
+    for it in range(1, W + 1):
+        acc = rng.uniform(0.3, 1.0, C)
+        got = drv.warmup_update(it, acc, np.zeros((C, P)), np.ones(C), refind)
+        want = np.array([refs[c].update(np.array([acc[c]]))[0] for c in range(C)])
+        if it in ends and it < W:
+            want = want * 0.5
+            refs = [inf.DualAveraging(np.array([s]), 0.8) for s in want]
+        assert np.allclose(got, want, rtol=1e-12), it
+    assert len(calls) == len([e for e in ends if e < W])
+    final = drv.warmup_finalize()
+    assert np.allclose(final, [r.final()[0] for r in refs], rtol=1e-12)
+
+
 def test_mass_adaptation_weights():
     w = inf._mass_adaptation_weights(0.5, [True, False, False, False], [0.3, 0.3, np.nan, 0.9], [False, False, False, True])
     assert w[0] == 1.0 and w[2] == 0.0 and w[3] == 0.0
