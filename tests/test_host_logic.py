@@ -194,6 +194,47 @@ def test_per_chain_step_driver_restarts_at_window_ends(monkeypatch):
     assert np.allclose(final, [r.final()[0] for r in refs], rtol=1e-12)
 
 
+def test_shared_step_driver_restarts_at_window_ends(monkeypatch):
+    """The shared-step warmup driver (warmup.jl:262-330): one dual-averaged step
+    on the pooled acceptance, the mass re-estimated at each slow-window end,
+    the step re-searched with that mass (before the last warmup iteration) and
+    dual averaging restarted from it; finalisation averages."""
+    P, C, W = 2, 4, 120
+
+    def host_update(self, positions, weights):
+        st = self.state.numpy()
+        for c in range(len(weights)):
+            st[2 * P + 1] += float(weights[c])
+            st[2 * P + 2] += float(weights[c]) ** 2
+        st[P:2 * P] += np.array([0.5, 2.0])
+        self.count += int(np.count_nonzero(np.asarray(weights) > 0))
+
+    monkeypatch.setattr(inf.DeviceRunningVariance, "update", host_update)
+    drv = inf.WarmupDriver(None, P, W, 0.3, 0.8, adapt_step_size=True, adapt_mass_matrix=True,
+                           mass_matrix_regularization=1e-3, mass_matrix_min_samples=10, device="cpu")
+    seen = []
+
+    def refind(step, inverse_mass):
+        seen.append(np.array(inverse_mass))
+        return step * 2.0
+
+    ref = inf.DualAveraging(0.3, 0.8)
+    ends = set(drv.schedule.slow_window_ends)
+    rng = np.random.default_rng(4)
+    for it in range(1, W + 1):
+        a = float(rng.uniform(0.4, 1.0))
+        got = drv.warmup_update(it, a, np.zeros((C, P)), np.ones(C), refind)
+        want = float(ref.update(a))
+        if it in ends and it < W:
+            want *= 2.0
+            ref = inf.DualAveraging(want, 0.8)
+            assert np.allclose(seen[-1], drv.inverse_mass_matrix)
+        assert got == pytest.approx(want, rel=1e-12), it
+    assert len(seen) == len([e for e in ends if e < W])
+    assert drv.inverse_mass_matrix[1] > drv.inverse_mass_matrix[0]   # the larger second moment
+    assert drv.warmup_finalize() == pytest.approx(float(ref.final()), rel=1e-12)
+
+
 def test_mass_adaptation_weights():
     w = inf._mass_adaptation_weights(0.5, [True, False, False, False], [0.3, 0.3, np.nan, 0.9], [False, False, False, True])
     assert w[0] == 1.0 and w[2] == 0.0 and w[3] == 0.0
