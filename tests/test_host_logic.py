@@ -235,6 +235,40 @@ def test_shared_step_driver_restarts_at_window_ends(monkeypatch):
     assert drv.warmup_finalize() == pytest.approx(float(ref.final()), rel=1e-12)
 
 
+def test_draw_buffer_and_finish_layout():
+    """Draws recorded per iteration come back as (chains, samples, ...) arrays,
+    constrained through the model's transform, with the run's step sizes and
+    mass; the diagnostics read that layout (host assembly on CPU tensors)."""
+    import torch
+    from uncertaintea_b200.models import NormalLocationScale
+
+    class Run:
+        pass
+
+    run = Run()
+    run.torch, run.device, run.C, run.P = torch, "cpu", 3, 2
+    run.model, run.args, run.constraints = NormalLocationScale(), (4,), {"y": np.zeros(4)}
+    for name, dt in (("position", torch.float32), ("logjoint", torch.float32), ("accept_prob", torch.float32),
+                     ("energy", torch.float32), ("energy_error", torch.float32), ("accepted", torch.uint8),
+                     ("divergent", torch.uint8)):
+        setattr(run, name, torch.zeros((3, 2) if name == "position" else 3, dtype=dt))
+    draws = inf._DrawBuffer(run, 6)
+    for s_ in range(6):
+        run.position.copy_(torch.tensor([[s_, 0.1 * s_], [10 + s_, 0.2], [20 + s_, -0.3]], dtype=torch.float32))
+        run.logjoint.fill_(-float(s_))
+        run.accept_prob.fill_(0.5)
+        run.divergent.copy_(torch.tensor([0, s_ == 3, 0], dtype=torch.uint8))
+        draws.record(s_, integration_steps=7)
+    out = inf._finish("hmc", run, draws, 0.25, np.ones(2), [], 1.0, 2.0)
+    assert out.unconstrained.shape == (3, 6, 2) and out.constrained.shape == (3, 6, 2)
+    assert out.unconstrained[1, 4, 0] == 14.0 and out.logjoint[2, 5] == -5.0
+    assert np.allclose(out.constrained[:, :, 1], np.exp(out.unconstrained[:, :, 1]))
+    assert out.divergent.dtype == bool and out.divergent[1, 3] and out.divergent.sum() == 1
+    assert np.all(out.integration_steps == 7) and np.all(out.step_size == 0.25)
+    assert out.num_chains == 3 and out.num_samples == 6
+    assert dg.rhat(out).shape == (2,) and dg.summarize(out)["diagnostics"]["divergence_rate"] == pytest.approx(1 / 18)
+
+
 def test_mass_adaptation_weights():
     w = inf._mass_adaptation_weights(0.5, [True, False, False, False], [0.3, 0.3, np.nan, 0.9], [False, False, False, True])
     assert w[0] == 1.0 and w[2] == 0.0 and w[3] == 0.0
