@@ -269,6 +269,42 @@ def test_draw_buffer_and_finish_layout():
     assert dg.rhat(out).shape == (2,) and dg.summarize(out)["diagnostics"]["divergence_rate"] == pytest.approx(1 / 18)
 
 
+@pytest.mark.parametrize("velocity", ["reference", "forward"])
+def test_chees_trajectory_adaptation_on_the_conjugate_model(velocity):
+    """The reference's ChEES T-trace gate (device_chees.jl:70-79) on the oracle:
+    16 chains of the conjugate gauss model (y = 0.3), trajectories and the
+    cross-chain reduction from the oracle, the trajectory length adapted by the
+    package's Adam update on log T.  T stays finite, ends in (0.5, 200) and its
+    last 150 values vary by less than a factor 3, for both trajectory-gradient
+    estimators."""
+    import math
+    import oracle
+    from uncertaintea_b200.models import NormalKnownScale
+    om = oracle.OracleModel(NormalKnownScale().lower((1,), {"y": np.array([0.3])}))
+    C, eps, im = 16, 0.8, np.full(1, 0.5, dtype=np.float32)
+    rng = np.random.default_rng(161)
+    q = rng.normal(0, 1, size=(C, 1)).astype(np.float32)
+    t, g = om.logjoint_gradient_f32(q)
+    traj = inf.ChEESTrajectoryState(10 * eps, math.log(10 * eps), inf.ChEESAdamState(0.5, 0.0, 0.95, 1e-8), 1,
+                                    0.5, 1000)
+    trace = []
+    for it in range(1, 401):
+        jit = inf._chees_jitter_value(1.0, it)
+        L = inf._chees_leapfrog_steps_from_jitter(jit, traj.trajectory_length, eps)
+        init = q.copy()
+        out = om.hmc_iteration(q, g, t, im, np.full(C, eps, np.float32), L, it, want_proposal=True)
+        num, den = oracle.chees_reduce(init, out["proposal"], out["endpoint_momentum"], out["accept_prob"],
+                                       out["divergent"], im)
+        if velocity == "forward":
+            num = -num
+        inf._chees_apply_trajectory_gradient(traj, num, den, jit, eps)
+        trace.append(traj.trajectory_length)
+    trace = np.asarray(trace)
+    assert np.all(np.isfinite(trace)) and 0.5 < trace[-1] < 200.0, trace[-1]
+    assert trace[-150:].max() / trace[-150:].min() < 3.0
+    assert abs(float(q.mean()) - 0.15) < 0.5     # the chains sit in the posterior (sd 0.71)
+
+
 def test_mass_adaptation_weights():
     w = inf._mass_adaptation_weights(0.5, [True, False, False, False], [0.3, 0.3, np.nan, 0.9], [False, False, False, True])
     assert w[0] == 1.0 and w[2] == 0.0 and w[3] == 0.0
