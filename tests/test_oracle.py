@@ -249,6 +249,65 @@ def test_initial_positions_every_family(case):
     assert ok.mean() >= 0.95, ok.mean()
 
 
+def _conjugate_oracle():
+    return oracle.OracleModel(NormalKnownScale().lower((1,), {"y": np.array([0.3])}))
+
+
+def _check_conjugate_draws(draws, tol_mean, tol_sd):
+    """draws (iterations, chains) of mu against the exact posterior normal(0.15, sqrt(0.5))."""
+    assert abs(draws.mean() - 0.15) <= tol_mean, draws.mean()
+    assert abs(draws.std() - np.sqrt(0.5)) <= tol_sd, draws.std()
+
+
+def test_oracle_nuts_samples_the_conjugate_posterior():
+    """The oracle's NUTS (the checker of the device trees) is itself a correct
+    sampler: 64 chains, fixed step 0.9, 100 + 1000 iterations on the reference's
+    conjugate gate model reproduce the posterior mean and sd within 0.03 (the
+    reference's own gate, device_persistent_nuts.jl:58-72)."""
+    om, C = _conjugate_oracle(), 64
+    q = np.random.default_rng(1).normal(0, 1, (C, 1)).astype(np.float32)
+    t, g = om.logjoint_gradient_f32(q)
+    draws = []
+    for it in range(1, 1101):
+        out = om.nuts_iteration(q, g, t, np.ones(1), np.full(C, 0.9), 10, it)
+        assert not np.any(out["divergent"])
+        if it > 100:
+            draws.append(q[:, 0].copy())
+    _check_conjugate_draws(np.asarray(draws), 0.03, 0.03)
+
+
+def test_oracle_hmc_samples_the_conjugate_posterior():
+    """The oracle's HMC iteration: 64 chains, step 0.3, 5 leapfrog steps."""
+    om, C = _conjugate_oracle(), 64
+    q = np.random.default_rng(2).normal(0, 1, (C, 1)).astype(np.float32)
+    t, g = om.logjoint_gradient_f32(q)
+    draws = []
+    for it in range(1, 1101):
+        om.hmc_iteration(q, g, t, np.ones(1), np.full(C, 0.3), 5, it)
+        if it > 100:
+            draws.append(q[:, 0].copy())
+    _check_conjugate_draws(np.asarray(draws), 0.03, 0.03)
+
+
+def test_oracle_meads_samples_the_conjugate_posterior():
+    """The oracle's MEADS iteration (the checker of the device fold updates):
+    64 chains in 4 folds, 500 + 1500 iterations, mean within 0.05 and sd within
+    0.08 (the reference's MEADS gate, batched_meads.jl:71-87)."""
+    om, C = _conjugate_oracle(), 64
+    rng = np.random.default_rng(3)
+    st = {"position": rng.normal(0, 1, (C, 1)).astype(np.float32)}
+    st["logjoint"], st["gradient"] = om.logjoint_gradient_f32(st["position"])
+    st["momentum"] = rng.standard_normal((C, 1)).astype(np.float32)
+    st["slice"] = rng.uniform(-1, 1, C).astype(np.float32)
+    draws = []
+    for it in range(1, 2001):
+        st = om.meads_iteration(st["position"], st["gradient"], st["logjoint"], st["momentum"], st["slice"], 4, it,
+                                1000 + it)
+        if it > 500:
+            draws.append(st["position"][:, 0].copy())
+    _check_conjugate_draws(np.asarray(draws), 0.05, 0.08)
+
+
 def test_oracle_hmc_reversibility():
     """A trajectory followed by the same trajectory from the (flipped) end
     returns to the start: leapfrog is reversible and the final flip is applied."""
