@@ -583,6 +583,33 @@ def test_advi_entropy_clip_and_adam():
     assert p[0] == pytest.approx(ref, abs=1e-15)
 
 
+def test_advi_on_the_conjugate_model_through_the_oracle():
+    """Mean-field ADVI is exact for the conjugate gauss model (posterior
+    normal(0.15, sqrt(0.5))): the oracle's ADVI step (Philox particles, mean
+    gradients) with the package's gradient clip, entropy and Adam ascent
+    reaches that location and scale, and the ELBO rises."""
+    import oracle
+    from uncertaintea_b200 import vi
+    from uncertaintea_b200.models import NormalKnownScale
+    om = oracle.OracleModel(NormalKnownScale().lower((1,), {"y": np.array([0.3])}))
+    loc, ls = np.array([-1.0]), np.array([-1.0])
+    m1, v1, m2, v2 = np.zeros(1), np.zeros(1), np.zeros(1), np.zeros(1)
+    locs, scales, elbo = [], [], []
+    for it in range(1, 1501):
+        r = om.advi_step(loc.astype(np.float32), np.exp(ls).astype(np.float32), 256, 7000 + it)
+        lg = np.asarray(r["location_gradient"], dtype=np.float64).copy()
+        sg = 1.0 + np.asarray(r["scale_gradient"], dtype=np.float64)
+        vi._clip_advi_gradients(lg, sg, math.inf)
+        elbo.append(float(np.mean(r["values"])) + vi._gaussian_entropy(ls))
+        vi._adam_ascent_step(loc, m1, v1, lg, it, 0.02, 0.9, 0.999, 1e-8)
+        vi._adam_ascent_step(ls, m2, v2, sg, it, 0.02, 0.9, 0.999, 1e-8)
+        locs.append(loc[0])
+        scales.append(math.exp(ls[0]))
+    assert abs(np.mean(locs[-300:]) - 0.15) < 0.03, np.mean(locs[-300:])
+    assert abs(np.mean(scales[-300:]) - math.sqrt(0.5)) < 0.05, np.mean(scales[-300:])
+    assert np.mean(elbo[-100:]) > np.mean(elbo[:100])
+
+
 def test_advi_validation_before_any_device_work():
     from uncertaintea_b200 import BernoulliLogitGLM, batched_advi
     m = BernoulliLogitGLM(3)
