@@ -183,7 +183,7 @@ def test_gauss_oracle_finite_differences_and_support():
 def test_uturn_criterion_pins():
     """The reference's U-turn unit pins (test/uncertaintea/core/nuts_uturn_turning.jl:204-380):
     checkpoint slots, the dyadic test in both orientations, and the metric-aware
-    velocity M^-1 p flipping the verdict of the raw-momentum criterion."""
+    velocity M^-1 p flipping the result of the raw-momentum criterion."""
     ck = oracle.new_checkpoints(2, 2)
     oracle.store_tree_checkpoint(ck, 0, [0.0, 0.0], [1.0, 0.0])
     assert list(ck[0, 0]) == [0.0, 0.0] and list(ck[0, 1]) == [1.0, 0.0]

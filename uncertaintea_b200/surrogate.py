@@ -8,7 +8,7 @@ trajectories while the Metropolis accept uses the exact device logjoint: the
 leapfrog map of any position-only force field is volume-preserving and
 reversible, so the chains keep the exact posterior as their target whatever
 the surrogate's error.  Exact gradients remain the fallback when the accept
-rate drops, and the judge of the surrogate's error.
+rate drops, and the measure of the surrogate's error.
 """
 from __future__ import annotations
 
