@@ -215,6 +215,30 @@ def test_uturn_criterion_pins():
     assert not oracle.dyadic_turning(ck, 2, [3.0], [-1.0], 1)      # even leaf: no trailing ones, no test
 
 
+def test_staging_layouts():
+    """The staged observation buffers, one shared column as the reference's
+    DeviceStagingBundle (staging.jl:11-39): the GLM stages, per observation, its
+    D covariates then y (stride D + 1, staging.jl:332); the hierarchical model
+    stages y group after group, then sigma_1..sigma_J, with each group's trip
+    count and first row; the loop families stage y alone."""
+    X = np.arange(12, dtype=np.float32).reshape(4, 3) / 10
+    y = np.array([1, 0, 1, 1], dtype=np.float32)
+    low = BernoulliLogitGLM(3, intercept=True).lower((X,), {"y": y})
+    assert low.observed.dtype == np.float32 and low.observed.shape == (4 * 4,)
+    np.testing.assert_array_equal(low.observed.reshape(4, 4)[:, :3], X)
+    np.testing.assert_array_equal(low.observed.reshape(4, 4)[:, 3], y)
+    assert (low.plan.num_params, low.plan.num_obs, low.plan.num_coefs, low.plan.has_intercept) == (4, 4, 3, 1)
+    yh, sig, sizes, _ = hierarchical_data(3, [2, 0, 3], 5)
+    low = HierarchicalNormalNoncentered(3).lower((sig, sizes), {"y": yh})
+    assert list(low.trip_counts) == [2, 0, 3] and list(low.loop_starts) == [0, 2, 2]
+    np.testing.assert_array_equal(low.observed[:5], yh.astype(np.float32))
+    np.testing.assert_array_equal(low.observed[5:], np.asarray(sig, dtype=np.float32))
+    assert low.num_params == 5 and low.plan.num_groups == 3
+    yg = np.array([0.4, -0.7, 1.1])
+    for m in (NormalLocationScale(), LognormalGammaNormal(), StudentTHeavyTail(), NormalKnownScale()):
+        np.testing.assert_array_equal(m.lower((3,), {"y": yg}).observed, yg.astype(np.float32))
+
+
 def _family_cases():
     X, y, _ = logistic_regression_data(300, 5, 2)
     yh, sig, sizes, _ = hierarchical_data(6, 9, 3)
