@@ -255,6 +255,20 @@ def _family_cases():
     ]
 
 
+def test_lowering_report_every_family():
+    """device_lowering_report (workspace.jl:24-35): every family's description is
+    supported; a model that cannot be lowered reports why instead of raising."""
+    from uncertaintea_b200 import device_lowering_report
+    for m, args, cons in _family_cases():
+        ok, issues = device_lowering_report(m, args, cons)
+        assert ok and issues == [], (m.name, issues)
+    X, y, _ = logistic_regression_data(20, 3, 0)
+    ok, issues = device_lowering_report(BernoulliLogitGLM(3, coef_sigma=0.0), (X,), {"y": y})
+    assert not ok and any("coefficient prior scale" in i for i in issues)
+    ok, issues = device_lowering_report(BernoulliLogitGLM(3), (X[:, :2],), {"y": y})
+    assert not ok and issues
+
+
 @pytest.mark.parametrize("case", range(7))
 def test_initial_positions_every_family(case):
     """init_strategy=:uniform draws every unconstrained coordinate from U[-2, 2)
