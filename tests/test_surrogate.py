@@ -81,6 +81,22 @@ def test_oracle_weight_gradient_matches_finite_differences(P):
         assert abs(fd - wg[k]) <= 1e-4 * max(abs(wg[k]), 1e-3), (k, fd, wg[k])
 
 
+def test_weight_layout_matches_the_oracle_mlp():
+    """The flat weight layout (W1, b1, W2, b2, W3, b3 with the parameter
+    dimension padded to 16) has the oracle MLP's size for every P, its slices
+    tile it without gaps, and the unpadded 100 -> 256 -> 256 -> 100 network has
+    117 348 weights."""
+    for P in (1, 7, 16, 100, 255, 256):
+        lay = weight_layout(P)
+        assert lay["total"] == oracle.mlp_num_weights(P), P
+        spans = sorted((lay[k][0].start, lay[k][0].stop) for k in ("W1", "b1", "W2", "b2", "W3", "b3"))
+        assert spans[0][0] == 0 and spans[-1][1] == lay["total"]
+        assert all(a[1] == b[0] for a, b in zip(spans, spans[1:]))
+        assert lay["padded_params"] % 16 == 0 and lay["padded_params"] - P < 16
+    P, H = 100, 256
+    assert P * H + H + H * H + H + H * P + P == 117348
+
+
 def test_oracle_bf16_mode_is_close_to_fp64():
     P = 12
     r = np.random.default_rng(0)
