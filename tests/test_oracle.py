@@ -352,6 +352,52 @@ def test_oracle_nuts_samples_the_normal_location_scale_posterior():
         assert abs(d[:, :, k].mean() - exact) <= 5 * mcse, (k, d[:, :, k].mean(), exact, mcse)
 
 
+def test_oracle_nuts_samples_the_hierarchical_marginal_posterior():
+    """The non-centred hierarchical model (8 groups x 3 observations, weakly
+    informative): the oracle's NUTS reproduces the posterior means of mu and tau
+    of the exact marginal posterior (theta integrated out analytically:
+    ybar_j | mu, tau ~ normal(mu, sqrt(tau^2 + sigma_j^2 / n_j)), on a 2-D grid)
+    within 5 Monte-Carlo standard errors."""
+    from uncertaintea_b200 import diagnostics as dg
+    y, sig, sizes, _ = hierarchical_data(8, 3, 11)
+    m = HierarchicalNormalNoncentered(8)
+    om = oracle.OracleModel(m.lower((sig, sizes), {"y": y}))
+    starts = np.concatenate([[0], np.cumsum(sizes)[:-1]])
+    yf = y.astype(np.float32).astype(np.float64)
+    ybar = np.array([yf[s_:s_ + n].mean() for s_, n in zip(starts, sizes)])
+    se2 = np.asarray(sig, dtype=np.float32).astype(np.float64) ** 2 / np.asarray(sizes)
+    mu = np.linspace(ybar.mean() - 15, ybar.mean() + 15, 801)[:, None]
+    lt = np.linspace(-6.0, np.log(ybar.std() + 1.0) + 3.0, 801)[None, :]
+    tau = np.exp(lt)
+    lp = -0.5 * (mu / 5.0) ** 2 - np.log1p((tau / 2.5) ** 2) + lt
+    for j in range(8):
+        v = tau ** 2 + se2[j]
+        lp = lp - 0.5 * np.log(v) - 0.5 * (ybar[j] - mu) ** 2 / v
+    w = np.exp(lp - lp.max())
+    w /= w.sum()
+    mu_ex, tau_ex = float((w * mu).sum()), float((w * tau).sum())
+    C = 64
+    q = (0.5 * np.random.default_rng(6).standard_normal((C, 10))).astype(np.float32)
+    t, g = om.logjoint_gradient_f32(q)
+    draws, div = [], []
+    for it in range(1, 1201):
+        out = om.nuts_iteration(q, g, t, np.ones(10), np.full(C, 0.1), 10, it)
+        div.append(np.asarray(out["divergent"]).mean())
+        if it > 200:
+            draws.append(np.asarray(m.constrain(q.astype(np.float64)))[:, :2].copy())
+    d = np.asarray(draws).swapaxes(0, 1)            # chains x draws x (mu, tau)
+    assert np.mean(div) < 0.02, np.mean(div)
+
+    class Chains:
+        constrained = d
+        unconstrained = d
+
+    ess = dg.ess(Chains)
+    for k, exact in ((0, mu_ex), (1, tau_ex)):
+        mcse = d[:, :, k].std() / np.sqrt(ess[k])
+        assert abs(d[:, :, k].mean() - exact) <= 5 * mcse, (k, d[:, :, k].mean(), exact, mcse, ess[k])
+
+
 def test_oracle_hmc_samples_the_conjugate_posterior():
     """The oracle's HMC iteration: 64 chains, step 0.3, 5 leapfrog steps."""
     om, C = _conjugate_oracle(), 64
