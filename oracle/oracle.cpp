@@ -6,7 +6,12 @@
 // Parity pinning: Philox4x32-10 is pinned by the Random123 known-answer
 // vectors the reference's own test holds (test/uncertaintea/core/device_rng.jl:77-93);
 // the ChEES scalar helpers by the reference's unit pins
-// (test/uncertaintea/core/batched_chees_adaptation.jl:29-72).  The reference is
+// (test/uncertaintea/core/batched_chees_adaptation.jl:29-72); the NUTS U-turn
+// helpers by its U-turn unit vectors (nuts_uturn_turning.jl:204-380); the MEADS
+// eigenvalue estimator and slice drift by its MEADS pins (batched_meads.jl:32-57).
+// The samplers (NUTS, HMC, MEADS, the ADVI step) are checked on the CPU against
+// exact posteriors (the reference's conjugate gate model, a grid posterior, an
+// analytic hierarchical marginal).  The reference is
 // Julia, which is not installed here, so its density/gradient/sampler code
 // cannot be run: those functions are restated from the cited source lines and
 // checked against closed forms and central finite differences instead, on
