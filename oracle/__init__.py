@@ -3,9 +3,11 @@
 TEST INFRASTRUCTURE: only the tests, ``__graft_entry__.smoke`` and the CPU
 baseline leg of ``bench.py`` use this package, as the test oracle.  The product
 library never calls it.  See oracle.cpp for what each function restates and
-how far parity is pinned (Philox and the ChEES scalar helpers by the
-reference's own known-answer tests; the densities and samplers by closed
-forms and finite differences, not by reference outputs).
+how far parity is pinned: Philox, the ChEES scalar helpers, the NUTS U-turn
+helpers and the MEADS estimator / slice drift by the reference's own unit
+tests; the densities by closed forms and finite differences on the
+reference's parity-case inputs; the samplers by exact posteriors.  None of it
+is pinned by reference outputs, which need Julia.
 """
 from __future__ import annotations
 
