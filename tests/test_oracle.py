@@ -398,6 +398,24 @@ def test_oracle_nuts_samples_the_hierarchical_marginal_posterior():
         assert abs(d[:, :, k].mean() - exact) <= 5 * mcse, (k, d[:, :, k].mean(), exact, mcse, ess[k])
 
 
+def test_oracle_keyed_nuts_shifts_only_the_philox_keys():
+    """The keyed NUTS iteration (chains of one model sitting at an offset of a
+    larger batch, as in the uneven batch) equals the plain one at offset 0, and
+    at offset k its chain c draws what chain c + k of the plain iteration draws."""
+    om = _conjugate_oracle()
+    C = 8
+    q0 = np.random.default_rng(9).normal(0, 1, (C + 3, 1)).astype(np.float32)
+    t0, g0 = om.logjoint_gradient_f32(q0)
+    def run(q, g, t, offset):
+        q, g, t = q.copy(), g.copy(), t.copy()
+        out = om.nuts_iteration(q, g, t, np.ones(1), np.full(q.shape[0], 0.9), 10, 42, chain_key_offset=offset)
+        return q, out
+    plain_q, plain = run(q0, g0, t0, 0)
+    keyed_q, keyed = run(q0[3:], g0[3:], t0[3:], 3)
+    np.testing.assert_array_equal(keyed_q, plain_q[3:])
+    np.testing.assert_array_equal(keyed["tree_depth"], plain["tree_depth"][3:])
+
+
 def test_oracle_hmc_samples_the_conjugate_posterior():
     """The oracle's HMC iteration: 64 chains, step 0.3, 5 leapfrog steps."""
     om, C = _conjugate_oracle(), 64
