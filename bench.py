@@ -151,23 +151,84 @@ def cpu_reference_rate(model, X, y, params, budget_s=12.0, threads=0):
     return done / el, cores, f"{done} chain-gradients of the full N=100000 x D=100 model in {el:.1f} s"
 
 
+def _emit(name, result):
+    """One sub-result of the run as its own JSON line (before the headline line)."""
+    if result is not None:
+        print(json.dumps({"sub": name, **result}), flush=True)
+
+
+def _profiled_traffic():
+    """DRAM bytes (read + write) of one tensor-core launch on this workload, from
+    the committed ncu summary (its `traffic_bytes_per_launch:` line), or None."""
+    path = os.path.join(ROOT, "profiles", "tc_glm_kernel_config3.md")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        for ln in f:
+            if ln.strip().startswith("traffic_bytes_per_launch:"):
+                return float(ln.split(":", 1)[1].strip().split()[0])
+    return None
+
+
+# Gradient tolerance of the FP64 check, elementwise:
+#   |g - g64| <= GRAD_RTOL * |g64| + GRAD_ATOL_MAG * m,
+# m = the sum of the magnitudes of the terms g adds up (oracle gradient_magnitude).
+GRAD_RTOL = 1e-5
+GRAD_ATOL_MAG = 2e-6
+
+
+def fp64_error(model, X, y, params, totals, grads):
+    """The measured error of one timed evaluation (all 4096 chains) against
+    the FP64 oracle: max relative logjoint error; max elementwise relative
+    gradient error over components whose magnitude does not cancel (|g64| at
+    least 1% of the sum of the magnitudes of its terms); and the max of the
+    elementwise error over its tolerance (<= 1 passes)."""
+    import oracle
+    om = oracle.OracleModel(model.lower((X,), {"y": y}))
+    t0 = time.perf_counter()
+    q64 = params.astype(np.float64)
+    t64, g64 = om.logjoint_gradient_f64(q64)
+    mag = om.gradient_magnitude_f64(q64)
+    err = np.abs(grads.astype(np.float64) - g64)
+    keep = np.abs(g64) >= 1e-2 * mag
+    return {"chains": int(params.shape[0]),
+            "logjoint_max_rel_err": float(np.max(np.abs(totals.astype(np.float64) - t64) / np.abs(t64))),
+            "gradient_max_rel_err": float(np.max(err[keep] / np.abs(g64[keep]))),
+            "gradient_components_checked_relative": float(keep.mean()),
+            "gradient_max_err_over_bound": float(np.max(err / (GRAD_RTOL * np.abs(g64) + GRAD_ATOL_MAG * mag))),
+            "gradient_max_norm_rel_err": float(np.max(np.max(err, 1) / np.max(np.abs(g64), 1))),
+            "tolerance": f"|g - g64| <= {GRAD_RTOL:g} |g64| + {GRAD_ATOL_MAG:g} * sum_i |term_i|",
+            "oracle_s": time.perf_counter() - t0}
+
+
 def run_reference(args):
+    """The reference arm: the CPU restatement of the reference's batched GLM
+    logjoint + gradient (chain-parallel over every host thread).  Each step is
+    one full evaluation of the same 4096-chain batch; warm-up steps are
+    untimed, every timed step is timed by itself."""
     world, rank, _ = _dist()
     if rank != 0:
         return
+    import oracle
     model, X, y, params = _data()
-    vals = []
+    om = oracle.OracleModel(model.lower((X,), {"y": y}))
+    cores = oracle.max_threads()
+    step_s = []
     for i in range(args.warmup + args.steps):
-        rate, cores, sample = cpu_reference_rate(model, X, y, params, budget_s=4.0)
+        t0 = time.perf_counter()
+        om.logjoint_gradient_f32(params)
         if i >= args.warmup:
-            vals.append(rate)
-    value = float(np.mean(vals))
+            step_s.append(time.perf_counter() - t0)
+    total_s = float(sum(step_s))
+    value = N_CHAINS * args.steps / total_s
+    sample = (f"every step: all {N_CHAINS} chain-gradients of the full N=100000 x D=100 model "
+              f"(C++ restatement of the reference's CPU batched path; Julia is not runnable here)")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * N_CHAINS / value,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total_s / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "global_batch": N_CHAINS, "parallelism": "replicas"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": sample + " per step (Julia reference not runnable here; C++ restatement)"},
+            "config": {"workload": WORKLOAD, "global_batch": N_CHAINS, "n_obs": N_OBS, "n_coefs": N_COEF,
+                       "parallelism": "replicas"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -235,42 +296,45 @@ def run_b200(args):
 
     hbm, bf16, peak_kind = _peaks()
     tc = bool(getattr(ws, "tensor_core_path", lambda: False)())
-    if tc:
-        work = 3.0 * FLOP_FP32 / 1e12          # 3xTF32: three TF32 products per FP32 product
-        peak = bf16 / 2.0                      # dense TF32 = half of dense bf16
-        bound = "tensor"
-    else:
-        work = FLOP_FP32 / 1e12
-        peak = bf16 / 2.0
-        bound = "tensor"
+    work = (3.0 if tc else 1.0) * FLOP_FP32 / 1e12   # 3xTF32: three TF32 products per FP32 product
+    peak = bf16 / 2.0                                  # dense TF32 = half of dense bf16
     avg_s = (total_ms / args.steps) / 1000.0
     achieved = work / avg_s
-    roof = {"bound": bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "traffic": None, "peak_source": f"{peak_kind} bf16/2 (dense TF32)",
-            "note": ("3xTF32 TF32-FLOPs" if tc else "FP32 CUDA-core FLOPs (no tensor-core path active)")}
-    cpu = None
+    roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "traffic": _profiled_traffic() if tc else None, "peak_source": f"{peak_kind} bf16/2 (dense TF32)",
+            "note": ("3xTF32 TF32-FLOPs; traffic = ncu DRAM read+write bytes of one launch "
+                     "(profiles/tc_glm_kernel_config3.md)" if tc
+                     else "FP32 CUDA-core FLOPs (no tensor-core path active)")}
+    cpu = fp64 = None
     if rank == 0 and world == 1 and not args.no_cpu:
         rate, cores, sample = cpu_reference_rate(model, X, y, params, budget_s=args.cpu_seconds)
         cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+        fp64 = fp64_error(model, X, y, params, totals.cpu().numpy(), grads.cpu().numpy())
     launches = int(ws.launches_per_gradient()) * args.steps if hasattr(ws, "launches_per_gradient") else 2 * args.steps
     ws.close()
-    sur = uneven = sweep = samplers = None
-    if rank == 0 and world == 1:
-        sweep = hbm_sweep()
-        if not args.no_samplers:
-            samplers = sampler_configs()
-            samplers["glm100000x100_nuts"] = glm_large_nuts()
-            samplers["glm100000x100_meads"] = glm_large_meads()
-    if rank == 0 and world == 1 and not args.no_surrogate:
-        sur = surrogate_comparison()
-        if samplers is not None:
-            # the headline comparison: surrogate-driven trajectories vs plain NUTS on the same model
-            nuts = samplers["glm100000x100_nuts"]
-            sur["plain_nuts"] = {k: nuts[k] for k in ("min_ess_per_s", "min_ess", "max_rhat", "sampling_s")}
-            sur["ratio_vs_plain_nuts"] = sur["surrogate"]["min_ess_per_s"] / nuts["min_ess_per_s"]
-    if rank == 0 and world == 1 and not args.no_uneven:
-        uneven = uneven_batch()
     if rank == 0:
+        # every sub-result is its own short line, printed when it is done; the
+        # headline line comes last
+        _emit("fp64_error", fp64)
+        if world == 1:
+            _emit("hbm_sweep", hbm_sweep())
+            samplers = None
+            if not args.no_samplers:
+                samplers = {}
+                for name, fn in (("glm1000x10_hmc", sampler_glm_hmc), ("hier64x20_nuts", sampler_hier_nuts),
+                                 ("glm100000x100_nuts", glm_large_nuts), ("glm100000x100_meads", glm_large_meads)):
+                    samplers[name] = fn()
+                    _emit("samplers." + name, samplers[name])
+            if not args.no_surrogate:
+                sur = surrogate_comparison()
+                if samplers is not None:
+                    # the metric's own comparison: surrogate-driven trajectories vs plain NUTS on the same model
+                    nuts = samplers["glm100000x100_nuts"]
+                    sur["plain_nuts"] = {k: nuts[k] for k in ("min_ess_per_s", "min_ess", "max_rank_rhat", "sampling_s")}
+                    sur["ratio_vs_plain_nuts"] = sur["surrogate"]["min_ess_per_s"] / nuts["min_ess_per_s"]
+                _emit("surrogate_chees", sur)
+            if not args.no_uneven:
+                _emit("uneven_batch", uneven_batch())
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -280,14 +344,9 @@ def run_b200(args):
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": N_CHAINS * N_COEF * 4,
                         "d2h_bytes_per_step": N_CHAINS * (N_COEF + 1) * 4},
                 "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches}
-        if sweep is not None:
-            line["hbm_sweep"] = sweep
-        if samplers is not None:
-            line["samplers"] = samplers
-        if sur is not None:
-            line["surrogate_chees"] = sur
-        if uneven is not None:
-            line["uneven_batch"] = uneven
+        if fp64 is not None:
+            line["fp64_error"] = {k: fp64[k] for k in ("logjoint_max_rel_err", "gradient_max_rel_err",
+                                                       "gradient_max_err_over_bound")}
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
@@ -383,33 +442,46 @@ def hbm_sweep(chain_counts=(1, 4, 8, 16), steps=20, warmup=5):
             "rows": out, "yardsticks": yard}
 
 
-def sampler_configs():
-    """The two sampler workloads of the small models, timed end to end: batched
-    HMC on the 1000 x 10 logistic regression (256 chains, 8 leapfrog steps, step
-    0.05 without step adaptation, 1000 warmup + 1000 draws, seed 1) and batched
-    persistent NUTS on the non-centred hierarchical model with J = 64 groups x 20
-    observations (sigma_j ~ U(0.5, 2), y from the prior at seed 7; 4096 chains, max
-    tree depth 10, 1000 warmup + 1000 draws).  Min bulk ESS over
-    parameters per second of sampling, max split R-hat, gradient evaluations/s."""
-    from uncertaintea_b200 import (BernoulliLogitGLM, HierarchicalNormalNoncentered, batched_hmc, batched_nuts, ess,
-                                   hierarchical_data, logistic_regression_data, rhat)
-    out = {}
-    X, y, _ = logistic_regression_data(1000, 10, seed=1)
-    c1 = batched_hmc(BernoulliLogitGLM(10), (X,), {"y": y}, num_chains=256, num_samples=1000, num_warmup=1000,
-                     step_size=0.05, num_leapfrog_steps=8, adapt_step_size=False, rng=1)
-    yh, sig, sizes, _ = hierarchical_data(64, 20, 7)
-    c2 = batched_nuts(HierarchicalNormalNoncentered(64), (sig, sizes), {"y": yh}, num_chains=4096, num_samples=1000,
-                      num_warmup=1000, max_tree_depth=10, rng=7)
-    for name, ch, cfg in (("glm1000x10_hmc", c1, "256 chains, L=8, step 0.05, 1000+1000, GLM 1000x10"),
-                          ("hier64x20_nuts", c2, "4096 chains, depth 10, 1000+1000, hierarchical J=64 x 20")):
-        e, r = ess(ch, space="unconstrained"), rhat(ch, space="unconstrained")
-        total_s = ch.warmup_seconds + ch.sampling_seconds
-        out[name] = {"min_ess_per_s": float(np.min(e) / ch.sampling_seconds), "min_ess": float(np.min(e)),
-                     "max_rhat": float(np.max(r)), "warmup_s": ch.warmup_seconds, "sampling_s": ch.sampling_seconds,
-                     "grad_evals_per_s": ch.gradient_evaluations / total_s, "mean_accept": float(ch.accept_prob.mean()),
-                     "config": cfg}
-    out["hier64x20_nuts"]["mean_tree_depth"] = float(c2.tree_depth.mean())
+def _chain_summary(ch, cfg, extra=None):
+    """Min bulk ESS/s and both R-hats of a sampler run.  The gate is the
+    reference's: rank-normalised split R-hat < 1.01 (diagnostics.jl:607-612,
+    docs/benchmarks.md:8-13); the plain split R-hat is reported beside it."""
+    from uncertaintea_b200 import ess, rhat
+    e = ess(ch, space="unconstrained")
+    r_rank = rhat(ch, space="unconstrained", method="rank")
+    r_split = rhat(ch, space="unconstrained")
+    total_s = ch.warmup_seconds + ch.sampling_seconds
+    out = {"min_ess_per_s": float(np.min(e) / ch.sampling_seconds), "min_ess": float(np.min(e)),
+           "max_rank_rhat": float(np.max(r_rank)), "max_split_rhat": float(np.max(r_split)),
+           "gate_rank_rhat_lt_1.01": bool(np.max(r_rank) < 1.01),
+           "warmup_s": ch.warmup_seconds, "sampling_s": ch.sampling_seconds,
+           "grad_evals_per_s": ch.gradient_evaluations / total_s, "mean_accept": float(ch.accept_prob.mean()),
+           "config": cfg}
+    out.update(extra or {})
     return out
+
+
+def sampler_glm_hmc(num_samples=1000):
+    """Batched HMC on the 1000 x 10 logistic regression: 256 chains, 8 leapfrog
+    steps, step 0.05 without step adaptation, 1000 warmup + num_samples draws,
+    seed 1."""
+    from uncertaintea_b200 import BernoulliLogitGLM, batched_hmc, logistic_regression_data
+    X, y, _ = logistic_regression_data(1000, 10, seed=1)
+    ch = batched_hmc(BernoulliLogitGLM(10), (X,), {"y": y}, num_chains=256, num_samples=num_samples,
+                     num_warmup=1000, step_size=0.05, num_leapfrog_steps=8, adapt_step_size=False, rng=1)
+    return _chain_summary(ch, f"256 chains, L=8, step 0.05, 1000+{num_samples}, GLM 1000x10")
+
+
+def sampler_hier_nuts(num_samples=1000):
+    """Batched persistent NUTS on the non-centred hierarchical model with J = 64
+    groups x 20 observations (sigma_j ~ U(0.5, 2), y from the prior at seed 7;
+    4096 chains, max tree depth 10, 1000 warmup + num_samples draws)."""
+    from uncertaintea_b200 import HierarchicalNormalNoncentered, batched_nuts, hierarchical_data
+    yh, sig, sizes, _ = hierarchical_data(64, 20, 7)
+    ch = batched_nuts(HierarchicalNormalNoncentered(64), (sig, sizes), {"y": yh}, num_chains=4096,
+                      num_samples=num_samples, num_warmup=1000, max_tree_depth=10, rng=7)
+    return _chain_summary(ch, f"4096 chains, depth 10, 1000+{num_samples}, hierarchical J=64 x 20",
+                          {"mean_tree_depth": float(ch.tree_depth.mean())})
 
 
 def glm_large_nuts(num_chains=4096, num_warmup=200, num_samples=200):
@@ -418,19 +490,14 @@ def glm_large_nuts(num_chains=4096, num_warmup=200, num_samples=200):
     whose trees are still growing (compacted).  Fewer iterations than the small-model runs
     (200 + 200) keep the bench within minutes; the draws are still nearly
     independent (min ESS at the draw count)."""
-    from uncertaintea_b200 import batched_nuts, ess, rhat
+    from uncertaintea_b200 import batched_nuts
     model, X, y, _ = _data()
     ch = batched_nuts(model, (X,), {"y": y}, num_chains=num_chains, num_samples=num_samples, num_warmup=num_warmup,
                       max_tree_depth=10, tree_strategy="masked", rng=1)
-    e, r = ess(ch, space="unconstrained"), rhat(ch, space="unconstrained")
-    total_s = ch.warmup_seconds + ch.sampling_seconds
-    return {"min_ess_per_s": float(np.min(e) / ch.sampling_seconds), "min_ess": float(np.min(e)),
-            "max_rhat": float(np.max(r)), "warmup_s": ch.warmup_seconds, "sampling_s": ch.sampling_seconds,
-            "ms_per_sampling_iteration": 1e3 * ch.sampling_seconds / num_samples,
-            "grad_evals_per_s": ch.gradient_evaluations / total_s, "mean_accept": float(ch.accept_prob.mean()),
-            "mean_tree_depth": float(ch.tree_depth.mean()), "max_tree_depth": int(ch.tree_depth.max()),
-            "mean_leapfrog_steps": float(ch.integration_steps.mean()),
-            "config": f"{num_chains} chains, masked NUTS depth 10, {num_warmup}+{num_samples}, GLM 100000x100"}
+    return _chain_summary(ch, f"{num_chains} chains, masked NUTS depth 10, {num_warmup}+{num_samples}, GLM 100000x100",
+                          {"ms_per_sampling_iteration": 1e3 * ch.sampling_seconds / num_samples,
+                           "mean_tree_depth": float(ch.tree_depth.mean()), "max_tree_depth": int(ch.tree_depth.max()),
+                           "mean_leapfrog_steps": float(ch.integration_steps.mean())})
 
 
 def glm_large_meads(num_chains=4096, num_warmup=3000, num_samples=1000):
@@ -440,16 +507,13 @@ def glm_large_meads(num_chains=4096, num_warmup=3000, num_samples=1000):
     posterior ~15x narrower than the prior) the ensemble step size grows from
     3e-4 to ~0.5 over ~2500 iterations as the folds contract, so the first 3000
     draws are discarded."""
-    from uncertaintea_b200 import batched_meads, ess, rhat
+    from uncertaintea_b200 import batched_meads
     model, X, y, _ = _data()
     ch = batched_meads(model, (X,), {"y": y}, num_chains=num_chains, num_samples=num_samples,
                        num_warmup=num_warmup, rng=1)
-    e, r = ess(ch, space="unconstrained"), rhat(ch, space="unconstrained")
-    return {"min_ess_per_s": float(np.min(e) / ch.sampling_seconds), "min_ess": float(np.min(e)),
-            "max_rhat": float(np.max(r)), "warmup_s": ch.warmup_seconds, "sampling_s": ch.sampling_seconds,
-            "ms_per_iteration": 1e3 * ch.sampling_seconds / num_samples,
-            "mean_accept": float(ch.accept_prob.mean()), "step_size": float(np.mean(ch.step_size)),
-            "config": f"{num_chains} chains, MEADS 4 folds, {num_warmup} discarded + {num_samples}, GLM 100000x100"}
+    return _chain_summary(ch, f"{num_chains} chains, MEADS 4 folds, {num_warmup} discarded + {num_samples}, "
+                          "GLM 100000x100", {"ms_per_iteration": 1e3 * ch.sampling_seconds / num_samples,
+                                             "step_size": float(np.mean(ch.step_size))})
 
 
 def surrogate_comparison(num_chains=4096, num_warmup=500, num_samples=500):

@@ -40,6 +40,11 @@ extern "C" {
 #define UT_ERR_NO_DEVICE       6  /* no CUDA device visible                      */
 #define UT_ERR_DEVICE_TIMEOUT  7  /* a bounded in-kernel wait gave up            */
 
+/* Largest observation count of a kernel description (and of the
+ * allocation-free GLM entry point): the kernels index observations in 32-bit
+ * arithmetic, and 2^30 keeps every split end in range. */
+#define UT_MAX_OBS (1 << 30)
+
 /* ---- model families a kernel description can hold ---------------------- */
 /* Bernoulli-logit GLM: optional intercept ~ normal, coefficients ~ iid normal,
  * y_i ~ bernoullilogit(intercept + x_i . beta).  Lowered form of the
@@ -162,6 +167,133 @@ int32_t ut_workspace_info(const ut_workspace* ws, int32_t* num_params, int32_t* 
  * 4 = HBM-streaming path for a few chains (C <= 16, GLM with P % 4 == 0 and
  * P <= 128). */
 int32_t ut_workspace_path(const ut_workspace* ws);
+
+/* ---- composable kernel description: the step program -----------------------
+ * reference: the step tuple of DeviceExecutionPlan (src/device/plan/steps.jl:
+ * 6-489) that _lower_device_plan produces (src/device/plan/lowering.jl:1360),
+ * walked by _device_logjoint_kernel! (src/device/logjoint_kernel.jl:724) and
+ * _device_gradient_kernel! (src/device/gradient_kernel.jl:1124).  Where a
+ * model matches none of the fixed families above, the host passes its plan
+ * step by step: choice steps (a distribution, argument expressions, a value
+ * that is a latent parameter row or a staged observation, a transform, a
+ * binding slot), deterministic steps, loops, the iid normal vector prior
+ * (DeviceDiagNormalChoiceStepDyn, steps.jl:334-340) and the fused
+ * Bernoulli-logit GLM likelihood (DeviceBernoulliLogitGLMChoiceStep[Dyn],
+ * steps.jl:181-225).  The logjoint and its full gradient come from one pass.
+ *
+ * Observations: the staged buffer is read in blocks.  The top level is one
+ * block (row 0 ..); a loop's iteration t is the block that starts at row
+ * `obs_offset + t * width` of the enclosing block; an observed value, an
+ * observation leaf of an expression and a nested loop each name their row in
+ * the block of their own loop depth, so the host fixes every row statically
+ * (the reference's cursor, src/device/logjoint_kernel.jl:68-78, 620-634).
+ * Slots (0 .. num_slots-1) hold the values of bindings and iterators, as the
+ * reference's `slots` buffer; parameters rows are 0-based. */
+#define UT_FAMILY_PROGRAM 8
+
+#define UT_STEP_CHOICE              1  /* value ~ dist(args...)                         */
+#define UT_STEP_DETERMINISTIC       2  /* slot = expression (DeviceDeterministicStep)   */
+#define UT_STEP_LOOP                3  /* `count` iterations of the next `body` steps    */
+#define UT_STEP_IID_NORMAL          4  /* `count` latent rows ~ normal(arg0, arg1)      */
+#define UT_STEP_GLM_BERNOULLI_LOGIT 5  /* `count` observations, each `width` covariates
+                                        * then y ~ bernoullilogit(arg0 + x . beta), beta
+                                        * = `width` latent rows from value_source       */
+
+/* Distributions of UT_STEP_CHOICE; the argument order is the reference step's
+ * field order (math.jl:88-300).  Values of 18-23 must be observed. */
+#define UT_DIST_NORMAL             1  /* mu, sigma          */
+#define UT_DIST_LOGNORMAL          2  /* mu, sigma          */
+#define UT_DIST_EXPONENTIAL        3  /* rate               */
+#define UT_DIST_GAMMA              4  /* shape, rate        */
+#define UT_DIST_LAPLACE            5  /* loc, scale         */
+#define UT_DIST_CAUCHY             6  /* mu, sigma          */
+#define UT_DIST_HALFNORMAL         7  /* sigma              */
+#define UT_DIST_HALFCAUCHY         8  /* scale              */
+#define UT_DIST_LOGISTIC           9  /* mu, scale          */
+#define UT_DIST_GUMBEL            10  /* mu, scale          */
+#define UT_DIST_FRECHET           11  /* shape, scale       */
+#define UT_DIST_RAYLEIGH          12  /* scale              */
+#define UT_DIST_INVERSEGAUSSIAN   13  /* mu, lambda         */
+#define UT_DIST_BETA              14  /* alpha, beta        */
+#define UT_DIST_STUDENTT          15  /* nu, mu, sigma      */
+#define UT_DIST_INVERSEGAMMA      16  /* shape, scale       */
+#define UT_DIST_WEIBULL           17  /* shape, scale       */
+#define UT_DIST_BERNOULLI         18  /* p                  */
+#define UT_DIST_BERNOULLI_LOGIT   19  /* eta                */
+#define UT_DIST_POISSON           20  /* lambda             */
+#define UT_DIST_GEOMETRIC         21  /* p                  */
+#define UT_DIST_NEGATIVE_BINOMIAL 22  /* successes, p       */
+#define UT_DIST_BINOMIAL          23  /* trials, p          */
+
+/* Transforms of a latent scalar value (math.jl:1137-1159). */
+#define UT_TRANSFORM_IDENTITY 0
+#define UT_TRANSFORM_LOG      1       /* value = exp(u), log|J| = u                    */
+#define UT_TRANSFORM_LOGIT    2       /* value = logistic(u), log|J| = -|u| - 2 log1p(exp(-|u|)) */
+
+/* Expression nodes (reference DeviceLiteralExpr / DeviceSlotExpr /
+ * DevicePrimitiveExpr / DeviceObservedColumnExpr, src/device/plan/exprs.jl).
+ * An operand `a` / `b` is the index of an earlier node. */
+#define UT_EXPR_LITERAL  0   /* `value`                                                     */
+#define UT_EXPR_SLOT     1   /* slot `a`                                                    */
+#define UT_EXPR_OBS      2   /* observation row `a` of the block at loop depth `b` (0 = top) */
+#define UT_EXPR_NEG      3
+#define UT_EXPR_ADD      4
+#define UT_EXPR_SUB      5
+#define UT_EXPR_MUL      6
+#define UT_EXPR_DIV      7
+#define UT_EXPR_POW      8
+#define UT_EXPR_EXP      9
+#define UT_EXPR_LOG     10
+#define UT_EXPR_LOG1P   11
+#define UT_EXPR_SQRT    12
+#define UT_EXPR_ABS     13
+#define UT_EXPR_MIN     14
+#define UT_EXPR_MAX     15
+#define UT_EXPR_SIN     16
+#define UT_EXPR_COS     17
+#define UT_EXPR_TAN     18
+#define UT_EXPR_TANH    19
+#define UT_EXPR_SINH    20
+#define UT_EXPR_COSH    21
+#define UT_EXPR_ATAN    22
+#define UT_EXPR_EXPM1   23
+
+typedef struct ut_expr_node {
+    int32_t op;            /* UT_EXPR_*                                           */
+    int32_t a;             /* operand node / slot / observation row               */
+    int32_t b;             /* operand node / loop depth of an observation row     */
+    int32_t reserved;      /* 0                                                   */
+    double value;          /* UT_EXPR_LITERAL                                     */
+} ut_expr_node;
+
+typedef struct ut_program_step {
+    int32_t kind;          /* UT_STEP_*                                                  */
+    int32_t dist;          /* UT_STEP_CHOICE: UT_DIST_*                                  */
+    int32_t arg[4];        /* root node of each argument expression, -1 = none          */
+    int32_t value_source;  /* >= 0: first parameter row of a latent value; -1: observed */
+    int32_t obs_offset;    /* row of an observed value / of a loop's first block         */
+    int32_t transform;     /* UT_TRANSFORM_* of a latent scalar choice                   */
+    int32_t binding_slot;  /* slot that receives the value, -1 = none                    */
+    int32_t count;         /* LOOP: iterations; IID_NORMAL: rows; GLM: observations      */
+    int32_t width;         /* LOOP: rows per iteration block; GLM: covariates            */
+    int32_t body;          /* LOOP: number of following steps in its body (nested too)   */
+    int32_t iterator_slot; /* LOOP: slot holding iterator_start + t, -1 = none           */
+    int32_t iterator_start;
+} ut_program_step;
+
+/* Checks a step program (the device_lowering_report of a program): UT_OK or
+ * UT_ERR_UNSUPPORTED with the issues.  observed_rows = the staged rows. */
+int32_t ut_program_report(const ut_program_step* steps, int32_t num_steps, const ut_expr_node* nodes,
+                          int32_t num_nodes, int32_t num_slots, int32_t num_params, int64_t observed_rows,
+                          char* issues, size_t len);
+/* A workspace over a step program (DeviceBatchedWorkspace of a model outside
+ * the fixed families); every other workspace entry point and every sampler
+ * accepts it.  Parameters: 1 <= P <= 256, every row read by exactly one
+ * latent step. */
+int32_t ut_workspace_create_program(const ut_program_step* steps, int32_t num_steps, const ut_expr_node* nodes,
+                                    int32_t num_nodes, int32_t num_slots, int32_t num_params,
+                                    const float* observed, int64_t observed_rows, int32_t batch_size,
+                                    int32_t precision_bits, ut_workspace** out);
 /* Synchronises the workspace's work and reports the sticky device error word:
  * UT_ERR_DEVICE_TIMEOUT when a bounded in-kernel wait gave up since the last
  * check (the word is cleared by this call), else UT_OK.  Until it is cleared,
@@ -350,11 +482,15 @@ int32_t ut_running_variance_update(const float* d_positions, const double* d_wei
  *   d_y        : N outcomes in {0, 1}
  *   d_params   : C x P chain-major parameters;  d_totals: C;  d_gradients: C x P
  * Scratch memory is a fixed 16 MiB device array owned by the library (held by
- * every GPU that loads it until exit): C * (P + 1) may be at most 4,194,304,
- * larger batches are rejected with UT_ERR_ARGUMENT.  The first call on a device
- * performs a one-time set-up for that device; make it before any stream
- * capture.  All calls share the array, so calls that overlap on the GPU race:
- * serialise them.  Returns once the work is queued on `stream`. */
+ * every GPU that uses it until exit): C * (P + 1) may be at most 4,194,304,
+ * and 1 <= N <= UT_MAX_OBS; other sizes are rejected with UT_ERR_ARGUMENT.
+ * The first call on a device performs a one-time set-up for that device, and
+ * with CUDA's lazy module loading that first call is also when the 16 MiB and
+ * the module's code are committed on the device: a host that reserves its
+ * whole memory budget at start-up should make one call per device first (and
+ * before any stream capture).  All calls share the array, so calls that
+ * overlap on the GPU race: serialise them.  Returns once the work is queued
+ * on `stream`. */
 int32_t ut_glm_logjoint_gradient_noalloc(const float* d_design, const float* d_y, int64_t num_obs,
                                          int32_t num_params, int32_t has_intercept, double intercept_mu,
                                          double intercept_sigma, double coef_mu, double coef_sigma,

@@ -37,6 +37,8 @@ def load():
                                                 c_void_p, c_int32]),
         "orc_logjoint_gradient_f32": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p,
                                                 c_void_p, c_int32]),
+        "orc_gradient_magnitude_f64": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p,
+                                                 c_int32]),
         "orc_max_threads": (c_int32, []),
         "orc_meads_max_eig": (c_double, [c_void_p, c_int32, c_int32]),
         "orc_meads_iteration_f32": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32,
@@ -171,6 +173,14 @@ class OracleModel:
         grads = np.empty_like(q) if want_grad else None
         load().orc_logjoint_gradient_f64(*self._common(), _p(q), C, _p(totals), _p(grads), threads)
         return totals, grads
+
+    def gradient_magnitude_f64(self, params_cp, threads=0):
+        """Per gradient element, the sum of the magnitudes of the terms it adds
+        up (the scale FP32 rounding errors of the gradient are relative to)."""
+        q = np.ascontiguousarray(params_cp, dtype=np.float64)
+        out = np.empty_like(q)
+        load().orc_gradient_magnitude_f64(*self._common(), _p(q), q.shape[0], _p(out), threads)
+        return out
 
     def logjoint_gradient_f32(self, params_cp, threads=0, want_grad=True):
         q = np.ascontiguousarray(params_cp, dtype=np.float32)

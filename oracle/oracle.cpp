@@ -398,6 +398,110 @@ W logjoint_grad(const ModelData& m, const T* q, T* g) {
 }
 
 // ---------------------------------------------------------------------------
+// Gradient magnitudes (float64): for every gradient element, the sum of the
+// absolute values of the terms the gradient adds up, each term's magnitude
+// taken over the inputs of its own subtractions (so a term whose FP32 inputs
+// cancel keeps the size of those inputs).  An FP32 evaluation of a sum errs by
+// a multiple of the unit roundoff times this magnitude, not times the sum
+// itself, so it is the scale of the absolute part of the elementwise gradient
+// tolerance.  The GLM also carries the error a residual inherits from its
+// FP32 linear predictor: sigma'(eta) * sum_f |theta_f x_if| per observation.
+// Same terms as the *_logjoint_grad functions above.
+// ---------------------------------------------------------------------------
+void grad_magnitude(const ModelData& m, const double* q, double* a) {
+    const ut_plan_desc& p = m.plan;
+    const int P = p.num_params;
+    for (int k = 0; k < P; ++k) a[k] = 0.0;
+    switch (p.family) {
+    case UT_FAMILY_GLM_BERNOULLI_LOGIT: {
+        const int N = p.num_obs, D = p.num_coefs, off = p.has_intercept ? 1 : 0;
+        const double al = off ? q[0] : 0.0;
+        if (off) a[0] += (std::fabs(al) + std::fabs(p.intercept_mu)) / (p.intercept_sigma * p.intercept_sigma);
+        for (int d = 0; d < D; ++d)
+            a[off + d] += (std::fabs(q[off + d]) + std::fabs(p.coef_mu)) / (p.coef_sigma * p.coef_sigma);
+        for (int i = 0; i < N; ++i) {
+            const double* x = &m.X[(size_t)i * D];
+            double eta = al, A = std::fabs(al);
+            for (int d = 0; d < D; ++d) {
+                eta += q[off + d] * x[d];
+                A += std::fabs(q[off + d] * x[d]);
+            }
+            const double s = 1.0 / (1.0 + std::exp(-eta));
+            const double w = std::fabs(m.y[i] - s) + s * (1.0 - s) * A;
+            if (off) a[0] += w;
+            for (int d = 0; d < D; ++d) a[off + d] += w * std::fabs(x[d]);
+        }
+        break;
+    }
+    case UT_FAMILY_HIER_NORMAL_NONCENTERED: {
+        const double mu = q[0], tau = std::exp(q[1]), s2 = p.tau_scale * p.tau_scale;
+        a[0] = (std::fabs(mu) + std::fabs(p.mu_loc)) / (p.mu_scale * p.mu_scale);
+        a[1] = 1.0 + 2.0 * tau * tau / (s2 + tau * tau);
+        for (int j = 0; j < p.num_groups; ++j) {
+            const double z = q[2 + j], thm = std::fabs(mu) + std::fabs(tau * z), sj2 = m.sig[j] * m.sig[j];
+            double S = 0.0;
+            for (int k = 0; k < m.count[j]; ++k) S += (std::fabs(m.y[m.start[j] + k]) + thm) / sj2;
+            a[0] += S;
+            a[1] += std::fabs(tau * z) * S;
+            a[2 + j] = std::fabs(z) + tau * S;
+        }
+        break;
+    }
+    case UT_FAMILY_NORMAL_LOCATION_SCALE: {
+        const double mu = q[0], s = std::exp(q[1]);
+        a[0] = (std::fabs(mu) + std::fabs(p.mu_loc)) / (p.mu_scale * p.mu_scale);
+        a[1] = p.scale_shape + p.scale_rate * s;
+        for (size_t i = 0; i < m.y.size(); ++i) {
+            const double d = std::fabs(m.y[i]) + std::fabs(mu);
+            a[0] += d / (s * s);
+            a[1] += d * d / (s * s) + 1.0;
+        }
+        break;
+    }
+    case UT_FAMILY_NORMAL_KNOWN_SCALE: {
+        const double mu = q[0], s2 = p.obs_scale * p.obs_scale;
+        a[0] = (std::fabs(mu) + std::fabs(p.mu_loc)) / (p.mu_scale * p.mu_scale);
+        for (size_t i = 0; i < m.y.size(); ++i) a[0] += (std::fabs(m.y[i]) + std::fabs(mu)) / s2;
+        break;
+    }
+    case UT_FAMILY_BERNOULLI_BETA: {
+        const double pr = 1.0 / (1.0 + std::exp(-q[0]));
+        a[0] = std::fabs(p.prob_alpha - 1.0) * (1.0 + pr) + std::fabs(p.prob_beta - 1.0) * pr + 1.0 + 2.0 * pr;
+        for (size_t i = 0; i < m.y.size(); ++i) a[0] += m.y[i] > 0.5 ? 1.0 + pr : pr;
+        break;
+    }
+    case UT_FAMILY_LOGNORMAL_GAMMA_NORMAL: {
+        const double ea = std::exp(q[0]), b = std::exp(q[1]), s = std::exp(ea);
+        a[0] = (std::fabs(q[0]) + std::fabs(p.mu_loc)) / (p.mu_scale * p.mu_scale);
+        a[1] = p.scale_shape + p.scale_rate * b;
+        for (size_t i = 0; i < m.y.size(); ++i) {
+            const double d = std::fabs(m.y[i]) + b;
+            a[0] += ea * (1.0 + d * d / (s * s));
+            a[1] += b * d / (s * s);
+        }
+        break;
+    }
+    case UT_FAMILY_STUDENTT_HEAVY_TAIL: {
+        const double loc = q[0], s = std::exp(q[1]), w = std::exp(q[2]), sig = s + w;
+        const double nu0 = p.nu_prior, s0 = p.mu_scale, nu1 = p.nu_obs, d0 = loc - p.mu_loc;
+        a[0] = (nu0 + 1.0) * (std::fabs(loc) + std::fabs(p.mu_loc)) / (nu0 * s0 * s0 + d0 * d0);
+        const double ns2 = nu1 * sig * sig;
+        double md = 0.0;
+        for (size_t i = 0; i < m.y.size(); ++i) {
+            const double r = m.y[i] - loc, t = r * r, ra = std::fabs(m.y[i]) + std::fabs(loc);
+            a[0] += (nu1 + 1.0) * ra / (ns2 + t);
+            md += 1.0 / sig + (nu1 + 1.0) * ra * ra / (sig * (ns2 + t));
+        }
+        a[1] = p.scale_shape + p.scale_rate / s + s * md;
+        a[2] = p.weibull_shape + p.weibull_shape * std::pow(w / p.weibull_scale, p.weibull_shape) + w * md;
+        break;
+    }
+    default:
+        break;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // HMC iteration with Philox randomness (f32).  Momentum p = z / sqrt(M^-1)
 // (hmc_support.jl:350-367, persistent_nuts.jl:244-249); leapfrog as
 // _device_leapfrog_integrate_perchain! (hmc_kernels.jl:255-287) / host
@@ -750,6 +854,18 @@ int orc_logjoint_gradient_f32(const ut_plan_desc* plan, const float* observed, c
     for (int c = 0; c < C; ++c) {
         totals[c] = logjoint_grad<float, float>(m, params + (size_t)c * P, grads ? grads + (size_t)c * P : nullptr);
     }
+    return 0;
+}
+
+// Gradient magnitudes (see grad_magnitude) in float64; params C x P, out C x P.
+int orc_gradient_magnitude_f64(const ut_plan_desc* plan, const float* observed, const int32_t* trip_counts,
+                               const int32_t* loop_starts, const double* params, int32_t C, double* out,
+                               int32_t threads) {
+    ModelData m = make_model(plan, observed, trip_counts, loop_starts);
+    const int P = plan->num_params;
+    set_threads(threads);
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < C; ++c) grad_magnitude(m, params + (size_t)c * P, out + (size_t)c * P);
     return 0;
 }
 

@@ -6,8 +6,10 @@ Tolerances (stated per test):
 * Box-Muller normals: |gpu - oracle| <= 2e-6 * max(1, |oracle|) (libm vs CUDA
   logf/cosf differ in the last bits, rng.jl:185-194).
 * logjoint (FP32) vs the FP64 oracle: |lj - lj64| <= 1e-5 * |lj64|.
-* gradient (FP32) vs the FP64 oracle, per chain:
-  max_p |g - g64| <= 1e-5 * max_p |g64|.
+* gradient (FP32) vs the FP64 oracle, elementwise:
+  |g - g64| <= 1e-5 |g64| + 1e-6 m, m = the sum of the magnitudes of the terms
+  the component adds up (the scale of FP32 summation error, see GRAD_ATOL_MAG),
+  and per chain max_p |g - g64| <= 1e-5 max_p |g64|.
 * HMC / NUTS iterations vs the FP32 oracle under identical Philox streams:
   the same accept / tree decisions for >= 98% of chains, and states of the
   chains with identical decisions within rtol 1e-3, atol 1e-4.
@@ -34,9 +36,37 @@ def _ws(model, args, constraints, C):
     return DeviceBatchedWorkspace(model, C, args=args, constraints=constraints)
 
 
+GRAD_RTOL = 1e-5
+# Absolute part of the elementwise gradient tolerance, as a fraction of the
+# gradient magnitude m: the sum of the magnitudes of the terms a component adds
+# up (oracle gradient_magnitude_f64).  An FP32 sum errs by a multiple of the
+# unit roundoff times m, not times the sum itself, so a component whose terms
+# cancel (|g64| << m) cannot meet a purely relative bound in FP32 however it
+# is summed.  1e-6 m is about 17 FP32 roundoffs of m; the largest error
+# measured on any kernel path (warp, tiled, tensor core, streaming, live-chain
+# re-split, all 4096 chains of the 100000 x 100 design) is 3.9e-7 m.
+GRAD_ATOL_MAG = 1e-6
+
+
+def _ref(om, q):
+    """FP64 oracle logjoint, gradient and gradient magnitude of chain-major q."""
+    q64 = np.asarray(q, dtype=np.float64)
+    t64, g64 = om.logjoint_gradient_f64(q64)
+    return t64, g64, om.gradient_magnitude_f64(q64)
+
+
 def _grad_err(g, g64):
+    """Per-chain norm-relative error: max_p |g - g64| / max_p |g64|."""
     scale = np.maximum(np.max(np.abs(g64), axis=1), 1e-30)
     return np.max(np.max(np.abs(g.astype(np.float64) - g64), axis=1) / scale)
+
+
+def _grad_ok(g, g64, mag):
+    """Both gradient bounds: elementwise |g - g64| <= 1e-5 |g64| + 1e-6 m, and
+    the per-chain norm bound max_p |g - g64| <= 1e-5 max_p |g64|."""
+    g = np.asarray(g, dtype=np.float64)
+    over = np.max(np.abs(g - g64) / (GRAD_RTOL * np.abs(g64) + GRAD_ATOL_MAG * mag))
+    return over <= 1.0 and _grad_err(g, g64) <= GRAD_RTOL
 
 
 def _lj_err(t, t64):
@@ -92,28 +122,54 @@ def test_glm_density_vs_fp64_oracle(lib, N, D, C, intercept, scale):
     t, g = ws.logjoint_gradient(q.T)
     t_only = ws.logjoint(q.T)
     om = oracle.OracleModel(ws.lowered)
-    t64, g64 = om.logjoint_gradient_f64(q.astype(np.float64))
+    t64, g64, mag = _ref(om, q.astype(np.float64))
     assert _lj_err(t, t64) <= 1e-5
     assert _lj_err(t_only, t64) <= 1e-5
-    assert _grad_err(np.asarray(g.T), g64) <= 1e-5
+    assert _grad_ok(np.asarray(g.T), g64, mag)
     ws.close()
 
 
-def test_glm_density_full_size_subset(lib):
-    """Full size (N=100000, D=100, C=4096): every chain computed on the
-    GPU, 12 chains checked against the FP64 oracle."""
+def test_glm_density_full_size_all_chains(lib):
+    """Full size (N=100000, D=100, C=4096) on the tensor-core path: every one of
+    the 4096 chains against the FP64 oracle, elementwise."""
     m, args, cons, q = _glm_case(100000, 100, 4096, False, 3, 0.1)
     ws = _ws(m, args, cons, 4096)
+    assert ws.kernel_path() == "tensor_core"
     qd = torch.from_numpy(q).cuda()
     t, g = ws.logjoint_gradient_device(qd)
     torch.cuda.synchronize()
+    ws.check()
     t, g = t.cpu().numpy(), g.cpu().numpy()
-    idx = np.array([0, 1, 63, 64, 65, 1000, 2047, 2048, 3000, 4032, 4094, 4095])
-    om = oracle.OracleModel(ws.lowered)
-    t64, g64 = om.logjoint_gradient_f64(q[idx].astype(np.float64))
-    assert _lj_err(t[idx], t64) <= 1e-5
-    assert _grad_err(g[idx], g64) <= 1e-5
-    assert np.all(np.isfinite(t)) and np.all(np.isfinite(g))
+    t64, g64, mag = _ref(oracle.OracleModel(ws.lowered), q)
+    assert _lj_err(t, t64) <= 1e-5
+    assert _grad_ok(g, g64, mag)
+    ws.close()
+
+
+@pytest.mark.parametrize("live", [1, 127, 300, 2049])
+def test_tensor_core_live_chains_vs_oracle(lib, live):
+    """The live-chain launch masked NUTS makes at every leaf (only the first
+    `live` of 4096 chains evaluated; few live chain tiles re-split the
+    observations so the launch still fills the SMs) at the full 100000 x 100
+    size: the live rows against the FP64 oracle, the rows past them untouched."""
+    m, args, cons, q = _glm_case(100000, 100, 4096, False, 3, 0.1)
+    ws = _ws(m, args, cons, 4096)
+    assert ws.kernel_path() == "tensor_core"
+    fn = lib.ut_internal_tc_glm_live
+    fn.restype = ctypes.c_int32
+    fn.argtypes = [ctypes.c_void_p] * 6
+    qd = torch.from_numpy(q).cuda()
+    t = torch.full((4096,), float("nan"), device="cuda")
+    g = torch.full((4096, 100), float("nan"), device="cuda")
+    n = torch.tensor([live], dtype=torch.int32, device="cuda")
+    nat.check(fn(ws.handle, nat.ptr(qd), nat.ptr(t), nat.ptr(g), nat.ptr(n), None))
+    torch.cuda.synchronize()
+    ws.check()
+    t, g = t.cpu().numpy(), g.cpu().numpy()
+    assert np.all(np.isnan(t[live:])) and np.all(np.isnan(g[live:]))
+    t64, g64, mag = _ref(oracle.OracleModel(ws.lowered), q[:live])
+    assert _lj_err(t[:live], t64) <= 1e-5
+    assert _grad_ok(g[:live], g64, mag)
     ws.close()
 
 
@@ -145,9 +201,9 @@ def test_hier_density_vs_fp64_oracle(lib, J, n, C):
     ws = _ws(m, (sig, sizes), {"y": y}, C)
     t, g = ws.logjoint_gradient(q.T)
     om = oracle.OracleModel(ws.lowered)
-    t64, g64 = om.logjoint_gradient_f64(q.astype(np.float64))
+    t64, g64, mag = _ref(om, q.astype(np.float64))
     assert _lj_err(t, t64) <= 1e-5
-    assert _grad_err(np.asarray(g.T), g64) <= 1e-5
+    assert _grad_ok(np.asarray(g.T), g64, mag)
     ws.close()
 
 
@@ -165,9 +221,9 @@ def test_gauss_density_vs_fp64_oracle(lib, n, C):
     ws = _ws(m, (n,), {"y": y}, C)
     assert ws.kernel_path() == "warp"
     t, g = ws.logjoint_gradient(q.T)
-    t64, g64 = oracle.OracleModel(ws.lowered).logjoint_gradient_f64(q.astype(np.float64))
+    t64, g64, mag = _ref(oracle.OracleModel(ws.lowered), q.astype(np.float64))
     assert _lj_err(t, t64) <= 1e-5
-    assert _grad_err(np.asarray(g.T), g64) <= 1e-5
+    assert _grad_ok(np.asarray(g.T), g64, mag)
     ws.close()
 
 
@@ -183,9 +239,9 @@ def test_bernoulli_beta_density_vs_fp64_oracle(lib, n, C):
         q = (np.random.default_rng(4).standard_normal((C, 1)) * 2).astype(np.float32)
     ws = _ws(BernoulliBeta(), (n,), {"z": z}, C)
     t, g = ws.logjoint_gradient(q.T)
-    t64, g64 = oracle.OracleModel(ws.lowered).logjoint_gradient_f64(q.astype(np.float64))
+    t64, g64, mag = _ref(oracle.OracleModel(ws.lowered), q.astype(np.float64))
     assert _lj_err(t, t64) <= 1e-5
-    assert _grad_err(np.asarray(g.T), g64) <= 1e-5
+    assert _grad_ok(np.asarray(g.T), g64, mag)
     ws.close()
 
 
@@ -201,9 +257,9 @@ def test_lognormal_gamma_density_vs_fp64_oracle(lib, n, C):
         q = (np.array([0.0, 0.4]) + 0.3 * np.random.default_rng(4).standard_normal((C, 2))).astype(np.float32)
     ws = _ws(LognormalGammaNormal(), (n,), {"y": y}, C)
     t, g = ws.logjoint_gradient(q.T)
-    t64, g64 = oracle.OracleModel(ws.lowered).logjoint_gradient_f64(q.astype(np.float64))
+    t64, g64, mag = _ref(oracle.OracleModel(ws.lowered), q.astype(np.float64))
     assert _lj_err(t, t64) <= 1e-5
-    assert _grad_err(np.asarray(g.T), g64) <= 1e-5
+    assert _grad_ok(np.asarray(g.T), g64, mag)
     ws.close()
 
 
@@ -219,9 +275,9 @@ def test_heavy_tail_density_vs_fp64_oracle(lib, n, C):
         q = (np.array([0.5, -0.3, 0.0]) + 0.3 * np.random.default_rng(4).standard_normal((C, 3))).astype(np.float32)
     ws = _ws(StudentTHeavyTail(), (n,), {"y": y}, C)
     t, g = ws.logjoint_gradient(q.T)
-    t64, g64 = oracle.OracleModel(ws.lowered).logjoint_gradient_f64(q.astype(np.float64))
+    t64, g64, mag = _ref(oracle.OracleModel(ws.lowered), q.astype(np.float64))
     assert _lj_err(t, t64) <= 1e-5
-    assert _grad_err(np.asarray(g.T), g64) <= 1e-5
+    assert _grad_ok(np.asarray(g.T), g64, mag)
     ws.close()
 
 
@@ -235,8 +291,8 @@ def test_hier_ragged_groups_with_empty_group(lib):
     q = rng.standard_normal((5, J + 2)).astype(np.float32)
     ws = _ws(m, (sig, sizes), {"y": y}, 5)
     t, g = ws.logjoint_gradient(q.T)
-    t64, g64 = oracle.OracleModel(ws.lowered).logjoint_gradient_f64(q.astype(np.float64))
-    assert _lj_err(t, t64) <= 1e-5 and _grad_err(np.asarray(g.T), g64) <= 1e-5
+    t64, g64, mag = _ref(oracle.OracleModel(ws.lowered), q.astype(np.float64))
+    assert _lj_err(t, t64) <= 1e-5 and _grad_ok(np.asarray(g.T), g64, mag)
     ws.close()
 
 
@@ -428,7 +484,7 @@ def test_bernoulli_beta_float32_logit_cliff(lib):
     ws = _ws(m, (1,), {"z": np.array([1.0])}, len(q))
     t, g = ws.logjoint_gradient(q.T)
     g = np.asarray(g.T)[:, 0]
-    t64, g64 = oracle.OracleModel(ws.lowered).logjoint_gradient_f64(q.astype(np.float64))
+    t64, g64, mag = _ref(oracle.OracleModel(ws.lowered), q.astype(np.float64))
     assert np.all(t[:3] == -np.inf) and not np.any(np.isnan(g[:3]))
     tol = 4 * np.finfo(np.float32).eps * np.exp(q[3:6, 0].astype(np.float64)) + 1e-5
     assert np.all(np.isfinite(t[3:6])) and np.all(np.abs(t[3:6] - t64[3:6]) <= tol)
@@ -450,9 +506,9 @@ def test_known_scale_density_vs_fp64_oracle(lib, n, C):
     ws = _ws(m, (n,), {"y": y}, C)
     assert ws.kernel_path() == "warp"
     t, g = ws.logjoint_gradient(q.T)
-    t64, g64 = oracle.OracleModel(ws.lowered).logjoint_gradient_f64(q.astype(np.float64))
+    t64, g64, mag = _ref(oracle.OracleModel(ws.lowered), q.astype(np.float64))
     assert _lj_err(t, t64) <= 1e-5
-    assert _grad_err(np.asarray(g.T), g64) <= 1e-5
+    assert _grad_ok(np.asarray(g.T), g64, mag)
     ws.close()
 
 
@@ -673,10 +729,10 @@ def test_tensor_core_path_vs_cuda_core_and_oracle(lib, N, D, C, intercept, monke
     torch.cuda.synchronize()
     t1, g1, t0, t2, g2 = (x.cpu().numpy() for x in (t1, g1, t0, t2, g2))
     idx = np.unique(np.linspace(0, C - 1, min(C, 16)).astype(int))
-    t64, g64 = oracle.OracleModel(ws_tc.lowered).logjoint_gradient_f64(q[idx].astype(np.float64))
-    assert _lj_err(t1[idx], t64) <= 1e-5 and _grad_err(g1[idx], g64) <= 1e-5
+    t64, g64, mag = _ref(oracle.OracleModel(ws_tc.lowered), q[idx].astype(np.float64))
+    assert _lj_err(t1[idx], t64) <= 1e-5 and _grad_ok(g1[idx], g64, mag)
     assert _lj_err(t0[idx], t64) <= 1e-5
-    assert _lj_err(t2[idx], t64) <= 1e-5 and _grad_err(g2[idx], g64) <= 1e-5
+    assert _lj_err(t2[idx], t64) <= 1e-5 and _grad_ok(g2[idx], g64, mag)
     assert _lj_err(t1, t2.astype(np.float64)) <= 2e-5
     ws_tc.close()
     ws_cc.close()
@@ -708,9 +764,9 @@ def test_streaming_path_vs_oracle_and_tiled(lib, N, D, C, intercept, monkeypatch
     ws.check()
     t1, g1, t0, t2, g2 = (x.cpu().numpy() for x in (t1, g1, t0, t2, g2))
     assert np.array_equal(t1, t1b.cpu().numpy()) and np.array_equal(g1, g1b.cpu().numpy())
-    t64, g64 = oracle.OracleModel(ws.lowered).logjoint_gradient_f64(q.astype(np.float64))
+    t64, g64, mag = _ref(oracle.OracleModel(ws.lowered), q.astype(np.float64))
     assert _lj_err(t1, t64) <= 1e-5 and _lj_err(t0, t64) <= 1e-5
-    assert _grad_err(g1, g64) <= 1e-5
+    assert _grad_ok(g1, g64, mag)
     np.testing.assert_allclose(t1, t2, rtol=2e-6)
     np.testing.assert_allclose(g1, g2, rtol=1e-4, atol=1e-4 * np.abs(g64).max())
     ws.close()

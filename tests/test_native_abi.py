@@ -168,6 +168,13 @@ def test_lowering_report_flags_bad_descriptions(lib):
     gauss.num_params = 3
     assert lib.ut_lowering_report(ctypes.byref(gauss), buf, len(buf)) == nat.UT_ERR_UNSUPPORTED
     assert b"num_params must equal 2" in buf.value and b"gamma shape and rate" in buf.value
+    # the observation count bound of the 32-bit observation index arithmetic
+    glm.num_obs = (1 << 30) + 1
+    assert lib.ut_lowering_report(ctypes.byref(glm), buf, len(buf)) == nat.UT_ERR_UNSUPPORTED
+    assert b"num_obs must be <= 2^30" in buf.value
+    glm.num_obs = 1 << 30
+    assert lib.ut_lowering_report(ctypes.byref(glm), buf, len(buf)) == nat.UT_OK
+
     nks = nat.PlanDesc(family=nat.UT_FAMILY_NORMAL_KNOWN_SCALE, num_params=1, num_obs=1, mu_scale=1.0, obs_scale=1.0)
     assert lib.ut_lowering_report(ctypes.byref(nks), buf, len(buf)) == nat.UT_OK
     nks.obs_scale = 0.0
@@ -176,6 +183,22 @@ def test_lowering_report_flags_bad_descriptions(lib):
     assert b"num_params must equal 1 (mu)" in buf.value and b"observation scale" in buf.value
     nks.num_params, nks.obs_scale = 1, float("inf")
     assert lib.ut_lowering_report(ctypes.byref(nks), buf, len(buf)) == nat.UT_ERR_UNSUPPORTED
+
+
+
+def test_noalloc_rejects_observation_counts_past_the_bound(lib):
+    """The allocation-free entry point checks its sizes before it touches a
+    device: num_obs beyond 2^30 (where the split plan's 32-bit observation
+    bounds could overflow) is an argument error with a clear message, and so
+    is a batch past the fixed scratch."""
+    from uncertaintea_b200 import _native as nat
+    fake = ctypes.c_void_p(16)   # never dereferenced: the size checks come first
+    fn = lib.ut_glm_logjoint_gradient_noalloc
+    for n in ((1 << 30) + 1, 0, -5):
+        assert fn(fake, fake, n, 4, 0, 0.0, 1.0, 0.0, 1.0, fake, 8, fake, fake, None) == nat.UT_ERR_ARGUMENT
+        assert "num_obs must be in 1..2^30" in nat.last_error()
+    assert fn(fake, fake, 100, 64, 0, 0.0, 1.0, 0.0, 1.0, fake, 70_000, fake, fake, None) == nat.UT_ERR_ARGUMENT
+    assert "exceeds the fixed scratch" in nat.last_error()
 
 
 def test_workspace_create_validates_before_touching_device(lib):

@@ -610,3 +610,36 @@ def test_heavy_tail_oracle_on_the_reference_parity_case():
             qm[c, k] -= h
             fd = (om.logjoint_gradient_f64(qp)[0][c] - om.logjoint_gradient_f64(qm)[0][c]) / (2 * h)
             assert abs(fd - g[c, k]) <= 1e-6 * max(1.0, abs(g[c, k]))
+
+
+@pytest.mark.parametrize("case", range(7))
+def test_gradient_magnitude_bounds_the_gradient(case):
+    """The gradient magnitude (the sum of the absolute values of the terms each
+    gradient element adds up) is at least |gradient| elementwise -- the
+    triangle inequality -- and is positive wherever a term contributes."""
+    m, args, cons = _family_cases()[case]
+    low = m.lower(args, cons)
+    om = oracle.OracleModel(low)
+    q = m.initial_positions(np.random.default_rng(5), 16, args, cons, "prior")
+    t, g = om.logjoint_gradient_f64(q)
+    a = om.gradient_magnitude_f64(q)
+    ok = np.isfinite(t)
+    assert a.shape == g.shape and ok.mean() >= 0.9
+    assert np.all(a[ok] >= np.abs(g[ok]) * (1 - 1e-12))
+    assert np.all(a[ok] > 0)
+
+
+def test_gradient_magnitude_glm_matches_direct_sum():
+    """GLM: per coefficient d, sum_i |x_id| (|y_i - s_i| + s_i (1 - s_i) sum_f |q_f x_if|)
+    plus the prior's (|q_d| + |mu|) / sigma^2, restated with numpy."""
+    m, low, X, y = _glm(N=200, D=4, intercept=True)
+    q = np.random.default_rng(2).standard_normal((5, 5))
+    a = oracle.OracleModel(low).gradient_magnitude_f64(q)
+    Xa = np.hstack([np.ones((200, 1)), X])
+    for c in range(5):
+        eta = Xa @ q[c]
+        s = 1 / (1 + np.exp(-eta))
+        w = np.abs(y - s) + s * (1 - s) * (np.abs(Xa) @ np.abs(q[c]))
+        prior = (np.abs(q[c]) + np.abs([m.intercept_mu] + [m.coef_mu] * 4)) / \
+            np.array([m.intercept_sigma] + [m.coef_sigma] * 4) ** 2
+        np.testing.assert_allclose(a[c], np.abs(Xa).T @ w + prior, rtol=1e-12)

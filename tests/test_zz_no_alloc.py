@@ -10,11 +10,16 @@ stopping at the first failure has already run every other test.
 Checked here, through the C ABI on a GPU: two calls in a row each agree with
 the workspace entry point (ut_logjoint_gradient_device) on the same inputs,
 within the density tests' tolerances (logjoint 1e-5 relative, gradient 1e-5 of
-the chain's max |g|), and a batch larger than the fixed scratch is rejected.
+the chain's max |g|), and a few chains with the FP64 oracle; the second call
+leaves the device's free memory unchanged (nothing is allocated); a batch so
+large that the scratch, not the SM count, sets the observation split count
+(C * (P + 1) above half of the scratch) agrees too; and a batch larger than the
+fixed scratch is rejected.
 """
 import numpy as np
 import pytest
 
+import oracle
 from uncertaintea_b200 import _native as nat
 from uncertaintea_b200.device import DeviceBatchedWorkspace
 from uncertaintea_b200.models import BernoulliLogitGLM, logistic_regression_data
@@ -30,30 +35,56 @@ def _call(design, y, P, intercept, m, params, totals, grads):
         m.coef_mu, m.coef_sigma, nat.ptr(params), int(params.shape[0]), nat.ptr(totals), nat.ptr(grads), None)
 
 
-@pytest.mark.parametrize("intercept", [True, False])
-def test_noalloc_matches_workspace_entry_point_twice(intercept):
-    N, D, C = 20_000, 50, 300
-    X, y, _ = logistic_regression_data(N, D, 17, x_scale=0.2)
+def _check_against_workspace_and_oracle(N, D, C, intercept, seed, calls=2):
+    X, y, _ = logistic_regression_data(N, D, seed, x_scale=0.2)
     m = BernoulliLogitGLM(D, intercept=intercept)
     P = m.num_params()
     ws = DeviceBatchedWorkspace(m, C, args=(X,), constraints={"y": y})
+    om = oracle.OracleModel(ws.lowered)
     design = np.concatenate([np.ones((N, 1), np.float32), X], axis=1) if intercept else X
     d_design = torch.from_numpy(np.ascontiguousarray(design, dtype=np.float32)).cuda()
     d_y = torch.from_numpy(y.astype(np.float32)).cuda()
     rng = np.random.default_rng(3)
-    for call in range(2):
-        q = torch.from_numpy(rng.standard_normal((C, P)).astype(np.float32)).cuda()
-        ref_t, ref_g = ws.logjoint_gradient_device(q)
-        tot = torch.full((C,), float("nan"), device="cuda")
-        grd = torch.full((C, P), float("nan"), device="cuda")
-        nat.check(_call(d_design, d_y, P, intercept, m, q, tot, grd))
+    qs = [torch.from_numpy(rng.standard_normal((C, P)).astype(np.float32)).cuda() for _ in range(calls)]
+    refs = [ws.logjoint_gradient_device(q) for q in qs]
+    tot = torch.empty(C, device="cuda")
+    grd = torch.empty((C, P), device="cuda")
+    torch.cuda.synchronize()
+    for call in range(calls):
+        tot.fill_(float("nan"))
+        grd.fill_(float("nan"))
         torch.cuda.synchronize()
-        t, g, rt, rg = (x.double().cpu().numpy() for x in (tot, grd, ref_t, ref_g))
+        free_before = torch.cuda.mem_get_info()[0]
+        nat.check(_call(d_design, d_y, P, intercept, m, qs[call], tot, grd))
+        torch.cuda.synchronize()
+        free_after = torch.cuda.mem_get_info()[0]
+        if call > 0:
+            # the first call on the device did its one-time set-up; later calls
+            # leave the device's free memory exactly as it was
+            assert free_after == free_before, (call, free_before, free_after)
+        (ref_t, ref_g) = refs[call]
+        t, g, rt, rg = (x.cpu().double().numpy() for x in (tot, grd, ref_t, ref_g))
         assert np.all(np.isfinite(t)) and np.all(np.isfinite(g)), call
         assert np.max(np.abs(t - rt) / np.abs(rt)) <= 1e-5, call
         scale = np.max(np.abs(rg), axis=1)
         assert np.max(np.max(np.abs(g - rg), axis=1) / scale) <= 1e-5, call
+        idx = np.unique(np.linspace(0, C - 1, 6).astype(int))
+        t64, g64 = om.logjoint_gradient_f64(qs[call][idx].cpu().double().numpy())
+        assert np.max(np.abs(t[idx] - t64) / np.abs(t64)) <= 1e-5, call
+        assert np.max(np.max(np.abs(g[idx] - g64), axis=1) / np.max(np.abs(g64), axis=1)) <= 1e-5, call
     ws.close()
+
+
+@pytest.mark.parametrize("intercept", [True, False])
+def test_noalloc_matches_workspace_entry_point_twice(intercept):
+    _check_against_workspace_and_oracle(20_000, 50, 300, intercept, 17)
+
+
+def test_noalloc_split_count_set_by_the_scratch_limit():
+    """C * (P + 1) = 40000 * 102 > 4,194,304 / 2: the scratch holds one split's
+    partials only, so the observation split count is the scratch's, not the
+    SM-count plan's."""
+    _check_against_workspace_and_oracle(3_000, 100, 40_000, True, 19)
 
 
 def test_noalloc_rejects_batches_beyond_the_fixed_scratch():

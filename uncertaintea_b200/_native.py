@@ -58,6 +58,34 @@ class PlanDesc(ctypes.Structure):
     ]
 
 
+UT_FAMILY_PROGRAM = 8
+UT_MAX_OBS = 1 << 30
+
+UT_STEP_CHOICE, UT_STEP_DETERMINISTIC, UT_STEP_LOOP, UT_STEP_IID_NORMAL, UT_STEP_GLM_BERNOULLI_LOGIT = 1, 2, 3, 4, 5
+UT_TRANSFORM_IDENTITY, UT_TRANSFORM_LOG, UT_TRANSFORM_LOGIT = 0, 1, 2
+DISTRIBUTIONS = {
+    "normal": 1, "lognormal": 2, "exponential": 3, "gamma": 4, "laplace": 5, "cauchy": 6, "halfnormal": 7,
+    "halfcauchy": 8, "logistic": 9, "gumbel": 10, "frechet": 11, "rayleigh": 12, "inversegaussian": 13, "beta": 14,
+    "studentt": 15, "inversegamma": 16, "weibull": 17, "bernoulli": 18, "bernoullilogit": 19, "poisson": 20,
+    "geometric": 21, "negativebinomial": 22, "binomial": 23,
+}
+EXPR_OPS = {
+    "literal": 0, "slot": 1, "obs": 2, "neg": 3, "+": 4, "-": 5, "*": 6, "/": 7, "^": 8, "exp": 9, "log": 10,
+    "log1p": 11, "sqrt": 12, "abs": 13, "min": 14, "max": 15, "sin": 16, "cos": 17, "tan": 18, "tanh": 19,
+    "sinh": 20, "cosh": 21, "atan": 22, "expm1": 23,
+}
+
+
+class ExprNode(ctypes.Structure):
+    _fields_ = [("op", c_int32), ("a", c_int32), ("b", c_int32), ("reserved", c_int32), ("value", c_double)]
+
+
+class ProgramStep(ctypes.Structure):
+    _fields_ = [("kind", c_int32), ("dist", c_int32), ("arg", c_int32 * 4), ("value_source", c_int32),
+                ("obs_offset", c_int32), ("transform", c_int32), ("binding_slot", c_int32), ("count", c_int32),
+                ("width", c_int32), ("body", c_int32), ("iterator_slot", c_int32), ("iterator_start", c_int32)]
+
+
 class MeadsBuffers(ctypes.Structure):
     _fields_ = [(n, c_void_p) for n in ("position", "gradient", "logjoint", "momentum", "slice", "accept_prob",
                                          "energy", "energy_error", "accepted", "divergent", "integration_steps",
@@ -133,6 +161,11 @@ SIGNATURES = [
     ("ut_workspace_destroy", c_int32, [c_void_p]),
     ("ut_workspace_info", c_int32, [c_void_p, POINTER(c_int32), POINTER(c_int32)]),
     ("ut_workspace_path", c_int32, [c_void_p]),
+    ("ut_program_report", c_int32,
+     [POINTER(ProgramStep), c_int32, POINTER(ExprNode), c_int32, c_int32, c_int32, c_int64, c_char_p, c_size_t]),
+    ("ut_workspace_create_program", c_int32,
+     [POINTER(ProgramStep), c_int32, POINTER(ExprNode), c_int32, c_int32, c_int32, c_void_p, c_int64, c_int32,
+      c_int32, POINTER(c_void_p)]),
     ("ut_workspace_check", c_int32, [c_void_p, c_void_p]),
     ("ut_logjoint", c_int32, [c_void_p, c_void_p, c_void_p]),
     ("ut_logjoint_gradient", c_int32, [c_void_p, c_void_p, c_void_p, c_void_p]),

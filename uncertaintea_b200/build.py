@@ -3,7 +3,8 @@
 The C ABI and its kernels are compiled by nvcc for sm_100a only, from
 csrc/ut_api.cu, csrc/ut_noalloc.cu (the allocation-free entry point, whose
 kernels are private to its file), csrc/ut_surrogate.cu (the learned
-gradient surrogate) and csrc/ut_multi.cu (many models in one batched launch).  Run: python -m uncertaintea_b200.build [--force]
+gradient surrogate) and csrc/ut_multi.cu (many models in one batched launch),
+each in its own process, then linked into one shared library.  Run: python -m uncertaintea_b200.build [--force]
 """
 from __future__ import annotations
 
@@ -33,18 +34,28 @@ def sources():
                   + [os.path.join(ROOT, "include", "ut_b200.h")])
 
 
+UNITS = ["ut_api.cu", "ut_noalloc.cu", "ut_surrogate.cu", "ut_multi.cu"]
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     newest = max(os.path.getmtime(s) for s in sources())
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= newest:
         return LIB
-    cmd = [nvcc()] + NVCC_FLAGS + ["-o", LIB + ".tmp", os.path.join(HERE, "csrc", "ut_api.cu"),
-                                   os.path.join(HERE, "csrc", "ut_noalloc.cu"),
-                                   os.path.join(HERE, "csrc", "ut_surrogate.cu"),
-                                   os.path.join(HERE, "csrc", "ut_multi.cu")]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    subprocess.run(cmd, check=True)
+    # each translation unit compiles in its own nvcc process (the kernel
+    # template instantiations make ut_api.cu the longest), then one link
+    import concurrent.futures as cf
+    objs = [os.path.join(HERE, "csrc", u[:-3] + ".o") for u in UNITS]
+    flags = [f for f in NVCC_FLAGS if f != "-shared"] + (["-Xptxas=-v"] if verbose else [])
+
+    def compile_unit(i):
+        subprocess.run([nvcc()] + flags + ["-c", "-o", objs[i], os.path.join(HERE, "csrc", UNITS[i])], check=True)
+
+    with cf.ThreadPoolExecutor(len(UNITS)) as pool:
+        list(pool.map(compile_unit, range(len(UNITS))))
+    subprocess.run([nvcc()] + ARCH_FLAGS + ["-shared", "-o", LIB + ".tmp"] + objs, check=True)
     os.replace(LIB + ".tmp", LIB)
+    for o in objs:
+        os.remove(o)
     return LIB
 
 

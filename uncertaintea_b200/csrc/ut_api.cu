@@ -147,6 +147,9 @@ std::string plan_issues(const ut_plan_desc* p) {
     std::string s;
     auto add = [&](const std::string& m) { s += (s.empty() ? "" : "\n") + m; };
     if (!p) { add("null kernel description"); return s; }
+    // the kernels' observation index arithmetic is 32-bit: an observation
+    // count of at most 2^30 keeps every split end and tile bound in range
+    if (p->num_obs > UT_MAX_OBS) add("num_obs must be <= 2^30 (1073741824)");
     if (p->family == UT_FAMILY_GLM_BERNOULLI_LOGIT) {
         if (p->num_coefs < 1) add("GLM needs at least one covariate (num_coefs >= 1)");
         if (p->has_intercept != 0 && p->has_intercept != 1) add("has_intercept must be 0 or 1");
@@ -223,6 +226,14 @@ int32_t need_device() {
             KERNEL(kFamLgn, 1, 1, __VA_ARGS__);                                                              \
         } else if ((ws)->dm.family == kFamHt) {                                                              \
             KERNEL(kFamHt, 1, 1, __VA_ARGS__);                                                               \
+        } else if ((ws)->dm.family == kFamProg) {                                                            \
+            switch ((ws)->K) {                                                                               \
+                case 1: KERNEL(kFamProg, 1, 1, __VA_ARGS__); break;                                          \
+                case 2: KERNEL(kFamProg, 2, 1, __VA_ARGS__); break;                                          \
+                case 3: KERNEL(kFamProg, 3, 1, __VA_ARGS__); break;                                          \
+                case 4: KERNEL(kFamProg, 4, 1, __VA_ARGS__); break;                                          \
+                default: KERNEL(kFamProg, 8, 1, __VA_ARGS__); break;                                         \
+            }                                                                                                \
         } else {                                                                                             \
             switch ((ws)->K) {                                                                               \
                 case 1: KERNEL(kFamHier, 1, 1, __VA_ARGS__); break;                                          \
@@ -744,6 +755,95 @@ int32_t ut_workspace_create(const ut_plan_desc* plan, const float* observed, int
     return UT_OK;
 }
 
+int32_t ut_program_report(const ut_program_step* steps, int32_t num_steps, const ut_expr_node* nodes,
+                          int32_t num_nodes, int32_t num_slots, int32_t num_params, int64_t observed_rows,
+                          char* issues, size_t len) {
+    ProgCompiled pc;
+    const std::string msg = ProgCompiler(steps, num_steps, nodes, num_nodes, num_slots, num_params, observed_rows).run(&pc);
+    if (issues && len) {
+        const size_t n = std::min(len - 1, msg.size());
+        memcpy(issues, msg.data(), n);
+        issues[n] = 0;
+    }
+    return msg.empty() ? UT_OK : UT_ERR_UNSUPPORTED;
+}
+
+int32_t ut_workspace_create_program(const ut_program_step* steps, int32_t num_steps, const ut_expr_node* nodes,
+                                    int32_t num_nodes, int32_t num_slots, int32_t num_params, const float* observed,
+                                    int64_t observed_rows, int32_t batch_size, int32_t precision_bits,
+                                    ut_workspace** out) {
+    if (!out) return fail(UT_ERR_ARGUMENT, "null output handle");
+    *out = nullptr;
+    if (precision_bits != 32)
+        return fail(UT_ERR_PRECISION,
+                    "the B200 backend does not support Float%d arithmetic; request precision=Float32 instead",
+                    (int)precision_bits);
+    ProgCompiled pc;
+    const std::string issues =
+        ProgCompiler(steps, num_steps, nodes, num_nodes, num_slots, num_params, observed_rows).run(&pc);
+    if (!issues.empty())
+        return fail(UT_ERR_UNSUPPORTED, "kernel description cannot be lowered to the device path:\n%s", issues.c_str());
+    if (batch_size < 1) return fail(UT_ERR_ARGUMENT, "batch size must be >= 1, got %d", (int)batch_size);
+    if (observed_rows > 0 && !observed) return fail(UT_ERR_ARGUMENT, "null observation buffer");
+    int32_t rc = need_device();
+    if (rc) return rc;
+
+    ut_workspace* ws = new ut_workspace();
+    memset(&ws->plan, 0, sizeof(ws->plan));
+    ws->plan.family = UT_FAMILY_PROGRAM;
+    ws->plan.num_params = num_params;
+    ws->plan.num_obs = (int32_t)observed_rows;
+    ws->P = num_params;
+    ws->C = batch_size;
+    ws->N = (int)observed_rows;
+    cudaGetDevice(&ws->device);
+    auto bail = [&](int32_t code) {
+        ut_workspace_destroy(ws);
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(UT_ERR_CUDA, "cudaStreamCreate failed"));
+    DevModel& dm = ws->dm;
+    memset(&dm, 0, sizeof(dm));
+    dm.family = kFamProg;
+    dm.P = num_params;
+    ws->K = inst_k(num_params);
+    ws->path = kPathWarp;
+    ProgModel& m = dm.prog;
+    m.nsteps = (int)pc.steps.size();
+    m.nnodes = (int)pc.nodes.size();
+    m.nslots = pc.nslots;
+    m.nobs = (int)observed_rows;
+    m.P = num_params;
+    m.pp = ((num_params + 31) / 32) * 32;
+    dm.Ppad = prog_scratch_floats(num_params, pc.nslots);
+    float* d_obs = nullptr;
+    PStep* d_steps = nullptr;
+    PNode* d_nodes = nullptr;
+    if ((rc = dalloc(ws, &d_obs, (size_t)std::max<int64_t>(observed_rows, 1)))) return bail(rc);
+    if ((rc = dalloc(ws, &d_steps, pc.steps.size()))) return bail(rc);
+    if ((rc = dalloc(ws, &d_nodes, std::max<size_t>(pc.nodes.size(), 1)))) return bail(rc);
+    if (observed_rows > 0)
+        UT_CUDA(cudaMemcpy(d_obs, observed, sizeof(float) * (size_t)observed_rows, cudaMemcpyHostToDevice));
+    UT_CUDA(cudaMemcpy(d_steps, pc.steps.data(), sizeof(PStep) * pc.steps.size(), cudaMemcpyHostToDevice));
+    if (!pc.nodes.empty())
+        UT_CUDA(cudaMemcpy(d_nodes, pc.nodes.data(), sizeof(PNode) * pc.nodes.size(), cudaMemcpyHostToDevice));
+    m.obs = d_obs;
+    m.steps = d_steps;
+    m.nodes = d_nodes;
+    ws->d_y = d_obs;
+    // the program and its observations go to shared memory when they fit beside
+    // the per-warp scratch of the widest launch
+    const size_t staged = ((size_t)(observed_rows + 3) / 4) * 4 + pc.nodes.size() * (sizeof(PNode) / 4) +
+                          pc.steps.size() * (sizeof(PStep) / 4);
+    dm.stage = (staged * 4 + (size_t)kWarpsDensity * dm.Ppad * 4) <= kSmemBudget ? 1 : 0;
+    dm.staged_floats = dm.stage ? (int)(((staged + 3) / 4) * 4) : 0;
+    if ((size_t)dm.staged_floats * 4 + (size_t)kWarpsDensity * dm.Ppad * 4 > kSmemBudget)
+        return bail(fail(UT_ERR_UNSUPPORTED, "the program's per-chain scratch does not fit shared memory"));
+    *out = ws;
+    return UT_OK;
+}
+
 int32_t ut_workspace_destroy(ut_workspace* ws) {
     if (!ws) return UT_OK;
     for (void* p : ws->allocations) cudaFree(p);
@@ -839,6 +939,23 @@ extern "C" int32_t ut_internal_tc_live_split(int32_t num_obs, int32_t num_chains
     p.nact = live >= 0 ? &n : nullptr;
     const TcSplit r = tc_split(p);
     out[0] = r.nt; out[1] = r.S; out[2] = r.tps; out[3] = r.Cl;
+    return UT_OK;
+}
+
+// Test hook (not part of the C ABI in ut_b200.h): one tensor-core evaluation of
+// only the first *d_live chains of d_params -- the live-chain launch masked NUTS
+// makes at every leaf, with its observation re-split -- on device buffers.
+// Rows of chains at or past *d_live are left untouched.  d_grads may be NULL
+// (logjoint only).  UT_ERR_UNSUPPORTED when the workspace is not on the
+// tensor-core path.
+extern "C" int32_t ut_internal_tc_glm_live(ut_workspace* ws, const float* d_params, float* d_totals, float* d_grads,
+                                           const int32_t* d_live, void* stream) {
+    int32_t rc = check_ws(ws);
+    if (rc) return rc;
+    if (!ws->tc.enabled) return fail(UT_ERR_UNSUPPORTED, "the workspace is not on the tensor-core path");
+    if (!d_params || !d_totals || !d_live) return fail(UT_ERR_ARGUMENT, "null device buffer");
+    if (tc_glm_launch(ws->tc, d_params, d_totals, d_grads, (cudaStream_t)stream, d_live) != cudaSuccess)
+        return fail(UT_ERR_CUDA, "tensor-core GLM launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     return UT_OK;
 }
 

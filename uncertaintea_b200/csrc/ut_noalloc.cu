@@ -115,7 +115,7 @@ extern "C" int32_t ut_glm_logjoint_gradient_noalloc(const float* d_design, const
     if (num_params < 1 || num_params > ut::kGlmMaxF)
         return noalloc_fail(UT_ERR_ARGUMENT, "num_params must be in 1..%d, got %d", ut::kGlmMaxF, (int)num_params);
     if (has_intercept != 0 && has_intercept != 1) return noalloc_fail(UT_ERR_ARGUMENT, "has_intercept must be 0 or 1");
-    if (num_obs < 1 || num_obs > INT32_MAX) return noalloc_fail(UT_ERR_ARGUMENT, "num_obs must be in 1..2^31-1");
+    if (num_obs < 1 || num_obs > UT_MAX_OBS) return noalloc_fail(UT_ERR_ARGUMENT, "num_obs must be in 1..2^30");
     if (num_chains < 1) return noalloc_fail(UT_ERR_ARGUMENT, "num_chains must be >= 1, got %d", (int)num_chains);
     if (!(coef_sigma > 0.0) || (has_intercept && !(intercept_sigma > 0.0)))
         return noalloc_fail(UT_ERR_ARGUMENT, "prior scales must be > 0");
@@ -134,14 +134,18 @@ extern "C" int32_t ut_glm_logjoint_gradient_noalloc(const float* d_design, const
     int32_t rc = setup_device(dev, &scratch, &sms);
     if (rc) return rc;
 
+    // The split plan in 64-bit arithmetic: S observation splits of whole chunks,
+    // at most 3 CTAs per SM in all and at most what the scratch holds
+    // (S * C * (P + 1) floats).  With N <= 2^30 every value fits the kernels' int.
     const int N = (int)num_obs, F = num_params, C = num_chains;
     const int ctiles = (C + ut::kGlmCT - 1) / ut::kGlmCT;
-    const int chunks = (N + ut::kGlmOT - 1) / ut::kGlmOT;
-    int S = std::max(1, std::min(chunks, (3 * sms + ctiles - 1) / ctiles));
-    S = std::max(1, std::min<int>(S, (int)(kNoAllocScratchFloats / per_split)));
-    const int per = (chunks + S - 1) / S;
-    const int obs_per_split = per * ut::kGlmOT;
-    S = (N + obs_per_split - 1) / obs_per_split;
+    const int64_t chunks = (num_obs + ut::kGlmOT - 1) / ut::kGlmOT;
+    int64_t S64 = std::max<int64_t>(1, std::min<int64_t>(chunks, (3 * (int64_t)sms + ctiles - 1) / ctiles));
+    S64 = std::max<int64_t>(1, std::min<int64_t>(S64, (int64_t)(kNoAllocScratchFloats / per_split)));
+    const int64_t per = (chunks + S64 - 1) / S64;
+    const int64_t ops64 = per * ut::kGlmOT;
+    const int obs_per_split = (int)ops64;
+    const int S = (int)((num_obs + ops64 - 1) / ops64);
 
     ut::GlmTiledArgs a;
     a.Xa = d_design; a.y = d_y; a.params = d_params;

@@ -20,6 +20,11 @@
 // owning 8 of a tile's observation columns and a quarter of the gradient columns.
 // Pipelines: 3 X stages, 2 H/R TMEM buffers, so GEMM1 of tile t+1 runs on the
 // tensor cores while the epilogue of tile t runs on the CUDA cores / SFUs.
+// The tensor pipe stays busy while the epilogue's round trip (GEMM1(t) done ->
+// R(t) in TMEM) is shorter than GEMM2(t-1) + GEMM1(t+1), so the epilogue keeps
+// that path short: one mbarrier arrival per warp (not per thread), and the
+// periodic drain of the gradient accumulator rides on the next tile's epilogue
+// instead of stalling the MMA issuer.
 //
 // Every mbarrier wait is bounded (~2^31 clocks).  A wait that gives up sets the
 // error word, the role stops issuing, all threads meet at the final barrier and
@@ -43,6 +48,7 @@ constexpr int kTcObs = 32;              // observations per tile (N of GEMM1, K 
 constexpr int kTcMaxFp = 128;           // padded feature count the TMEM plan holds (3 Fp + 128 <= 512)
 constexpr int kTcThreads = 576;         // warp 0 TMA, warp 1 MMA, warps 2-17 epilogue
 constexpr int kTcEpiThreads = 512;
+constexpr int kTcEpiWarps = kTcEpiThreads / 32;   // arrivals per epilogue barrier phase
 constexpr long long kTcWaitClocks = 1ll << 31;
 // Per-CTA set-up (barriers, TMEM allocation, theta into TMEM, pipeline fill) in
 // units of one 32-observation tile's time at one CTA per SM: ~27 us vs ~2.4 us
@@ -252,6 +258,9 @@ constexpr int kTcStages = 3;
 constexpr int kTcDrainTiles = 4;   // observation tiles per TMEM gradient accumulation run
 
 __host__ __device__ inline int tc_kblocks(int Fp) { return Fp / 8; }
+// K-blocks GEMM1 needs: the features rounded up to 8 (the TF32 MMA's K), not to
+// the 16 of Fp (GEMM2's N); the blocks past it hold zero padding.
+__host__ __device__ inline int tc_kblocks_used(int F) { return (F + 7) / 8; }
 __host__ __device__ inline int tc_matoms(int Fp) { return (Fp + 31) / 32; }
 __host__ __device__ inline int tc_xk_bytes(int Fp) { return tc_kblocks(Fp) * kTcObs * 32; }
 __host__ __device__ inline int tc_xm_bytes(int Fp) { return tc_matoms(Fp) * kTcObs * 128; }
@@ -313,7 +322,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int Fp = p.Fp;
-    const int KB = tc_kblocks(Fp), MA = tc_matoms(Fp);
+    const int KB1 = tc_kblocks_used(p.F), MA = tc_matoms(Fp);
     const int xk_bytes = tc_xk_bytes(Fp), xm_bytes = tc_xm_bytes(Fp), stage_bytes = tc_stage_bytes(Fp);
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kTcStages * stage_bytes);
     uint64_t* bar_xfull = bars;                    // [3]
@@ -322,7 +331,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     uint64_t* bar_rfull = bars + 8;                // [2]
     uint64_t* bar_d2full = bars + 10;
     uint64_t* bar_theta = bars + 11;
-    uint64_t* bar_d2empty = bars + 12;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 13);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -344,11 +352,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
         for (int i = 0; i < 2; ++i) {
             mbar_init(bar_d1full + i, 1);
-            mbar_init(bar_rfull + i, kTcEpiThreads);
+            mbar_init(bar_rfull + i, kTcEpiWarps);
         }
         mbar_init(bar_d2full, 1);
-        mbar_init(bar_theta, kTcEpiThreads);
-        mbar_init(bar_d2empty, kTcEpiThreads);
+        mbar_init(bar_theta, kTcEpiWarps);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) tmem_alloc(tmem_slot, 512);
@@ -365,9 +372,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 const int s = i % kTcStages;
                 if (i >= kTcStages && !mbar_wait(bar_xempty + s, ((i / kTcStages) - 1) & 1, p.err)) break;
                 uint8_t* st = smem + s * stage_bytes;
-                mbar_expect_tx(bar_xfull + s, stage_bytes - 1024 + kTcObs * 4);
+                mbar_expect_tx(bar_xfull + s, 2 * KB1 * (kTcObs * 32) + 2 * xm_bytes + kTcObs * 4);
                 const int n0 = (t_begin + i) * kTcObs;
-                for (int kb = 0; kb < KB; ++kb) {
+                for (int kb = 0; kb < KB1; ++kb) {
                     tma_load_2d(st + kb * (kTcObs * 32), &map_xk_hi, bar_xfull + s, kb * 8, n0);
                     tma_load_2d(st + xk_bytes + kb * (kTcObs * 32), &map_xk_lo, bar_xfull + s, kb * 8, n0);
                 }
@@ -389,14 +396,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             // GEMM2 of tile j.  The G^T accumulator in TMEM restarts every
             // kTcDrainTiles tiles: the epilogue drains it into FP32 registers
             // (round-to-nearest adds) so only a short run of tensor-core
-            // accumulations ever lands in one TMEM value.
-            auto gemm2 = [&](int j) -> bool {
+            // accumulations ever lands in one TMEM value.  The restart needs no
+            // wait of its own: GEMM2(j) is issued after R(j) is in TMEM, and the
+            // epilogue drains the previous group before it signals R(j).
+            auto gemm2 = [&](int j) {
                 const int s = j % kTcStages, b = j & 1;
-                const int group = j / kTcDrainTiles;
-                if (j % kTcDrainTiles == 0 && group > 0) {
-                    if (!mbar_wait(bar_d2empty, (group - 1) & 1, p.err)) return false;
-                    tc_fence_after();
-                }
                 const uint32_t xm = smem_u32(smem + s * stage_bytes + 2 * xk_bytes);
                 const uint32_t rhi = tmem + col_buf + b * 64, rlo = rhi + 32;
                 for (int kk = 0; kk < kTcObs / 8; ++kk) {
@@ -408,7 +412,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     mma_ts(tmem + col_d2, rhi + kk * 8, bl, id2, 1u);
                 }
                 if ((j + 1) % kTcDrainTiles == 0 || j == ntiles - 1) mma_commit(bar_d2full);
-                return true;
             };
             for (int i = 0; ok && i < ntiles; ++i) {
                 const int s = i % kTcStages, b = i & 1;
@@ -416,7 +419,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 tc_fence_after();
                 const uint32_t xk = smem_u32(smem + s * stage_bytes);
                 const uint32_t d1 = tmem + col_buf + b * 64;
-                for (int kb = 0; kb < KB; ++kb) {
+                for (int kb = 0; kb < KB1; ++kb) {
                     const uint64_t bh = sdesc_sw32(xk + kb * (kTcObs * 32), 16, 256);
                     const uint64_t bl = sdesc_sw32(xk + xk_bytes + kb * (kTcObs * 32), 16, 256);
                     mma_ts(d1, tmem + col_thi + kb * 8, bh, id1, kb > 0 ? 1u : 0u);
@@ -428,7 +431,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     const int j = i - 1;
                     if (!mbar_wait(bar_rfull + (j & 1), (j >> 1) & 1, p.err)) { ok = false; break; }
                     tc_fence_after();
-                    if (p.want_grad && !gemm2(j)) { ok = false; break; }
+                    if (p.want_grad) gemm2(j);
                     mma_commit(bar_xempty + (j % kTcStages));
                 }
             }
@@ -443,6 +446,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
     } else {
         // ---------------- epilogue: thread = chain (TMEM lane) ----------------
+        // Every wait's verdict is made warp-uniform (a lane that gave up makes
+        // the whole warp give up), so the warp's lanes always meet at the same
+        // __syncwarp and the single-lane arrivals stay matched.
+        auto warp_wait = [&](uint64_t* bar, uint32_t parity) -> bool {
+            const bool r = mbar_wait(bar, parity, p.err);
+            return __all_sync(0xffffffffu, r);
+        };
         const int q = warp & 3;                 // TMEM lane quadrant
         const int slot = (warp - 2) >> 2;       // which quarter of the columns this warp owns
         const int c_local = q * 32 + lane;
@@ -464,19 +474,36 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
         asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
         tc_fence_before();
-        mbar_arrive(bar_theta);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(bar_theta);
 
         float ll = 0.0f;
         constexpr int kOwnCols = kTcMaxFp / 4;     // gradient columns owned by this warp
         float gacc[kOwnCols];
 #pragma unroll
         for (int f = 0; f < kOwnCols; ++f) gacc[f] = 0.0f;
+        // Drain group g (tiles g*kTcDrainTiles ...) of the G^T accumulator into registers.
+        auto drain = [&](int g) -> bool {
+            if (!warp_wait(bar_d2full, g & 1)) return false;
+            tc_fence_after();
+#pragma unroll
+            for (int k = 0; k < kOwnCols / 16; ++k) {
+                const int f0 = 16 * slot + 64 * k;
+                if (f0 < Fp) {
+                    float gv[16];
+                    tmem_ld16(tmem + lane_off + col_d2 + f0, gv);
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) gacc[16 * k + j] += gv[j];
+                }
+            }
+            return true;
+        };
         bool ok = ntiles > 0;
         for (int i = 0; ok && i < ntiles; ++i) {
             const int b = i & 1, s = i % kTcStages;
             // the y tile arrived with the X stage; d1_full(i) implies GEMM1(i) consumed stage s,
             // which the producer only refills after GEMM2(i) -- after this tile's r_full
-            if (!mbar_wait(bar_d1full + b, (i >> 1) & 1, p.err)) { ok = false; break; }
+            if (!warp_wait(bar_d1full + b, (i >> 1) & 1)) { ok = false; break; }
             tc_fence_after();
             const int n0 = (t_begin + i) * kTcObs + 8 * slot;
             const float* ys = reinterpret_cast<const float*>(smem + s * stage_bytes + 2 * xk_bytes + 2 * xm_bytes) +
@@ -497,7 +524,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 const float e = __expf(-fabsf(hv));
                 const float onepe = 1.0f + e;
                 const float lpe = fmaxf(hv, 0.0f) + __logf(onepe);
-                const float inv = __frcp_rn(onepe);
+                const float inv = __fdividef(1.0f, onepe);
                 const float sig = hv >= 0.0f ? inv : e * inv;
                 const bool sup = (yv == 0.0f) | (yv == 1.0f);
                 ll += live ? (sup ? yv * hv - lpe : -INFINITY) : 0.0f;
@@ -509,26 +536,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             tmem_st8(d1, rh);        // R_hi overwrites the consumed H^T columns
             tmem_st8(d1 + 32, rl);
             asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+            // the group that ended with tile i-1: GEMM2(i-1) ran while this tile's
+            // residuals were computed; draining it before R(i) is signalled frees
+            // the accumulator for GEMM2(i)
+            if (p.want_grad && i > 0 && i % kTcDrainTiles == 0 && !drain(i / kTcDrainTiles - 1)) { ok = false; break; }
             tc_fence_before();
-            mbar_arrive(bar_rfull + b);
-            if (p.want_grad && ((i + 1) % kTcDrainTiles == 0 || i == ntiles - 1)) {
-                // drain the G^T accumulator of this group of tiles into registers
-                if (!mbar_wait(bar_d2full, (i / kTcDrainTiles) & 1, p.err)) { ok = false; break; }
-                tc_fence_after();
-#pragma unroll
-                for (int k = 0; k < kOwnCols / 16; ++k) {
-                    const int f0 = 16 * slot + 64 * k;
-                    if (f0 < Fp) {
-                        float g[16];
-                        tmem_ld16(tmem + lane_off + col_d2 + f0, g);
-#pragma unroll
-                        for (int j = 0; j < 16; ++j) gacc[16 * k + j] += g[j];
-                    }
-                }
-                tc_fence_before();
-                mbar_arrive(bar_d2empty);
-            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(bar_rfull + b);
         }
+        if (ok && p.want_grad) ok = drain((ntiles - 1) / kTcDrainTiles);
         // combine the four column quarters' log-likelihoods through shared memory
         float* ll_part = reinterpret_cast<float*>(tmem_slot + 4);   // [4][128]
         ll_part[slot * kTcChains + c_local] = ll;

@@ -6,10 +6,11 @@
 #pragma once
 
 #include "ut_models.cuh"
+#include "ut_program.cuh"
 
 namespace ut {
 
-enum Family : int { kFamGlm = 1, kFamHier = 2, kFamGauss = 3, kFamBern = 4, kFamLgn = 5, kFamHt = 6 };
+enum Family : int { kFamGlm = 1, kFamHier = 2, kFamGauss = 3, kFamBern = 4, kFamLgn = 5, kFamHt = 6, kFamProg = 7 };
 
 struct DevModel {
     int family;
@@ -23,6 +24,7 @@ struct DevModel {
     BernModel bern;
     LgnModel lgn;
     HtModel ht;
+    ProgModel prog;   // the step program (ut_program.cuh)
 };
 
 // Copies the model's observation data into shared memory (when dm.stage) and
@@ -58,6 +60,22 @@ __device__ __forceinline__ void stage_model(DevModel& dm, float* smem) {
         for (int i = threadIdx.x; i < dm.bern.N; i += blockDim.x) smem[i] = dm.bern.z[i];
         __syncthreads();
         dm.bern.z = smem;
+    } else if constexpr (FAM == kFamProg) {
+        // observations, then the compiled nodes and steps (all 4-byte words)
+        ProgModel& m = dm.prog;
+        float* o = smem;
+        PNode* nd = reinterpret_cast<PNode*>(smem + ((m.nobs + 3) / 4) * 4);
+        PStep* st = reinterpret_cast<PStep*>(nd + m.nnodes);
+        for (int i = threadIdx.x; i < m.nobs; i += blockDim.x) o[i] = m.obs[i];
+        const int nw = m.nnodes * (int)(sizeof(PNode) / 4), sw = m.nsteps * (int)(sizeof(PStep) / 4);
+        for (int i = threadIdx.x; i < nw; i += blockDim.x)
+            reinterpret_cast<int*>(nd)[i] = reinterpret_cast<const int*>(m.nodes)[i];
+        for (int i = threadIdx.x; i < sw; i += blockDim.x)
+            reinterpret_cast<int*>(st)[i] = reinterpret_cast<const int*>(m.steps)[i];
+        __syncthreads();
+        m.obs = o;
+        m.nodes = nd;
+        m.steps = st;
     } else {
         const int N = dm.hier.N, J = dm.hier.J;
         float* ys = smem;
@@ -86,6 +104,7 @@ __device__ __forceinline__ float eval_lj(const DevModel& dm, const float (&q)[K]
     else if constexpr (FAM == kFamBern) return bern_lj_grad<K>(dm.bern, q, g, want_grad);
     else if constexpr (FAM == kFamLgn) return lgn_lj_grad<K>(dm.lgn, q, g, want_grad);
     else if constexpr (FAM == kFamHt) return ht_lj_grad<K>(dm.ht, q, g, want_grad);
+    else if constexpr (FAM == kFamProg) return prog_lj_grad<K>(dm.prog, q, g, qs, want_grad);
     else return hier_lj_grad<K>(dm.hier, dm.P, q, g, want_grad);
 }
 
