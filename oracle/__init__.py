@@ -39,6 +39,7 @@ def load():
                                                 c_void_p, c_int32]),
         "orc_gradient_magnitude_f64": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p,
                                                  c_int32]),
+        "orc_program_set": (None, [c_void_p, c_int32, c_void_p, c_int32, c_int32, c_int32]),
         "orc_max_threads": (c_int32, []),
         "orc_meads_max_eig": (c_double, [c_void_p, c_int32, c_int32]),
         "orc_meads_iteration_f32": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32,
@@ -160,6 +161,11 @@ class OracleModel:
         self.ls = np.ascontiguousarray(lowered.loop_starts, dtype=np.int32)
 
     def _common(self):
+        prog = getattr(self.lowered, "program", None)
+        if prog is not None:  # a step program: the oracle walks the one set last
+            lw = self.lowered
+            load().orc_program_set(ctypes.addressof(lw.steps), len(prog.steps), ctypes.addressof(lw.nodes),
+                                   len(prog.nodes), prog.num_slots, prog.num_params)
         return (ctypes.byref(self.plan), _p(self.obs), _p(self.tc) if self.tc.size else None,
                 _p(self.ls) if self.ls.size else None)
 

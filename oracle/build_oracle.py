@@ -1,6 +1,6 @@
 """Build recipe of the CPU oracle (test infrastructure only).
 
-Compiles oracle/oracle.cpp and oracle/oracle_mlp.cpp into
+Compiles oracle/oracle.cpp, oracle/oracle_mlp.cpp and oracle/oracle_program.cpp into
 oracle/_build/liboracle.so with g++ and OpenMP.  Run: python oracle/build_oracle.py
 """
 from __future__ import annotations
@@ -15,8 +15,9 @@ LIB = os.path.join(OUT_DIR, "liboracle.so")
 
 
 def build(force: bool = False) -> str:
-    srcs = [os.path.join(HERE, "oracle.cpp"), os.path.join(HERE, "oracle_mlp.cpp")]
-    deps = srcs + [os.path.join(HERE, "oracle_mlp.h"), os.path.join(HERE, "..", "include", "ut_b200.h")]
+    srcs = [os.path.join(HERE, "oracle.cpp"), os.path.join(HERE, "oracle_mlp.cpp"), os.path.join(HERE, "oracle_program.cpp")]
+    deps = srcs + [os.path.join(HERE, "oracle_mlp.h"), os.path.join(HERE, "oracle_program.h"),
+                   os.path.join(HERE, "..", "include", "ut_b200.h")]
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(d) for d in deps):
         return LIB
     os.makedirs(OUT_DIR, exist_ok=True)

@@ -34,6 +34,7 @@
 
 #include "../include/ut_b200.h"
 #include "oracle_mlp.h"
+#include "oracle_program.h"
 
 namespace {
 
@@ -140,6 +141,7 @@ template <class T> inline T gamma_logpdf(T shape, T rate, T x) {
 // ---------------------------------------------------------------------------
 struct ModelData {
     ut_plan_desc plan;
+    oracle_program::Program prog;  // UT_FAMILY_PROGRAM: the step program (y holds its staged rows)
     std::vector<double> X;   // N x D row-major (observation-major), GLM
     std::vector<double> y;   // N
     std::vector<double> sig; // J, HIER
@@ -159,6 +161,9 @@ ModelData make_model(const ut_plan_desc* plan, const float* observed, const int3
             for (int d = 0; d < D; ++d) m.X[(size_t)i * D + d] = observed[(size_t)i * (D + 1) + d];
             m.y[i] = observed[(size_t)i * (D + 1) + D];
         }
+    } else if (plan->family == UT_FAMILY_PROGRAM) {
+        m.prog = oracle_program::current();
+        m.y.assign(observed, observed + N);
     } else if (plan->family == UT_FAMILY_NORMAL_LOCATION_SCALE || plan->family == UT_FAMILY_BERNOULLI_BETA ||
                plan->family == UT_FAMILY_LOGNORMAL_GAMMA_NORMAL || plan->family == UT_FAMILY_STUDENTT_HEAVY_TAIL ||
                plan->family == UT_FAMILY_NORMAL_KNOWN_SCALE) {
@@ -388,6 +393,13 @@ W ht_logjoint_grad(const ModelData& m, const T* q, T* g) {
 
 template <class T, class W>
 W logjoint_grad(const ModelData& m, const T* q, T* g) {
+    if (m.plan.family == UT_FAMILY_PROGRAM) {  // float64 plan walk, cast to T
+        const int P = m.plan.num_params;
+        std::vector<double> qd(q, q + P), gd(g ? P : 0);
+        const double v = oracle_program::logjoint_grad(m.prog, m.y, qd.data(), g ? gd.data() : nullptr);
+        if (g) for (int k = 0; k < P; ++k) g[k] = (T)gd[k];
+        return (W)v;
+    }
     if (m.plan.family == UT_FAMILY_STUDENTT_HEAVY_TAIL) return ht_logjoint_grad<T, W>(m, q, g);
     if (m.plan.family == UT_FAMILY_LOGNORMAL_GAMMA_NORMAL) return lgn_logjoint_grad<T, W>(m, q, g);
     if (m.plan.family == UT_FAMILY_BERNOULLI_BETA) return bern_logjoint_grad<T, W>(m, q, g);
@@ -413,6 +425,9 @@ void grad_magnitude(const ModelData& m, const double* q, double* a) {
     const int P = p.num_params;
     for (int k = 0; k < P; ++k) a[k] = 0.0;
     switch (p.family) {
+    case UT_FAMILY_PROGRAM:  // per row: the sum over the terms of |d term / d row|
+        oracle_program::logjoint_grad(m.prog, m.y, q, nullptr, a);
+        break;
     case UT_FAMILY_GLM_BERNOULLI_LOGIT: {
         const int N = p.num_obs, D = p.num_coefs, off = p.has_intercept ? 1 : 0;
         const double al = off ? q[0] : 0.0;
@@ -867,6 +882,17 @@ int orc_gradient_magnitude_f64(const ut_plan_desc* plan, const float* observed, 
 #pragma omp parallel for schedule(static)
     for (int c = 0; c < C; ++c) grad_magnitude(m, params + (size_t)c * P, out + (size_t)c * P);
     return 0;
+}
+
+// The step program that models of family UT_FAMILY_PROGRAM use from here on
+// (their plan carries num_params and the staged row count as num_obs).
+void orc_program_set(const ut_program_step* steps, int32_t num_steps, const ut_expr_node* nodes, int32_t num_nodes,
+                     int32_t num_slots, int32_t num_params) {
+    oracle_program::Program& p = oracle_program::current();
+    p.steps.assign(steps, steps + num_steps);
+    p.nodes.assign(nodes, nodes + num_nodes);
+    p.nslots = num_slots;
+    p.P = num_params;
 }
 
 int orc_max_threads(void) { return set_threads(0); }

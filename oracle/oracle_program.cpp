@@ -225,6 +225,12 @@ struct Walker {
     const Dual* q;
     std::vector<Dual> slots;
     std::vector<long long> base;   // block base row per loop depth
+    double absd = 0.0;             // sum over terms of |d term / d seeded row|
+
+    Dual term(Dual t) {
+        absd += std::fabs(t.d);
+        return t;
+    }
 
     Dual eval(int i) {
         const ut_expr_node& n = p.nodes[i];
@@ -278,14 +284,14 @@ struct Walker {
                     if (s.value_source >= 0) x = transform(s.transform, q[s.value_source], lad);
                     else x = C(obs[base[depth] + s.obs_offset]);
                     bind(s.binding_slot, x);
-                    total = total + logpdf(s.dist, a, x) + lad;
+                    total = total + term(logpdf(s.dist, a, x) + lad);
                     ++i;
                     break;
                 }
                 case UT_STEP_IID_NORMAL: {  // DeviceDiagNormalChoiceStepDyn (logjoint_kernel.jl:514-533)
                     const Dual mu = eval(s.arg[0]), sg = eval(s.arg[1]);
                     Dual a[2] = {mu, sg};
-                    for (int d = 0; d < s.count; ++d) total = total + logpdf(UT_DIST_NORMAL, a, q[s.value_source + d]);
+                    for (int d = 0; d < s.count; ++d) total = total + term(logpdf(UT_DIST_NORMAL, a, q[s.value_source + d]));
                     ++i;
                     break;
                 }
@@ -297,7 +303,7 @@ struct Walker {
                         Dual eta = icpt;
                         for (int d = 0; d < F; ++d) eta = eta + q[s.value_source + d] * C(obs[row + d]);
                         Dual a[1] = {eta};
-                        total = total + logpdf(UT_DIST_BERNOULLI_LOGIT, a, C(obs[row + F]));
+                        total = total + term(logpdf(UT_DIST_BERNOULLI_LOGIT, a, C(obs[row + F])));
                     }
                     ++i;
                     break;
@@ -323,17 +329,19 @@ struct Walker {
 
 }  // namespace
 
-double logjoint_grad(const Program& prog, const std::vector<double>& obs, const double* q, double* g) {
+double logjoint_grad(const Program& prog, const std::vector<double>& obs, const double* q, double* g, double* mag) {
     const int P = prog.P;
     std::vector<Dual> qd(P);
     double value = 0.0;
-    const int passes = g ? P : 1;
+    const bool seed = g || mag;
+    const int passes = seed ? P : 1;
     for (int s = 0; s < passes; ++s) {
-        for (int r = 0; r < P; ++r) qd[r] = {q[r], (g && r == s) ? 1.0 : 0.0};
+        for (int r = 0; r < P; ++r) qd[r] = {q[r], (seed && r == s) ? 1.0 : 0.0};
         Walker w{prog, obs, qd.data(), std::vector<Dual>(std::max(prog.nslots, 1)), std::vector<long long>(1, 0)};
         const Dual t = w.walk(0, (int)prog.steps.size(), 0);
         value = t.v;
         if (g) g[s] = t.d;
+        if (mag) mag[s] = w.absd;
     }
     return value;
 }

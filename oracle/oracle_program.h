@@ -20,7 +20,10 @@ struct Program {
 Program& current();
 
 // Logjoint (and, when g != nullptr, its gradient) of one chain in float64,
-// the gradient by forward-mode duals, one pass per parameter row.
-double logjoint_grad(const Program& prog, const std::vector<double>& obs, const double* q, double* g);
+// the gradient by forward-mode duals, one pass per parameter row.  With mag,
+// also the gradient magnitude: per row, the sum over the density's terms of
+// |d term / d row|.
+double logjoint_grad(const Program& prog, const std::vector<double>& obs, const double* q, double* g,
+                     double* mag = nullptr);
 
 }  // namespace oracle_program

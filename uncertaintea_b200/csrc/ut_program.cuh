@@ -144,6 +144,7 @@ class ProgCompiler {
     std::vector<int> covered_;
     std::vector<PStep> steps_;
     std::vector<PNode> nodes_;
+    std::vector<int64_t> blocks_;  // rows of the observation block at each loop depth
     int devslots_ = 0;
 
     void add(const std::string& m) {
@@ -187,6 +188,7 @@ class ProgCompiler {
             }
         } else if (e.op == UT_EXPR_OBS) {
             if (e.b > depth) { add(where + ": observation leaf of a deeper loop"); return false; }
+            if ((int64_t)e.a >= blocks_[e.b]) { add(where + ": observation leaf outside its block"); return false; }
             t.push_back(PNode{UT_EXPR_OBS, e.a, e.b, 0, 0.0f});
         } else if (e.op == UT_EXPR_LITERAL) {
             t.push_back(PNode{UT_EXPR_LITERAL, 0, 0, 0, (float)e.value});
@@ -239,6 +241,8 @@ class ProgCompiler {
 
     // Compiles steps [pc, end) at loop depth `depth` whose block holds `block` rows.
     void compile_block(int& pc, int end, int depth, int64_t block) {
+        blocks_.resize(depth + 1);
+        blocks_[depth] = block;
         while (pc < end && issues_.size() < 2000) {
             const ut_program_step& s = in_[pc];
             const std::string where = "step " + std::to_string(pc);

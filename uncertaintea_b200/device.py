@@ -78,7 +78,12 @@ def device_lowering_report(model: TeaModelSpec, args=(), constraints=None):
     except (ValueError, IndexError) as err:
         return False, [str(err)]
     buf = ctypes.create_string_buffer(4096)
-    status = lib.ut_lowering_report(ctypes.byref(lowered.plan), buf, len(buf))
+    prog = getattr(lowered, "program", None)
+    if prog is not None:
+        status = lib.ut_program_report(lowered.steps, len(prog.steps), lowered.nodes, len(prog.nodes), prog.num_slots,
+                                       prog.num_params, int(lowered.observed.size), buf, len(buf))
+    else:
+        status = lib.ut_lowering_report(ctypes.byref(lowered.plan), buf, len(buf))
     issues = [s for s in buf.value.decode().split("\n") if s]
     return status == nat.UT_OK, issues
 
@@ -103,11 +108,17 @@ class DeviceBatchedWorkspace:
         self.lowered = lowered
         handle = ctypes.c_void_p()
         obs = lowered.observed
-        status = self.lib.ut_workspace_create(
-            ctypes.byref(lowered.plan), nat.ptr(obs), int(obs.size), 1,
-            nat.ptr(lowered.trip_counts) if lowered.trip_counts.size else None,
-            nat.ptr(lowered.loop_starts) if lowered.loop_starts.size else None,
-            int(lowered.trip_counts.size), int(num_chains), 32, ctypes.byref(handle))
+        prog = getattr(lowered, "program", None)
+        if prog is not None:
+            status = self.lib.ut_workspace_create_program(
+                lowered.steps, len(prog.steps), lowered.nodes, len(prog.nodes), prog.num_slots, prog.num_params,
+                nat.ptr(obs) if obs.size else None, int(obs.size), int(num_chains), 32, ctypes.byref(handle))
+        else:
+            status = self.lib.ut_workspace_create(
+                ctypes.byref(lowered.plan), nat.ptr(obs), int(obs.size), 1,
+                nat.ptr(lowered.trip_counts) if lowered.trip_counts.size else None,
+                nat.ptr(lowered.loop_starts) if lowered.loop_starts.size else None,
+                int(lowered.trip_counts.size), int(num_chains), 32, ctypes.byref(handle))
         if status == nat.UT_ERR_UNSUPPORTED:
             msg = nat.last_error()
             raise ValueError(f"model {model.name} cannot be lowered to the device logjoint path. Issues:\n  - "
