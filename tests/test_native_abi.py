@@ -55,25 +55,64 @@ def test_plain_c_host_binds_the_library(tmp_path, lib):
     assert "all checks passed" in run.stdout
 
 
-def test_julia_shim_struct_matches_the_c_struct():
-    """The Julia mirror of ut_plan_desc in INTEGRATION.md has the C struct's
-    fields in the same order with the same widths (a ccall passes it by
-    reference, so any drift would shift every later field)."""
-    import ctypes as ct
-    from uncertaintea_b200 import _native as nat
-    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    body = text[text.index("struct UtPlanDesc"):]
+JULIA_EXT = os.path.join(ROOT, "julia", "UncertainTeaB200Ext.jl")
+
+
+def _julia_struct(text, name):
+    body = text[text.index(f"struct {name}"):]
     body = body[body.index("\n") + 1:body.index("\nend")]
     fields = []
     for line in body.splitlines():
         line = line.split("#")[0]
-        fields += re.findall(r"([a-z_]+)::(Int32|Float64)", line)
+        fields += re.findall(r"([a-z_]+)::([A-Za-z0-9_{}, ]+?)(?:;|$)", line.strip())
+    return [(n, t.strip()) for n, t in fields]
+
+
+def test_julia_shim_struct_matches_the_c_struct():
+    """The Julia mirror of ut_plan_desc (julia/UncertainTeaB200Ext.jl) has the C
+    struct's fields in the same order with the same widths (a ccall passes it
+    by reference, so any drift would shift every later field)."""
+    import ctypes as ct
+    from uncertaintea_b200 import _native as nat
+    fields = _julia_struct(open(JULIA_EXT).read(), "UtPlanDesc")
     widths = {"Int32": ct.c_int32, "Float64": ct.c_double}
     assert [(n, widths[t]) for n, t in fields] == [(n, t) for n, t in nat.PlanDesc._fields_]
     header = open(HEADER).read()
     c_body = header[header.index("typedef struct ut_plan_desc"):header.index("} ut_plan_desc;")]
     c_fields = re.findall(r"(int32_t|double)\s+([a-z_]+);", c_body)
     assert [n for _, n in c_fields] == [n for n, _ in nat.PlanDesc._fields_]
+
+
+def test_julia_program_mirrors_and_code_tables_match_the_header():
+    """The Julia mirrors of ut_program_step / ut_expr_node and its tables of
+    distribution and expression codes agree with include/ut_b200.h and the
+    Python binding."""
+    from uncertaintea_b200 import _native as nat
+    text = open(JULIA_EXT).read()
+    header = open(HEADER).read()
+    for c_name, jl, py in [("ut_program_step", "UtProgramStep", nat.ProgramStep),
+                           ("ut_expr_node", "UtExprNode", nat.ExprNode)]:
+        body = header[header.index(f"typedef struct {c_name} {{"):header.index(f"}} {c_name};")]
+        c_fields = re.findall(r"^\s*(?:int32_t|double)\s+([a-z_]+)(?:\[\d+\])?;", body, re.M)
+        jl_fields = [n for n, _ in _julia_struct(text, jl)]
+        assert jl_fields == c_fields == [n for n, _ in py._fields_], (c_name, jl_fields, c_fields)
+    codes = {m.group(1).lower(): int(m.group(2)) for m in re.finditer(r"#define UT_DIST_([A-Z_]+)\s+(\d+)", header)}
+    jl_dists = {m.group(1): int(m.group(2)) for m in re.finditer(r":Device(\w+)ChoiceStep => \(Int32\((\d+)\)", text)}
+    names = {"Normal": "normal", "Lognormal": "lognormal", "Exponential": "exponential", "Gamma": "gamma",
+             "Laplace": "laplace", "Cauchy": "cauchy", "HalfNormal": "halfnormal", "HalfCauchy": "halfcauchy",
+             "Logistic": "logistic", "Gumbel": "gumbel", "Frechet": "frechet", "Rayleigh": "rayleigh",
+             "InverseGaussian": "inversegaussian", "Beta": "beta", "StudentT": "studentt",
+             "InverseGamma": "inversegamma", "Weibull": "weibull", "Bernoulli": "bernoulli",
+             "BernoulliLogit": "bernoulli_logit", "Poisson": "poisson", "Geometric": "geometric",
+             "NegativeBinomial": "negative_binomial", "Binomial": "binomial"}
+    assert len(jl_dists) == 23
+    for jl_name, code in jl_dists.items():
+        assert codes[names[jl_name]] == code == nat.DISTRIBUTIONS[names[jl_name].replace("_", "")], jl_name
+    ops = {m.group(1).lower(): int(m.group(2)) for m in re.finditer(r"#define UT_EXPR_([A-Z0-9]+)\s+(\d+)", header)}
+    jl_ops = {m.group(1): int(m.group(2)) for m in re.finditer(r":(\S+?) => (\d+)", text[text.index("const EXPR_OPS"):])}
+    sym = {"+": "add", "-": "sub", "*": "mul", "/": "div", "^": "pow"}
+    for op, code in jl_ops.items():
+        assert ops[sym.get(op, op)] == code, op
 
 
 def _header_struct_fields(name):
@@ -83,10 +122,10 @@ def _header_struct_fields(name):
 
 
 def test_buffer_struct_mirrors_match_the_header():
-    """The Python (ctypes) and Julia mirrors of the sampler
-    buffer structs list the header's fields in its order."""
+    """The Python (ctypes) and Julia (julia/UncertainTeaB200Ext.jl) mirrors of
+    the sampler buffer structs list the header's fields in its order."""
     from uncertaintea_b200 import _native as nat
-    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    text = open(JULIA_EXT).read()
     for c_name, py, jl in [("ut_hmc_buffers", nat.HmcBuffers, "UtHmcBuffers"),
                            ("ut_nuts_buffers", nat.NutsBuffers, "UtNutsBuffers"),
                            ("ut_meads_buffers", nat.MeadsBuffers, "UtMeadsBuffers"),
