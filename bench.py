@@ -318,6 +318,7 @@ def run_b200(args):
         _emit("fp64_error", fp64)
         if world == 1:
             _emit("hbm_sweep", hbm_sweep())
+            _emit("hbm_sweep_large", hbm_sweep_large())
             samplers = None
             if not args.no_samplers:
                 samplers = {}
@@ -350,6 +351,52 @@ def run_b200(args):
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
+
+
+def hbm_sweep_large(num_obs=1_000_000, chain_counts=(1, 4, 16), steps=10, warmup=3):
+    """The few-chain streaming evaluation on a design larger than L2 (N =
+    1000000 x 100, 400 MB): every evaluation streams X from HBM, and one launch
+    is long enough (~60 us at the copy bandwidth) that the launch ramp and the
+    fused fold's tail no longer dominate, so this is the kernel's own HBM
+    roofline.  Back-to-back evaluations, one event pair per evaluation."""
+    import torch
+    from uncertaintea_b200.device import DeviceBatchedWorkspace
+    from uncertaintea_b200.models import BernoulliLogitGLM, logistic_regression_data
+    X, y, _ = logistic_regression_data(num_obs, N_COEF, seed=4, x_scale=1.0 / np.sqrt(N_COEF))
+    model = BernoulliLogitGLM(N_COEF)
+    hbm, _, kind = _peaks()
+    params = np.random.default_rng(1).standard_normal((16, N_COEF)).astype(np.float32)
+    stream = torch.cuda.current_stream()
+    rows = []
+    for C in chain_counts:
+        ws = DeviceBatchedWorkspace(model, C, args=(X,), constraints={"y": y})
+        qd = torch.from_numpy(params[:C].copy()).cuda()
+        totals, grads = torch.empty(C, device="cuda"), torch.empty_like(qd)
+        row = {"chains": C, "n_obs": num_obs, "kernel_path": ws.kernel_path()}
+        for name, grad in (("logjoint_gradient", True), ("logjoint", False)):
+            def step():
+                if grad:
+                    ws.logjoint_gradient_device(qd, totals, grads)
+                else:
+                    ws.logjoint_device(qd, totals)
+            for _ in range(max(warmup, 3)):
+                step()
+            evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+            for a, b in evs:
+                a.record(stream)
+                step()
+                b.record(stream)
+            torch.cuda.synchronize()
+            ms = float(np.median([a.elapsed_time(b) for a, b in evs]))
+            nbytes = num_obs * N_COEF * 4 + num_obs * 4 + (2 if grad else 1) * C * N_COEF * 4 + C * 4
+            gbs = nbytes / (ms / 1000.0) / 1e9
+            row[name] = {"ms": ms, "bytes": nbytes, "GB/s": gbs, "frac": gbs / hbm}
+        ws.check()
+        ws.close()
+        rows.append(row)
+    return {"metric": "few-chain logjoint(+gradient) HBM roofline, design larger than L2",
+            "peak_GB/s": hbm, "peak_source": f"{kind} HBM copy bandwidth",
+            "l2": "X (400 MB) > L2 (126 MB): every evaluation reads X from HBM", "rows": rows}
 
 
 def hbm_sweep(chain_counts=(1, 4, 8, 16), steps=20, warmup=5):

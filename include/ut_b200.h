@@ -470,6 +470,26 @@ int32_t ut_chees_reduce(ut_workspace* ws, const float* d_initials, const float* 
 int32_t ut_running_variance_update(const float* d_positions, const double* d_weights, int32_t num_params,
                                    int32_t num_chains, double* d_state, int32_t window_length, void* stream);
 
+/* One warmup iteration's adaptation on the device, so warmup copies nothing to
+ * the host between mass-window ends.  reference: the per-iteration
+ * warmup_update! of src/inference/warmup.jl:262-326 / 371-470: the running-
+ * variance weights of src/inference/nuts/adaptation.jl:225-260 into d_weights
+ * (C doubles; NULL skips them), the window progress taken from
+ * d_variance_state (the ut_running_variance_update state, its count at
+ * [2P]) and window_length; and with adapt_step, one dual-averaging update
+ * (adaptation.jl:1-28) of d_dual -- per chain (per_chain = 1, C x 5 doubles)
+ * with each chain's statistic (0 when divergent), or shared (5 doubles) with
+ * the mean statistic over the chains (hmc_support.jl:635-652) -- writing the
+ * new step sizes to d_step (C floats).  Dual-averaging state: mu, log step,
+ * log step average, hbar, iteration. */
+int32_t ut_warmup_adapt(const float* d_accept_prob, const uint8_t* d_accepted, const uint8_t* d_divergent,
+                        int32_t num_chains, int32_t num_params, const double* d_variance_state,
+                        int32_t window_length, double* d_weights, double* d_dual, int32_t per_chain,
+                        int32_t adapt_step, double target_accept, float* d_step, void* stream);
+/* The warmup's final step sizes exp(log step average) into d_step (C floats). */
+int32_t ut_dual_averaging_final(const double* d_dual, int32_t num_chains, int32_t per_chain, float* d_step,
+                                void* stream);
+
 /* ---- allocation-free GLM logjoint + gradient ------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory when they need a gradient (a host whose device memory all comes from

@@ -411,3 +411,22 @@ def test_no_cpu_fallback_without_device():
     X, y, _ = logistic_regression_data(10, 2, 0)
     with pytest.raises(Exception):
         device_batched_logjoint(BernoulliLogitGLM(2), np.zeros((2, 3)), (X,), {"y": y})
+
+
+def test_tensor_core_tmem_plan_fits_for_every_feature_count(lib):
+    """The tensor-core kernel's TMEM columns: Theta hi / lo (KC = F rounded up
+    to 8 each), the gradient accumulator (Fp = F rounded up to 16) and 2 or 3
+    H/R buffers of 64 columns fit the 512 allocated columns for every feature
+    count the path takes (1..128), with 3 buffers at 100 features."""
+    fn = lib.ut_internal_tc_tmem_plan
+    fn.restype = ctypes.c_int32
+    fn.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
+    out = (ctypes.c_int32 * 4)()
+    for F in range(1, 129):
+        assert fn(F, out) == 0
+        KC, Fp, nb, cols = list(out)
+        assert KC == 8 * ((F + 7) // 8) and Fp == 16 * ((F + 15) // 16)
+        assert 2 <= nb <= 3 and cols <= 512 and cols == 2 * KC + Fp + 64 * nb, (F, list(out))
+    fn(100, out)
+    assert list(out) == [104, 112, 3, 512]
+    assert fn(129, out) != 0 and fn(0, out) != 0

@@ -190,6 +190,10 @@ SIGNATURES = [
      [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, POINTER(c_double), c_void_p]),
     ("ut_running_variance_update", c_int32,
      [c_void_p, c_void_p, c_int32, c_int32, c_void_p, c_int32, c_void_p]),
+    ("ut_warmup_adapt", c_int32,
+     [c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p, c_int32, c_void_p, c_void_p, c_int32, c_int32,
+      c_double, c_void_p, c_void_p]),
+    ("ut_dual_averaging_final", c_int32, [c_void_p, c_int32, c_int32, c_void_p, c_void_p]),
     ("ut_glm_logjoint_gradient_noalloc", c_int32,
      [c_void_p, c_void_p, c_int64, c_int32, c_int32, c_double, c_double, c_double, c_double, c_void_p, c_int32,
       c_void_p, c_void_p, c_void_p]),

@@ -942,6 +942,15 @@ extern "C" int32_t ut_internal_tc_live_split(int32_t num_obs, int32_t num_chains
     return UT_OK;
 }
 
+// Test hook (not part of the C ABI in ut_b200.h): the tensor-core kernel's TMEM
+// column plan for F features: out = {KC, Fp, buffers, columns used}.
+extern "C" int32_t ut_internal_tc_tmem_plan(int32_t F, int32_t* out) {
+    if (F < 1 || F > kTcMaxFp || !out) return UT_ERR_ARGUMENT;
+    const int KC = 8 * tc_kblocks_used(F), Fp = ((F + 15) / 16) * 16, nb = tc_nbuf(F, Fp);
+    out[0] = KC; out[1] = Fp; out[2] = nb; out[3] = 2 * KC + Fp + 64 * nb;
+    return UT_OK;
+}
+
 // Test hook (not part of the C ABI in ut_b200.h): one tensor-core evaluation of
 // only the first *d_live chains of d_params -- the live-chain launch masked NUTS
 // makes at every leaf, with its observation re-split -- on device buffers.
@@ -1465,6 +1474,34 @@ int32_t ut_running_variance_update(const float* d_positions, const double* d_wei
     UT_CUDA(allow_dynamic_smem(running_variance_kernel, smem));
     running_variance_kernel<<<1, threads, smem, (cudaStream_t)stream>>>(d_positions, d_weights, num_params, num_chains,
                                                                       d_state, window_length);
+    UT_LAUNCHED();
+    return UT_OK;
+}
+
+int32_t ut_warmup_adapt(const float* d_accept_prob, const uint8_t* d_accepted, const uint8_t* d_divergent,
+                        int32_t num_chains, int32_t num_params, const double* d_variance_state,
+                        int32_t window_length, double* d_weights, double* d_dual, int32_t per_chain,
+                        int32_t adapt_step, double target_accept, float* d_step, void* stream) {
+    if (!d_accept_prob || !d_divergent) return fail(UT_ERR_ARGUMENT, "null accept / divergence buffer");
+    if (num_chains < 1) return fail(UT_ERR_ARGUMENT, "num_chains must be >= 1, got %d", (int)num_chains);
+    if (d_weights && (!d_variance_state || num_params < 1 || window_length < 1))
+        return fail(UT_ERR_ARGUMENT, "weights need the running-variance state, num_params and window_length");
+    if (adapt_step && (!d_dual || !d_step)) return fail(UT_ERR_ARGUMENT, "null dual-averaging state or step buffer");
+    if (!(target_accept > 0.0 && target_accept < 1.0)) return fail(UT_ERR_ARGUMENT, "target_accept must be in (0, 1)");
+    warmup_adapt_kernel<<<1, 1024, 0, (cudaStream_t)stream>>>(d_accept_prob, d_accepted, d_divergent, num_chains,
+                                                              num_params, d_weights ? d_variance_state : nullptr,
+                                                              window_length, d_weights, d_dual, per_chain ? 1 : 0,
+                                                              adapt_step ? 1 : 0, target_accept, d_step);
+    UT_LAUNCHED();
+    return UT_OK;
+}
+
+int32_t ut_dual_averaging_final(const double* d_dual, int32_t num_chains, int32_t per_chain, float* d_step,
+                                void* stream) {
+    if (!d_dual || !d_step) return fail(UT_ERR_ARGUMENT, "null dual-averaging state or step buffer");
+    if (num_chains < 1) return fail(UT_ERR_ARGUMENT, "num_chains must be >= 1, got %d", (int)num_chains);
+    dual_averaging_final_kernel<<<(num_chains + 255) / 256, 256, 0, (cudaStream_t)stream>>>(d_dual, num_chains,
+                                                                                           per_chain ? 1 : 0, d_step);
     UT_LAUNCHED();
     return UT_OK;
 }

@@ -324,4 +324,67 @@ __global__ void __launch_bounds__(1024) running_variance_kernel(const float* __r
     if (threadIdx.x == 0) { state[2 * P] = count; state[2 * P + 1] = wsum; state[2 * P + 2] = wsq; }
 }
 
+// One warmup iteration's adaptation on the device, so the single-model
+// samplers copy nothing to the host between mass-window ends (one CTA):
+//  * running-variance weights (adaptation.jl:225-260): 1 for an accepted
+//    chain, 0 for a divergent one, else the rejection weight
+//    1 + (clamp(accept_prob, 0, 1) - 1) * progress (0 when accept_prob is not
+//    finite), with the window progress of adaptation.jl:56-65 taken from the
+//    running-variance state's count (var[2P]);
+//  * one dual-averaging update (adaptation.jl:1-28; gamma 0.05, t0 10, kappa
+//    0.75) of each chain's state (per_chain) with the chain's statistic, 0 when
+//    divergent, or of one shared state with the mean statistic over chains
+//    (hmc_support.jl:635-652, summed in a fixed order); the new step sizes go
+//    to step[C].  State: [mu, log step, log step avg, hbar, iteration] doubles.
+__device__ __forceinline__ double dual_averaging_update(double* s, double stat, double target) {
+    const double it = s[4] + 1.0;
+    const double eta = 1.0 / (it + 10.0);
+    s[3] = (1.0 - eta) * s[3] + eta * (target - stat);
+    s[1] = s[0] - sqrt(it) / 0.05 * s[3];
+    const double eta_bar = pow(it, -0.75);
+    s[2] = eta_bar * s[1] + (1.0 - eta_bar) * s[2];
+    s[4] = it;
+    return s[1];
+}
+
+__global__ void __launch_bounds__(1024) warmup_adapt_kernel(const float* __restrict__ ap, const uint8_t* __restrict__ acc,
+                                                            const uint8_t* __restrict__ div, int C, int P,
+                                                            const double* __restrict__ var, int window_length,
+                                                            double* weights, double* dual, int per_chain, int adapt,
+                                                            double target, float* step) {
+    __shared__ double red[1024];
+    __shared__ float shared_step;
+    const double count = var ? var[2 * P] : 0.0;
+    const double prog = window_length <= 4 ? 1.0 : fmin(fmax(count - 4.0, 0.0) / (double)(window_length - 4), 1.0);
+    double part = 0.0;
+    for (int c = threadIdx.x; c < C; c += blockDim.x) {
+        const double a = (double)ap[c];
+        const bool dv = div[c] != 0;
+        if (weights) {
+            double w = isfinite(a) ? 1.0 + (fmin(fmax(a, 0.0), 1.0) - 1.0) * prog : 0.0;
+            if (acc && acc[c]) w = 1.0;
+            weights[c] = dv ? 0.0 : w;
+        }
+        const double stat = dv ? 0.0 : a;
+        if (adapt && per_chain) step[c] = (float)exp(dual_averaging_update(dual + 5 * (size_t)c, stat, target));
+        part += stat;
+    }
+    if (!adapt || per_chain) return;
+    red[threadIdx.x] = part;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) shared_step = (float)exp(dual_averaging_update(dual, red[0] / (double)C, target));
+    __syncthreads();
+    for (int c = threadIdx.x; c < C; c += blockDim.x) step[c] = shared_step;
+}
+
+// Final warmup step sizes exp(log step avg) (adaptation.jl:25-28).
+__global__ void dual_averaging_final_kernel(const double* dual, int C, int per_chain, float* step) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < C) step[c] = (float)exp(dual[per_chain ? 5 * (size_t)c + 2 : 2]);
+}
+
 }  // namespace ut

@@ -18,8 +18,10 @@
 // Warp roles (576 threads): warp 0 = TMA producer, warp 1 = MMA issuer (and
 // TMEM owner), warps 2-17 = epilogue: four warps per TMEM lane quadrant, each
 // owning 8 of a tile's observation columns and a quarter of the gradient columns.
-// Pipelines: 3 X stages, 2 H/R TMEM buffers, so GEMM1 of tile t+1 runs on the
-// tensor cores while the epilogue of tile t runs on the CUDA cores / SFUs.
+// Pipelines: 3 X stages and up to 3 H/R TMEM buffers (as many as TMEM holds
+// beside Theta and the gradient accumulator: 3 for 100 features), so GEMM1 of
+// the next tiles runs on the tensor cores while the epilogue of tile t runs on
+// the CUDA cores / SFUs.
 // The tensor pipe stays busy while the epilogue's round trip (GEMM1(t) done ->
 // R(t) in TMEM) is shorter than GEMM2(t-1) + GEMM1(t+1), so the epilogue keeps
 // that path short: one mbarrier arrival per warp (not per thread), and the
@@ -67,6 +69,7 @@ struct TcGlmParams {
     int want_grad;
     int ctiles, S, sms;    // chain tiles, observation splits of the full grid, SMs
     const int* nact;       // optional: only the first *nact chains are live
+    int nbuf;              // H/R TMEM buffers (2 or 3)
 };
 
 // Work split of one launch.  Without nact: the (chain tile, split) grid of the
@@ -112,6 +115,19 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Non-blocking test of a phase (no suspension, unlike try_wait).
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
 }
 
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
@@ -246,21 +262,30 @@ __host__ __device__ constexpr uint32_t idesc_tf32(int M, int N, int b_mn_major) 
 // ---------------------------------------------------------------------------
 // the kernel
 // ---------------------------------------------------------------------------
-// TMEM columns (512 allocated), Fp = padded features (multiple of 16, <= 128):
-//   Theta_hi [0, Fp)   Theta_lo [Fp, 2Fp)   D2 = G^T [2Fp, 3Fp)
-//   buffer b (0,1): H^T / R_hi [3Fp + 64b, +32)   R_lo [3Fp + 64b + 32, +32)
+// TMEM columns (512 allocated), KC = features rounded up to 8 (GEMM1's K),
+// Fp = features rounded up to 16 (GEMM2's N), both <= 128:
+//   Theta_hi [0, KC)   Theta_lo [KC, 2KC)   D2 = G^T [2KC, 2KC + Fp)
+//   buffer b (0 .. nbuf-1): H^T / R_hi [2KC + Fp + 64b, +32)   R_lo [.. + 32, +32)
+// nbuf = min(3, (512 - 2KC - Fp) / 64): 3 for 100 features (208 + 112 + 192).
 // Shared memory per pipeline stage (3 stages), Fp features x 32 observations:
 //   XK_hi, XK_lo : K-major SWIZZLE_32B, Fp/8 blocks of [32 rows][32 B]     (GEMM1 B)
 //   XM_hi, XM_lo : MN-major SWIZZLE_128B_BASE32B, Fp/32 atoms of [32 rows][128 B] (GEMM2 B)
 // (TF32 operands that are MN-major must use the 128B_BASE32B layout, which no
 // K-major layout shares, so each X tile is loaded twice, once per view.)
 constexpr int kTcStages = 3;
+constexpr int kTcMaxBufs = 3;      // H/R buffers: at most the X stages (GEMM1(i) needs stage i's
+                                   // release after GEMM2(i - 3), which the same thread issues)
 constexpr int kTcDrainTiles = 4;   // observation tiles per TMEM gradient accumulation run
 
 __host__ __device__ inline int tc_kblocks(int Fp) { return Fp / 8; }
 // K-blocks GEMM1 needs: the features rounded up to 8 (the TF32 MMA's K), not to
 // the 16 of Fp (GEMM2's N); the blocks past it hold zero padding.
 __host__ __device__ inline int tc_kblocks_used(int F) { return (F + 7) / 8; }
+// H/R TMEM buffers the 512 columns hold beside Theta hi/lo and the accumulator.
+__host__ __device__ inline int tc_nbuf(int F, int Fp) {
+    const int n = (512 - 16 * tc_kblocks_used(F) - Fp) / 64;
+    return n < kTcMaxBufs ? n : kTcMaxBufs;
+}
 __host__ __device__ inline int tc_matoms(int Fp) { return (Fp + 31) / 32; }
 __host__ __device__ inline int tc_xk_bytes(int Fp) { return tc_kblocks(Fp) * kTcObs * 32; }
 __host__ __device__ inline int tc_xm_bytes(int Fp) { return tc_matoms(Fp) * kTcObs * 128; }
@@ -327,11 +352,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kTcStages * stage_bytes);
     uint64_t* bar_xfull = bars;                    // [3]
     uint64_t* bar_xempty = bars + 3;               // [3]
-    uint64_t* bar_d1full = bars + 6;               // [2]
-    uint64_t* bar_rfull = bars + 8;                // [2]
-    uint64_t* bar_d2full = bars + 10;
-    uint64_t* bar_theta = bars + 11;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 13);
+    uint64_t* bar_d1full = bars + 6;               // [kTcMaxBufs]
+    uint64_t* bar_rfull = bars + 9;                // [kTcMaxBufs]
+    uint64_t* bar_d2full = bars + 12;
+    uint64_t* bar_theta = bars + 13;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 14);
+    const int nbuf = p.nbuf;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // chain tiles fastest: concurrent CTAs share X ranges in L2
@@ -350,7 +376,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             mbar_init(bar_xfull + i, 1);
             mbar_init(bar_xempty + i, 1);
         }
-        for (int i = 0; i < 2; ++i) {
+        for (int i = 0; i < kTcMaxBufs; ++i) {
             mbar_init(bar_d1full + i, 1);
             mbar_init(bar_rfull + i, kTcEpiWarps);
         }
@@ -363,7 +389,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-    const uint32_t col_thi = 0, col_tlo = Fp, col_d2 = 2 * Fp, col_buf = 3 * Fp;
+    const int KC = 8 * KB1;
+    const uint32_t col_thi = 0, col_tlo = KC, col_d2 = 2 * KC, col_buf = 2 * KC + Fp;
 
     if (warp == 0) {
         // ---------------- TMA producer ----------------
@@ -400,7 +427,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             // wait of its own: GEMM2(j) is issued after R(j) is in TMEM, and the
             // epilogue drains the previous group before it signals R(j).
             auto gemm2 = [&](int j) {
-                const int s = j % kTcStages, b = j & 1;
+                const int s = j % kTcStages, b = j % nbuf;
                 const uint32_t xm = smem_u32(smem + s * stage_bytes + 2 * xk_bytes);
                 const uint32_t rhi = tmem + col_buf + b * 64, rlo = rhi + 32;
                 for (int kk = 0; kk < kTcObs / 8; ++kk) {
@@ -413,8 +440,23 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 }
                 if ((j + 1) % kTcDrainTiles == 0 || j == ntiles - 1) mma_commit(bar_d2full);
             };
+            // GEMM2 of tile j (when the gradient is wanted), then the release of its X stage
+            auto finish = [&](int j) {
+                tc_fence_after();
+                if (p.want_grad) gemm2(j);
+                mma_commit(bar_xempty + (j % kTcStages));
+            };
+            int g2 = 0;  // next tile whose GEMM2 / stage release is due
             for (int i = 0; ok && i < ntiles; ++i) {
-                const int s = i % kTcStages, b = i & 1;
+                // buffer i % nbuf is reused: the epilogue has to be done with tile i - nbuf
+                while (g2 <= i - nbuf) {
+                    if (!mbar_wait(bar_rfull + (g2 % nbuf), (g2 / nbuf) & 1, p.err)) { ok = false; break; }
+                    finish(g2++);
+                }
+                if (!ok) break;
+                // GEMM2s whose residuals are already in TMEM go ahead of the next GEMM1
+                while (g2 < i && mbar_test_wait(bar_rfull + (g2 % nbuf), (g2 / nbuf) & 1)) finish(g2++);
+                const int s = i % kTcStages, b = i % nbuf;
                 if (!mbar_wait(bar_xfull + s, (i / kTcStages) & 1, p.err)) { ok = false; break; }
                 tc_fence_after();
                 const uint32_t xk = smem_u32(smem + s * stage_bytes);
@@ -427,21 +469,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     mma_ts(d1, tmem + col_tlo + kb * 8, bh, id1, 1u);
                 }
                 mma_commit(bar_d1full + b);
-                if (i > 0) {
-                    const int j = i - 1;
-                    if (!mbar_wait(bar_rfull + (j & 1), (j >> 1) & 1, p.err)) { ok = false; break; }
-                    tc_fence_after();
-                    if (p.want_grad) gemm2(j);
-                    mma_commit(bar_xempty + (j % kTcStages));
-                }
             }
-            if (ok) {
-                const int j = ntiles - 1;
-                if (mbar_wait(bar_rfull + (j & 1), (j >> 1) & 1, p.err)) {
-                    tc_fence_after();
-                    if (p.want_grad) gemm2(j);
-                    mma_commit(bar_xempty + (j % kTcStages));
-                }
+            while (ok && g2 < ntiles) {
+                if (!mbar_wait(bar_rfull + (g2 % nbuf), (g2 / nbuf) & 1, p.err)) break;
+                finish(g2++);
             }
         }
     } else {
@@ -458,19 +489,19 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const int c_local = q * 32 + lane;
         const int c = ctile * kTcChains + c_local;
         const uint32_t lane_off = (uint32_t)(q * 32) << 16;
-        // Theta row of this chain -> TF32 hi / lo in TMEM (A operand of GEMM1);
-        // 16-column chunks f0 = 16*slot + 64*k belong to this warp (also for the gradient)
-        for (int f0 = 16 * slot; f0 < Fp; f0 += 64) {
-            uint32_t hi[16], lo[16];
+        // Theta row of this chain -> TF32 hi / lo in TMEM (A operand of GEMM1):
+        // 8-column chunks f0 = 8*slot + 32*k < KC belong to this warp
+        for (int f0 = 8 * slot; f0 < KC; f0 += 32) {
+            uint32_t hi[8], lo[8];
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
+            for (int j = 0; j < 8; ++j) {
                 const int f = f0 + j;
                 const float x = (c < p.C && f < p.F) ? __ldg(params + (size_t)c * p.F + f) : 0.0f;
                 hi[j] = tf32_bits(x);
                 lo[j] = tf32_bits(x - __uint_as_float(hi[j]));
             }
-            tmem_st16(tmem + lane_off + col_thi + f0, hi);
-            tmem_st16(tmem + lane_off + col_tlo + f0, lo);
+            tmem_st8(tmem + lane_off + col_thi + f0, hi);
+            tmem_st8(tmem + lane_off + col_tlo + f0, lo);
         }
         asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
         tc_fence_before();
@@ -500,10 +531,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         };
         bool ok = ntiles > 0;
         for (int i = 0; ok && i < ntiles; ++i) {
-            const int b = i & 1, s = i % kTcStages;
+            const int b = i % nbuf, s = i % kTcStages;
             // the y tile arrived with the X stage; d1_full(i) implies GEMM1(i) consumed stage s,
             // which the producer only refills after GEMM2(i) -- after this tile's r_full
-            if (!warp_wait(bar_d1full + b, (i >> 1) & 1)) { ok = false; break; }
+            if (!warp_wait(bar_d1full + b, (i / nbuf) & 1)) { ok = false; break; }
             tc_fence_after();
             const int n0 = (t_begin + i) * kTcObs + 8 * slot;
             const float* ys = reinterpret_cast<const float*>(smem + s * stage_bytes + 2 * xk_bytes + 2 * xm_bytes) +
@@ -774,6 +805,7 @@ inline cudaError_t tc_glm_launch(const TcGlmPlan& t, const float* params, float*
     p.tiles_per_split = t.tiles_per_split; p.num_tiles = t.num_tiles; p.want_grad = grads ? 1 : 0;
     p.ctiles = t.ctiles; p.S = t.S; p.sms = t.sms;
     p.nact = nact;
+    p.nbuf = tc_nbuf(t.F, t.Fp);
     dim3 grid(t.ctiles, t.S);
     tc_glm_kernel<<<grid, kTcThreads, t.smem, st>>>(t.map_xk_hi, t.map_xk_lo, t.map_xm_hi, t.map_xm_lo, params, p);
     tc_reduce_kernel<<<t.C, 128, 0, st>>>(params, totals, grads, p, t.off, t.icpt_mu, t.icpt_sigma, t.coef_mu,

@@ -136,6 +136,20 @@ class DualAveraging:
         return np.exp(self.log_step_size_avg)
 
 
+class DeviceDualAveraging:
+    """The DualAveraging state on the device (C x 5 or 5 doubles: mu, log step,
+    log step average, hbar, iteration), made from a host DualAveraging and
+    updated by ut_warmup_adapt without host copies."""
+
+    def __init__(self, host: DualAveraging, device):
+        torch = _torch()
+        mu = np.atleast_1d(host.mu)
+        cols = [mu, np.atleast_1d(host.log_step_size), np.atleast_1d(host.log_step_size_avg),
+                np.atleast_1d(host.hbar), np.full(mu.shape, float(host.iteration))]
+        self.per_chain = np.ndim(host.mu) > 0
+        self.state = torch.from_numpy(np.ascontiguousarray(np.stack(cols, axis=1), dtype=np.float64)).to(device)
+
+
 # ---------------------------------------------------------------------------
 # running variance with the update on device (adaptation.jl:30-41, 138-223)
 # ---------------------------------------------------------------------------
@@ -151,13 +165,27 @@ class DeviceRunningVariance:
         self.count = 0  # tracked on host: +1 per non-zero weight
 
     def progress(self) -> float:
+        self.sync_count()
         return _window_progress(self.count, self.window_length)
 
     def clip_scale(self) -> float:
+        self.sync_count()
         if self.count <= _RUNNING_VARIANCE_CLIP_START:
             return _RUNNING_VARIANCE_CLIP_SCALE_EARLY
         return _RUNNING_VARIANCE_CLIP_SCALE_EARLY + (
             _RUNNING_VARIANCE_CLIP_SCALE_LATE - _RUNNING_VARIANCE_CLIP_SCALE_EARLY) * self.progress()
+
+    def update_device(self, positions, weights_device):
+        """Welford update with device-resident weights (no host copy); the host
+        count is then refreshed from the device state when it is needed."""
+        nat.check(self.lib.ut_running_variance_update(nat.ptr(positions), nat.ptr(weights_device), self.P,
+                                                      positions.shape[0], nat.ptr(self.state), self.window_length,
+                                                      _stream_handle()))
+        self.count = None
+
+    def sync_count(self):
+        if self.count is None:
+            self.count = int(round(float(self.state[2 * self.P].item())))
 
     def update(self, positions, weights: np.ndarray):
         torch = _torch()
@@ -167,6 +195,7 @@ class DeviceRunningVariance:
         wd = torch.from_numpy(w).to(positions.device, non_blocking=False)
         nat.check(self.lib.ut_running_variance_update(nat.ptr(positions), nat.ptr(wd), self.P, positions.shape[0],
                                                       nat.ptr(self.state), self.window_length, _stream_handle()))
+        self.sync_count()
         self.count += int(np.count_nonzero(w))
         self._wd = wd  # keep alive until the stream has consumed it
 
@@ -260,27 +289,38 @@ class WarmupDriver:
         return (self.adapt_mass_matrix and self.mass_window_index <= len(s.slow_window_ends)
                 and iteration > s.initial_buffer and iteration == s.slow_window_ends[self.mass_window_index - 1])
 
+    def in_mass_window(self, iteration: int) -> bool:
+        s = self.schedule
+        return (self.adapt_mass_matrix and self.mass_window_index <= len(s.slow_window_ends)
+                and iteration > s.initial_buffer)
+
+    def end_window(self):
+        """A slow window's end (warmup.jl:262-326): the new inverse mass when the
+        window pooled enough samples, the window's record, the next window's
+        running variance."""
+        s = self.schedule
+        updated = False
+        if self.variance.effective_count() >= self.min_samples:
+            self.inverse_mass_matrix = self.variance.inverse_mass(self.regularization)
+            updated = True
+        self.mass_adaptation_windows.append(_mass_adaptation_window_summary(
+            s, self.mass_window_index, self.variance, self.inverse_mass_matrix, updated))
+        self.mass_window_index += 1
+        if self.mass_window_index <= len(s.slow_window_ends):
+            self.variance = DeviceRunningVariance(
+                self.lib, self.num_params, _warmup_window_length(s, self.mass_window_index), self.device)
+        else:
+            self.variance = DeviceRunningVariance(self.lib, self.num_params,
+                                                  _RUNNING_VARIANCE_CLIP_START + 16, self.device)
+
     def warmup_update(self, iteration, accept_statistic, positions, mass_weights, refind):
         if self.adapt_step_size:
             self.step_size = float(self.dual.update(accept_statistic))
         s = self.schedule
-        if (self.adapt_mass_matrix and self.mass_window_index <= len(s.slow_window_ends)
-                and iteration > s.initial_buffer):
+        if self.in_mass_window(iteration):
             self.variance.update(positions, mass_weights)
             if iteration == s.slow_window_ends[self.mass_window_index - 1]:
-                updated = False
-                if self.variance.effective_count() >= self.min_samples:
-                    self.inverse_mass_matrix = self.variance.inverse_mass(self.regularization)
-                    updated = True
-                self.mass_adaptation_windows.append(_mass_adaptation_window_summary(
-                    s, self.mass_window_index, self.variance, self.inverse_mass_matrix, updated))
-                self.mass_window_index += 1
-                if self.mass_window_index <= len(s.slow_window_ends):
-                    self.variance = DeviceRunningVariance(
-                        self.lib, self.num_params, _warmup_window_length(s, self.mass_window_index), self.device)
-                else:
-                    self.variance = DeviceRunningVariance(self.lib, self.num_params,
-                                                          _RUNNING_VARIANCE_CLIP_START + 16, self.device)
+                self.end_window()
                 if self.adapt_step_size and iteration < self.num_warmup and refind is not None:
                     self.step_size = float(refind(self.step_size, self.inverse_mass_matrix))
                     self.dual = DualAveraging(self.step_size, self.target_accept)
@@ -331,6 +371,55 @@ class PooledMassPerChainStepDriver:
             self.step_sizes = self.dual.final()
         self.mass.warmup_finalize()
         return self.step_sizes
+
+
+def _device_warmup_iteration(run, driver, per_chain, iteration, num_warmup, accepted, refind, weights):
+    """One warmup iteration's adaptation with the per-iteration work on the
+    device: ut_warmup_adapt (running-variance weights + dual averaging, the new
+    steps written into the sampler's step buffer) and the Welford update with
+    device weights -- no host copies.  The host takes over at a mass-window end
+    (new inverse mass, window record, step re-search and dual-averaging
+    restart, warmup.jl:262-326 / 371-470) and at the end of warmup (final
+    steps, final mass).  Same order of operations as the host drivers."""
+    lib = run.lib
+    mass = driver.mass if per_chain else driver
+    adapt = driver.adapt_step_size
+    if adapt and getattr(driver, "dual_device", None) is None:
+        driver.dual_device = DeviceDualAveraging(driver.dual, run.device)
+    in_window = mass.in_mass_window(iteration)
+    var = mass.variance
+    nat.check(lib.ut_warmup_adapt(
+        nat.ptr(run.accept_prob), nat.ptr(accepted), nat.ptr(run.divergent), run.C, run.P, nat.ptr(var.state),
+        var.window_length, nat.ptr(weights) if in_window else None,
+        nat.ptr(driver.dual_device.state) if adapt else None, 1 if per_chain else 0, 1 if adapt else 0,
+        float(driver.target_accept), nat.ptr(run.step), _stream_handle()))
+    if in_window:
+        var.update_device(run.position, weights)
+        if iteration == mass.schedule.slow_window_ends[mass.mass_window_index - 1]:
+            mass.end_window()
+            steps = run.step.double().cpu().numpy()
+            if adapt and iteration < num_warmup and refind is not None:
+                steps = np.asarray(refind(steps if per_chain else float(steps[0]), mass.inverse_mass_matrix),
+                                   dtype=np.float64)
+                driver.dual = DualAveraging(steps if per_chain else float(steps), driver.target_accept)
+                driver.dual_device = DeviceDualAveraging(driver.dual, run.device)
+            if per_chain:
+                driver.step_sizes = np.broadcast_to(steps, (run.C,)).copy()
+            else:
+                driver.step_size = float(np.ravel(steps)[0])
+            run.set_mass_and_step(mass.inverse_mass_matrix, driver.step_sizes if per_chain else driver.step_size)
+    if iteration == num_warmup:
+        if adapt:
+            nat.check(lib.ut_dual_averaging_final(nat.ptr(driver.dual_device.state), run.C, 1 if per_chain else 0,
+                                                  nat.ptr(run.step), _stream_handle()))
+        steps = run.step.double().cpu().numpy()
+        if per_chain:
+            driver.step_sizes = steps
+        else:
+            driver.step_size = float(steps[0])
+        if mass.adapt_mass_matrix and mass.variance.effective_count() >= mass.min_samples:
+            mass.inverse_mass_matrix = mass.variance.inverse_mass(mass.regularization)
+        run.set_mass_and_step(mass.inverse_mass_matrix, driver.step_sizes if per_chain else driver.step_size)
 
 
 # ---------------------------------------------------------------------------
@@ -742,7 +831,13 @@ def batched_hmc(model, args=(), constraints=None, *, num_chains, num_samples, nu
                 adapt_mass_matrix=True, per_chain_adaptation=None, find_reasonable_step_size=False,
                 divergence_threshold=1000.0, mass_matrix_regularization=1e-3, mass_matrix_min_samples=10,
                 callback=None, callback_every=10, backend="cuda", precision=None, rng=None,
-                init_strategy="prior", init_max_retries=100) -> HMCChains:
+                init_strategy="prior", init_max_retries=100, device_adaptation=True) -> HMCChains:
+    """reference: batched_hmc (src/inference/api_batched_hmc.jl:16-300; device loop
+    src/device/hmc_kernels.jl:306-723).  With device_adaptation (the default,
+    when no callback is given) every warmup iteration's step-size and
+    mass-window bookkeeping runs on the device (ut_warmup_adapt), so the host
+    only synchronises at mass-window ends; device_adaptation=False runs the
+    same arithmetic on the host from O(C) copies per iteration."""
     _validate_init("batched_hmc", init_strategy, init_max_retries)
     _validate_common(num_chains, num_samples, num_warmup, step_size, target_accept, divergence_threshold,
                      mass_matrix_regularization, mass_matrix_min_samples)
@@ -773,17 +868,27 @@ def batched_hmc(model, args=(), constraints=None, *, num_chains, num_samples, nu
     draws = _DrawBuffer(run, num_samples)
     total = num_warmup + num_samples
     divergences = 0
+    on_device = device_adaptation and callback is None
+    div_count = torch.zeros((), dtype=torch.int64, device=run.device)
+    weights = torch.empty(C, dtype=torch.float64, device=run.device)
+    run.set_mass_and_step(driver.inverse_mass_matrix, driver.step_sizes if per_chain else driver.step_size)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     t_sample = None
     for it in range(1, total + 1):
         steps = driver.step_sizes if per_chain else driver.step_size
-        run.set_mass_and_step(driver.inverse_mass_matrix, steps)
+        if not on_device:
+            run.set_mass_and_step(driver.inverse_mass_matrix, steps)
         if it == num_warmup + 1:
             torch.cuda.synchronize()
             t_sample = time.perf_counter()
         run.hmc_iteration(num_leapfrog_steps, it, divergence_threshold)
-        if it <= num_warmup:
+        if it <= num_warmup and on_device:
+            div_count += run.divergent.sum()
+            _device_warmup_iteration(run, driver, per_chain, it, num_warmup, run.accepted, refind, weights)
+            if it == num_warmup:
+                divergences = int(div_count.item())
+        elif it <= num_warmup:
             ap = run.accept_prob.double().cpu().numpy()
             acc = run.accepted.cpu().numpy().astype(bool)
             div = run.divergent.cpu().numpy().astype(bool)
@@ -826,8 +931,13 @@ def batched_nuts(model, args=(), constraints=None, *, num_chains, num_samples, n
                  find_reasonable_step_size=False, divergence_threshold=1000.0, mass_matrix_regularization=1e-3,
                  mass_matrix_min_samples=10, callback=None, callback_every=10, tree_strategy="persistent",
                  backend="cuda", precision=None, persistent_gradient="auto", device_sync_per_leaf=False,
-                 adtype="auto", rng=None) -> HMCChains:
+                 adtype="auto", rng=None, device_adaptation=True) -> HMCChains:
     """Batched multinomial NUTS on the device (api_batched_nuts.jl:22-51).
+
+    With device_adaptation (the default, when no callback is given) every
+    warmup iteration's dual averaging and mass-window weights run on the device
+    (ut_warmup_adapt): warmup copies nothing to the host between mass-window
+    ends.  device_adaptation=False runs the same arithmetic on the host.
 
     tree_strategy "persistent" runs a whole iteration per chain in one launch;
     "masked" grows every chain's tree in lockstep, one leaf per batched
@@ -874,18 +984,29 @@ def batched_nuts(model, args=(), constraints=None, *, num_chains, num_samples, n
     total = num_warmup + num_samples
     divergences = 0
     grad_evals = torch.zeros((), dtype=torch.int64, device=run.device)
+    on_device = device_adaptation and callback is None
+    div_count = torch.zeros((), dtype=torch.int64, device=run.device)
+    weights = torch.empty(C, dtype=torch.float64, device=run.device)
+    run.set_mass_and_step(driver.inverse_mass_matrix, driver.step_sizes if per_chain else driver.step_size)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     t_sample = None
     for it in range(1, total + 1):
         steps = driver.step_sizes if per_chain else driver.step_size
-        run.set_mass_and_step(driver.inverse_mass_matrix, steps)
+        if not on_device:
+            run.set_mass_and_step(driver.inverse_mass_matrix, steps)
         if it == num_warmup + 1:
             torch.cuda.synchronize()
             t_sample = time.perf_counter()
         run.nuts_iteration(max_tree_depth, it, divergence_threshold, tree_strategy)
         grad_evals += run.integration_steps.sum()
-        if it <= num_warmup:
+        if it <= num_warmup and on_device:
+            div_count += run.divergent.sum()
+            # NUTS has no accept flag: its weights are the rejection weights of the accept statistic
+            _device_warmup_iteration(run, driver, per_chain, it, num_warmup, None, refind, weights)
+            if it == num_warmup:
+                divergences = int(div_count.item())
+        elif it <= num_warmup:
             ap = run.accept_prob.double().cpu().numpy()
             div = run.divergent.cpu().numpy().astype(bool)
             divergences += int(div.sum())
