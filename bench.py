@@ -332,7 +332,8 @@ def run_b200(args):
                     # the metric's own comparison: surrogate-driven trajectories vs plain NUTS on the same model
                     nuts = samplers["glm100000x100_nuts"]
                     sur["plain_nuts"] = {k: nuts[k] for k in ("min_ess_per_s", "min_ess", "max_rank_rhat", "sampling_s")}
-                    sur["ratio_vs_plain_nuts"] = sur["surrogate"]["min_ess_per_s"] / nuts["min_ess_per_s"]
+                    for v in ("fixed16", "adapted_reference", "adapted_forward"):
+                        sur[v]["ratio_vs_plain_nuts"] = sur[v]["surrogate"]["min_ess_per_s"] / nuts["min_ess_per_s"]
                 _emit("surrogate_chees", sur)
             if not args.no_uneven:
                 _emit("uneven_batch", uneven_batch())
@@ -563,39 +564,57 @@ def glm_large_meads(num_chains=4096, num_warmup=3000, num_samples=1000):
                                              "step_size": float(np.mean(ch.step_size))})
 
 
-def surrogate_comparison(num_chains=4096, num_warmup=500, num_samples=500):
-    """The learned-surrogate workload on the same model: ChEES-HMC with exact
-    gradients vs ChEES-HMC whose trajectories the trained MLP drives (exact
-    logjoint in the accept), same seeds and settings (16 initial leapfrog
-    steps, trajectory length and step size adapted in warmup).  The surrogate
-    is trained on 2^20 (theta, gradient) pairs of the last 256 warmup
-    iterations.  Min ESS over the 100 coefficients per second of sampling
-    (warmup, training and step-size re-tuning excluded, reported apart).
-    Both arms adapt the trajectory length with the forward endpoint velocity
-    (an ascent on the ChEES criterion); the reference's own estimator descends
-    it and on this workload can collapse T to the step size."""
+def _surrogate_pair(model, X, y, **kw):
+    """Plain ChEES-HMC and surrogate-driven ChEES-HMC with the same settings:
+    min ESS per sampling second (and per total second: warmup + surrogate
+    training + sampling), rank R-hat, mean trajectory steps, the ratio, and
+    the largest difference of posterior means in posterior SDs."""
     from uncertaintea_b200 import batched_chees, batched_chees_surrogate, ess, rhat
-    model, X, y, _ = _data()
-    kw = dict(num_chains=num_chains, num_samples=num_samples, num_warmup=num_warmup, num_leapfrog_steps=16, rng=1,
-              trajectory_velocity="forward")
-    out = {}
     runs = {"plain": batched_chees(model, (X,), {"y": y}, **kw),
             "surrogate": batched_chees_surrogate(model, (X,), {"y": y}, **kw)}
+    out = {}
     for name, ch in runs.items():
-        e, r = ess(ch, space="unconstrained"), rhat(ch, space="unconstrained")
+        e, r = ess(ch, space="unconstrained"), rhat(ch, space="unconstrained", method="rank")
+        total_s = ch.warmup_seconds + ch.sampling_seconds
         out[name] = {"min_ess_per_s": float(np.min(e) / ch.sampling_seconds), "min_ess": float(np.min(e)),
-                     "max_rhat": float(np.max(r)), "sampling_s": ch.sampling_seconds, "warmup_s": ch.warmup_seconds,
+                     "min_ess_per_total_s": float(np.min(e) / total_s), "max_rank_rhat": float(np.max(r)),
+                     "sampling_s": ch.sampling_seconds, "warmup_s": ch.warmup_seconds,
                      "mean_leapfrog_steps": float(ch.integration_steps.mean()),
                      "mean_accept": float(ch.accept_prob.mean()), "step_size": float(np.mean(ch.step_size))}
     rep = runs["surrogate"].surrogate
-    out["surrogate"].update({"pairs": rep.num_pairs, "train_steps": rep.train_steps,
-                             "train_s": rep.train_seconds, "relative_error": rep.relative_error_after_training,
-                             "fallback_at": rep.fallback_at})
+    out["surrogate"].update({"pairs": rep.num_pairs, "train_steps": rep.train_steps, "train_s": rep.train_seconds,
+                             "relative_error": rep.relative_error_after_training, "fallback_at": rep.fallback_at})
     up = runs["plain"].unconstrained.reshape(-1, N_COEF)
     us = runs["surrogate"].unconstrained.reshape(-1, N_COEF)
     out["max_mean_diff_in_sd"] = float(np.max(np.abs(up.mean(0) - us.mean(0)) / up.std(0)))
     out["ratio"] = out["surrogate"]["min_ess_per_s"] / out["plain"]["min_ess_per_s"]
-    out["metric"] = "min ESS/s (R-hat<1.01), surrogate ChEES-HMC vs plain ChEES-HMC"
+    out["ratio_including_warmup_and_training"] = (out["surrogate"]["min_ess_per_total_s"]
+                                                  / out["plain"]["min_ess_per_total_s"])
+    out["gate_rank_rhat_lt_1.01"] = bool(max(out["plain"]["max_rank_rhat"], out["surrogate"]["max_rank_rhat"]) < 1.01)
+    return out
+
+
+def surrogate_comparison(num_chains=4096, num_warmup=500, num_samples=500):
+    """The learned-surrogate workload on the same model: ChEES-HMC with exact
+    gradients vs ChEES-HMC whose trajectories the trained MLP drives (exact
+    logjoint in the accept), same seeds and settings.  The surrogate is trained
+    on 2^20 (theta, gradient) pairs of the last 256 warmup iterations.
+    Variants:
+      fixed16            -- 16 leapfrog steps every iteration (the trajectory
+                            budget of the configuration), step size adapted;
+      adapted_reference  -- trajectory length adapted with the reference's
+                            estimator (16 initial steps);
+      adapted_forward    -- adapted with the forward endpoint velocity (an
+                            ascent on the ChEES criterion).
+    Min ESS over the 100 coefficients per second of sampling, and per second
+    of warmup + training + sampling."""
+    model, X, y, _ = _data()
+    base = dict(num_chains=num_chains, num_samples=num_samples, num_warmup=num_warmup, rng=1)
+    out = {"fixed16": _surrogate_pair(model, X, y, fixed_leapfrog_steps=16, **base),
+           "adapted_reference": _surrogate_pair(model, X, y, num_leapfrog_steps=16, **base),
+           "adapted_forward": _surrogate_pair(model, X, y, num_leapfrog_steps=16, trajectory_velocity="forward",
+                                              **base)}
+    out["metric"] = "min ESS/s (rank R-hat<1.01), surrogate ChEES-HMC vs plain ChEES-HMC"
     out["unit"] = "effective samples/s"
     out["config"] = (f"learned gradient surrogate on the 100000x100 logistic regression, {num_chains} chains, "
                      f"{num_warmup} warmup + {num_samples} sampling iterations")
@@ -618,15 +637,19 @@ def uneven_models(num_models=512, seed=5):
     return models
 
 
-def uneven_batch(num_models=512, chains=64, num_warmup=500, num_samples=500):
+def uneven_batch(num_models=512, chains=64, num_warmup=500, num_samples=1500):
     """All models in one batched persistent-NUTS run (one launch per
     parameter-slot class per iteration, replayed from a CUDA graph, launch
     shapes from the autotuner): aggregate min-ESS per sampling second and the
-    per-model time to R-hat < 1.01 (checked every 50 draws)."""
+    per-model time to R-hat < 1.01 (checked every 50 draws).  Per-model
+    stopping: a model that reaches the target stops there and the rest run on,
+    up to num_samples draws (the cap); ESS and R-hat are over each model's own
+    draws."""
     from uncertaintea_b200.multi import batched_nuts_multi
     models = uneven_models(num_models)
     res = batched_nuts_multi(models, chains_per_model=chains, num_warmup=num_warmup, num_samples=num_samples,
-                             rng=1, rhat_check_every=50)
+                             rng=1, rhat_check_every=50, stop_converged=True)
+    drawn = int(res.draws_per_model.max())
     fin = lambda v: v if np.isfinite(v) else None  # noqa: E731  (null: not reached within the run)
     p50, p99 = (fin(v) for v in res.time_to_rhat_quantiles())
     s50, s99 = (fin(v) for v in res.time_to_rhat_quantiles(from_sampling=True))
@@ -638,15 +661,17 @@ def uneven_batch(num_models=512, chains=64, num_warmup=500, num_samples=500):
            "time_to_rhat_note": "null = that share of models did not reach R-hat < 1.01 within the run",
            "converged_fraction": res.converged_fraction, "median_model_min_ess": float(np.median(res.min_ess)),
            "warmup_s": res.warmup_seconds, "sampling_s": res.sampling_seconds,
-           "ms_per_iteration": 1000.0 * res.sampling_seconds / num_samples,
+           "ms_per_iteration": 1000.0 * res.sampling_seconds / max(drawn, 1),
+           "draws_cap": num_samples, "draws_run": drawn,
+           "draws_per_model_p50": float(np.median(res.draws_per_model)),
            "mean_tree_depth": res.mean_tree_depth, "divergences": res.divergences,
            "total_obs": int(sum(int(m[1][1].sum()) for m in models)), "total_chains": int(res.num_chains.sum()),
            "classes": {"slots": cls["slots"].tolist(), "models": cls["models"].tolist(),
                        "chains_per_block": cls["chains_per_block"].tolist(),
                        "stage_limit_bytes": cls["stage_limit_bytes"].tolist()},
            "config": (f"uneven batch: {num_models} non-centred hierarchical models, J~U[8,512], obs/group~U[5,100], "
-                      f"{chains} chains each, max tree depth 10, {num_warmup} warmup + {num_samples} draws, "
-                      "CUDA graph replay, autotuned launch shapes")}
+                      f"{chains} chains each, max tree depth 10, {num_warmup} warmup + up to {num_samples} draws, "
+                      "per-model stopping at R-hat<1.01, CUDA graph replay, autotuned launch shapes")}
     res.batch.close()
     return out
 

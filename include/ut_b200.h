@@ -668,6 +668,13 @@ int32_t ut_multi_autotune(ut_multi* mm, int32_t trials, float* timings_ms, void*
 /* Max split R-hat over each model's parameters from its first num_draws
  * recorded draws (d_out: num_models floats). */
 int32_t ut_multi_split_rhat(ut_multi* mm, int32_t num_draws, float* d_out, void* stream);
+/* Per-model stopping: stopped[m] != 0 (host array of num_models bytes) makes
+ * the following iterations skip model m's chains -- their positions, steps and
+ * adaptation state stay as they are -- so the batch's work goes to the models
+ * still running.  The draw buffer keeps recording every model; a stopped
+ * model's later draws repeat its last state and are not its samples.  Reset
+ * to all-running by ut_multi_begin.  No counterpart in the reference. */
+int32_t ut_multi_set_stopped(ut_multi* mm, const uint8_t* stopped, void* stream);
 int32_t ut_multi_buffers(const ut_multi* mm, ut_multi_view* view);
 
 #ifdef __cplusplus

@@ -425,7 +425,7 @@ void grad_magnitude(const ModelData& m, const double* q, double* a) {
     const int P = p.num_params;
     for (int k = 0; k < P; ++k) a[k] = 0.0;
     switch (p.family) {
-    case UT_FAMILY_PROGRAM:  // per row: the sum over the terms of |d term / d row|
+    case UT_FAMILY_PROGRAM:  // per row: the magnitudes of every contribution to the derivative
         oracle_program::logjoint_grad(m.prog, m.y, q, nullptr, a);
         break;
     case UT_FAMILY_GLM_BERNOULLI_LOGIT: {

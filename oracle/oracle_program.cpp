@@ -30,38 +30,53 @@ Program& current() {
 
 namespace {
 
+// Forward-mode dual seeded on one parameter row: value v, derivative d, and m,
+// the sum of the magnitudes of every contribution to d (each operation adds
+// |partial| x |operand's m| instead of partial x operand's d).  m is the scale
+// of the rounding error of an evaluation of d, cancellation included.
 struct Dual {
-    double v, d;
+    double v, d, m;
 };
-inline Dual C(double v) { return {v, 0.0}; }
-inline Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
-inline Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
-inline Dual operator-(Dual a) { return {-a.v, -a.d}; }
-inline Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
-inline Dual operator/(Dual a, Dual b) { return {a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v)}; }
-inline Dual operator+(Dual a, double b) { return {a.v + b, a.d}; }
-inline Dual operator-(Dual a, double b) { return {a.v - b, a.d}; }
-inline Dual operator-(double a, Dual b) { return {a - b.v, -b.d}; }
-inline Dual operator*(double a, Dual b) { return {a * b.v, a * b.d}; }
-inline Dual operator/(Dual a, double b) { return {a.v / b, a.d / b}; }
-inline Dual dlog(Dual a) { return {std::log(a.v), a.d / a.v}; }
-inline Dual dexp(Dual a) { const double e = std::exp(a.v); return {e, a.d * e}; }
-inline Dual dlog1p(Dual a) { return {std::log1p(a.v), a.d / (1.0 + a.v)}; }
-inline Dual dsqrt(Dual a) { const double s = std::sqrt(a.v); return {s, a.d * 0.5 / s}; }
+inline Dual C(double v) { return {v, 0.0, 0.0}; }
+inline Dual un(double v, double dv, const Dual& a) { return {v, dv * a.d, std::fabs(dv) * a.m}; }
+inline Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d, a.m + b.m}; }
+inline Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d, a.m + b.m}; }
+inline Dual operator-(Dual a) { return {-a.v, -a.d, a.m}; }
+inline Dual operator*(Dual a, Dual b) {
+    return {a.v * b.v, a.d * b.v + a.v * b.d, a.m * std::fabs(b.v) + std::fabs(a.v) * b.m};
+}
+inline Dual operator/(Dual a, Dual b) {
+    return {a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v),
+            a.m / std::fabs(b.v) + std::fabs(a.v) * b.m / (b.v * b.v)};
+}
+inline Dual operator+(Dual a, double b) { return {a.v + b, a.d, a.m}; }
+inline Dual operator-(Dual a, double b) { return {a.v - b, a.d, a.m}; }
+inline Dual operator-(double a, Dual b) { return {a - b.v, -b.d, b.m}; }
+inline Dual operator*(double a, Dual b) { return {a * b.v, a * b.d, std::fabs(a) * b.m}; }
+inline Dual operator/(Dual a, double b) { return {a.v / b, a.d / b, a.m / std::fabs(b)}; }
+inline Dual dlog(Dual a) { return un(std::log(a.v), 1.0 / a.v, a); }
+inline Dual dexp(Dual a) { const double e = std::exp(a.v); return un(e, e, a); }
+inline Dual dlog1p(Dual a) { return un(std::log1p(a.v), 1.0 / (1.0 + a.v), a); }
+inline Dual dsqrt(Dual a) { const double s = std::sqrt(a.v); return un(s, 0.5 / s, a); }
 inline Dual dabs(Dual a) { return a.v < 0 ? -a : a; }
-inline Dual dsin(Dual a) { return {std::sin(a.v), a.d * std::cos(a.v)}; }
-inline Dual dcos(Dual a) { return {std::cos(a.v), -a.d * std::sin(a.v)}; }
-inline Dual dtan(Dual a) { const double t = std::tan(a.v); return {t, a.d * (1.0 + t * t)}; }
-inline Dual dtanh(Dual a) { const double t = std::tanh(a.v); return {t, a.d * (1.0 - t * t)}; }
-inline Dual dsinh(Dual a) { return {std::sinh(a.v), a.d * std::cosh(a.v)}; }
-inline Dual dcosh(Dual a) { return {std::cosh(a.v), a.d * std::sinh(a.v)}; }
-inline Dual datan(Dual a) { return {std::atan(a.v), a.d / (1.0 + a.v * a.v)}; }
-inline Dual dexpm1(Dual a) { return {std::expm1(a.v), a.d * std::exp(a.v)}; }
+inline Dual dsin(Dual a) { return un(std::sin(a.v), std::cos(a.v), a); }
+inline Dual dcos(Dual a) { return un(std::cos(a.v), -std::sin(a.v), a); }
+inline Dual dtan(Dual a) { const double t = std::tan(a.v); return un(t, 1.0 + t * t, a); }
+inline Dual dtanh(Dual a) { const double t = std::tanh(a.v); return un(t, 1.0 - t * t, a); }
+inline Dual dsinh(Dual a) { return un(std::sinh(a.v), std::cosh(a.v), a); }
+inline Dual dcosh(Dual a) { return un(std::cosh(a.v), std::sinh(a.v), a); }
+inline Dual datan(Dual a) { return un(std::atan(a.v), 1.0 / (1.0 + a.v * a.v), a); }
+inline Dual dexpm1(Dual a) { return un(std::expm1(a.v), std::exp(a.v), a); }
 inline Dual dpow(Dual a, Dual b) {
     const double p = std::pow(a.v, b.v);
-    double d = b.v * std::pow(a.v, b.v - 1.0) * a.d;
-    if (b.d != 0.0) d += p * std::log(a.v) * b.d;
-    return {p, d};
+    const double pa = b.v * std::pow(a.v, b.v - 1.0);
+    double d = pa * a.d, m = std::fabs(pa) * a.m;
+    if (b.d != 0.0 || b.m != 0.0) {
+        const double pb = p * std::log(a.v);
+        d += pb * b.d;
+        m += std::fabs(pb) * b.m;
+    }
+    return {p, d, m};
 }
 inline Dual dmin(Dual a, Dual b) { return a.v <= b.v ? a : b; }
 inline Dual dmax(Dual a, Dual b) { return a.v >= b.v ? a : b; }
@@ -79,7 +94,7 @@ double digamma(double x) {
                                                                                                       r2 * (691.0 / 32760))))));
     return acc + std::log(x) - 0.5 * r - s;
 }
-inline Dual dlgamma(Dual a) { return {std::lgamma(a.v), a.d * digamma(a.v)}; }
+inline Dual dlgamma(Dual a) { return un(std::lgamma(a.v), digamma(a.v), a); }
 
 const double kNegInf = -std::numeric_limits<double>::infinity();
 const double kHalfLog2Pi = 0.9189385332046727;  // math.jl:90
@@ -225,12 +240,6 @@ struct Walker {
     const Dual* q;
     std::vector<Dual> slots;
     std::vector<long long> base;   // block base row per loop depth
-    double absd = 0.0;             // sum over terms of |d term / d seeded row|
-
-    Dual term(Dual t) {
-        absd += std::fabs(t.d);
-        return t;
-    }
 
     Dual eval(int i) {
         const ut_expr_node& n = p.nodes[i];
@@ -284,14 +293,14 @@ struct Walker {
                     if (s.value_source >= 0) x = transform(s.transform, q[s.value_source], lad);
                     else x = C(obs[base[depth] + s.obs_offset]);
                     bind(s.binding_slot, x);
-                    total = total + term(logpdf(s.dist, a, x) + lad);
+                    total = total + logpdf(s.dist, a, x) + lad;
                     ++i;
                     break;
                 }
                 case UT_STEP_IID_NORMAL: {  // DeviceDiagNormalChoiceStepDyn (logjoint_kernel.jl:514-533)
                     const Dual mu = eval(s.arg[0]), sg = eval(s.arg[1]);
                     Dual a[2] = {mu, sg};
-                    for (int d = 0; d < s.count; ++d) total = total + term(logpdf(UT_DIST_NORMAL, a, q[s.value_source + d]));
+                    for (int d = 0; d < s.count; ++d) total = total + logpdf(UT_DIST_NORMAL, a, q[s.value_source + d]);
                     ++i;
                     break;
                 }
@@ -303,7 +312,7 @@ struct Walker {
                         Dual eta = icpt;
                         for (int d = 0; d < F; ++d) eta = eta + q[s.value_source + d] * C(obs[row + d]);
                         Dual a[1] = {eta};
-                        total = total + term(logpdf(UT_DIST_BERNOULLI_LOGIT, a, C(obs[row + F])));
+                        total = total + logpdf(UT_DIST_BERNOULLI_LOGIT, a, C(obs[row + F]));
                     }
                     ++i;
                     break;
@@ -336,12 +345,12 @@ double logjoint_grad(const Program& prog, const std::vector<double>& obs, const 
     const bool seed = g || mag;
     const int passes = seed ? P : 1;
     for (int s = 0; s < passes; ++s) {
-        for (int r = 0; r < P; ++r) qd[r] = {q[r], (seed && r == s) ? 1.0 : 0.0};
+        for (int r = 0; r < P; ++r) qd[r] = {q[r], (seed && r == s) ? 1.0 : 0.0, (seed && r == s) ? 1.0 : 0.0};
         Walker w{prog, obs, qd.data(), std::vector<Dual>(std::max(prog.nslots, 1)), std::vector<long long>(1, 0)};
         const Dual t = w.walk(0, (int)prog.steps.size(), 0);
         value = t.v;
         if (g) g[s] = t.d;
-        if (mag) mag[s] = w.absd;
+        if (mag) mag[s] = t.m;
     }
     return value;
 }

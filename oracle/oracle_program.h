@@ -21,8 +21,9 @@ Program& current();
 
 // Logjoint (and, when g != nullptr, its gradient) of one chain in float64,
 // the gradient by forward-mode duals, one pass per parameter row.  With mag,
-// also the gradient magnitude: per row, the sum over the density's terms of
-// |d term / d row|.
+// also the gradient magnitude: per row, the sum of the magnitudes of every
+// contribution to the derivative (each operation's |partial| times its
+// operand's magnitude), the scale of the FP32 rounding error of the gradient.
 double logjoint_grad(const Program& prog, const std::vector<double>& obs, const double* q, double* g,
                      double* mag = nullptr);
 

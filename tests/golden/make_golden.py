@@ -6,7 +6,7 @@ pins of test/uncertaintea/core/batched_chees_adaptation.jl:50-72, and writes
 them as a small JSON fixture that the test suite loads.  The GPU box never
 needs the reference tree.
 
-Usage: python tests/golden/make_golden.py [reference_root]
+Usage: python tests/golden/make_golden.py <reference_root>   (a checkout of shohei81/uncertaintea)
 """
 from __future__ import annotations
 
@@ -61,4 +61,6 @@ def main(root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <checkout of shohei81/uncertaintea>")
+    main(sys.argv[1])

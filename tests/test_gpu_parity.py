@@ -65,8 +65,14 @@ def _grad_ok(g, g64, mag):
     """Both gradient bounds: elementwise |g - g64| <= 1e-5 |g64| + 1e-6 m, and
     the per-chain norm bound max_p |g - g64| <= 1e-5 max_p |g64|."""
     g = np.asarray(g, dtype=np.float64)
-    over = np.max(np.abs(g - g64) / (GRAD_RTOL * np.abs(g64) + GRAD_ATOL_MAG * mag))
-    return over <= 1.0 and _grad_err(g, g64) <= GRAD_RTOL
+    ratio = np.abs(g - g64) / (GRAD_RTOL * np.abs(g64) + GRAD_ATOL_MAG * mag)
+    over = np.max(ratio)
+    ok = over <= 1.0 and _grad_err(g, g64) <= GRAD_RTOL
+    if not ok:  # the worst component, shown with the failing assert
+        i = np.unravel_index(np.argmax(ratio), ratio.shape)
+        print(f"gradient bound: worst {i}: g={g[i]!r} g64={g64[i]!r} m={mag[i]!r} over={over:.3g}; "
+              f"norm error {_grad_err(g, g64):.3g}")
+    return ok
 
 
 def _lj_err(t, t64):

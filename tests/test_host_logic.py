@@ -328,6 +328,64 @@ def test_diagnostics_iid_draws():
     assert np.all(rr < 1.02)
 
 
+def _rank_rhat_loops(chains):
+    """The reference's rank-normalised R-hat of one parameter, restated with
+    loops (diagnostics.jl:500-511 split matrix, :589-600 ranks of the
+    column-major flattening by a stable sort, :602-612 bulk and folded)."""
+    from statistics import NormalDist
+    C, S = len(chains), len(chains[0])
+    h = S // 2
+    split = []
+    for c in range(C):
+        split.append(list(chains[c][:h]))
+        split.append(list(chains[c][h:2 * h]))
+
+    def rhat_of(m):
+        means = [sum(r) / h for r in m]
+        var = [sum((v - mu) ** 2 for v in r) / (h - 1) for r, mu in zip(m, means)]
+        W = sum(var) / len(m)
+        gm = sum(means) / len(m)
+        B = h * sum((mu - gm) ** 2 for mu in means) / (len(m) - 1)
+        return math.sqrt(max(((h - 1) / h * W + B / h) / W, 1.0))
+
+    def rank_normal(m):
+        flat = [m[i][j] for j in range(h) for i in range(len(m))]  # column-major
+        order = sorted(range(len(flat)), key=lambda k: flat[k])   # stable
+        ranks = [0] * len(flat)
+        for pos, k in enumerate(order):
+            ranks[k] = pos + 1
+        n = len(flat)
+        z = [NormalDist().inv_cdf((r - 0.375) / (n + 0.25)) for r in ranks]
+        return [[z[j * len(m) + i] for j in range(h)] for i in range(len(m))]
+
+    vals = sorted(v for r in split for v in r)
+    n = len(vals)
+    med = 0.5 * (vals[(n - 1) // 2] + vals[n // 2])
+    folded = [[abs(v - med) for v in r] for r in split]
+    return max(rhat_of(rank_normal(split)), rhat_of(rank_normal(folded)))
+
+
+def test_rank_rhat_ties_follow_reference_order():
+    """Repeated states (rejected proposals) tie; their ranks follow the
+    reference's order, in the host diagnostics and the device gate alike."""
+    import torch
+    from uncertaintea_b200.multi import rank_split_rhat
+    rng = np.random.default_rng(11)
+    d = np.round(rng.standard_normal((5, 41, 2)), 1)   # (C, S, P) with many ties
+    d[0] += 0.3
+
+    class Fake:
+        constrained = d
+        unconstrained = d
+
+    host = dg.rhat(Fake, method="rank")
+    dev = rank_split_rhat(torch.from_numpy(d.transpose(1, 0, 2).copy())).numpy()
+    for p in range(2):
+        ref = _rank_rhat_loops(d[:, :, p].tolist())
+        assert host[p] == pytest.approx(ref, rel=1e-12)
+        assert dev[p] == pytest.approx(ref, rel=1e-12)
+
+
 def test_diagnostics_detect_disagreeing_chains():
     rng = np.random.default_rng(1)
 

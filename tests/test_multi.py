@@ -195,6 +195,73 @@ def test_batched_nuts_multi_end_to_end(lib):
 
 
 @pytest.mark.gpu
+def test_stopped_model_keeps_its_state(lib):
+    """ut_multi_set_stopped: a stopped model's positions, step sizes and
+    adaptation state stay as they were through warmup and sampling
+    iterations, its later draw rows repeat its last state, and the other
+    models' iterations are bitwise those of a run without the stop (each
+    chain's Philox key is its global chain index)."""
+    torch = pytest.importorskip("torch")
+    from uncertaintea_b200.multi import MultiModelBatch
+    models = _models(SPEC, seed=4)
+    ref = _run_state(models, CHAINS, 14, seed=13)
+    batch = MultiModelBatch(models, CHAINS, max_tree_depth=8)
+    r = np.random.default_rng(5)
+    qs = [_near_mode(ma, c, r) for ma, c in zip(models, CHAINS)]
+    batch.set_positions(np.concatenate([q.reshape(-1) for q in qs]))
+    batch.begin(6, 8, 13, initial_step=0.05)
+    batch.run(4, use_graph=False)
+    torch.cuda.synchronize()
+    a, b = int(batch.state_offsets[1]), int(batch.state_offsets[2])
+    c0, c1 = int(batch.chain_offsets[1]), int(batch.chain_offsets[2])
+    p0, p1 = int(batch.param_offsets[1]), int(batch.param_offsets[2])
+    v = batch.view()
+    before = {k: v[k].cpu().numpy().copy() for k in ("position", "step", "inverse_mass")}
+    batch.set_stopped(np.array([0, 1, 0, 0], dtype=np.uint8))
+    batch.run(10, use_graph=True)
+    torch.cuda.synchronize()
+    v = batch.view()
+    after = {k: v[k].cpu().numpy() for k in ("position", "step", "inverse_mass")}
+    assert np.array_equal(after["position"][a:b], before["position"][a:b])
+    assert np.array_equal(after["step"][c0:c1], before["step"][c0:c1])
+    assert np.array_equal(after["inverse_mass"][p0:p1], before["inverse_mass"][p0:p1])
+    d = v["draws"].cpu().numpy()
+    assert np.all(d[:, a:b] == before["position"][a:b][None, :])   # all 8 draws follow the stop
+    others = np.ones(ref["position"].shape[0], dtype=bool)
+    others[a:b] = False
+    assert np.array_equal(after["position"][others], ref["position"][others])
+    batch.close()
+
+
+@pytest.mark.gpu
+def test_per_model_stopping_run(lib):
+    """batched_nuts_multi(stop_converged=True): converged models stop at the
+    checkpoint that confirmed R-hat < 1.01 (rank-normalised, over their own
+    draws), the others run to the cap, and each model's summary covers its
+    own draws only."""
+    from uncertaintea_b200 import batched_nuts_multi
+    easy = _models([(8, 3), (30, 2), (64, 2)], seed=21, sigma_range=(4.0, 8.0))
+    hard = _models([(200, 60)], seed=2, sigma_range=(0.5, 0.6))  # informative: slow in the non-centred form
+    models = easy + hard
+    cap = 400
+    res = batched_nuts_multi(models, chains_per_model=32, num_warmup=300, num_samples=cap, rng=5,
+                             rhat_check_every=50, stop_converged=True)
+    own = res.draws_per_model
+    stopped = np.isfinite(res.time_to_rhat)
+    assert stopped[:3].all(), res.max_rhat
+    assert np.all(own[stopped] % 50 == 0) and np.all(own[stopped] <= cap)
+    assert np.all(res.max_rhat[stopped] < 1.01)
+    assert np.all(own[~stopped] == own.max())
+    if (~stopped).any():
+        assert own.max() == cap
+    d = res.batch.view()["draws"].cpu().numpy()
+    for m in np.flatnonzero(stopped & (own < own.max())):
+        a, b = int(res.batch.state_offsets[m]), int(res.batch.state_offsets[m + 1])
+        assert np.all(d[own[m]:own.max(), a:b] == d[own[m] - 1, a:b][None, :])
+    res.batch.close()
+
+
+@pytest.mark.gpu
 def test_multi_validation(lib):
     from uncertaintea_b200 import BernoulliLogitGLM, logistic_regression_data
     from uncertaintea_b200.multi import MultiModelBatch

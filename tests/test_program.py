@@ -295,3 +295,65 @@ def test_program_report_accepts_and_rejects(lib):
                         with p.loop(1, 1):
                             p.observe("normal", 0.0, 1.0, row=0)
     bad(deep, 1, "nest at most 4 deep")
+
+
+def _host_math(tmp_path):
+    """The device interpreter's distribution math compiled for the host."""
+    import ctypes
+    import os
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    lib = str(tmp_path / "program_math.so")
+    subprocess.run(["nvcc", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "-gencode",
+                    "arch=compute_100a,code=sm_100a", "-o", lib,
+                    os.path.join(root, "tests", "c_host", "program_math.cu")], check=True)
+    h = ctypes.CDLL(lib)
+    h.prog_dist_host.restype = ctypes.c_float
+    h.prog_dist_host.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_float), ctypes.c_float,
+                                 ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]
+    h.prog_digamma_host.restype = ctypes.c_float
+    h.prog_digamma_host.argtypes = [ctypes.c_float]
+    return h
+
+
+def test_device_distribution_math_matches_scipy_and_its_derivatives(tmp_path):
+    """Every distribution of the device interpreter (compiled for the host):
+    the float32 log-density against scipy in float64, and each partial
+    derivative (arguments and value) against float64 central differences of
+    scipy's density, at several argument points."""
+    import ctypes
+    h = _host_math(tmp_path)
+    r = np.random.default_rng(0)
+    discrete = ("bernoulli", "bernoullilogit", "poisson", "geometric", "negativebinomial", "binomial")
+    for name, args, x, ref in _CASES:
+        code = nat.DISTRIBUTIONS[name]
+        for trial in range(4):
+            a = np.array(args, dtype=np.float64)
+            if trial:   # perturb the continuous arguments (binomial trials stay integral)
+                scale = np.where(np.arange(a.size) == 0 if name == "binomial" else False, 0.0, 0.15)
+                a = a * np.exp(scale * r.standard_normal(a.size))
+            a32 = (ctypes.c_float * 3)(*[float(np.float32(v)) for v in a] + [0.0] * (3 - a.size))
+            da = (ctypes.c_float * 3)()
+            dx = ctypes.c_float()
+            x32 = float(np.float32(x))
+            lp = h.prog_dist_host(code, a32, x32, da, ctypes.byref(dx))
+            av = np.array([a32[k] for k in range(a.size)], dtype=np.float64)
+            want = ref(av, x32)
+            assert lp == pytest.approx(want, rel=2e-6, abs=2e-6), (name, trial)
+            for k in range(a.size):
+                if name == "binomial" and k == 0:
+                    continue
+                e = np.zeros_like(av)
+                e[k] = 1e-6 * max(1.0, abs(av[k]))
+                fd = (ref(av + e, x32) - ref(av - e, x32)) / (2 * e[k])
+                assert da[k] == pytest.approx(fd, rel=2e-4, abs=2e-4 * max(1.0, abs(fd))), (name, trial, k)
+            if name not in discrete:
+                hx = 1e-6 * max(1.0, abs(x32))
+                fd = (ref(av, x32 + hx) - ref(av, x32 - hx)) / (2 * hx)
+                assert dx.value == pytest.approx(fd, rel=2e-4, abs=2e-4 * max(1.0, abs(fd))), (name, trial, "x")
+
+
+def test_device_digamma_against_scipy(tmp_path):
+    h = _host_math(tmp_path)
+    for x in [1e-3, 0.05, 0.3, 0.5, 1.0, 1.7, 2.5, 4.0, 5.9, 6.0, 7.5, 12.0, 50.0, 1e3, 1e5]:
+        assert h.prog_digamma_host(x) == pytest.approx(special.digamma(x), rel=3e-6, abs=3e-6), x

@@ -362,24 +362,27 @@ def test_surrogate_validation_errors(lib):
 @pytest.mark.gpu
 def test_surrogate_chees_gains_over_plain_chees(lib):
     """The learned surrogate's gain on the large logistic regression (the
-    100000 x 100 design scaled by 1/10, at 1024 chains): the same ChEES run
-    with exact gradients and with surrogate-driven trajectories.  Both reach
-    R-hat < 1.01 with posterior means within 0.05 posterior SD of each other;
-    the surrogate run's min-ESS per sampling second is at least twice the
-    plain run's (about 4x measured on B200 at 4096 chains)."""
+    100000 x 100 design scaled by 1/10, at 1024 chains), at the trajectory
+    budget the learned-surrogate configuration states: 16 leapfrog steps every
+    iteration.  The same ChEES run with exact gradients and with
+    surrogate-driven trajectories (exact logjoint in the accept) both reach
+    rank-normalised R-hat < 1.01 with posterior means within 0.05 posterior SD
+    of each other, and the surrogate run's min-ESS per sampling second is at
+    least 3x the plain run's."""
     from uncertaintea_b200 import (BernoulliLogitGLM, batched_chees, batched_chees_surrogate,
                                    logistic_regression_data, min_ess_per_second, rhat)
     X, y, _ = logistic_regression_data(100000, 100, seed=3, x_scale=0.1)
     m = BernoulliLogitGLM(100)
-    kw = dict(num_chains=1024, num_samples=300, num_warmup=300, num_leapfrog_steps=16, rng=1)
+    kw = dict(num_chains=1024, num_samples=300, num_warmup=300, fixed_leapfrog_steps=16, rng=1)
     plain = batched_chees(m, (X,), {"y": y}, **kw)
     sur = batched_chees_surrogate(m, (X,), {"y": y}, **kw)
     rep = sur.surrogate
     assert rep.fallback_at is None and rep.surrogate_iterations == 300
     assert rep.relative_error_after_training < 0.2
     for ch in (plain, sur):
-        assert np.max(rhat(ch, space="unconstrained")) < 1.01
+        assert np.max(rhat(ch, space="unconstrained", method="rank")) < 1.01
+        assert np.all(ch.integration_steps == 16)
     up, us = plain.unconstrained.reshape(-1, 100), sur.unconstrained.reshape(-1, 100)
     assert np.max(np.abs(up.mean(0) - us.mean(0)) / up.std(0)) < 0.05
     gain = min_ess_per_second(sur, "unconstrained") / min_ess_per_second(plain, "unconstrained")
-    assert gain >= 2.0, gain
+    assert gain >= 3.0, gain

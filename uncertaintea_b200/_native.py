@@ -226,6 +226,7 @@ SIGNATURES = [
     ("ut_multi_run", c_int32, [c_void_p, c_int32, c_int32, c_void_p]),
     ("ut_multi_autotune", c_int32, [c_void_p, c_int32, c_void_p, c_void_p]),
     ("ut_multi_split_rhat", c_int32, [c_void_p, c_int32, c_void_p, c_void_p]),
+    ("ut_multi_set_stopped", c_int32, [c_void_p, c_void_p, c_void_p]),
     ("ut_multi_buffers", c_int32, [c_void_p, POINTER(MultiView)]),
 ]
 

@@ -947,7 +947,9 @@ extern "C" int32_t ut_internal_tc_live_split(int32_t num_obs, int32_t num_chains
 extern "C" int32_t ut_internal_tc_tmem_plan(int32_t F, int32_t* out) {
     if (F < 1 || F > kTcMaxFp || !out) return UT_ERR_ARGUMENT;
     const int KC = 8 * tc_kblocks_used(F), Fp = ((F + 15) / 16) * 16, nb = tc_nbuf(F, Fp);
-    out[0] = KC; out[1] = Fp; out[2] = nb; out[3] = 2 * KC + Fp + 64 * nb;
+    int cols[3];
+    tc_columns(F, Fp, false, cols);
+    out[0] = KC; out[1] = Fp; out[2] = nb; out[3] = cols[2] + 64 * nb;
     return UT_OK;
 }
 

@@ -124,6 +124,7 @@ struct MmArgs {
     double* da;                // per chain dual-averaging state: mu, log_eps, log_eps_avg, hbar, t
     const uint8_t* actions;
     int num_warmup;
+    const uint8_t* model_done; // per model: 1 = stopped (its items do nothing)
 };
 
 // log accept ratio H0 - H1 of one leapfrog step of size h from (q, g, lj)
@@ -185,6 +186,7 @@ template <int K>
 __global__ void __launch_bounds__(32 * kMaxWarps) mm_nuts_kernel(MmArgs a) {
     extern __shared__ float smem[];
     const MmItem item = a.items[blockIdx.x];
+    if (a.model_done[item.model]) return;  // a stopped model's chains keep their state (uniform per CTA)
     const MmModel m = a.models[item.model];
     const float* pack = a.packs + m.pack_off;
     if ((int64_t)m.pack_floats * 4 <= (int64_t)a.stage_limit) pack = mm_stage(pack, m.pack_floats, smem);
@@ -261,6 +263,7 @@ struct MmAdaptArgs {
     double* wmean;            // per parameter
     double* wm2;
     double* wcount;           // per model
+    const uint8_t* model_done; // per model: 1 = stopped (its adaptation state stays)
 };
 
 constexpr double kDaGamma = 0.05, kDaT0 = 10.0, kDaKappa = 0.75;
@@ -268,6 +271,7 @@ constexpr double kDaGamma = 0.05, kDaT0 = 10.0, kDaKappa = 0.75;
 __global__ void __launch_bounds__(256) mm_adapt_kernel(MmAdaptArgs a) {
     const int it = *a.counter;
     if (it >= a.num_warmup) return;
+    if (a.model_done[blockIdx.x]) return;
     const MmModel m = a.models[blockIdx.x];
     const uint8_t act = a.actions[it];
     __shared__ int included;
@@ -454,6 +458,7 @@ struct ut_multi {
     // adaptation and run state
     double *da = nullptr, *wmean = nullptr, *wm2 = nullptr, *wcount = nullptr;
     uint8_t* actions = nullptr;
+    uint8_t* model_done = nullptr;  // per model stop flags (device)
     int num_warmup = 0, num_samples = 0;
     float target_accept = 0.8f, thr = 1000.0f;
     uint32_t seed = 0;
@@ -522,6 +527,7 @@ MmArgs base_args(const ut_multi* mm, const MmClass& cl) {
     a.ckpt = cl.ckpt; a.class_slot = mm->class_slot; a.counter = mm->counter; a.seed = mm->seed;
     a.max_depth = mm->max_depth; a.thr = mm->thr; a.stage_limit = cl.stage_limit;
     a.step_out = mm->step; a.da = mm->da; a.actions = mm->actions; a.num_warmup = mm->num_warmup;
+    a.model_done = mm->model_done;
     return a;
 }
 
@@ -592,6 +598,7 @@ int32_t enqueue_iteration(ut_multi* mm, cudaStream_t st) {
     ad.position = mm->position;
     ad.inverse_mass = mm->inverse_mass; ad.step = mm->step; ad.da = mm->da; ad.wmean = mm->wmean; ad.wm2 = mm->wm2;
     ad.wcount = mm->wcount;
+    ad.model_done = mm->model_done;
     mm_adapt_kernel<<<mm->M, 256, 0, st>>>(ad);
     MM_LAUNCHED();
     if (mm->draws_capacity > 0) {
@@ -733,7 +740,8 @@ int32_t ut_multi_create(int32_t num_models, const ut_plan_desc* plans, const flo
         (rc = malloc_into(L, &mm->divergent, chain_total)) || (rc = malloc_into(L, &mm->moved, chain_total)) ||
         (rc = malloc_into(L, &mm->class_slot, chain_total)) || (rc = malloc_into(L, &mm->da, 5 * (size_t)chain_total)) ||
         (rc = malloc_into(L, &mm->wmean, param_total)) || (rc = malloc_into(L, &mm->wm2, param_total)) ||
-        (rc = malloc_into(L, &mm->wcount, num_models)) || (rc = malloc_into(L, &mm->counter, 1)))
+        (rc = malloc_into(L, &mm->wcount, num_models)) || (rc = malloc_into(L, &mm->counter, 1)) ||
+        (rc = malloc_into(L, &mm->model_done, num_models)))
         return bail(rc);
     std::vector<int32_t> slot((size_t)chain_total);
     for (int k = 0; k < kNumClasses; ++k) {
@@ -888,7 +896,18 @@ int32_t ut_multi_begin(ut_multi* mm, int32_t num_warmup, int32_t num_samples, ui
     MM_CUDA(cudaMemset(mm->wcount, 0, mm->M * sizeof(double)));
     MM_CUDA(cudaMemset(mm->counter, 0, sizeof(int32_t)));
     MM_CUDA(cudaMemset(mm->accept_prob, 0, mm->total_chains * sizeof(float)));
+    MM_CUDA(cudaMemset(mm->model_done, 0, mm->M));
     mm->begun = true;
+    return UT_OK;
+}
+
+int32_t ut_multi_set_stopped(ut_multi* mm, const uint8_t* stopped, void* stream) {
+    int32_t rc = check_mm(mm);
+    if (rc) return rc;
+    if (!stopped) return mfail(UT_ERR_ARGUMENT, "null stop flags");
+    if (!mm->begun) return mfail(UT_ERR_ARGUMENT, "call ut_multi_begin before ut_multi_set_stopped");
+    MM_CUDA(cudaMemcpyAsync(mm->model_done, stopped, mm->M, cudaMemcpyHostToDevice, (cudaStream_t)stream));
+    MM_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
     return UT_OK;
 }
 

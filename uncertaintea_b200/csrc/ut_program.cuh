@@ -26,6 +26,7 @@
 #include <cmath>
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "ut_common.cuh"
@@ -112,6 +113,12 @@ class ProgCompiler {
         covered_.assign(P_, 0);
         int pc = 0;
         compile_block(pc, ns_, 0, rows_);
+        for (const auto& gr : glm_rows_)
+            for (int r = gr.first; r < gr.first + gr.second; ++r)
+                if (covered_[r] == 0) {
+                    add("GLM coefficient row " + std::to_string(r) + " is not a latent value");
+                    break;
+                }
         for (int r = 0; r < P_; ++r)
             if (covered_[r] != 1) {
                 add("parameter row " + std::to_string(r) + (covered_[r] ? " is read by more than one latent step"
@@ -145,6 +152,7 @@ class ProgCompiler {
     std::vector<PStep> steps_;
     std::vector<PNode> nodes_;
     std::vector<int64_t> blocks_;  // rows of the observation block at each loop depth
+    std::vector<std::pair<int, int>> glm_rows_;  // (first row, count) read by GLM steps
     int devslots_ = 0;
 
     void add(const std::string& m) {
@@ -305,7 +313,13 @@ class ProgCompiler {
                     add(where + ": GLM observation rows outside the staged buffer");
                 bool ok = true;
                 if (s.arg[0] >= 0) ok = arg(s.arg[0], depth, ps, 0, where);
-                if (ok && claim_rows(s.value_source, s.width, where)) {
+                // the coefficients are read here; a latent step (their prior) owns the rows
+                if (s.value_source < 0 || (int64_t)s.value_source + s.width > P_) {
+                    add(where + ": GLM coefficient rows out of range");
+                    ok = false;
+                }
+                if (ok) glm_rows_.push_back({s.value_source, s.width});
+                if (ok) {
                     ps.vs = s.value_source;
                     ps.count = s.count;
                     ps.width = s.width;
@@ -357,7 +371,7 @@ class ProgCompiler {
 // digamma: recurrence psi(x) = psi(x + 1) - 1/x up to x >= 6, then the
 // asymptotic series psi(x) ~ ln x - 1/(2x) - sum_k B_2k / (2k x^2k) with the
 // Bernoulli numbers B_2 .. B_8 (1/6, -1/30, 1/42, -1/30).
-__device__ __forceinline__ float prog_digamma(float x) {
+__host__ __device__ __forceinline__ float prog_digamma(float x) {
     float acc = 0.0f;
     for (int i = 0; i < 8 && x < 6.0f; ++i) {
         acc -= 1.0f / x;
@@ -369,7 +383,7 @@ __device__ __forceinline__ float prog_digamma(float x) {
 }
 
 // loggamma(x + 1/2) - loggamma(x), large-x safe (math.jl:80-86, crossover 12 in Float32).
-__device__ __forceinline__ float prog_lgamma_half_ratio(float x) {
+__host__ __device__ __forceinline__ float prog_lgamma_half_ratio(float x) {
     if (x > 12.0f)
         return x * log1pf(1.0f / (2.0f * x)) + 0.5f * logf(x) - 0.5f + (1.0f / (x + 0.5f) - 1.0f / x) / 12.0f;
     return lgammaf(x + 0.5f) - lgammaf(x);
@@ -382,7 +396,7 @@ constexpr float kProgLog2 = 0.6931471805599453f;
 // Log-density of one choice term (math.jl:88-300) and its partials with
 // respect to the arguments (da) and the value (dx), which are only written
 // when `grad`.
-__device__ float prog_dist(int dist, const float* a, float x, bool grad, float* da, float& dx) {
+__host__ __device__ float prog_dist(int dist, const float* a, float x, bool grad, float* da, float& dx) {
     const float ninf = -INFINITY;
     float lp = 0.0f;
     da[0] = da[1] = da[2] = 0.0f;
@@ -550,7 +564,7 @@ __device__ float prog_dist(int dist, const float* a, float x, bool grad, float* 
 }
 
 // Latent transform (math.jl:1144-1159): value, log|J|, d value/du, d log|J|/du.
-__device__ __forceinline__ float prog_transform(int tr, float u, float& lad, float& dxdu, float& dlad) {
+__host__ __device__ __forceinline__ float prog_transform(int tr, float u, float& lad, float& dxdu, float& dlad) {
     if (tr == UT_TRANSFORM_LOG) {
         const float x = expf(u);
         lad = u; dxdu = x; dlad = 1.0f;
@@ -737,7 +751,7 @@ __device__ float prog_lj_grad(const ProgModel& m, const float (&q)[K], float (&g
                 const float z = (qs[s.vs + d] - mu) * inv;
                 lj += -lsg - kProgHalfLog2Pi - 0.5f * z * z;
                 if (want_grad) {
-                    gs[s.vs + d] = -z * inv;
+                    gs[s.vs + d] -= z * inv;
                     dmu += z * inv;
                     dsg += (z * z - 1.0f) * inv;
                 }
@@ -834,7 +848,7 @@ __device__ float prog_lj_grad(const ProgModel& m, const float (&q)[K], float (&g
             if (s.kind == UT_STEP_CHOICE && s.vs >= 0) {
                 float lad, dxdu, dlad;
                 prog_transform(s.tr, qs[s.vs], lad, dxdu, dlad);
-                gs[s.vs] = adj[s.slot * 33 + 32] * dxdu + dlad;
+                gs[s.vs] += adj[s.slot * 33 + 32] * dxdu + dlad;  // a GLM step may have added to the row
             }
         }
         __syncwarp();

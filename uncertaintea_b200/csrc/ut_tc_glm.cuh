@@ -69,7 +69,7 @@ struct TcGlmParams {
     int want_grad;
     int ctiles, S, sms;    // chain tiles, observation splits of the full grid, SMs
     const int* nact;       // optional: only the first *nact chains are live
-    int nbuf;              // H/R TMEM buffers (2 or 3)
+    int col_tlo, col_d2, col_buf;  // TMEM columns of Theta_lo, the accumulator, the first H/R buffer
 };
 
 // Work split of one launch.  Without nact: the (chain tile, split) grid of the
@@ -286,6 +286,16 @@ __host__ __device__ inline int tc_nbuf(int F, int Fp) {
     const int n = (512 - 16 * tc_kblocks_used(F) - Fp) / 64;
     return n < kTcMaxBufs ? n : kTcMaxBufs;
 }
+// TMEM column plan {Theta_lo, D2, first H/R buffer} for nbuf buffers.  The
+// compact plan packs Theta hi/lo at KC columns each; the wide plan (2 buffers
+// only) spaces everything at Fp: Theta_lo at Fp, D2 at 2Fp, buffers at 3Fp.
+__host__ __device__ inline void tc_columns(int F, int Fp, bool wide, int cols[3]) {
+    const int KC = 8 * tc_kblocks_used(F);
+    const int a = wide ? Fp : KC;
+    cols[0] = a;
+    cols[1] = 2 * a;
+    cols[2] = 2 * a + Fp;
+}
 __host__ __device__ inline int tc_matoms(int Fp) { return (Fp + 31) / 32; }
 __host__ __device__ inline int tc_xk_bytes(int Fp) { return tc_kblocks(Fp) * kTcObs * 32; }
 __host__ __device__ inline int tc_xm_bytes(int Fp) { return tc_matoms(Fp) * kTcObs * 128; }
@@ -340,6 +350,7 @@ __device__ __forceinline__ uint64_t sdesc_sw128b32(uint32_t saddr, uint32_t lbo_
     return d;
 }
 
+template <int NBUF>
 __global__ void __launch_bounds__(kTcThreads, 1)
     tc_glm_kernel(const __grid_constant__ CUtensorMap map_xk_hi, const __grid_constant__ CUtensorMap map_xk_lo,
                   const __grid_constant__ CUtensorMap map_xm_hi, const __grid_constant__ CUtensorMap map_xm_lo,
@@ -357,7 +368,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     uint64_t* bar_d2full = bars + 12;
     uint64_t* bar_theta = bars + 13;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 14);
-    const int nbuf = p.nbuf;
+    constexpr int nbuf = NBUF;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // chain tiles fastest: concurrent CTAs share X ranges in L2
@@ -390,7 +401,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
     const int KC = 8 * KB1;
-    const uint32_t col_thi = 0, col_tlo = KC, col_d2 = 2 * KC, col_buf = 2 * KC + Fp;
+    const uint32_t col_thi = 0, col_tlo = p.col_tlo, col_d2 = p.col_d2, col_buf = p.col_buf;
 
     if (warp == 0) {
         // ---------------- TMA producer ----------------
@@ -619,6 +630,8 @@ struct TcGlmPlan {
     float icpt_mu = 0, icpt_sigma = 1, coef_mu = 0, coef_sigma = 1;
     CUtensorMap map_xk_hi, map_xk_lo, map_xm_hi, map_xm_lo;
     size_t smem = 0;
+    int nbuf = 2;        // H/R TMEM buffers
+    bool wide = false;   // TMEM column plan (tc_columns)
 };
 
 inline std::string& tc_err_string() {
@@ -749,8 +762,21 @@ inline int tc_glm_setup(TcGlmPlan& t, const float* d_Xa, const float* d_y, int N
         tc_err_string() = "cuTensorMapEncodeTiled failed";
         return 1;
     }
+    // H/R buffers: as many as TMEM holds (tc_nbuf); UT_TC_BUFFERS=2 keeps two (a tuning knob)
+    t.nbuf = tc_nbuf(F, Fp);
+    const char* nb_env = getenv("UT_TC_BUFFERS");
+    if (nb_env && nb_env[0] == '2') t.nbuf = 2;
+    // UT_TC_LAYOUT=wide: the wide column plan (2 buffers), a tuning knob
+    const char* lay_env = getenv("UT_TC_LAYOUT");
+    if (lay_env && lay_env[0] == 'w' && 3 * Fp + 128 <= 512) {
+        t.wide = true;
+        t.nbuf = 2;
+    }
     t.smem = 1024 + (size_t)kTcStages * tc_stage_bytes(Fp) + 128 + 16 + 4 * kTcChains * sizeof(float);
-    if (cudaFuncSetAttribute(tc_glm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem) != cudaSuccess) {
+    if (cudaFuncSetAttribute(tc_glm_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(tc_glm_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem) !=
+            cudaSuccess) {
         tc_err_string() = "shared-memory opt-in failed";
         return 1;
     }
@@ -805,9 +831,14 @@ inline cudaError_t tc_glm_launch(const TcGlmPlan& t, const float* params, float*
     p.tiles_per_split = t.tiles_per_split; p.num_tiles = t.num_tiles; p.want_grad = grads ? 1 : 0;
     p.ctiles = t.ctiles; p.S = t.S; p.sms = t.sms;
     p.nact = nact;
-    p.nbuf = tc_nbuf(t.F, t.Fp);
+    int cols[3];
+    tc_columns(t.F, t.Fp, t.wide, cols);
+    p.col_tlo = cols[0]; p.col_d2 = cols[1]; p.col_buf = cols[2];
     dim3 grid(t.ctiles, t.S);
-    tc_glm_kernel<<<grid, kTcThreads, t.smem, st>>>(t.map_xk_hi, t.map_xk_lo, t.map_xm_hi, t.map_xm_lo, params, p);
+    if (t.nbuf == 3)
+        tc_glm_kernel<3><<<grid, kTcThreads, t.smem, st>>>(t.map_xk_hi, t.map_xk_lo, t.map_xm_hi, t.map_xm_lo, params, p);
+    else
+        tc_glm_kernel<2><<<grid, kTcThreads, t.smem, st>>>(t.map_xk_hi, t.map_xk_lo, t.map_xm_hi, t.map_xm_lo, params, p);
     tc_reduce_kernel<<<t.C, 128, 0, st>>>(params, totals, grads, p, t.off, t.icpt_mu, t.icpt_sigma, t.coef_mu,
                                           t.coef_sigma);
     return cudaGetLastError();

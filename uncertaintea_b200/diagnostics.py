@@ -78,13 +78,15 @@ def _split_ess_of(split: np.ndarray) -> float:
 
 
 def _rank_normal(draws: np.ndarray) -> np.ndarray:
-    """diagnostics.jl:589-600: (r - 3/8) / (S + 1/4) through the normal quantile."""
-    flat = draws.reshape(-1)
+    """diagnostics.jl:589-600: (r - 3/8) / (S + 1/4) through the normal quantile.
+    Ties take ranks in the reference's order: a stable sort of the (2C, S/2)
+    split matrix flattened column-major (draw-major, split chain minor)."""
+    flat = draws.reshape(-1, order="F")
     S = flat.size
     order = np.argsort(flat, kind="stable")
     ranks = np.empty(S, dtype=np.float64)
     ranks[order] = np.arange(1, S + 1)
-    return ndtri((ranks - 0.375) / (S + 0.25)).reshape(draws.shape)
+    return ndtri((ranks - 0.375) / (S + 0.25)).reshape(draws.shape, order="F")
 
 
 def _draws(chains, space):

@@ -227,6 +227,7 @@ def _mass_adaptation_window_summary(schedule, window_index, variance, inverse_ma
     variance, the clip scale at its start and end, whether the mass was updated,
     and the mean / min / max of the diagonal mass (1 / inverse mass) it left."""
     _, _, _, ws, wss = variance.host_state()
+    variance.sync_count()
     pooled = int(variance.count)
     mass = 1.0 / np.asarray(inverse_mass, dtype=np.float64)
     return {"window": window_index, "start": _warmup_window_start(schedule, window_index),
@@ -1048,8 +1049,8 @@ def batched_chees(model, args=(), constraints=None, *, num_chains, num_samples, 
                   init_strategy="prior", init_max_retries=100, target_accept=0.651, adapt_step_size=True,
                   adapt_mass_matrix=True, find_reasonable_step_size=False, divergence_threshold=1000.0,
                   mass_matrix_regularization=1e-3, mass_matrix_min_samples=10, callback=None, callback_every=10,
-                  backend="cuda", precision=None, rng=None, trajectory_velocity="reference", _trajectory_trace=None,
-                  _surrogate=None) -> HMCChains:
+                  backend="cuda", precision=None, rng=None, trajectory_velocity="reference", fixed_leapfrog_steps=None,
+                  _trajectory_trace=None, _surrogate=None) -> HMCChains:
     """ChEES-HMC (api_batched_chees.jl:314-347).
 
     trajectory_velocity selects the endpoint velocity of the trajectory-length
@@ -1060,7 +1061,16 @@ def batched_chees(model, args=(), constraints=None, *, num_chains, num_samples, 
     -dChEES/dlog T.  "forward" uses the velocity the trajectory ends with
     (the criterion's own derivative), so the ascent maximises ChEES as the
     reference documents; it is the same reduction with the numerator negated.
+
+    fixed_leapfrog_steps (an addition; default None = the reference's rule)
+    makes every iteration run exactly that many leapfrog steps, with no
+    trajectory-length adaptation: a fixed trajectory budget, as the learned-
+    surrogate comparison at 16 steps uses.
     """
+    if fixed_leapfrog_steps is not None:
+        if int(fixed_leapfrog_steps) < 1:
+            raise ValueError(f"fixed_leapfrog_steps must be >= 1, got {fixed_leapfrog_steps}")
+        adapt_trajectory_length = False
     _validate_init("batched_chees", init_strategy, init_max_retries)
     if trajectory_velocity not in ("reference", "forward"):
         raise ValueError(f"batched_chees trajectory_velocity must be 'reference' or 'forward', got {trajectory_velocity!r}")
@@ -1118,6 +1128,8 @@ def batched_chees(model, args=(), constraints=None, *, num_chains, num_samples, 
         run.set_mass_and_step(driver.inverse_mass_matrix, eps)
         jitter = _chees_jitter_value(jitter_amount, it)
         L = _chees_leapfrog_steps_from_jitter(jitter, traj.trajectory_length, eps)
+        if fixed_leapfrog_steps is not None:
+            L = int(fixed_leapfrog_steps)
         if it == num_warmup + 1:
             torch.cuda.synchronize()
             t_sample = time.perf_counter()
@@ -1159,8 +1171,10 @@ def batched_chees(model, args=(), constraints=None, *, num_chains, num_samples, 
                 driver.warmup_finalize()
                 if _surrogate is not None:
                     # Philox coordinates past the run's own iterations
+                    steps_fn = _chees_leapfrog_steps_from_jitter if fixed_leapfrog_steps is None else \
+                        (lambda _j, _t, _e: int(fixed_leapfrog_steps))
                     _surrogate.end_warmup(run, driver, traj, lambda i: _chees_jitter_value(jitter_amount, i),
-                                          _chees_leapfrog_steps_from_jitter, divergence_threshold, total + 1)
+                                          steps_fn, divergence_threshold, total + 1)
             _invoke_callback(callback, callback_every, "warmup", it, num_warmup, driver.step_size, divergences)
         else:
             draws.record(it - num_warmup - 1, integration_steps=L)

@@ -111,6 +111,57 @@ def split_ess(draws):
     return torch.where((W == 0) & (var_plus == 0), torch.full_like(ess, float("nan")), ess)
 
 
+def _split_rhat_cols(split):
+    """Split R-hat per column of (M, h, P) split chains (diagnostics.jl:514-540)."""
+    torch = _torch()
+    M, h, _ = split.shape
+    means = split.mean(dim=1)
+    W = split.var(dim=1, unbiased=True).mean(dim=0)
+    B = h * means.var(dim=0, unbiased=True)
+    var_plus = (h - 1) / h * W + B / h
+    r = torch.sqrt(torch.clamp(var_plus / W, min=1.0))
+    r = torch.where(W == 0, torch.where(var_plus == 0, torch.full_like(r, float("nan")),
+                                        torch.full_like(r, float("inf"))), r)
+    return r
+
+
+def _rank_normal_cols(split):
+    """Rank-normalise every column of (M, h, P) over its M*h values:
+    (rank - 3/8) / (n + 1/4) through the normal quantile, ranks 1..n with ties
+    in the reference's order, a stable sort over draw-major, split-chain-minor
+    values (diagnostics.jl:589-600 on the column-major (2C, S/2) matrix)."""
+    torch = _torch()
+    M, h, P = split.shape
+    flat = split.permute(1, 0, 2).reshape(h * M, P)
+    n = M * h
+    order = torch.argsort(flat, dim=0, stable=True)
+    ranks = torch.empty_like(flat)
+    ranks.scatter_(0, order, torch.arange(1, n + 1, dtype=flat.dtype, device=flat.device)[:, None].expand(n, P))
+    z = torch.special.ndtri((ranks - 0.375) / (n + 0.25))
+    return z.reshape(h, M, P).permute(1, 0, 2)
+
+
+def rank_split_rhat(draws):
+    """Rank-normalised split R-hat per parameter of draws (S, C, P) -- a torch
+    tensor on any device: max of the bulk R-hat of the rank-normalised split
+    chains and the tail R-hat of the rank-normalised |x - median|
+    (diagnostics.jl:602-612, the sampler gate's estimator)."""
+    torch = _torch()
+    x = draws.double()
+    S, C, P = x.shape
+    h = S // 2
+    if h < 2:
+        return torch.full((P,), float("nan"), dtype=torch.float64, device=x.device)
+    # (2C, h, P): chain c's first half is split chain 2c, its second half 2c + 1
+    split = torch.stack([x[:h], x[h:2 * h]], dim=2).reshape(h, 2 * C, P).permute(1, 0, 2)
+    bulk = _split_rhat_cols(_rank_normal_cols(split))
+    srt = torch.sort(split.reshape(-1, P), dim=0).values
+    n = srt.shape[0]
+    med = 0.5 * (srt[(n - 1) // 2] + srt[n // 2])  # the 0.5 quantile with linear interpolation
+    tail = _split_rhat_cols(_rank_normal_cols(torch.abs(split - med)))
+    return torch.maximum(bulk, tail)
+
+
 class MultiModelBatch:
     """A batch of (model, args, constraints) hierarchical models on the current
     CUDA device (library-owned state, see ut_multi_* in include/ut_b200.h)."""
@@ -188,6 +239,11 @@ class MultiModelBatch:
     def run(self, num_iterations: int, use_graph: bool = True) -> None:
         nat.check(self.lib.ut_multi_run(self.handle, int(num_iterations), int(bool(use_graph)), _stream_handle()))
 
+    def set_stopped(self, stopped) -> None:
+        """Per-model stop flags (nonzero = the model's chains no longer move)."""
+        flags = np.ascontiguousarray(np.asarray(stopped, dtype=np.uint8))
+        nat.check(self.lib.ut_multi_set_stopped(self.handle, nat.ptr(flags), _stream_handle()))
+
     def split_rhat(self, num_draws: int) -> np.ndarray:
         torch = _torch()
         out = torch.empty(self.M, dtype=torch.float32, device="cuda")
@@ -250,6 +306,7 @@ class MultiChains:
     warmup_seconds: float
     sampling_seconds: float            # device time of the sampling iterations (checkpoints excluded)
     autotune_ms: np.ndarray | None = None
+    draws_per_model: np.ndarray | None = None  # the draws that are each model's own (per-model stopping)
     classes: dict = field(default_factory=dict)
     divergences: int = 0
     mean_tree_depth: float = float("nan")
@@ -276,7 +333,8 @@ class MultiChains:
 def batched_nuts_multi(models, *, chains_per_model=64, num_warmup=1000, num_samples=1000, max_tree_depth=10,
                        target_accept=0.8, initial_step_size=0.1, divergence_threshold=1000.0, rng=None,
                        init_strategy="prior", autotune=True, autotune_after=None, autotune_trials=2,
-                       rhat_check_every=50, rhat_target=1.01, use_graph=True, callback=None) -> MultiChains:
+                       rhat_check_every=50, rhat_target=1.01, use_graph=True, callback=None,
+                       stop_converged=False) -> MultiChains:
     """Batched persistent NUTS over many hierarchical models at once.
 
     models: list of (HierarchicalNormalNoncentered, args, constraints).  Warmup
@@ -284,8 +342,15 @@ def batched_nuts_multi(models, *, chains_per_model=64, num_warmup=1000, num_samp
     autotuner runs after ``autotune_after`` warmup iterations (default: a
     fifth of the warmup), when the trees look like the stationary ones.
     Every ``rhat_check_every`` sampling iterations the per-model split R-hat of
-    the draws so far is computed; a model's time-to-R-hat is the first
-    checkpoint where its max R-hat is below ``rhat_target``."""
+    the draws so far is computed on the device; a model below ``rhat_target``
+    there is confirmed with the rank-normalised split R-hat (the gate's
+    estimator), and its time-to-R-hat is the first checkpoint where that max
+    over its parameters is below the target.  Reported R-hats are rank-normalised.
+
+    stop_converged: a model that reaches the target stops there (its chains no
+    longer move, ut_multi_set_stopped) and the run continues for the others up
+    to ``num_samples`` draws (the cap), or until every model has stopped; each
+    model's R-hat and ESS are then over its own draws."""
     torch = _torch()
     if num_warmup < 0 or num_samples < 4:
         raise ValueError("need num_warmup >= 0 and num_samples >= 4")
@@ -319,6 +384,8 @@ def batched_nuts_multi(models, *, chains_per_model=64, num_warmup=1000, num_samp
         timings = batch.autotune(autotune_trials)
     ttr = np.full(M, np.inf)
     sttr = np.full(M, np.inf)
+    stopped = np.zeros(M, dtype=np.uint8)
+    own = np.full(M, num_samples, dtype=np.int64)   # draws that are the model's own
     samp_ms = 0.0
     t_samp0 = time.perf_counter()
     s = 0
@@ -331,21 +398,39 @@ def batched_nuts_multi(models, *, chains_per_model=64, num_warmup=1000, num_samp
         s += k
         if s >= 4:
             r = batch.split_rhat(s)  # synchronises
+            hit = (r < rhat_target) & ~np.isfinite(sttr) & (stopped == 0)
+            for m in np.flatnonzero(hit):  # confirm with the gate's rank-normalised R-hat
+                hit[m] = float(torch.nan_to_num(rank_split_rhat(batch.model_draws(int(m), s)),
+                                                nan=float("inf")).max()) < rhat_target
             now = time.perf_counter()
-            hit = (r < rhat_target) & ~np.isfinite(sttr)
             sttr[hit] = now - t_samp0
             ttr[hit] = now - t0
+            if stop_converged and hit.any():
+                stopped[hit] = 1
+                own[hit] = s
+                batch.set_stopped(stopped)
         torch.cuda.synchronize()
         samp_ms += e0.elapsed_time(e1)
         if callback is not None:
             callback("sample", s, num_samples)
-    final_rhat = batch.split_rhat(num_samples)
+        if stop_converged and stopped.all():
+            break
+    own = np.minimum(own, s)
+    final_rhat = np.empty(M)  # rank-normalised, each model over its own draws
     ess = np.empty(M)
     for m in range(M):
-        ess[m] = float(torch.nan_to_num(split_ess(batch.model_draws(m)), nan=float("inf")).min())
+        d = batch.model_draws(m, int(own[m]))
+        final_rhat[m] = float(torch.nan_to_num(rank_split_rhat(d), nan=float("inf")).max())
+        ess[m] = float(torch.nan_to_num(split_ess(d), nan=float("inf")).min())
     v = batch.view()
+    div, depth_sum, depth_n = 0, 0.0, 0
+    for m in range(M):  # each model's own draws (a stopped model's later rows repeat its last state)
+        a, b = int(batch.chain_offsets[m]), int(batch.chain_offsets[m + 1])
+        n = int(own[m])
+        div += int(v["draw_divergent"][:n, a:b].sum())
+        depth_sum += float(v["draw_tree_depth"][:n, a:b].double().sum())
+        depth_n += n * (b - a)
     return MultiChains(batch=batch, num_params=batch.P.copy(), num_chains=batch.chains.copy(), min_ess=ess,
                        max_rhat=final_rhat, time_to_rhat=ttr, sampling_time_to_rhat=sttr, warmup_seconds=t_warm,
                        sampling_seconds=samp_ms / 1000.0, autotune_ms=timings, classes=batch.class_info(),
-                       divergences=int(v["draw_divergent"].sum()),
-                       mean_tree_depth=float(v["draw_tree_depth"].float().mean()))
+                       divergences=div, mean_tree_depth=depth_sum / max(depth_n, 1), draws_per_model=own)
