@@ -70,6 +70,7 @@ struct TcGlmParams {
     int ctiles, S, sms;    // chain tiles, observation splits of the full grid, SMs
     const int* nact;       // optional: only the first *nact chains are live
     int col_tlo, col_d2, col_buf;  // TMEM columns of Theta_lo, the accumulator, the first H/R buffer
+    int xk3d;              // the K-major maps are 3-D (8 features, rows, K-blocks): one copy per tile
 };
 
 // Work split of one launch.  Without nact: the (chain tile, split) grid of the
@@ -206,6 +207,75 @@ __device__ __forceinline__ void mma_ts(uint32_t d, uint32_t a, uint64_t b, uint3
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                  : "memory");
+}
+
+// Warp-wide forms: the whole (converged) warp runs the issuing code, so the
+// descriptors and addresses are warp-uniform values, and one elected lane --
+// always the same one, since tcgen05.commit tracks the MMAs of the thread that
+// issues it -- issues the instruction.
+__device__ __forceinline__ void mma_ts_warp(uint32_t d, uint32_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p, e;\n\t.reg .b32 r;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "elect.sync r|e, 0xffffffff;\n\t"
+        "@e tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}"
+        ::"r"(d), "r"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void mma_commit_warp(uint64_t* bar) {
+    asm volatile(
+        "{\n\t.reg .pred e;\n\t.reg .b32 r;\n\t"
+        "elect.sync r|e, 0xffffffff;\n\t"
+        "@e tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n\t}"
+        ::"r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx_warp(uint64_t* bar, uint32_t bytes) {
+    asm volatile(
+        "{\n\t.reg .pred e;\n\t.reg .b32 r;\n\t"
+        "elect.sync r|e, 0xffffffff;\n\t"
+        "@e mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n\t}"
+        ::"r"(smem_u32(bar)), "r"(bytes)
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d_warp(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+    asm volatile(
+        "{\n\t.reg .pred e;\n\t.reg .b32 r;\n\t"
+        "elect.sync r|e, 0xffffffff;\n\t"
+        "@e cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];\n\t}"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d_warp(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y,
+                                                 int z) {
+    asm volatile(
+        "{\n\t.reg .pred e;\n\t.reg .b32 r;\n\t"
+        "elect.sync r|e, 0xffffffff;\n\t"
+        "@e cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];\n\t}"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+
+__device__ __forceinline__ void bulk_load_warp(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "{\n\t.reg .pred e;\n\t.reg .b32 r;\n\t"
+        "elect.sync r|e, 0xffffffff;\n\t"
+        "@e cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n\t}"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool elect_one() {
+    uint32_t is = 0;
+    asm volatile(
+        "{\n\t.reg .pred e;\n\t.reg .b32 r;\n\t"
+        "elect.sync r|e, 0xffffffff;\n\t"
+        "selp.u32 %0, 1, 0, e;\n\t}"
+        : "=r"(is));
+    return is != 0;
 }
 
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
@@ -350,11 +420,27 @@ __device__ __forceinline__ uint64_t sdesc_sw128b32(uint32_t saddr, uint32_t lbo_
     return d;
 }
 
-template <int NBUF>
+// TMEM load of a warp's kCols (8 or 16) consecutive columns.
+template <int kCols>
+__device__ __forceinline__ void tmem_ld_cols(uint32_t taddr, float (&v)[kCols]) {
+    if constexpr (kCols == 8) tmem_ld8(taddr, v);
+    else tmem_ld16(taddr, v);
+}
+
+// NBUF H/R TMEM buffers; G epilogue warp groups.  G = 1: all 16 epilogue
+// warps work on every tile, 8 observation columns each.  G = 2: two groups of
+// 8 warps take alternate tiles, 16 columns each, so two tiles' epilogues
+// overlap (each warp's per-tile chain of waits, TMEM round trips and arrivals
+// is paid once per 16 columns instead of once per 8); this needs 3 buffers,
+// two tiles in the epilogue while GEMM1 of the next one runs.
+template <int NBUF, int G>
 __global__ void __launch_bounds__(kTcThreads, 1)
     tc_glm_kernel(const __grid_constant__ CUtensorMap map_xk_hi, const __grid_constant__ CUtensorMap map_xk_lo,
                   const __grid_constant__ CUtensorMap map_xm_hi, const __grid_constant__ CUtensorMap map_xm_lo,
                   const float* __restrict__ params, TcGlmParams p) {
+    static_assert(G == 1 || (G == 2 && NBUF == 3), "two epilogue groups need three H/R buffers");
+    constexpr int kGroupWarps = kTcEpiWarps / G;          // arrivals per tile
+    constexpr int kCols = kTcObs / (kGroupWarps / 4);     // observation columns per warp and tile
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int Fp = p.Fp;
@@ -367,7 +453,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     uint64_t* bar_rfull = bars + 9;                // [kTcMaxBufs]
     uint64_t* bar_d2full = bars + 12;
     uint64_t* bar_theta = bars + 13;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 14);
+    uint64_t* bar_drained = bars + 14;             // every epilogue warp has read the accumulator run
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 15);
     constexpr int nbuf = NBUF;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -389,10 +476,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
         for (int i = 0; i < kTcMaxBufs; ++i) {
             mbar_init(bar_d1full + i, 1);
-            mbar_init(bar_rfull + i, kTcEpiWarps);
+            mbar_init(bar_rfull + i, kGroupWarps);
         }
         mbar_init(bar_d2full, 1);
         mbar_init(bar_theta, kTcEpiWarps);
+        mbar_init(bar_drained, kTcEpiWarps);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) tmem_alloc(tmem_slot, 512);
@@ -403,86 +491,139 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int KC = 8 * KB1;
     const uint32_t col_thi = 0, col_tlo = p.col_tlo, col_d2 = p.col_d2, col_buf = p.col_buf;
 
+    // waits of the producer and issuer warps, with warp-uniform verdicts
+    auto wwait = [&](uint64_t* bar, uint32_t parity) -> bool {
+        return __all_sync(0xffffffffu, mbar_wait(bar, parity, p.err));
+    };
+    auto wtest = [&](uint64_t* bar, uint32_t parity) -> bool {
+        return __all_sync(0xffffffffu, mbar_test_wait(bar, parity));
+    };
     if (warp == 0) {
-        // ---------------- TMA producer ----------------
-        if (lane == 0) {
-            for (int i = 0; i < ntiles; ++i) {
-                const int s = i % kTcStages;
-                if (i >= kTcStages && !mbar_wait(bar_xempty + s, ((i / kTcStages) - 1) & 1, p.err)) break;
-                uint8_t* st = smem + s * stage_bytes;
-                mbar_expect_tx(bar_xfull + s, 2 * KB1 * (kTcObs * 32) + 2 * xm_bytes + kTcObs * 4);
-                const int n0 = (t_begin + i) * kTcObs;
+        // ---------------- TMA producer (the whole warp; an elected lane issues) ----------------
+        for (int i = 0; i < ntiles; ++i) {
+            const int s = i % kTcStages;
+            if (i >= kTcStages && !wwait(bar_xempty + s, ((i / kTcStages) - 1) & 1)) break;
+            uint8_t* st = smem + s * stage_bytes;
+            mbar_expect_tx_warp(bar_xfull + s, 2 * KB1 * (kTcObs * 32) + 2 * xm_bytes + kTcObs * 4);
+            const int n0 = (t_begin + i) * kTcObs;
+            if (p.xk3d) {
+                // [K-block][32 rows][8 features] in one copy per view
+                tma_load_3d_warp(st, &map_xk_hi, bar_xfull + s, 0, n0, 0);
+                tma_load_3d_warp(st + xk_bytes, &map_xk_lo, bar_xfull + s, 0, n0, 0);
+            } else {
                 for (int kb = 0; kb < KB1; ++kb) {
-                    tma_load_2d(st + kb * (kTcObs * 32), &map_xk_hi, bar_xfull + s, kb * 8, n0);
-                    tma_load_2d(st + xk_bytes + kb * (kTcObs * 32), &map_xk_lo, bar_xfull + s, kb * 8, n0);
+                    tma_load_2d_warp(st + kb * (kTcObs * 32), &map_xk_hi, bar_xfull + s, kb * 8, n0);
+                    tma_load_2d_warp(st + xk_bytes + kb * (kTcObs * 32), &map_xk_lo, bar_xfull + s, kb * 8, n0);
                 }
-                for (int a = 0; a < MA; ++a) {
-                    tma_load_2d(st + 2 * xk_bytes + a * (kTcObs * 128), &map_xm_hi, bar_xfull + s, a * 32, n0);
-                    tma_load_2d(st + 2 * xk_bytes + xm_bytes + a * (kTcObs * 128), &map_xm_lo, bar_xfull + s, a * 32,
-                                n0);
-                }
-                bulk_load(st + 2 * xk_bytes + 2 * xm_bytes, p.y + n0, kTcObs * 4, bar_xfull + s);
             }
+            for (int a = 0; a < MA; ++a) {
+                tma_load_2d_warp(st + 2 * xk_bytes + a * (kTcObs * 128), &map_xm_hi, bar_xfull + s, a * 32, n0);
+                tma_load_2d_warp(st + 2 * xk_bytes + xm_bytes + a * (kTcObs * 128), &map_xm_lo, bar_xfull + s,
+                                 a * 32, n0);
+            }
+            bulk_load_warp(st + 2 * xk_bytes + 2 * xm_bytes, p.y + n0, kTcObs * 4, bar_xfull + s);
         }
     } else if (warp == 1) {
-        // ---------------- MMA issuer ----------------
-        if (lane == 0 && ntiles > 0) {
+        // ---------------- MMA issuer (the whole warp; an elected lane issues) ----------------
+        if (ntiles > 0) {
             const uint32_t id1 = idesc_tf32(kTcChains, kTcObs, 0);
             const uint32_t id2 = idesc_tf32(kTcChains, Fp, 1);
-            bool ok = mbar_wait(bar_theta, 0, p.err);
+            bool ok = wwait(bar_theta, 0);
             tc_fence_after();
             // GEMM2 of tile j.  The G^T accumulator in TMEM restarts every
             // kTcDrainTiles tiles: the epilogue drains it into FP32 registers
             // (round-to-nearest adds) so only a short run of tensor-core
-            // accumulations ever lands in one TMEM value.  The restart needs no
-            // wait of its own: GEMM2(j) is issued after R(j) is in TMEM, and the
-            // epilogue drains the previous group before it signals R(j).
+            // accumulations ever lands in one TMEM value.  A restart waits for
+            // every epilogue warp's drain of the previous run (bar_drained).
+            // descriptors advance by whole 1 KB blocks: +64 in the address field (addr >> 4)
             auto gemm2 = [&](int j) {
                 const int s = j % kTcStages, b = j % nbuf;
                 const uint32_t xm = smem_u32(smem + s * stage_bytes + 2 * xk_bytes);
-                const uint32_t rhi = tmem + col_buf + b * 64, rlo = rhi + 32;
+                uint32_t rhi = tmem + col_buf + b * 64, rlo = rhi + 32;
+                uint64_t bh = sdesc_sw128b32(xm, kTcObs * 128, 512);
+                uint64_t bl = sdesc_sw128b32(xm + xm_bytes, kTcObs * 128, 512);
+                const uint32_t d2 = tmem + col_d2;
+#pragma unroll
                 for (int kk = 0; kk < kTcObs / 8; ++kk) {
-                    const uint64_t bh = sdesc_sw128b32(xm + kk * 1024, kTcObs * 128, 512);
-                    const uint64_t bl = sdesc_sw128b32(xm + xm_bytes + kk * 1024, kTcObs * 128, 512);
                     const uint32_t first = (j % kTcDrainTiles == 0 && kk == 0) ? 0u : 1u;
-                    mma_ts(tmem + col_d2, rhi + kk * 8, bh, id2, first);
-                    mma_ts(tmem + col_d2, rlo + kk * 8, bh, id2, 1u);
-                    mma_ts(tmem + col_d2, rhi + kk * 8, bl, id2, 1u);
+                    mma_ts_warp(d2, rhi, bh, id2, first);
+                    mma_ts_warp(d2, rlo, bh, id2, 1u);
+                    mma_ts_warp(d2, rhi, bl, id2, 1u);
+                    bh += 64;
+                    bl += 64;
+                    rhi += 8;
+                    rlo += 8;
                 }
-                if ((j + 1) % kTcDrainTiles == 0 || j == ntiles - 1) mma_commit(bar_d2full);
+                if ((j + 1) % kTcDrainTiles == 0 || j == ntiles - 1) mma_commit_warp(bar_d2full);
+            };
+            // whether GEMM2(j) may restart the accumulator (1), not yet (0), or a wait gave up (-1)
+            auto restart_ok = [&](int j, bool block) -> int {
+                if (!p.want_grad || j == 0 || j % kTcDrainTiles) return 1;
+                const uint32_t par = ((j / kTcDrainTiles) - 1) & 1;
+                if (!block) return wtest(bar_drained, par) ? 1 : 0;
+                return wwait(bar_drained, par) ? 1 : -1;
             };
             // GEMM2 of tile j (when the gradient is wanted), then the release of its X stage
             auto finish = [&](int j) {
                 tc_fence_after();
                 if (p.want_grad) gemm2(j);
-                mma_commit(bar_xempty + (j % kTcStages));
+                mma_commit_warp(bar_xempty + (j % kTcStages));
             };
-            int g2 = 0;  // next tile whose GEMM2 / stage release is due
-            for (int i = 0; ok && i < ntiles; ++i) {
-                // buffer i % nbuf is reused: the epilogue has to be done with tile i - nbuf
-                while (g2 <= i - nbuf) {
-                    if (!mbar_wait(bar_rfull + (g2 % nbuf), (g2 / nbuf) & 1, p.err)) { ok = false; break; }
-                    finish(g2++);
-                }
-                if (!ok) break;
-                // GEMM2s whose residuals are already in TMEM go ahead of the next GEMM1
-                while (g2 < i && mbar_test_wait(bar_rfull + (g2 % nbuf), (g2 / nbuf) & 1)) finish(g2++);
+            auto gemm1 = [&](int i) -> bool {
                 const int s = i % kTcStages, b = i % nbuf;
-                if (!mbar_wait(bar_xfull + s, (i / kTcStages) & 1, p.err)) { ok = false; break; }
+                if (!wwait(bar_xfull + s, (i / kTcStages) & 1)) return false;
                 tc_fence_after();
                 const uint32_t xk = smem_u32(smem + s * stage_bytes);
                 const uint32_t d1 = tmem + col_buf + b * 64;
-                for (int kb = 0; kb < KB1; ++kb) {
-                    const uint64_t bh = sdesc_sw32(xk + kb * (kTcObs * 32), 16, 256);
-                    const uint64_t bl = sdesc_sw32(xk + xk_bytes + kb * (kTcObs * 32), 16, 256);
-                    mma_ts(d1, tmem + col_thi + kb * 8, bh, id1, kb > 0 ? 1u : 0u);
-                    mma_ts(d1, tmem + col_thi + kb * 8, bl, id1, 1u);
-                    mma_ts(d1, tmem + col_tlo + kb * 8, bh, id1, 1u);
+                uint64_t bh = sdesc_sw32(xk, 16, 256), bl = sdesc_sw32(xk + xk_bytes, 16, 256);
+                uint32_t ahi = tmem + col_thi, alo = tmem + col_tlo;
+                mma_ts_warp(d1, ahi, bh, id1, 0u);
+                mma_ts_warp(d1, ahi, bl, id1, 1u);
+                mma_ts_warp(d1, alo, bh, id1, 1u);
+                for (int kb = 1; kb < KB1; ++kb) {
+                    bh += 64;
+                    bl += 64;
+                    ahi += 8;
+                    alo += 8;
+                    mma_ts_warp(d1, ahi, bh, id1, 1u);
+                    mma_ts_warp(d1, ahi, bl, id1, 1u);
+                    mma_ts_warp(d1, alo, bh, id1, 1u);
                 }
-                mma_commit(bar_d1full + b);
+                mma_commit_warp(bar_d1full + b);
+                return true;
+            };
+            int g2 = 0;  // next tile whose GEMM2 / stage release is due
+            if (G == 1) {
+                // GEMM1(i), then tile i-1's GEMM2 as soon as its residuals are in TMEM
+                for (int i = 0; ok && i < ntiles; ++i) {
+                    if (!gemm1(i)) { ok = false; break; }
+                    if (i > 0) {
+                        if (!wwait(bar_rfull + (g2 % nbuf), (g2 / nbuf) & 1) || restart_ok(g2, true) < 0) {
+                            ok = false;
+                            break;
+                        }
+                        finish(g2++);
+                    }
+                }
+            } else {
+                for (int i = 0; ok && i < ntiles; ++i) {
+                    // buffer i % nbuf is reused: the epilogue has to be done with tile i - nbuf
+                    while (g2 <= i - nbuf) {
+                        if (!wwait(bar_rfull + (g2 % nbuf), (g2 / nbuf) & 1) || restart_ok(g2, true) < 0) {
+                            ok = false;
+                            break;
+                        }
+                        finish(g2++);
+                    }
+                    if (!ok) break;
+                    // GEMM2s that are ready go ahead of the next GEMM1: they free X stages for the producer
+                    while (g2 < i && wtest(bar_rfull + (g2 % nbuf), (g2 / nbuf) & 1) && restart_ok(g2, false) == 1)
+                        finish(g2++);
+                    if (!gemm1(i)) { ok = false; break; }
+                }
             }
             while (ok && g2 < ntiles) {
-                if (!mbar_wait(bar_rfull + (g2 % nbuf), (g2 / nbuf) & 1, p.err)) break;
+                if (!wwait(bar_rfull + (g2 % nbuf), (g2 / nbuf) & 1) || restart_ok(g2, true) < 0) break;
                 finish(g2++);
             }
         }
@@ -496,13 +637,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             return __all_sync(0xffffffffu, r);
         };
         const int q = warp & 3;                 // TMEM lane quadrant
-        const int slot = (warp - 2) >> 2;       // which quarter of the columns this warp owns
+        const int e = (warp - 2) >> 2;          // which of the quadrant's four warps
+        const int grp = G == 1 ? 0 : (e & 1);   // the tiles i with i % G == grp are this warp's
+        const int slot = G == 1 ? e : (e >> 1); // its kCols observation columns of such a tile
         const int c_local = q * 32 + lane;
         const int c = ctile * kTcChains + c_local;
         const uint32_t lane_off = (uint32_t)(q * 32) << 16;
         // Theta row of this chain -> TF32 hi / lo in TMEM (A operand of GEMM1):
-        // 8-column chunks f0 = 8*slot + 32*k < KC belong to this warp
-        for (int f0 = 8 * slot; f0 < KC; f0 += 32) {
+        // 8-column chunks f0 = 8*e + 32*k < KC belong to this warp
+        for (int f0 = 8 * e; f0 < KC; f0 += 32) {
             uint32_t hi[8], lo[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
@@ -524,13 +667,18 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         float gacc[kOwnCols];
 #pragma unroll
         for (int f = 0; f < kOwnCols; ++f) gacc[f] = 0.0f;
-        // Drain group g (tiles g*kTcDrainTiles ...) of the G^T accumulator into registers.
-        auto drain = [&](int g) -> bool {
-            if (!warp_wait(bar_d2full, g & 1)) return false;
+        // the k-th 16-column chunk of the gradient this warp owns (G = 1: 16 e + 64 k;
+        // G = 2: group grp owns [64 grp, 64 grp + 64), its warps 32 columns each)
+        auto own_col = [&](int k) { return G == 1 ? 16 * e + 64 * k : 64 * grp + 32 * slot + 16 * k; };
+        int drained = 0;  // accumulator runs this warp has drained
+        // Drain the next run of the G^T accumulator into registers; arrive when
+        // a later run will restart the accumulator after it.
+        auto drain_next = [&](bool arrive) -> bool {
+            if (!warp_wait(bar_d2full, drained & 1)) return false;
             tc_fence_after();
 #pragma unroll
             for (int k = 0; k < kOwnCols / 16; ++k) {
-                const int f0 = 16 * slot + 64 * k;
+                const int f0 = own_col(k);
                 if (f0 < Fp) {
                     float gv[16];
                     tmem_ld16(tmem + lane_off + col_d2 + f0, gv);
@@ -538,61 +686,80 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     for (int j = 0; j < 16; ++j) gacc[16 * k + j] += gv[j];
                 }
             }
+            ++drained;
+            if (arrive) {
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(bar_drained);
+            }
             return true;
         };
         bool ok = ntiles > 0;
-        for (int i = 0; ok && i < ntiles; ++i) {
+        for (int i = grp; ok && i < ntiles; i += G) {
             const int b = i % nbuf, s = i % kTcStages;
             // the y tile arrived with the X stage; d1_full(i) implies GEMM1(i) consumed stage s,
             // which the producer only refills after GEMM2(i) -- after this tile's r_full
             if (!warp_wait(bar_d1full + b, (i / nbuf) & 1)) { ok = false; break; }
             tc_fence_after();
-            const int n0 = (t_begin + i) * kTcObs + 8 * slot;
-            const float* ys = reinterpret_cast<const float*>(smem + s * stage_bytes + 2 * xk_bytes + 2 * xm_bytes) +
-                              8 * slot;
-            const uint32_t d1 = tmem + lane_off + col_buf + b * 64 + 8 * slot;
-            float h[8];
-            tmem_ld8(d1, h);
-            const float4 y0 = *reinterpret_cast<const float4*>(ys);
-            const float4 y1 = *reinterpret_cast<const float4*>(ys + 4);
-            const float yt[8] = {y0.x, y0.y, y0.z, y0.w, y1.x, y1.y, y1.z, y1.w};
-            uint32_t rh[8], rl[8];
+            const int c0 = kCols * slot;
+            const int n0 = (t_begin + i) * kTcObs + c0;
+            const float* ys = reinterpret_cast<const float*>(smem + s * stage_bytes + 2 * xk_bytes + 2 * xm_bytes) + c0;
+            const uint32_t d1 = tmem + lane_off + col_buf + b * 64 + c0;
+            float h[kCols];
+            tmem_ld_cols<kCols>(d1, h);
+            // residuals in runs of 8 columns (few live registers beside the gradient accumulators)
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const bool live = n0 + j < p.N;
-                const float yv = live ? yt[j] : 0.0f;
-                const float hv = h[j];
-                // log1p_exp(h) = max(h,0) + log1p(exp(-|h|)); logistic(h) from the same exp (math.jl:202-224)
-                const float e = __expf(-fabsf(hv));
-                const float onepe = 1.0f + e;
-                const float lpe = fmaxf(hv, 0.0f) + __logf(onepe);
-                const float inv = __fdividef(1.0f, onepe);
-                const float sig = hv >= 0.0f ? inv : e * inv;
-                const bool sup = (yv == 0.0f) | (yv == 1.0f);
-                ll += live ? (sup ? yv * hv - lpe : -INFINITY) : 0.0f;
-                const float r = live ? yv - sig : 0.0f;
-                const uint32_t hb = tf32_bits(r);
-                rh[j] = hb;
-                rl[j] = tf32_bits(r - __uint_as_float(hb));
+            for (int j8 = 0; j8 < kCols; j8 += 8) {
+                uint32_t rh[8], rl[8];
+#pragma unroll
+                for (int j0 = 0; j0 < 8; j0 += 4) {
+                    const float4 y4 = *reinterpret_cast<const float4*>(ys + j8 + j0);
+                    const float yt[4] = {y4.x, y4.y, y4.z, y4.w};
+#pragma unroll
+                    for (int jj = 0; jj < 4; ++jj) {
+                        const int j = j0 + jj;
+                        const bool live = n0 + j8 + j < p.N;
+                        const float yv = live ? yt[jj] : 0.0f;
+                        const float hv = h[j8 + j];
+                        // log1p_exp(h) = max(h,0) + log1p(exp(-|h|)); logistic(h) from the same exp (math.jl:202-224)
+                        const float ex = __expf(-fabsf(hv));
+                        const float onepe = 1.0f + ex;
+                        const float lpe = fmaxf(hv, 0.0f) + __logf(onepe);
+                        const float inv = __fdividef(1.0f, onepe);
+                        const float sig = hv >= 0.0f ? inv : ex * inv;
+                        const bool sup = (yv == 0.0f) | (yv == 1.0f);
+                        ll += live ? (sup ? yv * hv - lpe : -INFINITY) : 0.0f;
+                        const float r = live ? yv - sig : 0.0f;
+                        const uint32_t hb = tf32_bits(r);
+                        rh[j] = hb;
+                        rl[j] = tf32_bits(r - __uint_as_float(hb));
+                    }
+                }
+                tmem_st8(d1 + j8, rh);        // R_hi overwrites the consumed H^T columns
+                tmem_st8(d1 + 32 + j8, rl);
             }
-            tmem_st8(d1, rh);        // R_hi overwrites the consumed H^T columns
-            tmem_st8(d1 + 32, rl);
             asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-            // the group that ended with tile i-1: GEMM2(i-1) ran while this tile's
-            // residuals were computed; draining it before R(i) is signalled frees
-            // the accumulator for GEMM2(i)
-            if (p.want_grad && i > 0 && i % kTcDrainTiles == 0 && !drain(i / kTcDrainTiles - 1)) { ok = false; break; }
+            // the first tile of run g (g >= 1) that this warp's group takes: drain
+            // run g-1 (its GEMM2s ran while this tile's residuals were computed)
+            // before the residuals are signalled
+            if (p.want_grad && i >= kTcDrainTiles && i % kTcDrainTiles == grp && !drain_next(true)) {
+                ok = false;
+                break;
+            }
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(bar_rfull + b);
         }
-        if (ok && p.want_grad) ok = drain((ntiles - 1) / kTcDrainTiles);
+        if (ok && p.want_grad) {
+            const int last = (ntiles - 1) / kTcDrainTiles;
+            while (ok && drained <= last) ok = drain_next(drained < last);
+        }
         // combine the four column quarters' log-likelihoods through shared memory
         float* ll_part = reinterpret_cast<float*>(tmem_slot + 4);   // [4][128]
-        ll_part[slot * kTcChains + c_local] = ll;
+        ll_part[e * kTcChains + c_local] = ll;
         asm volatile("bar.sync 1, %0;" ::"n"(kTcEpiThreads));
         if (ok) {
-            if (slot == 0 && c < p.C)
+            if (e == 0 && c < p.C)
                 p.part_ll[(size_t)split * sp.Cl + c] = ((ll_part[c_local] + ll_part[kTcChains + c_local]) +
                                                       ll_part[2 * kTcChains + c_local]) + ll_part[3 * kTcChains + c_local];
             if (p.want_grad && c < p.C) {
@@ -601,7 +768,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 for (int k = 0; k < kOwnCols / 16; ++k) {
 #pragma unroll
                     for (int j = 0; j < 16; ++j) {
-                        const int f = 16 * slot + 64 * k + j;
+                        const int f = own_col(k) + j;
                         if (f < p.F) dst[f] = gacc[16 * k + j];
                     }
                 }
@@ -629,8 +796,10 @@ struct TcGlmPlan {
     int off = 0;
     float icpt_mu = 0, icpt_sigma = 1, coef_mu = 0, coef_sigma = 1;
     CUtensorMap map_xk_hi, map_xk_lo, map_xm_hi, map_xm_lo;
+    bool xk3d = false;   // the K-major maps are 3-D (tc_make_map_kblocks)
     size_t smem = 0;
     int nbuf = 2;        // H/R TMEM buffers
+    int groups = 1;      // epilogue warp groups (2 needs 3 buffers)
     bool wide = false;   // TMEM column plan (tc_columns)
 };
 
@@ -667,6 +836,22 @@ inline bool tc_make_map(CUtensorMap* m, float* base, int rows, int Fp, int box_c
     cuuint32_t estr[2] = {1, 1};
     CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+// The K-major view as a 3-D map: (8 features, rows, K-blocks), the K-block
+// stride 32 bytes inside a row, so one box of (8, 32 rows, kblocks) lands as
+// [K-block][row][8 features] -- the layout of kblocks separate 2-D copies.
+inline bool tc_make_map_kblocks(CUtensorMap* m, float* base, int rows, int Fp, int kblocks, int box_rows) {
+    PFN_encodeTiled enc = tc_encode_fn();
+    if (!enc) return false;
+    cuuint64_t dims[3] = {8, (cuuint64_t)rows, (cuuint64_t)kblocks};
+    cuuint64_t strides[2] = {(cuuint64_t)Fp * sizeof(float), 8 * sizeof(float)};
+    cuuint32_t box[3] = {8, (cuuint32_t)box_rows, (cuuint32_t)kblocks};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
 }
@@ -762,6 +947,18 @@ inline int tc_glm_setup(TcGlmPlan& t, const float* d_Xa, const float* d_y, int N
         tc_err_string() = "cuTensorMapEncodeTiled failed";
         return 1;
     }
+    // the K-major view in one copy per tile and view, where the driver takes the
+    // 3-D map (UT_TC_XK2D=1 keeps the per-K-block copies: a tuning knob)
+    {
+        const char* e2 = getenv("UT_TC_XK2D");
+        CUtensorMap k3h, k3l;
+        if (!(e2 && e2[0] == '1') && tc_make_map_kblocks(&k3h, t.xhi, N, Fp, tc_kblocks_used(F), kTcObs) &&
+            tc_make_map_kblocks(&k3l, t.xlo, N, Fp, tc_kblocks_used(F), kTcObs)) {
+            t.map_xk_hi = k3h;
+            t.map_xk_lo = k3l;
+            t.xk3d = true;
+        }
+    }
     // H/R buffers: as many as TMEM holds (tc_nbuf); UT_TC_BUFFERS=2 keeps two (a tuning knob)
     t.nbuf = tc_nbuf(F, Fp);
     const char* nb_env = getenv("UT_TC_BUFFERS");
@@ -772,10 +969,17 @@ inline int tc_glm_setup(TcGlmPlan& t, const float* d_Xa, const float* d_y, int N
         t.wide = true;
         t.nbuf = 2;
     }
+    // one epilogue group; UT_TC_GROUPS=2 splits it in two on alternate tiles when 3 buffers fit
+    // (a tuning knob: measured slower on config 3)
+    t.groups = 1;
+    const char* g_env = getenv("UT_TC_GROUPS");
+    if (g_env && g_env[0] == '2' && t.nbuf == 3) t.groups = 2;
     t.smem = 1024 + (size_t)kTcStages * tc_stage_bytes(Fp) + 128 + 16 + 4 * kTcChains * sizeof(float);
-    if (cudaFuncSetAttribute(tc_glm_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem) !=
+    if (cudaFuncSetAttribute(tc_glm_kernel<2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem) !=
             cudaSuccess ||
-        cudaFuncSetAttribute(tc_glm_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem) !=
+        cudaFuncSetAttribute(tc_glm_kernel<3, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(tc_glm_kernel<3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem) !=
             cudaSuccess) {
         tc_err_string() = "shared-memory opt-in failed";
         return 1;
@@ -834,11 +1038,17 @@ inline cudaError_t tc_glm_launch(const TcGlmPlan& t, const float* params, float*
     int cols[3];
     tc_columns(t.F, t.Fp, t.wide, cols);
     p.col_tlo = cols[0]; p.col_d2 = cols[1]; p.col_buf = cols[2];
+    p.xk3d = t.xk3d ? 1 : 0;
     dim3 grid(t.ctiles, t.S);
-    if (t.nbuf == 3)
-        tc_glm_kernel<3><<<grid, kTcThreads, t.smem, st>>>(t.map_xk_hi, t.map_xk_lo, t.map_xm_hi, t.map_xm_lo, params, p);
+    if (t.nbuf == 3 && t.groups == 2)
+        tc_glm_kernel<3, 2><<<grid, kTcThreads, t.smem, st>>>(t.map_xk_hi, t.map_xk_lo, t.map_xm_hi, t.map_xm_lo,
+                                                              params, p);
+    else if (t.nbuf == 3)
+        tc_glm_kernel<3, 1><<<grid, kTcThreads, t.smem, st>>>(t.map_xk_hi, t.map_xk_lo, t.map_xm_hi, t.map_xm_lo,
+                                                              params, p);
     else
-        tc_glm_kernel<2><<<grid, kTcThreads, t.smem, st>>>(t.map_xk_hi, t.map_xk_lo, t.map_xm_hi, t.map_xm_lo, params, p);
+        tc_glm_kernel<2, 1><<<grid, kTcThreads, t.smem, st>>>(t.map_xk_hi, t.map_xk_lo, t.map_xm_hi, t.map_xm_lo,
+                                                              params, p);
     tc_reduce_kernel<<<t.C, 128, 0, st>>>(params, totals, grads, p, t.off, t.icpt_mu, t.icpt_sigma, t.coef_mu,
                                           t.coef_sigma);
     return cudaGetLastError();
