@@ -174,7 +174,7 @@ def _profiled_traffic():
 #   |g - g64| <= GRAD_RTOL * |g64| + GRAD_ATOL_MAG * m,
 # m = the sum of the magnitudes of the terms g adds up (oracle gradient_magnitude).
 GRAD_RTOL = 1e-5
-GRAD_ATOL_MAG = 2e-6
+GRAD_ATOL_MAG = 1e-6
 
 
 def fp64_error(model, X, y, params, totals, grads):
@@ -319,6 +319,7 @@ def run_b200(args):
         if world == 1:
             _emit("hbm_sweep", hbm_sweep())
             _emit("hbm_sweep_large", hbm_sweep_large())
+            _emit("hbm_trajectory", hbm_trajectory())
             samplers = None
             if not args.no_samplers:
                 samplers = {}
@@ -398,6 +399,71 @@ def hbm_sweep_large(num_obs=1_000_000, chain_counts=(1, 4, 16), steps=10, warmup
     return {"metric": "few-chain logjoint(+gradient) HBM roofline, design larger than L2",
             "peak_GB/s": hbm, "peak_source": f"{kind} HBM copy bandwidth",
             "l2": "X (400 MB) > L2 (126 MB): every evaluation reads X from HBM", "rows": rows}
+
+
+def hbm_trajectory(designs=((100_000, "config-3 design, 40 MB: steps 2..L read X from L2"),
+                            (1_000_000, "400 MB design > L2: every step reads X from HBM")),
+                   chain_counts=(1, 4), L=8, reps=10, warmup=3):
+    """Whole HMC trajectories of L leapfrog steps on the streaming path: the L
+    gradient evaluations and the kicks and drifts between them in one
+    cooperative launch (bracketed by the momentum and accept kernels), against
+    one launch per step (UT_DISABLE_STREAM_TRAJECTORY=1, the same values bit for
+    bit).  Achieved GB/s = L x the algorithmic bytes of one evaluation (X and y)
+    / the iteration's device time; L2 flushed (256 MB write) before every timed
+    iteration, so each trajectory's first read of X comes from HBM."""
+    import ctypes
+    import torch
+    from uncertaintea_b200 import _native as nat
+    from uncertaintea_b200.device import DeviceBatchedWorkspace, _stream_handle
+    from uncertaintea_b200.models import BernoulliLogitGLM, logistic_regression_data
+    hbm, _, kind = _peaks()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    lib = nat.load()
+    out = []
+    for num_obs, note in designs:
+        X, y, _ = logistic_regression_data(num_obs, N_COEF, seed=4, x_scale=1.0 / np.sqrt(N_COEF))
+        model = BernoulliLogitGLM(N_COEF)
+        nbytes = num_obs * N_COEF * 4 + num_obs * 4
+        for C in chain_counts:
+            ws = DeviceBatchedWorkspace(model, C, args=(X,), constraints={"y": y})
+            q0 = torch.from_numpy((0.05 * np.random.default_rng(2).standard_normal((C, N_COEF))).astype(np.float32)).cuda()
+            f = lambda dt=torch.float32: torch.zeros(C, dtype=dt, device="cuda")  # noqa: E731
+            outs = [f(), f(), f(), f(torch.uint8), f(torch.uint8)]
+            im = torch.ones(N_COEF, device="cuda")
+            stp = torch.full((C,), 1e-3, device="cuda")
+            row = {"chains": C, "n_obs": num_obs, "L": L, "kernel_path": ws.kernel_path(), "note": note}
+            for name, env in (("one_launch", None), ("launch_per_step", "1")):
+                if env:
+                    os.environ["UT_DISABLE_STREAM_TRAJECTORY"] = env
+                else:
+                    os.environ.pop("UT_DISABLE_STREAM_TRAJECTORY", None)
+                qd = q0.clone()
+                t, g = ws.logjoint_gradient_device(qd)
+                buf = nat.HmcBuffers(nat.ptr(qd), nat.ptr(g), nat.ptr(t), nat.ptr(im), nat.ptr(stp),
+                                     *[nat.ptr(o) for o in outs], None, None)
+                times = []
+                for it in range(warmup + reps):
+                    flush.fill_(1.0)
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record(stream)
+                    nat.check(lib.ut_hmc_iteration(ws.handle, ctypes.byref(buf), L, 1000 + it, 1000.0,
+                                                   _stream_handle()))
+                    b.record(stream)
+                    torch.cuda.synchronize()
+                    if it >= warmup:
+                        times.append(a.elapsed_time(b))
+                ms = float(np.median(times))
+                gbs = L * nbytes / (ms / 1000.0) / 1e9
+                row[name] = {"ms": ms, "us_per_step": 1000.0 * ms / L, "GB/s": gbs, "frac": gbs / hbm}
+                ws.check()
+            os.environ.pop("UT_DISABLE_STREAM_TRAJECTORY", None)
+            ws.check()
+            ws.close()
+            out.append(row)
+    return {"metric": "few-chain HMC trajectory (L leapfrog evaluations), achieved GB/s of L x (X + y)",
+            "peak_GB/s": hbm, "peak_source": f"{kind} HBM copy bandwidth",
+            "l2": "flushed (256 MB write) before every timed iteration", "rows": out}
 
 
 def hbm_sweep(chain_counts=(1, 4, 8, 16), steps=20, warmup=5):
@@ -509,26 +575,75 @@ def _chain_summary(ch, cfg, extra=None):
     return out
 
 
-def sampler_glm_hmc(num_samples=1000):
+def _gate_prefixes(ch, lengths):
+    """The gate on the first S draws of every chain, for each S in lengths: max
+    rank-normalised split R-hat and min bulk ESS over parameters (the
+    reference's estimators, computed per parameter on the device:
+    multi.rank_split_rhat / multi.split_ess), and min-ESS/s over the device
+    time of those S sampling iterations (a sampling iteration's cost does not
+    depend on its index, so that time is the run's times S / S_total)."""
+    import torch
+    from uncertaintea_b200.multi import rank_split_rhat, split_ess
+    d = ch.unconstrained                        # (C, S_total, P)
+    C, S_tot, P = d.shape
+    rows = []
+    for S in lengths:
+        if S > S_tot:
+            break
+        r_max, e_min = 0.0, float("inf")
+        for p in range(P):
+            x = torch.from_numpy(np.ascontiguousarray(d[:, :S, p].T)).cuda()[:, :, None]   # (S, C, 1)
+            r_max = max(r_max, float(torch.nan_to_num(rank_split_rhat(x), nan=float("inf"))[0]))
+            e_min = min(e_min, float(torch.nan_to_num(split_ess(x), nan=float("inf"))[0]))
+        t = ch.sampling_seconds * S / S_tot
+        rows.append({"draws": S, "max_rank_rhat": r_max, "min_ess": e_min, "min_ess_per_s": e_min / t,
+                     "gate_rank_rhat_lt_1.01": bool(r_max < 1.01)})
+    return rows
+
+
+def _gated_summary(ch, cfg, lengths, extra=None):
+    """The 1000-draw figures (as configured) and the gate over longer prefixes of
+    the same run: `gate` is the shortest prefix whose rank R-hat is below 1.01
+    (null when none is)."""
+    rows = _gate_prefixes(ch, lengths)
+    first = rows[0]
+    passed = [r for r in rows if r["gate_rank_rhat_lt_1.01"]]
+    total_s = ch.warmup_seconds + ch.sampling_seconds
+    out = {"min_ess_per_s": first["min_ess_per_s"], "min_ess": first["min_ess"],
+           "max_rank_rhat": first["max_rank_rhat"], "gate_rank_rhat_lt_1.01": first["gate_rank_rhat_lt_1.01"],
+           "draws": first["draws"], "gate": passed[0] if passed else None, "prefixes": rows,
+           "warmup_s": ch.warmup_seconds, "sampling_s_all_draws": ch.sampling_seconds,
+           "grad_evals_per_s": ch.gradient_evaluations / total_s, "mean_accept": float(ch.accept_prob.mean()),
+           "config": cfg}
+    out.update(extra or {})
+    return out
+
+
+def sampler_glm_hmc(num_samples=16000):
     """Batched HMC on the 1000 x 10 logistic regression: 256 chains, 8 leapfrog
-    steps, step 0.05 without step adaptation, 1000 warmup + num_samples draws,
-    seed 1."""
+    steps, step 0.05 without step adaptation, 1000 warmup, seed 1.  The
+    configured 1000 draws are the first 1000 of one run of num_samples; the
+    gate is evaluated on longer prefixes of it."""
     from uncertaintea_b200 import BernoulliLogitGLM, batched_hmc, logistic_regression_data
     X, y, _ = logistic_regression_data(1000, 10, seed=1)
     ch = batched_hmc(BernoulliLogitGLM(10), (X,), {"y": y}, num_chains=256, num_samples=num_samples,
                      num_warmup=1000, step_size=0.05, num_leapfrog_steps=8, adapt_step_size=False, rng=1)
-    return _chain_summary(ch, f"256 chains, L=8, step 0.05, 1000+{num_samples}, GLM 1000x10")
+    return _gated_summary(ch, f"256 chains, L=8, step 0.05, 1000 warmup + 1000 draws (gate on up to "
+                              f"{num_samples}), GLM 1000x10", [1000, 2000, 4000, 8000, 16000])
 
 
-def sampler_hier_nuts(num_samples=1000):
+def sampler_hier_nuts(num_samples=8000):
     """Batched persistent NUTS on the non-centred hierarchical model with J = 64
     groups x 20 observations (sigma_j ~ U(0.5, 2), y from the prior at seed 7;
-    4096 chains, max tree depth 10, 1000 warmup + num_samples draws)."""
+    4096 chains, max tree depth 10, 1000 warmup).  The configured 1000 draws are
+    the first 1000 of one run of num_samples; the gate is evaluated on longer
+    prefixes of it."""
     from uncertaintea_b200 import HierarchicalNormalNoncentered, batched_nuts, hierarchical_data
     yh, sig, sizes, _ = hierarchical_data(64, 20, 7)
     ch = batched_nuts(HierarchicalNormalNoncentered(64), (sig, sizes), {"y": yh}, num_chains=4096,
                       num_samples=num_samples, num_warmup=1000, max_tree_depth=10, rng=7)
-    return _chain_summary(ch, f"4096 chains, depth 10, 1000+{num_samples}, hierarchical J=64 x 20",
+    return _gated_summary(ch, f"4096 chains, depth 10, 1000 warmup + 1000 draws (gate on up to {num_samples}), "
+                              "hierarchical J=64 x 20", [1000, 2000, 4000, 8000],
                           {"mean_tree_depth": float(ch.tree_depth.mean())})
 
 
@@ -607,17 +722,20 @@ def surrogate_comparison(num_chains=4096, num_warmup=500, num_samples=500):
       adapted_forward    -- adapted with the forward endpoint velocity (an
                             ascent on the ChEES criterion).
     Min ESS over the 100 coefficients per second of sampling, and per second
-    of warmup + training + sampling."""
+    of warmup + training + sampling.  The fixed-16 pair samples twice as many
+    iterations: at 16 steps of the adapted step size its draws are more
+    autocorrelated, and 500 of them stop just short of rank R-hat < 1.01."""
     model, X, y, _ = _data()
     base = dict(num_chains=num_chains, num_samples=num_samples, num_warmup=num_warmup, rng=1)
-    out = {"fixed16": _surrogate_pair(model, X, y, fixed_leapfrog_steps=16, **base),
+    fixed = dict(base, num_samples=2 * num_samples)
+    out = {"fixed16": _surrogate_pair(model, X, y, fixed_leapfrog_steps=16, **fixed),
            "adapted_reference": _surrogate_pair(model, X, y, num_leapfrog_steps=16, **base),
            "adapted_forward": _surrogate_pair(model, X, y, num_leapfrog_steps=16, trajectory_velocity="forward",
                                               **base)}
     out["metric"] = "min ESS/s (rank R-hat<1.01), surrogate ChEES-HMC vs plain ChEES-HMC"
     out["unit"] = "effective samples/s"
     out["config"] = (f"learned gradient surrogate on the 100000x100 logistic regression, {num_chains} chains, "
-                     f"{num_warmup} warmup + {num_samples} sampling iterations")
+                     f"{num_warmup} warmup + {num_samples} sampling iterations ({2 * num_samples} for fixed16)")
     return out
 
 
@@ -637,7 +755,7 @@ def uneven_models(num_models=512, seed=5):
     return models
 
 
-def uneven_batch(num_models=512, chains=64, num_warmup=500, num_samples=1500):
+def uneven_batch(num_models=512, chains=64, num_warmup=500, num_samples=1000):
     """All models in one batched persistent-NUTS run (one launch per
     parameter-slot class per iteration, replayed from a CUDA graph, launch
     shapes from the autotuner): aggregate min-ESS per sampling second and the
@@ -660,6 +778,10 @@ def uneven_batch(num_models=512, chains=64, num_warmup=500, num_samples=1500):
            "sampling_time_to_rhat_p50_s": s50, "sampling_time_to_rhat_p99_s": s99,
            "time_to_rhat_note": "null = that share of models did not reach R-hat < 1.01 within the run",
            "converged_fraction": res.converged_fraction, "median_model_min_ess": float(np.median(res.min_ess)),
+           "converged_models_time_to_rhat_p50_s": (float(np.median(res.time_to_rhat[np.isfinite(res.time_to_rhat)]))
+                                                   if np.isfinite(res.time_to_rhat).any() else None),
+           "final_rank_rhat_p50": float(np.median(res.max_rhat)),
+           "final_rank_rhat_p99": float(np.quantile(res.max_rhat, 0.99)),
            "warmup_s": res.warmup_seconds, "sampling_s": res.sampling_seconds,
            "ms_per_iteration": 1000.0 * res.sampling_seconds / max(drawn, 1),
            "draws_cap": num_samples, "draws_run": drawn,

@@ -390,6 +390,48 @@ def test_chees_iteration_is_the_hmc_iteration_with_its_outputs(lib):
     ws.close()
 
 
+@pytest.mark.parametrize("C,N,D,intercept,L", [(1, 50000, 20, False, 8), (4, 20000, 99, True, 8),
+                                                (16, 8000, 36, False, 5), (3, 12000, 12, False, 1),
+                                                # more chunks per CTA than ring stages: refills
+                                                (4, 100000, 99, True, 4), (1, 100000, 100, False, 3)])
+def test_stream_trajectory_in_one_launch_is_the_step_path(lib, monkeypatch, C, N, D, intercept, L):
+    """Few chains on the streaming path: ut_hmc_iteration runs the L gradient
+    evaluations of a trajectory, and the kicks and drifts between them, in one
+    cooperative launch.  Its state and outputs equal those of one launch per
+    step bit for bit (the fold keeps the streaming kernel's summation order),
+    again on a second call (the grid barrier's state carries over), and the
+    iteration agrees with the oracle's under the same Philox streams."""
+    m, args, cons, _ = _glm_case(N, D, C, intercept, 7, 0.3)
+    X = args[0]
+    Xa = np.hstack([np.ones((N, 1)), X]) if intercept else X
+    mode = _glm_mode(Xa, cons["y"])
+    r = np.random.default_rng(8)
+    P = m.num_params()
+    q = (mode + 0.02 * r.standard_normal((C, P))).astype(np.float32)
+    ws = _ws(m, args, cons, C)
+    assert ws.kernel_path() == "stream"
+    im = np.linspace(0.5, 1.5, P)
+    steps = np.full(C, 0.01) * np.linspace(0.8, 1.2, C)
+    monkeypatch.setenv("UT_DISABLE_STREAM_TRAJECTORY", "1")
+    a = _hmc_gpu(ws, *_state(ws, q), im, steps, L, 4242, want=True)
+    monkeypatch.delenv("UT_DISABLE_STREAM_TRAJECTORY")
+    for _ in range(2):
+        b = _hmc_gpu(ws, *_state(ws, q), im, steps, L, 4242, want=True)
+        for k in a:
+            assert np.array_equal(a[k], b[k]), k
+    ws.check()
+    om = oracle.OracleModel(ws.lowered)
+    qd, g, t = _state(ws, q)
+    qo, go, to = qd.cpu().numpy().copy(), g.cpu().numpy().copy(), t.cpu().numpy().copy()
+    ref = om.hmc_iteration(qo, go, to, im, steps, L, 4242, want_proposal=True)
+    assert np.array_equal(b["accepted"], ref["accepted"]) and not ref["divergent"].any()
+    np.testing.assert_allclose(b["proposal"], ref["proposal"], rtol=1e-3, atol=1e-4)
+    # the energy error is a difference of logjoints of magnitude ~1e4 here, whose
+    # FP32 roundoff (~1e-3 each) shows in the accept probability
+    np.testing.assert_allclose(b["accept_prob"], ref["accept_prob"], atol=1e-2)
+    ws.close()
+
+
 @pytest.mark.parametrize("case", ["glm_c1", "glm_tiled", "hier", "gauss"])
 def test_hmc_iteration_vs_oracle(lib, case):
     """One HMC iteration from near-posterior states with stable step sizes:

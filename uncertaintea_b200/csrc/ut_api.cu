@@ -96,6 +96,7 @@ struct ut_workspace {
     float* d_sgpart = nullptr;      // per-group partials
     unsigned* d_stickets = nullptr; // fold tickets (zero between launches)
     int* d_serr = nullptr;          // sticky error word of the streaming kernel
+    unsigned* d_sbar = nullptr;     // grid barrier of the one-launch trajectory: [arrivals, generation]
     // batched leapfrog scratch
     LfScratch lf = {};
     // NUTS checkpoint scratch
@@ -356,6 +357,43 @@ int32_t launch_stream(ut_workspace* ws, const float* params, float* totals, floa
     return UT_OK;
 }
 
+// Steps 1..L of a leapfrog trajectory on the streaming path in one cooperative
+// launch (glm_stream_traj_kernel): the L evaluations at ws->lf.wq and the
+// kicks and drifts between them; lf_begin_kernel runs before it and
+// lf_step_kernel (l = L) after it.  UT_ERR_UNSUPPORTED when the launch cannot
+// be made cooperative here (the caller then runs the steps one launch each).
+int32_t launch_stream_traj(ut_workspace* ws, const HmcArgs& h, int L, cudaStream_t st) {
+    int32_t rc;
+    if (!ws->d_sbar) {
+        if ((rc = dalloc(ws, &ws->d_sbar, 2))) return rc;
+        UT_CUDA(cudaMemset(ws->d_sbar, 0, 2 * sizeof(unsigned)));
+    }
+    int coop = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ws->device);
+    if (!coop) return UT_ERR_UNSUPPORTED;
+    GlmTrajArgs t;
+    GlmStreamArgs& a = t.s;
+    a.Xa = ws->d_Xa; a.ypad = ws->d_ypad; a.params = ws->lf.wq;
+    a.part = ws->d_spart; a.gpart = ws->d_sgpart; a.tickets = ws->d_stickets; a.err = ws->d_serr;
+    a.totals = ws->lf.wlj; a.grads = ws->lf.wg;
+    a.N = ws->N; a.F = ws->P; a.C = ws->C; a.stages = ws->stream_stages; a.slots = ws->stream_slots;
+    a.off = ws->plan.has_intercept;
+    a.icpt_mu = (float)ws->plan.intercept_mu; a.icpt_sigma = (float)ws->plan.intercept_sigma;
+    a.coef_mu = (float)ws->plan.coef_mu; a.coef_sigma = (float)ws->plan.coef_sigma;
+    t.wq = ws->lf.wq; t.wp = ws->lf.wp; t.wg = ws->lf.wg; t.wlj = ws->lf.wlj; t.valid = ws->lf.valid;
+    t.inverse_mass = h.inverse_mass; t.step = h.step; t.bar = ws->d_sbar; t.L = L;
+    const size_t smem = ws->stream_smem;
+    void* args[] = {&t};
+#define TRAJ_CASE(CBV)                                                                                      case CBV: {                                                                                                 auto kern = glm_stream_traj_kernel<CBV>;                                                               UT_CUDA(allow_dynamic_smem(kern, smem));                                                              int per_sm = 0;                                                                                         UT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kStreamThreads, smem));           int sms = 0;                                                                                            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ws->device);                               if (per_sm < 1 || ws->stream_splits > per_sm * sms) return UT_ERR_UNSUPPORTED;                          UT_CUDA(cudaLaunchCooperativeKernel((const void*)kern, dim3(ws->stream_splits), dim3(kStreamThreads),                                             args, smem, st));                                              } break;
+    switch (ws->stream_cb) {
+        TRAJ_CASE(1) TRAJ_CASE(2) TRAJ_CASE(4) TRAJ_CASE(8)
+        default: TRAJ_CASE(16)
+    }
+#undef TRAJ_CASE
+    UT_LAUNCHED();
+    return UT_OK;
+}
+
 // The streaming kernel over the first n (<= 16) rows of `params` of a GLM
 // workspace that normally uses another path (the lockstep tail): buffers for 16
 // chains are made on first use, the stage plan follows the chain bucket.
@@ -473,9 +511,10 @@ int32_t error_reads_status(ut_workspace* ws) {
                                            "its results are invalid");
     }
     if (ws->h_err[1]) {
+        const int code = ws->h_err[1];
         UT_CUDA(cudaMemset(ws->d_serr, 0, sizeof(int)));
-        return fail(UT_ERR_DEVICE_TIMEOUT, "a bounded wait inside the streaming GLM kernel gave up; "
-                                           "its results are invalid");
+        return fail(UT_ERR_DEVICE_TIMEOUT, "a bounded wait inside the streaming GLM kernel gave up (%s); "
+                                           "its results are invalid", code == 2 ? "grid barrier" : "ring wait");
     }
     return UT_OK;
 }
@@ -888,8 +927,8 @@ int32_t ut_workspace_check(ut_workspace* ws, void* stream) {
         UT_CUDA(cudaMemcpy(&h, ws->d_serr, sizeof(int), cudaMemcpyDeviceToHost));
         if (h) {
             UT_CUDA(cudaMemset(ws->d_serr, 0, sizeof(int)));
-            return fail(UT_ERR_DEVICE_TIMEOUT, "a bounded wait inside the streaming GLM kernel gave up; "
-                                               "its results are invalid");
+            return fail(UT_ERR_DEVICE_TIMEOUT, "a bounded wait inside the streaming GLM kernel gave up (%s); "
+                                               "its results are invalid", h == 2 ? "grid barrier" : "ring wait");
         }
     }
     return UT_OK;
@@ -1084,6 +1123,18 @@ int32_t ut_hmc_iteration(ut_workspace* ws, const ut_hmc_buffers* buf, int32_t nu
     const unsigned grid = (ws->C + 7) / 8;
     UT_K_SWITCH(ws->K, lf_begin_kernel<K><<<grid, 256, 0, st>>>(a, ws->lf, P));
     UT_LAUNCHED();
+    // few chains on the streaming path: the L evaluations in one launch
+    // (UT_DISABLE_STREAM_TRAJECTORY=1 keeps one launch per step; same values, bit for bit)
+    const char* no_traj = getenv("UT_DISABLE_STREAM_TRAJECTORY");
+    if (ws->streaming && !(no_traj && no_traj[0] == '1')) {
+        rc = launch_stream_traj(ws, a, num_leapfrog_steps, st);
+        if (rc == UT_OK) {
+            UT_K_SWITCH(ws->K, lf_step_kernel<K><<<grid, 256, 0, st>>>(a, ws->lf, P, num_leapfrog_steps));
+            UT_LAUNCHED();
+            return UT_OK;
+        }
+        if (rc != UT_ERR_UNSUPPORTED) return rc;
+    }
     for (int l = 1; l <= num_leapfrog_steps; ++l) {
         if ((rc = density(ws, ws->lf.wq, ws->lf.wlj, ws->lf.wg, st))) return rc;
         UT_K_SWITCH(ws->K, lf_step_kernel<K><<<grid, 256, 0, st>>>(a, ws->lf, P, l));

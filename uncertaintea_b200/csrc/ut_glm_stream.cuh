@@ -89,11 +89,18 @@ inline bool glm_stream_plan(int CB, int F, size_t smem_limit, int* stages, int* 
     return true;
 }
 
+// One CTA's share of one evaluation: load theta (a.params) into shared
+// memory, stream this CTA's chunks through the ring, and write the CTA's
+// partial sums ([ll, g_0..g_F-1] per chain, summed over its warps in
+// chunk-slot order) to a.part[blockIdx.x].  The ring's mbarriers are
+// initialised by the first call of a launch (call = 0); a later call (once
+// every thread of the CTA has left the previous one) keeps them and offsets
+// its wait parities by the phases each stage completed in the earlier calls:
+// stage s takes U_s = ceil((n - s) / NS) chunks per call and is released for
+// a refill U_s - 1 times.
 template <int CB, bool GRAD>
-__global__ void __launch_bounds__(kStreamThreads, 1) glm_stream_kernel(GlmStreamArgs a) {
+__device__ __forceinline__ void stream_cta_partial(const GlmStreamArgs& a, uint8_t* stream_smem, int call = 0) {
     constexpr int CG = glm_stream_cg(CB), CH = glm_stream_ch(CB), SLOTS = kStreamWarps / CG;
-    extern __shared__ __align__(1024) uint8_t stream_smem[];
-    __shared__ int s_last;
     const int F = a.F, F4 = F / 4, N = a.N, C = a.C, NS = a.stages, SL = a.slots;
     const int Wd = GRAD ? F + 1 : 1;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -109,7 +116,7 @@ __global__ void __launch_bounds__(kStreamThreads, 1) glm_stream_kernel(GlmStream
     const int c1 = (int)((long long)(blockIdx.x + 1) * NC / gridDim.x);
     const int n = c1 - c0;
 
-    if (tid == 0) {
+    if (tid == 0 && call == 0) {
         for (int s = 0; s < NS; ++s) {
             mbar_init(full + s, 1);
             mbar_init(empty + s, CG);
@@ -118,8 +125,11 @@ __global__ void __launch_bounds__(kStreamThreads, 1) glm_stream_kernel(GlmStream
     }
     for (int i = tid; i < CB * F; i += blockDim.x) {
         const int c = i / F, f = i % F;
-        Th[i] = c < C ? a.params[(size_t)c * F + f] : 0.0f;
+        Th[i] = c < C ? __ldcg(a.params + (size_t)c * F + f) : 0.0f;   // L2: another SM may have written it
     }
+    // the ring's previous contents were written through the generic proxy (partial
+    // sums, a fold's scratch): order them before the bulk copies that refill it
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
 
     float ll[CH];
@@ -133,6 +143,9 @@ __global__ void __launch_bounds__(kStreamThreads, 1) glm_stream_kernel(GlmStream
     // chunk i of this CTA -> slot i % SL, stage slot + SL * ((i / SL) % P), use (i / SL) / P
     const int P = NS / SL;
     auto stage_of = [&](int i) { return i % SL + SL * ((i / SL) % P); };
+    // phases stage s completed in the earlier calls of this launch (full, empty)
+    auto full_base = [&](int s) { return (uint32_t)call * (uint32_t)(s < n ? (n - s + NS - 1) / NS : 0); };
+    auto empty_base = [&](int s) { return (uint32_t)call * (uint32_t)(s < n ? (n - s + NS - 1) / NS - 1 : 0); };
     auto issue = [&](int i) {
         const int s = stage_of(i);
         const int r0 = (c0 + i) * kStreamRows;
@@ -153,7 +166,7 @@ __global__ void __launch_bounds__(kStreamThreads, 1) glm_stream_kernel(GlmStream
         for (int i = slot < SL ? slot : n; i < n; i += SL) {  // warps of unused slots stay idle
             const int s = stage_of(i);
             const uint32_t use = (uint32_t)((i / SL) / P);
-            if (!mbar_wait(full + s, use & 1, a.err)) break;
+            if (!mbar_wait(full + s, (full_base(s) + use) & 1, a.err)) break;
             const int nrows = min(kStreamRows, N - (c0 + i) * kStreamRows);
             const float* st = ring + s * stage_floats;
             const float4* X4 = reinterpret_cast<const float4*>(st);
@@ -236,7 +249,7 @@ __global__ void __launch_bounds__(kStreamThreads, 1) glm_stream_kernel(GlmStream
                     if (cb0 == 0) {
                         bool ok = true;
                         if (lane == 0) {
-                            ok = mbar_wait(empty + s, use & 1, a.err);
+                            ok = mbar_wait(empty + s, (empty_base(s) + use) & 1, a.err);
                             if (ok) issue(i + NS);
                         }
                         if (!__shfl_sync(UT_FULL_MASK, ok ? 1 : 0, 0)) break;
@@ -268,6 +281,19 @@ __global__ void __launch_bounds__(kStreamThreads, 1) glm_stream_kernel(GlmStream
         for (int w = 0; w < SLOTS; ++w) t += ring[(size_t)(w0 + w) * CH * Wd + cl * Wd + k];
         a.part[(size_t)b * CW + i] = t;
     }
+}
+
+template <int CB, bool GRAD>
+__global__ void __launch_bounds__(kStreamThreads, 1) glm_stream_kernel(GlmStreamArgs a) {
+    extern __shared__ __align__(1024) uint8_t stream_smem[];
+    __shared__ int s_last;
+    stream_cta_partial<CB, GRAD>(a, stream_smem);
+    const int F = a.F, C = a.C;
+    const int Wd = GRAD ? F + 1 : 1;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const float* Th = reinterpret_cast<const float*>(stream_smem + kStreamHeader);    // [CB][F]
+    float* ring = reinterpret_cast<float*>(stream_smem + kStreamHeader) + CB * F + kStreamWarps * kStreamRows * glm_stream_ch(CB);
+    const int S = gridDim.x, b = blockIdx.x, CW = C * Wd;
 
     // first-level fold: the last CTA of this group adds the group's partials in CTA
     // order.  The ticket is taken by one thread after the CTA barrier (its fence
@@ -329,6 +355,159 @@ __global__ void __launch_bounds__(kStreamThreads, 1) glm_stream_kernel(GlmStream
     }
     // every CTA has taken its tickets: reset them for the next launch
     for (int i = tid; i <= NG; i += blockDim.x) a.tickets[i] = 0u;
+}
+
+// ---------------------------------------------------------------------------
+// A whole leapfrog trajectory in one launch (few chains).
+//
+// The batched leapfrog path runs L x [batched gradient -> lf_step_kernel]: at
+// a design of 40 MB each evaluation is one launch whose ramp and fold tail
+// cost as much as its streaming.  glm_stream_traj_kernel runs the L
+// evaluations, and the L - 1 intermediate kicks and drifts between them, in
+// one cooperative launch (one CTA per SM, all resident): per step every CTA
+// streams its rows (stream_cta_partial), a grid barrier, then CTA c folds
+// chain c's per-CTA partials -- in exactly the order of glm_stream_kernel's
+// two-level fold, so every value is bit-identical to the step-by-step path --
+// adds the prior term, and applies lf_step_kernel's kick and drift; a second
+// grid barrier publishes the new positions.  After step L it leaves the
+// gradient and logjoint at the final position for lf_step_kernel (l = L),
+// which closes the trajectory.  Barrier waits are bounded: one that gives up
+// raises the error word and the CTA returns.
+// ---------------------------------------------------------------------------
+struct GlmTrajArgs {
+    GlmStreamArgs s;            // s.params = wq, s.part = per-CTA partials (S x C x (F + 1))
+    float* wq;                  // C x F working position
+    float* wp;                  // C x F working momentum
+    float* wg;                  // C x F gradient at wq
+    float* wlj;                 // C     logjoint at wq (written after the last step)
+    uint8_t* valid;             // C
+    const float* inverse_mass;  // F
+    const float* step;          // C
+    unsigned* bar;              // [arrivals, generation]: arrivals are 0 between barriers
+    int L;
+};
+
+// Grid-wide barrier of a cooperative launch.  gen: the generation thread 0
+// last saw.  Returns false (error word raised) when the wait gave up.
+__device__ __forceinline__ bool stream_grid_sync(unsigned* bar, unsigned& gen, int* err, int* s_ok) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned target = gen + 1u;
+        __threadfence();
+        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicExch(bar + 1, target);
+        } else {
+            const long long t0 = clock64();
+            for (unsigned it = 1;; ++it) {
+                if (*reinterpret_cast<volatile unsigned*>(bar + 1) == target) break;
+                if ((it & 255u) == 0u &&
+                    (clock64() - t0 > kTcWaitClocks || *reinterpret_cast<volatile int*>(err))) {
+                    atomicCAS(err, 0, 2);   // 2: a grid barrier gave up (1: a ring wait)
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        __threadfence();
+        gen = target;
+        *s_ok = ok;
+    }
+    __syncthreads();
+    return *s_ok != 0;
+}
+
+template <int CB>
+__global__ void __launch_bounds__(kStreamThreads, 1) glm_stream_traj_kernel(GlmTrajArgs t) {
+    extern __shared__ __align__(1024) uint8_t stream_smem[];
+    __shared__ int s_ok;
+    const GlmStreamArgs& a = t.s;
+    const int F = a.F, C = a.C, Wd = F + 1, S = gridDim.x, CW = C * Wd;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int NG = (S + kStreamGroup - 1) / kStreamGroup;
+    float* G = reinterpret_cast<float*>(stream_smem + kStreamHeader);  // [NG][Wd] group sums (reuses theta/ring)
+    float* V = G + (size_t)NG * Wd;                                     // [Wd] chain totals
+    unsigned gen = 0;
+    if (tid == 0) gen = *reinterpret_cast<volatile unsigned*>(t.bar + 1);
+    const int c = blockIdx.x;  // the chain this CTA folds and steps (c < C)
+    bool valid = c < C && __ldcg(t.valid + c) != 0;
+    for (int l = 1; l <= t.L; ++l) {
+        stream_cta_partial<CB, true>(a, stream_smem, l - 1);
+        if (!stream_grid_sync(t.bar, gen, a.err, &s_ok)) return;
+        if (c < C) {
+            // first level: groups of kStreamGroup CTAs, in CTA order
+            for (int idx = tid; idx < NG * Wd; idx += blockDim.x) {
+                const int grp = idx / Wd, k = idx % Wd, g0 = grp * kStreamGroup, g1 = min(S, g0 + kStreamGroup);
+                float v[kStreamGroup];
+#pragma unroll
+                for (int q = 0; q < kStreamGroup; ++q)
+                    v[q] = g0 + q < g1 ? __ldcg(a.part + (size_t)(g0 + q) * CW + (size_t)c * Wd + k) : 0.0f;
+                float sum = v[0];
+#pragma unroll
+                for (int q = 1; q < kStreamGroup; ++q) sum += v[q];
+                G[grp * Wd + k] = sum;
+            }
+            __syncthreads();
+            // second level: the groups in group order
+            for (int k = tid; k < Wd; k += blockDim.x) {
+                float sum = 0.0f;
+                for (int q0 = 0; q0 < NG; q0 += 16) {
+                    float v[16];
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) v[q] = q0 + q < NG ? G[(q0 + q) * Wd + k] : 0.0f;
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) sum += v[q];
+                }
+                V[k] = sum;
+            }
+            __syncthreads();
+            // the gradient as glm_stream_kernel writes it (likelihood + prior term)
+            const float h = t.step[c];
+            bool fin = true;
+            for (int f = tid; f < F; f += blockDim.x) {
+                const float th = __ldcg(t.wq + (size_t)c * F + f);
+                const bool icpt = a.off && f == 0;
+                const float mu = icpt ? a.icpt_mu : a.coef_mu, sg = icpt ? a.icpt_sigma : a.coef_sigma;
+                const float gv = V[1 + f] - (th - mu) / (sg * sg);
+                t.wg[(size_t)c * F + f] = gv;
+                fin &= (bool)isfinite(gv);
+                if (l < t.L && valid) V[1 + f] = gv;  // kept for the step below
+            }
+            fin = __syncthreads_and(fin) != 0;
+            if (l < t.L) {
+                // lf_step_kernel's intermediate step: kick and drift, or the chain turns invalid
+                if (valid) {
+                    if (!fin) {
+                        valid = false;
+                    } else {
+                        for (int f = tid; f < F; f += blockDim.x) {
+                            const float im = t.inverse_mass[f];
+                            float p = __ldcg(t.wp + (size_t)c * F + f), q = __ldcg(t.wq + (size_t)c * F + f);
+                            p = fmaf(h, V[1 + f], p);
+                            q = fmaf(h * im, p, q);
+                            t.wp[(size_t)c * F + f] = p;
+                            t.wq[(size_t)c * F + f] = q;
+                        }
+                    }
+                }
+                if (tid == 0) t.valid[c] = valid ? 1 : 0;
+            } else if (warp == 0) {
+                // the logjoint at the final position: likelihood + priors, as glm_stream_kernel sums them
+                float prior = 0.0f;
+                for (int f = lane; f < F; f += 32) {
+                    const float th = __ldcg(t.wq + (size_t)c * F + f);
+                    const bool icpt = a.off && f == 0;
+                    const float mu = icpt ? a.icpt_mu : a.coef_mu, sg = icpt ? a.icpt_sigma : a.coef_sigma;
+                    prior += normal_logpdf(mu, sg, th);
+                }
+                prior = warp_sum(prior);
+                if (lane == 0) t.wlj[c] = V[0] + prior;
+            }
+        }
+        if (l < t.L && !stream_grid_sync(t.bar, gen, a.err, &s_ok)) return;
+    }
 }
 
 }  // namespace ut
