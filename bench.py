@@ -288,7 +288,7 @@ def run_b200(args):
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
-    e2e_steps = max(3, args.steps // 2)
+    e2e_steps = max(10, args.steps)
     for _ in range(e2e_steps):
         vals, g = ws.logjoint_gradient(pt)
     e2e_s = _max_over_ranks(time.perf_counter() - t0, dist)
