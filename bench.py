@@ -814,6 +814,32 @@ def run_kernel_only(args):
     ws.close()
 
 
+def run_trajectory_only(args):
+    """Only one-launch HMC trajectories (L = 8) of one chain on the 1000000 x 100
+    design, args.steps of them: the command the trajectory kernel's ncu summary
+    under profiles/ was captured with."""
+    import ctypes
+    import torch
+    from uncertaintea_b200 import _native as nat
+    from uncertaintea_b200.device import DeviceBatchedWorkspace, _stream_handle
+    from uncertaintea_b200.models import BernoulliLogitGLM, logistic_regression_data
+    X, y, _ = logistic_regression_data(1_000_000, N_COEF, seed=4, x_scale=1.0 / np.sqrt(N_COEF))
+    ws = DeviceBatchedWorkspace(BernoulliLogitGLM(N_COEF), 1, args=(X,), constraints={"y": y})
+    qd = torch.from_numpy((0.05 * np.random.default_rng(2).standard_normal((1, N_COEF))).astype(np.float32)).cuda()
+    t, g = ws.logjoint_gradient_device(qd)
+    im, st = torch.ones(N_COEF, device="cuda"), torch.full((1,), 1e-3, device="cuda")
+    outs = [torch.zeros(1, device="cuda") for _ in range(3)] + [torch.zeros(1, dtype=torch.uint8, device="cuda")
+                                                               for _ in range(2)]
+    buf = nat.HmcBuffers(nat.ptr(qd), nat.ptr(g), nat.ptr(t), nat.ptr(im), nat.ptr(st), *[nat.ptr(o) for o in outs],
+                         None, None)
+    for it in range(args.steps):
+        nat.check(nat.load().ut_hmc_iteration(ws.handle, ctypes.byref(buf), 8, 100 + it, 1000.0, _stream_handle()))
+    torch.cuda.synchronize()
+    ws.check()
+    print(json.dumps({"kernel_path": ws.kernel_path(), "trajectories": args.steps, "L": 8}))
+    ws.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -823,6 +849,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--kernel-only", action="store_true")
+    ap.add_argument("--trajectory-only", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true",
                     help="skip the learned-surrogate ChEES comparison (about a minute) in the output line")
     ap.add_argument("--no-samplers", action="store_true",
@@ -830,6 +857,9 @@ def main():
     ap.add_argument("--no-uneven", action="store_true",
                     help="skip the uneven-batch run (512 hierarchical models, about two minutes)")
     args = ap.parse_args()
+    if args.trajectory_only:
+        run_trajectory_only(args)
+        return
     if args.kernel_only:
         run_kernel_only(args)
     elif args.impl == "reference":
