@@ -71,7 +71,31 @@ struct TcGlmParams {
     const int* nact;       // optional: only the first *nact chains are live
     int col_tlo, col_d2, col_buf;  // TMEM columns of Theta_lo, the accumulator, the first H/R buffer
     int xk3d;              // the K-major maps are 3-D (8 features, rows, K-blocks): one copy per tile
+    int yvalid;            // every y is 0 or 1: tiles without padding skip the support check
 };
+
+// The epilogue works in base 2: Theta is scaled by log2(e) before it enters
+// TMEM, so GEMM1 yields h' = log2(e) eta, and exp(-|eta|) = 2^-|h'|,
+// log1p_exp(eta) = ln(2) (max(h', 0) + log2(1 + 2^-|h'|)): the hardware base-2
+// exponential and logarithm apply directly, and the log-likelihood, summed in
+// base-2 units, is multiplied by ln(2) once per chain.
+constexpr float kTcLog2e = 1.4426950408889634f;
+constexpr float kTcLn2 = 0.6931471805599453f;
+__device__ __forceinline__ float tc_ex2(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float tc_lg2(float x) {
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float tc_rcp(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
 
 // Work split of one launch.  Without nact: the (chain tile, split) grid of the
 // plan and partial rows of C chains.  With nact: only ceil(nact / 128) chain
@@ -650,7 +674,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
                 const int f = f0 + j;
-                const float x = (c < p.C && f < p.F) ? __ldg(params + (size_t)c * p.F + f) : 0.0f;
+                const float x = (c < p.C && f < p.F) ? kTcLog2e * __ldg(params + (size_t)c * p.F + f) : 0.0f;
                 hi[j] = tf32_bits(x);
                 lo[j] = tf32_bits(x - __uint_as_float(hi[j]));
             }
@@ -707,6 +731,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             const uint32_t d1 = tmem + lane_off + col_buf + b * 64 + c0;
             float h[kCols];
             tmem_ld_cols<kCols>(d1, h);
+            // a tile with all its observations present and y known to be 0 / 1 needs no checks
+            const bool fast = p.yvalid && (t_begin + i + 1) * kTcObs <= p.N;
             // residuals in runs of 8 columns (few live registers beside the gradient accumulators)
 #pragma unroll
             for (int j8 = 0; j8 < kCols; j8 += 8) {
@@ -718,18 +744,26 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 #pragma unroll
                     for (int jj = 0; jj < 4; ++jj) {
                         const int j = j0 + jj;
-                        const bool live = n0 + j8 + j < p.N;
-                        const float yv = live ? yt[jj] : 0.0f;
-                        const float hv = h[j8 + j];
-                        // log1p_exp(h) = max(h,0) + log1p(exp(-|h|)); logistic(h) from the same exp (math.jl:202-224)
-                        const float ex = __expf(-fabsf(hv));
+                        const float hv = h[j8 + j];   // log2(e) eta
+                        // log1p_exp(eta) = max(eta,0) + log1p(exp(-|eta|)); logistic(eta) from the same exp
+                        // (math.jl:202-224), in base 2
+                        const float ex = tc_ex2(-fabsf(hv));
                         const float onepe = 1.0f + ex;
-                        const float lpe = fmaxf(hv, 0.0f) + __logf(onepe);
-                        const float inv = __fdividef(1.0f, onepe);
+                        const float lpe = fmaxf(hv, 0.0f) + tc_lg2(onepe);
+                        const float inv = tc_rcp(onepe);
                         const float sig = hv >= 0.0f ? inv : ex * inv;
-                        const bool sup = (yv == 0.0f) | (yv == 1.0f);
-                        ll += live ? (sup ? yv * hv - lpe : -INFINITY) : 0.0f;
-                        const float r = live ? yv - sig : 0.0f;
+                        float r;
+                        if (fast) {
+                            const float yv = yt[jj];
+                            ll += fmaf(yv, hv, -lpe);
+                            r = yv - sig;
+                        } else {
+                            const bool live = n0 + j8 + j < p.N;
+                            const float yv = live ? yt[jj] : 0.0f;
+                            const bool sup = (yv == 0.0f) | (yv == 1.0f);
+                            ll += live ? (sup ? fmaf(yv, hv, -lpe) : -INFINITY) : 0.0f;
+                            r = live ? yv - sig : 0.0f;
+                        }
                         const uint32_t hb = tf32_bits(r);
                         rh[j] = hb;
                         rl[j] = tf32_bits(r - __uint_as_float(hb));
@@ -760,8 +794,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         asm volatile("bar.sync 1, %0;" ::"n"(kTcEpiThreads));
         if (ok) {
             if (e == 0 && c < p.C)
-                p.part_ll[(size_t)split * sp.Cl + c] = ((ll_part[c_local] + ll_part[kTcChains + c_local]) +
-                                                      ll_part[2 * kTcChains + c_local]) + ll_part[3 * kTcChains + c_local];
+                p.part_ll[(size_t)split * sp.Cl + c] =
+                    kTcLn2 * (((ll_part[c_local] + ll_part[kTcChains + c_local]) + ll_part[2 * kTcChains + c_local]) +
+                              ll_part[3 * kTcChains + c_local]);
             if (p.want_grad && c < p.C) {
                 float* dst = p.part_g + ((size_t)split * sp.Cl + c) * p.F;
 #pragma unroll
@@ -797,6 +832,7 @@ struct TcGlmPlan {
     float icpt_mu = 0, icpt_sigma = 1, coef_mu = 0, coef_sigma = 1;
     CUtensorMap map_xk_hi, map_xk_lo, map_xm_hi, map_xm_lo;
     bool xk3d = false;   // the K-major maps are 3-D (tc_make_map_kblocks)
+    bool yvalid = false; // every y is 0 or 1
     size_t smem = 0;
     int nbuf = 2;        // H/R TMEM buffers
     int groups = 1;      // epilogue warp groups (2 needs 3 buffers)
@@ -933,6 +969,12 @@ inline int tc_glm_setup(TcGlmPlan& t, const float* d_Xa, const float* d_y, int N
         cudaMemset(yp, 0, ybytes);
         cudaMemcpy(yp, d_y, (size_t)N * sizeof(float), cudaMemcpyDeviceToDevice);
         t.y = yp;
+        std::vector<float> hy((size_t)N);
+        if (cudaMemcpy(hy.data(), d_y, (size_t)N * sizeof(float), cudaMemcpyDeviceToHost) == cudaSuccess) {
+            bool ok = true;
+            for (float v : hy) ok = ok && (v == 0.0f || v == 1.0f);
+            t.yvalid = ok;
+        }
     }
     const long long total = (long long)N * Fp;
     tc_split_x_kernel<<<(unsigned)((total + 255) / 256), 256>>>(d_Xa, t.xhi, t.xlo, N, F, Fp);
@@ -1039,6 +1081,7 @@ inline cudaError_t tc_glm_launch(const TcGlmPlan& t, const float* params, float*
     tc_columns(t.F, t.Fp, t.wide, cols);
     p.col_tlo = cols[0]; p.col_d2 = cols[1]; p.col_buf = cols[2];
     p.xk3d = t.xk3d ? 1 : 0;
+    p.yvalid = t.yvalid ? 1 : 0;
     dim3 grid(t.ctiles, t.S);
     if (t.nbuf == 3 && t.groups == 2)
         tc_glm_kernel<3, 2><<<grid, kTcThreads, t.smem, st>>>(t.map_xk_hi, t.map_xk_lo, t.map_xm_hi, t.map_xm_lo,
