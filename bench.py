@@ -716,7 +716,8 @@ def surrogate_comparison(num_chains=4096, num_warmup=500, num_samples=500):
     on 2^20 (theta, gradient) pairs of the last 256 warmup iterations.
     Variants:
       fixed16            -- 16 leapfrog steps every iteration (the trajectory
-                            budget of the configuration), step size adapted;
+                            budget of the configuration), step size adapted,
+                            then Halton-jittered per sampling iteration;
       adapted_reference  -- trajectory length adapted with the reference's
                             estimator (16 initial steps);
       adapted_forward    -- adapted with the forward endpoint velocity (an

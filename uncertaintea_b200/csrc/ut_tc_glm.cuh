@@ -892,7 +892,7 @@ inline bool tc_make_map_kblocks(CUtensorMap* m, float* base, int rows, int Fp, i
     return r == CUDA_SUCCESS;
 }
 
-__global__ void tc_split_x_kernel(const float* __restrict__ Xa, float* __restrict__ hi, float* __restrict__ lo,
+static __global__ void tc_split_x_kernel(const float* __restrict__ Xa, float* __restrict__ hi, float* __restrict__ lo,
                                   long long N, int F, int Fp) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N * Fp) return;
@@ -1032,7 +1032,7 @@ inline int tc_glm_setup(TcGlmPlan& t, const float* d_Xa, const float* d_y, int N
 
 // Prior terms + deterministic fold of the split partials, one 128-thread CTA
 // per chain (thread = feature; F <= 128 on this path), fixed summation order.
-__global__ void __launch_bounds__(128) tc_reduce_kernel(const float* params, float* totals, float* grads,
+static __global__ void __launch_bounds__(128) tc_reduce_kernel(const float* params, float* totals, float* grads,
                                                         TcGlmParams p, int off, float icpt_mu, float icpt_sigma,
                                                         float coef_mu, float coef_sigma) {
     const int c = blockIdx.x;
