@@ -151,10 +151,12 @@ def cpu_reference_rate(model, X, y, params, budget_s=12.0, threads=0):
     return done / el, cores, f"{done} chain-gradients of the full N=100000 x D=100 model in {el:.1f} s"
 
 
-def _emit(name, result):
-    """One sub-result of the run as its own JSON line (before the headline line)."""
+def _emit(name, result, t0=None):
+    """One sub-result of the run as its own JSON line (before the headline
+    line), with the wall seconds the section took since t0."""
     if result is not None:
-        print(json.dumps({"sub": name, **result}), flush=True)
+        took = {"section_s": round(time.perf_counter() - t0, 1)} if t0 is not None else {}
+        print(json.dumps({"sub": name, **result, **took}), flush=True)
 
 
 def _profiled_traffic():
@@ -317,17 +319,20 @@ def run_b200(args):
         # headline line comes last
         _emit("fp64_error", fp64)
         if world == 1:
-            _emit("hbm_sweep", hbm_sweep())
-            _emit("hbm_sweep_large", hbm_sweep_large())
-            _emit("hbm_trajectory", hbm_trajectory())
+            for name, fn in (("hbm_sweep", hbm_sweep), ("hbm_sweep_large", hbm_sweep_large),
+                             ("hbm_trajectory", hbm_trajectory)):
+                t0 = time.perf_counter()
+                _emit(name, fn(), t0)
             samplers = None
             if not args.no_samplers:
                 samplers = {}
                 for name, fn in (("glm1000x10_hmc", sampler_glm_hmc), ("hier64x20_nuts", sampler_hier_nuts),
                                  ("glm100000x100_nuts", glm_large_nuts), ("glm100000x100_meads", glm_large_meads)):
+                    t0 = time.perf_counter()
                     samplers[name] = fn()
-                    _emit("samplers." + name, samplers[name])
+                    _emit("samplers." + name, samplers[name], t0)
             if not args.no_surrogate:
+                t0 = time.perf_counter()
                 sur = surrogate_comparison()
                 if samplers is not None:
                     # the metric's own comparison: surrogate-driven trajectories vs plain NUTS on the same model
@@ -335,9 +340,10 @@ def run_b200(args):
                     sur["plain_nuts"] = {k: nuts[k] for k in ("min_ess_per_s", "min_ess", "max_rank_rhat", "sampling_s")}
                     for v in ("fixed16", "adapted_reference", "adapted_forward"):
                         sur[v]["ratio_vs_plain_nuts"] = sur[v]["surrogate"]["min_ess_per_s"] / nuts["min_ess_per_s"]
-                _emit("surrogate_chees", sur)
+                _emit("surrogate_chees", sur, t0)
             if not args.no_uneven:
-                _emit("uneven_batch", uneven_batch())
+                t0 = time.perf_counter()
+                _emit("uneven_batch", uneven_batch(), t0)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -556,14 +562,37 @@ def hbm_sweep(chain_counts=(1, 4, 8, 16), steps=20, warmup=5):
             "rows": out, "yardsticks": yard}
 
 
+def _device_diagnostics(ch, S=None, chunk=None):
+    """Rank-normalised split R-hat, plain split R-hat and bulk ESS per
+    parameter of the first S draws of ch's unconstrained draws, computed on the
+    device a few parameters at a time with the reference's estimators
+    (uncertaintea_b200.multi: rank_split_rhat, split_rhat, split_ess; they
+    agree with the host diagnostics to 1e-9).  The host estimators take
+    minutes on 4096 chains x 1000 draws x 100 parameters."""
+    import torch
+    from uncertaintea_b200.multi import rank_split_rhat, split_ess, split_rhat
+    d = ch.unconstrained                        # (C, S_total, P)
+    C, S_tot, P = d.shape
+    S = S_tot if S is None else S
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    if chunk is None:   # about 1.6 GB of float64 draws per chunk
+        chunk = max(1, min(16, int(2e8 // (S * C))))
+    r_rank, r_split, e = np.empty(P), np.empty(P), np.empty(P)
+    for p0 in range(0, P, chunk):
+        p1 = min(P, p0 + chunk)
+        x = torch.from_numpy(np.ascontiguousarray(d[:, :S, p0:p1].transpose(1, 0, 2))).to(dev)   # (S, C, p)
+        r_rank[p0:p1] = torch.nan_to_num(rank_split_rhat(x), nan=float("inf")).cpu().numpy()
+        r_split[p0:p1] = torch.nan_to_num(split_rhat(x), nan=float("inf")).cpu().numpy()
+        e[p0:p1] = torch.nan_to_num(split_ess(x), nan=float("inf")).cpu().numpy()
+        del x
+    return r_rank, r_split, e
+
+
 def _chain_summary(ch, cfg, extra=None):
     """Min bulk ESS/s and both R-hats of a sampler run.  The gate is the
     reference's: rank-normalised split R-hat < 1.01 (diagnostics.jl:607-612,
     docs/benchmarks.md:8-13); the plain split R-hat is reported beside it."""
-    from uncertaintea_b200 import ess, rhat
-    e = ess(ch, space="unconstrained")
-    r_rank = rhat(ch, space="unconstrained", method="rank")
-    r_split = rhat(ch, space="unconstrained")
+    r_rank, r_split, e = _device_diagnostics(ch)
     total_s = ch.warmup_seconds + ch.sampling_seconds
     out = {"min_ess_per_s": float(np.min(e) / ch.sampling_seconds), "min_ess": float(np.min(e)),
            "max_rank_rhat": float(np.max(r_rank)), "max_split_rhat": float(np.max(r_split)),
@@ -582,19 +611,13 @@ def _gate_prefixes(ch, lengths):
     multi.rank_split_rhat / multi.split_ess), and min-ESS/s over the device
     time of those S sampling iterations (a sampling iteration's cost does not
     depend on its index, so that time is the run's times S / S_total)."""
-    import torch
-    from uncertaintea_b200.multi import rank_split_rhat, split_ess
-    d = ch.unconstrained                        # (C, S_total, P)
-    C, S_tot, P = d.shape
+    S_tot = ch.unconstrained.shape[1]
     rows = []
     for S in lengths:
         if S > S_tot:
             break
-        r_max, e_min = 0.0, float("inf")
-        for p in range(P):
-            x = torch.from_numpy(np.ascontiguousarray(d[:, :S, p].T)).cuda()[:, :, None]   # (S, C, 1)
-            r_max = max(r_max, float(torch.nan_to_num(rank_split_rhat(x), nan=float("inf"))[0]))
-            e_min = min(e_min, float(torch.nan_to_num(split_ess(x), nan=float("inf"))[0]))
+        r_rank, _, e = _device_diagnostics(ch, S)
+        r_max, e_min = float(np.max(r_rank)), float(np.min(e))
         t = ch.sampling_seconds * S / S_tot
         rows.append({"draws": S, "max_rank_rhat": r_max, "min_ess": e_min, "min_ess_per_s": e_min / t,
                      "gate_rank_rhat_lt_1.01": bool(r_max < 1.01)})
@@ -684,12 +707,12 @@ def _surrogate_pair(model, X, y, **kw):
     min ESS per sampling second (and per total second: warmup + surrogate
     training + sampling), rank R-hat, mean trajectory steps, the ratio, and
     the largest difference of posterior means in posterior SDs."""
-    from uncertaintea_b200 import batched_chees, batched_chees_surrogate, ess, rhat
+    from uncertaintea_b200 import batched_chees, batched_chees_surrogate
     runs = {"plain": batched_chees(model, (X,), {"y": y}, **kw),
             "surrogate": batched_chees_surrogate(model, (X,), {"y": y}, **kw)}
     out = {}
     for name, ch in runs.items():
-        e, r = ess(ch, space="unconstrained"), rhat(ch, space="unconstrained", method="rank")
+        r, _, e = _device_diagnostics(ch)
         total_s = ch.warmup_seconds + ch.sampling_seconds
         out[name] = {"min_ess_per_s": float(np.min(e) / ch.sampling_seconds), "min_ess": float(np.min(e)),
                      "min_ess_per_total_s": float(np.min(e) / total_s), "max_rank_rhat": float(np.max(r)),

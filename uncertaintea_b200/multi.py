@@ -141,6 +141,19 @@ def _rank_normal_cols(split):
     return z.reshape(h, M, P).permute(1, 0, 2)
 
 
+def split_rhat(draws):
+    """Plain split R-hat per parameter of draws (S, C, P) -- a torch tensor on
+    any device (diagnostics.jl:514-540 on each parameter's split chains)."""
+    torch = _torch()
+    x = draws.double()
+    S, C, P = x.shape
+    h = S // 2
+    if h < 2:
+        return torch.full((P,), float("nan"), dtype=torch.float64, device=x.device)
+    split = torch.stack([x[:h], x[h:2 * h]], dim=2).reshape(h, 2 * C, P).permute(1, 0, 2)
+    return _split_rhat_cols(split)
+
+
 def rank_split_rhat(draws):
     """Rank-normalised split R-hat per parameter of draws (S, C, P) -- a torch
     tensor on any device: max of the bulk R-hat of the rank-normalised split
