@@ -72,6 +72,8 @@ struct TcGlmParams {
     int col_tlo, col_d2, col_buf;  // TMEM columns of Theta_lo, the accumulator, the first H/R buffer
     int xk3d;              // the K-major maps are 3-D (8 features, rows, K-blocks): one copy per tile
     int yvalid;            // every y is 0 or 1: tiles without padding skip the support check
+    int xkpair;            // paired GEMM1: the K-major view is [K-block][hi | lo][rows] (one 4-D copy),
+                           // Theta_hi meets X_hi and X_lo in one N = 64 MMA per K-block
 };
 
 // The epilogue works in base 2: Theta is scaled by log2(e) before it enters
@@ -283,6 +285,16 @@ __device__ __forceinline__ void tma_load_3d_warp(void* dst, const CUtensorMap* m
         : "memory");
 }
 
+__device__ __forceinline__ void tma_load_4d_warp(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y,
+                                                 int z, int w) {
+    asm volatile(
+        "{\n\t.reg .pred e;\n\t.reg .b32 r;\n\t"
+        "elect.sync r|e, 0xffffffff;\n\t"
+        "@e cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], [%2];\n\t}"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z), "r"(w)
+        : "memory");
+}
+
 __device__ __forceinline__ void bulk_load_warp(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
     asm volatile(
         "{\n\t.reg .pred e;\n\t.reg .b32 r;\n\t"
@@ -360,9 +372,12 @@ __host__ __device__ constexpr uint32_t idesc_tf32(int M, int N, int b_mn_major) 
 // Fp = features rounded up to 16 (GEMM2's N), both <= 128:
 //   Theta_hi [0, KC)   Theta_lo [KC, 2KC)   D2 = G^T [2KC, 2KC + Fp)
 //   buffer b (0 .. nbuf-1): H^T / R_hi [2KC + Fp + 64b, +32)   R_lo [.. + 32, +32)
+//   (paired GEMM1: H^T is the sum of the buffer's two halves, Theta_hi X_hi in the
+//   first, Theta_hi X_lo + Theta_lo X_hi in the second; R_hi / R_lo replace them)
 // nbuf = min(3, (512 - 2KC - Fp) / 64): 3 for 100 features (208 + 112 + 192).
 // Shared memory per pipeline stage (3 stages), Fp features x 32 observations:
 //   XK_hi, XK_lo : K-major SWIZZLE_32B, Fp/8 blocks of [32 rows][32 B]     (GEMM1 B)
+//                  (paired GEMM1: [K-block][XK_hi 32 rows, XK_lo 32 rows], 2 KB a K-block)
 //   XM_hi, XM_lo : MN-major SWIZZLE_128B_BASE32B, Fp/32 atoms of [32 rows][128 B] (GEMM2 B)
 // (TF32 operands that are MN-major must use the 128B_BASE32B layout, which no
 // K-major layout shares, so each X tile is loaded twice, once per view.)
@@ -451,6 +466,36 @@ __device__ __forceinline__ void tmem_ld_cols(uint32_t taddr, float (&v)[kCols]) 
     else tmem_ld16(taddr, v);
 }
 
+// The sum of two kCols-column TMEM ranges (both loads in flight, one wait).
+template <int kCols>
+__device__ __forceinline__ void tmem_ld_cols_sum(uint32_t ta, uint32_t tb, float (&v)[kCols]) {
+    uint32_t ra[kCols], rb[kCols];
+    if constexpr (kCols == 8) {
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                     : "=r"(ra[0]), "=r"(ra[1]), "=r"(ra[2]), "=r"(ra[3]), "=r"(ra[4]), "=r"(ra[5]), "=r"(ra[6]),
+                       "=r"(ra[7])
+                     : "r"(ta));
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                     : "=r"(rb[0]), "=r"(rb[1]), "=r"(rb[2]), "=r"(rb[3]), "=r"(rb[4]), "=r"(rb[5]), "=r"(rb[6]),
+                       "=r"(rb[7])
+                     : "r"(tb));
+    } else {
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                     : "=r"(ra[0]), "=r"(ra[1]), "=r"(ra[2]), "=r"(ra[3]), "=r"(ra[4]), "=r"(ra[5]), "=r"(ra[6]),
+                       "=r"(ra[7]), "=r"(ra[8]), "=r"(ra[9]), "=r"(ra[10]), "=r"(ra[11]), "=r"(ra[12]), "=r"(ra[13]),
+                       "=r"(ra[14]), "=r"(ra[15])
+                     : "r"(ta));
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                     : "=r"(rb[0]), "=r"(rb[1]), "=r"(rb[2]), "=r"(rb[3]), "=r"(rb[4]), "=r"(rb[5]), "=r"(rb[6]),
+                       "=r"(rb[7]), "=r"(rb[8]), "=r"(rb[9]), "=r"(rb[10]), "=r"(rb[11]), "=r"(rb[12]), "=r"(rb[13]),
+                       "=r"(rb[14]), "=r"(rb[15])
+                     : "r"(tb));
+    }
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < kCols; ++i) v[i] = __uint_as_float(ra[i]) + __uint_as_float(rb[i]);
+}
+
 // NBUF H/R TMEM buffers; G epilogue warp groups.  G = 1: all 16 epilogue
 // warps work on every tile, 8 observation columns each.  G = 2: two groups of
 // 8 warps take alternate tiles, 16 columns each, so two tiles' epilogues
@@ -530,7 +575,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             uint8_t* st = smem + s * stage_bytes;
             mbar_expect_tx_warp(bar_xfull + s, 2 * KB1 * (kTcObs * 32) + 2 * xm_bytes + kTcObs * 4);
             const int n0 = (t_begin + i) * kTcObs;
-            if (p.xk3d) {
+            if (p.xkpair) {
+                // [K-block][hi, lo][32 rows][8 features] in one copy
+                tma_load_4d_warp(st, &map_xk_hi, bar_xfull + s, 0, n0, 0, 0);
+            } else if (p.xk3d) {
                 // [K-block][32 rows][8 features] in one copy per view
                 tma_load_3d_warp(st, &map_xk_hi, bar_xfull + s, 0, n0, 0);
                 tma_load_3d_warp(st + xk_bytes, &map_xk_lo, bar_xfull + s, 0, n0, 0);
@@ -551,6 +599,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         // ---------------- MMA issuer (the whole warp; an elected lane issues) ----------------
         if (ntiles > 0) {
             const uint32_t id1 = idesc_tf32(kTcChains, kTcObs, 0);
+            const uint32_t id1p = idesc_tf32(kTcChains, 2 * kTcObs, 0);
             const uint32_t id2 = idesc_tf32(kTcChains, Fp, 1);
             bool ok = wwait(bar_theta, 0);
             tc_fence_after();
@@ -599,8 +648,23 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 tc_fence_after();
                 const uint32_t xk = smem_u32(smem + s * stage_bytes);
                 const uint32_t d1 = tmem + col_buf + b * 64;
-                uint64_t bh = sdesc_sw32(xk, 16, 256), bl = sdesc_sw32(xk + xk_bytes, 16, 256);
                 uint32_t ahi = tmem + col_thi, alo = tmem + col_tlo;
+                if (p.xkpair) {
+                    // per K-block (2 KB: 32 X_hi rows, then 32 X_lo rows): Theta_hi x [X_hi | X_lo]
+                    // into columns [0, 64) in one N = 64 MMA -- an N = 32 MMA costs as much -- and
+                    // Theta_lo x X_hi into [32, 64); H^T = columns [0, 32) + [32, 64)
+                    uint64_t bp = sdesc_sw32(xk, 16, 256);
+                    for (int kb = 0; kb < KB1; ++kb) {
+                        mma_ts_warp(d1, ahi, bp, id1p, kb > 0 ? 1u : 0u);
+                        mma_ts_warp(d1 + 32, alo, bp, id1, 1u);
+                        bp += 128;
+                        ahi += 8;
+                        alo += 8;
+                    }
+                    mma_commit_warp(bar_d1full + b);
+                    return true;
+                }
+                uint64_t bh = sdesc_sw32(xk, 16, 256), bl = sdesc_sw32(xk + xk_bytes, 16, 256);
                 mma_ts_warp(d1, ahi, bh, id1, 0u);
                 mma_ts_warp(d1, ahi, bl, id1, 1u);
                 mma_ts_warp(d1, alo, bh, id1, 1u);
@@ -730,7 +794,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             const float* ys = reinterpret_cast<const float*>(smem + s * stage_bytes + 2 * xk_bytes + 2 * xm_bytes) + c0;
             const uint32_t d1 = tmem + lane_off + col_buf + b * 64 + c0;
             float h[kCols];
-            tmem_ld_cols<kCols>(d1, h);
+            if (p.xkpair) tmem_ld_cols_sum<kCols>(d1, d1 + 32, h);
+            else tmem_ld_cols<kCols>(d1, h);
             // a tile with all its observations present and y known to be 0 / 1 needs no checks
             const bool fast = p.yvalid && (t_begin + i + 1) * kTcObs <= p.N;
             // residuals in runs of 8 columns (few live registers beside the gradient accumulators)
@@ -832,6 +897,7 @@ struct TcGlmPlan {
     float icpt_mu = 0, icpt_sigma = 1, coef_mu = 0, coef_sigma = 1;
     CUtensorMap map_xk_hi, map_xk_lo, map_xm_hi, map_xm_lo;
     bool xk3d = false;   // the K-major maps are 3-D (tc_make_map_kblocks)
+    bool xkpair = false; // paired GEMM1: map_xk_hi is the 4-D hi/lo map (tc_make_map_kblocks_pair)
     bool yvalid = false; // every y is 0 or 1
     size_t smem = 0;
     int nbuf = 2;        // H/R TMEM buffers
@@ -887,6 +953,24 @@ inline bool tc_make_map_kblocks(CUtensorMap* m, float* base, int rows, int Fp, i
     cuuint32_t box[3] = {8, (cuuint32_t)box_rows, (cuuint32_t)kblocks};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+// The paired K-major view as a 4-D map over X_hi and X_lo in one allocation
+// (X_lo = X_hi + hl_stride bytes): (8 features, rows, hi/lo, K-blocks), so one
+// box of (8, 32 rows, 2, kblocks) lands as [K-block][hi, lo][row][8 features]:
+// per K-block 32 X_hi rows and then 32 X_lo rows, one N = 64 B operand.
+inline bool tc_make_map_kblocks_pair(CUtensorMap* m, float* base, int rows, int Fp, int kblocks, int box_rows,
+                                     size_t hl_stride) {
+    PFN_encodeTiled enc = tc_encode_fn();
+    if (!enc) return false;
+    cuuint64_t dims[4] = {8, (cuuint64_t)rows, 2, (cuuint64_t)kblocks};
+    cuuint64_t strides[3] = {(cuuint64_t)Fp * sizeof(float), (cuuint64_t)hl_stride, 8 * sizeof(float)};
+    cuuint32_t box[4] = {8, (cuuint32_t)box_rows, 2, (cuuint32_t)kblocks};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
@@ -952,7 +1036,8 @@ inline int tc_glm_setup(TcGlmPlan& t, const float* d_Xa, const float* d_y, int N
         return true;
     };
     const size_t xbytes = (size_t)N * Fp * sizeof(float);
-    if (!alloc((void**)&t.xhi, xbytes) || !alloc((void**)&t.xlo, xbytes) ||
+    // X_hi and X_lo in one allocation, X_lo right after X_hi (the paired map spans both)
+    if (!alloc((void**)&t.xhi, 2 * xbytes) || !(t.xlo = t.xhi + (size_t)N * Fp) ||
         !alloc((void**)&t.part_ll, part_rows * sizeof(float)) ||
         !alloc((void**)&t.part_g, part_rows * F * sizeof(float)) || !alloc((void**)&t.err, sizeof(int))) {
         tc_err_string() = "cudaMalloc failed";
@@ -999,6 +1084,14 @@ inline int tc_glm_setup(TcGlmPlan& t, const float* d_Xa, const float* d_y, int N
             t.map_xk_hi = k3h;
             t.map_xk_lo = k3l;
             t.xk3d = true;
+        }
+        // paired GEMM1 (UT_TC_PAIRED=0 keeps the three N = 32 MMAs per K-block: a tuning knob)
+        const char* ep = getenv("UT_TC_PAIRED");
+        CUtensorMap kp;
+        if (t.xk3d && !(ep && ep[0] == '0') &&
+            tc_make_map_kblocks_pair(&kp, t.xhi, N, Fp, tc_kblocks_used(F), kTcObs, xbytes)) {
+            t.map_xk_hi = kp;
+            t.xkpair = true;
         }
     }
     // H/R buffers: as many as TMEM holds (tc_nbuf); UT_TC_BUFFERS=2 keeps two (a tuning knob)
@@ -1081,6 +1174,7 @@ inline cudaError_t tc_glm_launch(const TcGlmPlan& t, const float* params, float*
     tc_columns(t.F, t.Fp, t.wide, cols);
     p.col_tlo = cols[0]; p.col_d2 = cols[1]; p.col_buf = cols[2];
     p.xk3d = t.xk3d ? 1 : 0;
+    p.xkpair = t.xkpair ? 1 : 0;
     p.yvalid = t.yvalid ? 1 : 0;
     dim3 grid(t.ctiles, t.S);
     if (t.nbuf == 3 && t.groups == 2)
