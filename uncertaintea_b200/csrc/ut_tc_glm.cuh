@@ -1037,8 +1037,12 @@ inline int tc_glm_setup(TcGlmPlan& t, const float* d_Xa, const float* d_y, int N
     };
     const size_t xbytes = (size_t)N * Fp * sizeof(float);
     // X_hi and X_lo in one allocation, X_lo right after X_hi (the paired map spans both)
-    if (!alloc((void**)&t.xhi, 2 * xbytes) || !(t.xlo = t.xhi + (size_t)N * Fp) ||
-        !alloc((void**)&t.part_ll, part_rows * sizeof(float)) ||
+    if (!alloc((void**)&t.xhi, 2 * xbytes)) {
+        tc_err_string() = "cudaMalloc failed";
+        return 1;
+    }
+    t.xlo = t.xhi + (size_t)N * Fp;
+    if (!alloc((void**)&t.part_ll, part_rows * sizeof(float)) ||
         !alloc((void**)&t.part_g, part_rows * F * sizeof(float)) || !alloc((void**)&t.err, sizeof(int))) {
         tc_err_string() = "cudaMalloc failed";
         return 1;
