@@ -386,6 +386,24 @@ def test_rank_rhat_ties_follow_reference_order():
         assert dev[p] == pytest.approx(ref, rel=1e-12)
 
 
+def test_fixed_step_chees_jitters_the_step_size_after_warmup():
+    """With fixed_leapfrog_steps the Halton jitter moves from the step count to
+    the step size, from the first sampling iteration on; the reference's rule
+    (no fixed count) is unchanged."""
+    for it in (1, 2, 3, 50, 51, 52, 77):
+        j = inf._chees_jitter_value(1.0, it)
+        eps, L, jit = inf._chees_iteration_step_and_steps(0.5, 3.0, 1.0, it, 50, 16)
+        assert L == 16 and jit == j
+        assert eps == (0.5 * j if it > 50 else 0.5)
+        eps, L, _ = inf._chees_iteration_step_and_steps(0.5, 3.0, 1.0, it, 50)
+        assert eps == 0.5 and L == inf._chees_leapfrog_steps_from_jitter(j, 3.0, 0.5)
+    # jitter_amount = 0: no jitter anywhere
+    assert inf._chees_iteration_step_and_steps(0.5, 3.0, 0.0, 77, 50, 16)[:2] == (0.5, 16)
+    # the sampling-phase step sizes cover (0, eps): no fixed trajectory length repeats
+    eps = [inf._chees_iteration_step_and_steps(0.5, 3.0, 1.0, it, 0, 16)[0] for it in range(1, 65)]
+    assert len(set(eps)) == 64 and 0.0 < min(eps) and max(eps) < 0.5
+
+
 def test_device_diagnostics_match_the_host_estimators():
     """The torch estimators the bench runs on the device (plain split R-hat,
     rank-normalised split R-hat, bulk ESS) agree with the host diagnostics,

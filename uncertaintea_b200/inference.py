@@ -448,6 +448,20 @@ def _chees_leapfrog_steps_from_jitter(jitter_value: float, trajectory_length: fl
     return max(1, steps)
 
 
+def _chees_iteration_step_and_steps(step_size, trajectory_length, jitter_amount, iteration, num_warmup,
+                                    fixed_leapfrog_steps=None):
+    """The step size and leapfrog step count of ChEES iteration `iteration`
+    (1-based).  The reference's rule jitters the step count
+    (api_batched_chees.jl:51-56).  With a fixed step count the same Halton
+    jitter scales the step size instead, from the first sampling iteration on."""
+    jitter = _chees_jitter_value(jitter_amount, iteration)
+    L = _chees_leapfrog_steps_from_jitter(jitter, trajectory_length, step_size)
+    if fixed_leapfrog_steps is None:
+        return float(step_size), L, jitter
+    eps = step_size * jitter if iteration > num_warmup else step_size
+    return float(eps), int(fixed_leapfrog_steps), jitter
+
+
 def _chees_jittered_leapfrog_steps(trajectory_length, step_size, jitter_amount, iteration) -> int:
     return _chees_leapfrog_steps_from_jitter(_chees_jitter_value(jitter_amount, iteration), trajectory_length,
                                              step_size)
@@ -1130,13 +1144,8 @@ def batched_chees(model, args=(), constraints=None, *, num_chains, num_samples, 
     t0 = time.perf_counter()
     t_sample = None
     for it in range(1, total + 1):
-        eps = driver.step_size
-        jitter = _chees_jitter_value(jitter_amount, it)
-        L = _chees_leapfrog_steps_from_jitter(jitter, traj.trajectory_length, eps)
-        if fixed_leapfrog_steps is not None:
-            L = int(fixed_leapfrog_steps)
-            if it > num_warmup:
-                eps = eps * jitter   # the fixed step count's jitter is on the step size
+        eps, L, jitter = _chees_iteration_step_and_steps(driver.step_size, traj.trajectory_length, jitter_amount,
+                                                         it, num_warmup, fixed_leapfrog_steps)
         run.set_mass_and_step(driver.inverse_mass_matrix, eps)
         if it == num_warmup + 1:
             torch.cuda.synchronize()
