@@ -12,7 +12,9 @@ Tolerances (stated per test):
   and per chain max_p |g - g64| <= 1e-5 max_p |g64|.
 * HMC / NUTS iterations vs the FP32 oracle under identical Philox streams:
   the same accept / tree decisions for >= 98% of chains, and states of the
-  chains with identical decisions within rtol 1e-3, atol 1e-4.
+  chains with identical decisions within rtol 1e-3, atol 1e-4.  An HMC accept
+  decision that differs must be a near-tie: the chain's accept uniform lies
+  between the two sides' accept probabilities.
 """
 import ctypes
 
@@ -432,6 +434,21 @@ def test_stream_trajectory_in_one_launch_is_the_step_path(lib, monkeypatch, C, N
     ws.close()
 
 
+def _assert_accept_flips_are_near_ties(gpu, ref, coord):
+    """Every chain whose accept decision differs between the device and the
+    oracle is a near-tie: its accept uniform (Philox stream 4, draw 0 of the
+    chain at this coordinate, the same on both sides; hmc_kernels.jl:553-577)
+    lies between the two sides' accept probabilities, which differ only by the
+    FP32 roundoff of the energy error.  A flip with the uniform elsewhere would
+    mean the two sides drew different randomness or computed different
+    energies."""
+    live = (gpu["divergent"] == 0) & (ref["divergent"] == 0)
+    for c in np.flatnonzero((gpu["accepted"] != ref["accepted"]) & live):
+        u = float(oracle.rand_uniform(int(c), coord, 4, 0, 1)[0])
+        lo, hi = sorted((float(gpu["accept_prob"][c]), float(ref["accept_prob"][c])))
+        assert lo - 1e-6 <= u <= hi + 1e-6, (int(c), u, lo, hi)
+
+
 @pytest.mark.parametrize("case", ["glm_c1", "glm_tiled", "hier", "gauss"])
 def test_hmc_iteration_vs_oracle(lib, case):
     """One HMC iteration from near-posterior states with stable step sizes:
@@ -472,6 +489,7 @@ def test_hmc_iteration_vs_oracle(lib, case):
     ref = om.hmc_iteration(qo, go, to, im, steps, L, 12345, want_proposal=True)
     same = (gpu["accepted"] == ref["accepted"]) & (gpu["divergent"] == ref["divergent"])
     assert same.mean() >= 0.98
+    _assert_accept_flips_are_near_ties(gpu, ref, 12345)
     assert ref["divergent"].mean() <= 0.02
     ok = same & (ref["divergent"] == 0)
     np.testing.assert_allclose(gpu["proposal"][ok], ref["proposal"][ok], rtol=1e-3, atol=1e-4)
