@@ -2,6 +2,7 @@
 reference's unit tests), warmup schedule, dual averaging, mass weights,
 diagnostics."""
 import math
+import os
 
 import numpy as np
 import pytest
@@ -422,6 +423,37 @@ def test_device_diagnostics_match_the_host_estimators():
         np.testing.assert_allclose(split_rhat(x).numpy(), dg.rhat(Fake), rtol=1e-12)
         np.testing.assert_allclose(rank_split_rhat(x).numpy(), dg.rhat(Fake, method="rank"), rtol=1e-12)
         np.testing.assert_allclose(split_ess(x).numpy(), dg.ess(Fake), rtol=1e-9)
+
+
+def test_bench_diagnostics_and_gate_prefixes_match_the_host_estimators():
+    """bench.py's sampler rows compute rank R-hat, split R-hat and bulk ESS a
+    few parameters at a time with the torch estimators (on the device when
+    there is one); chunking and prefixes give the host diagnostics' values."""
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    rng = np.random.default_rng(3)
+    d = np.cumsum(rng.standard_normal((6, 300, 37)), axis=1) * 0.05 + rng.standard_normal((6, 300, 37))
+
+    class Fake:
+        constrained = d
+        unconstrained = d
+        sampling_seconds = 2.0
+
+    rr, rs, e = bench._device_diagnostics(Fake, chunk=5)
+    np.testing.assert_allclose(rr, dg.rhat(Fake, "unconstrained", method="rank"), rtol=1e-12)
+    np.testing.assert_allclose(rs, dg.rhat(Fake, "unconstrained"), rtol=1e-12)
+    np.testing.assert_allclose(e, dg.ess(Fake, "unconstrained"), rtol=1e-9)
+
+    class Half:
+        constrained = d[:, :151]
+        unconstrained = d[:, :151]
+
+    rows = bench._gate_prefixes(Fake, [151, 300, 400])
+    assert [r["draws"] for r in rows] == [151, 300]
+    assert rows[0]["max_rank_rhat"] == pytest.approx(np.max(dg.rhat(Half, "unconstrained", method="rank")), rel=1e-12)
+    assert rows[0]["min_ess"] == pytest.approx(np.min(dg.ess(Half, "unconstrained")), rel=1e-9)
+    assert rows[1]["min_ess_per_s"] == pytest.approx(np.min(e) / 2.0, rel=1e-9)
 
 
 def test_diagnostics_detect_disagreeing_chains():
