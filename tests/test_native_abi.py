@@ -430,3 +430,26 @@ def test_tensor_core_tmem_plan_fits_for_every_feature_count(lib):
     fn(100, out)
     assert list(out) == [104, 112, 3, 512]
     assert fn(129, out) != 0 and fn(0, out) != 0
+
+
+def test_tensor_core_paired_copy_stays_in_its_stage(lib):
+    """The paired GEMM1's 4-D TMA copy ([K-block][hi, lo][32 rows][8 features])
+    and its N = 64 B-operand reads (2 KB per K-block) stay inside the stage's
+    K-major region for every feature count, and the copy meets the tensor-map
+    rules: box dimensions <= 256, a 32-byte innermost box (the 32-byte swizzle
+    span), strides that are multiples of 16 bytes and below 2^40 up to 2^30
+    observations."""
+    fn = lib.ut_internal_tc_pair_plan
+    fn.restype = ctypes.c_int32
+    fn.argtypes = [ctypes.c_int32, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
+    out = (ctypes.c_int64 * 6)()
+    for F in range(1, 129):
+        for N in (1, 31, 32, 33, 100_000, 1 << 30):
+            assert fn(F, N, out) == 0
+            kb, box, region, read_end, hl, inner = list(out)
+            Fp = 16 * ((F + 15) // 16)
+            assert kb == (F + 7) // 8 and 1 <= kb <= 256
+            assert box == 2 * 1024 * kb and box <= region and read_end <= region, (F, list(out))
+            assert region == 2 * 1024 * (Fp // 8)
+            assert inner == 32 and (Fp * 4) % 16 == 0 and hl % 16 == 0 and hl < (1 << 40)
+    assert fn(0, 10, out) != 0 and fn(129, 10, out) != 0 and fn(10, 0, out) != 0

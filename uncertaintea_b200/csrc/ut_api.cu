@@ -992,6 +992,23 @@ extern "C" int32_t ut_internal_tc_tmem_plan(int32_t F, int32_t* out) {
     return UT_OK;
 }
 
+// Test hook (not part of the C ABI in ut_b200.h): the paired GEMM1's K-major copy
+// and the MMAs that read it, for F features and N observations, from the
+// kernel's own helpers: out = {K-blocks, box bytes of the 4-D copy, bytes of the
+// stage's K-major region, end offset of the last N = 64 B-operand read (2 KB per
+// K-block), hi/lo stride in bytes, innermost box bytes}.
+extern "C" int32_t ut_internal_tc_pair_plan(int32_t F, int64_t N, int64_t* out) {
+    if (F < 1 || F > kTcMaxFp || N < 1 || !out) return UT_ERR_ARGUMENT;
+    const int Fp = ((F + 15) / 16) * 16, KB1 = tc_kblocks_used(F);
+    out[0] = KB1;
+    out[1] = (int64_t)8 * kTcObs * 2 * KB1 * (int64_t)sizeof(float);
+    out[2] = 2 * (int64_t)tc_xk_bytes(Fp);
+    out[3] = (int64_t)(KB1 - 1) * 2 * (kTcObs * 32) + 2 * kTcObs * 32;
+    out[4] = N * Fp * (int64_t)sizeof(float);
+    out[5] = 8 * (int64_t)sizeof(float);
+    return UT_OK;
+}
+
 // Test hook (not part of the C ABI in ut_b200.h): one tensor-core evaluation of
 // only the first *d_live chains of d_params -- the live-chain launch masked NUTS
 // makes at every leaf, with its observation re-split -- on device buffers.
