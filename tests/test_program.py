@@ -357,3 +357,30 @@ def test_device_digamma_against_scipy(tmp_path):
     h = _host_math(tmp_path)
     for x in [1e-3, 0.05, 0.3, 0.5, 1.0, 1.7, 2.5, 4.0, 5.9, 6.0, 7.5, 12.0, 50.0, 1e3, 1e5]:
         assert h.prog_digamma_host(x) == pytest.approx(special.digamma(x), rel=3e-6, abs=3e-6), x
+
+
+def _reference_logpdf_pins():
+    import json
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_pins.json")
+    with open(path) as f:
+        return json.load(f)["logpdf"]
+
+
+@pytest.mark.parametrize("pin", _reference_logpdf_pins(), ids=lambda p: f"{p['family']}@{p['x']}")
+def test_program_oracle_matches_the_reference_tests_logpdf_pins(pin):
+    """The reference's own scalar log-density tests (test/uncertaintea/core/
+    dist_*.jl: `logpdf(family(args), x) ≈ closed form` and `== -Inf` outside the
+    support, extracted by tests/golden/make_golden.py) hold for the oracle's
+    plan walk, which the device's step programs are tested against: the
+    parameterisations (rate or scale, failures or trials, shape order) are the
+    reference's.  The staged observation is float32, so values agree to 1e-6."""
+    p = Program()
+    p.latent("u", "normal", 0.0, 1.0)
+    p.observe(pin["family"], *pin["args"], row=0)
+    t, _, _ = _eval(ProgramModel(p, [pin["x"]]), [[0.25]])
+    got = float(t[0]) - stats.norm.logpdf(0.25)
+    if np.isinf(pin["logpdf"]):
+        assert got == pin["logpdf"], (pin["source"], got)
+    else:
+        assert abs(got - pin["logpdf"]) <= 1e-6 * max(1.0, abs(pin["logpdf"])), (pin["source"], got)
